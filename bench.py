@@ -1,0 +1,393 @@
+"""Benchmark: 128^3 delta pressure projections per second on B200 (one JSON line on rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--size 128]
+
+Workload: the seeded 128^3 box-basin scene (16 submerged boxes cut by their signed distance, a
+sinusoidal free surface, a divergence-free background flow plus N(0, 0.5) m/s face noise; see
+fluidisim_b200/scenes.py), projected from p = 0 by the multigrid-preconditioned CG of water-core's
+`project_mobile3` to relative residual 1e-6 and plain divergence 1e-5.  One step = one projection.
+
+  value  device-resident: the input faces are restored from HBM each step (fd3_set_velocity_device,
+         which also checks them), p is zeroed, then fd3_project_mobile.  L2 is flushed (a 256 MiB
+         write) between steps, outside the timed events.
+  e2e    the same through the host-buffer C ABI: faces from pinned host memory (fd3_set_velocity),
+         projection, then the projected faces and the pressure back to pinned host memory.
+N > 1 runs N independent replicas (the projection of one domain does not shard: one 128^3 domain
+fits one GPU), one per rank, timed on the device, max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "128³ projections/s at rel. residual 1e-6: learned-FCG vs plain MGPCG, 1 B200"
+
+# Algorithmic bytes per cell of each fine-level kernel (f32 fields, cut geometry): every distinct
+# array a pass must touch, counted once (stencil neighbours are not re-counted).  Geometry = the
+# fluid fraction (4 B) and the three face apertures (12 B) the matrix-free rows read; the column
+# heights are per column and negligible.
+GEOM = 16
+BYTES_PER_CELL = {
+    "k_fine_sweep": 4 + 4 + 4 + 4 + GEOM,      # prec, r, z in, z out
+    "k_fine_sweep0": 4 + 4 + 4,                # prec, r, z out
+    "k_fine_restrict": 4 + 4 + GEOM + 0.5,     # r, z, geometry, coarse r (1/8 cell)
+    "k_fine_prolong": 4 + 4 + 4 + 0.5,         # z in/out, prec, coarse x
+    "k_apply_dot": 4 + 4 + GEOM,               # d, q, geometry
+    "k_update": 4 * 6,                         # p, r read+write; d, q
+    "k_dot": 8,
+    "k_mg_dir": 12,
+    "k_residual": 4 * 3 + GEOM,                # p, rhs, res
+    "k_rhs_mobile": 4 * 3 + GEOM,
+    "k_divergence": 4 * 3 + 4 + GEOM,          # three face families in, rhs out
+}
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples of the SM clock and throttle reasons while the timed region runs."""
+
+    FIELDS = "clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown," \
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown," \
+             "clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.index)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax.append(float(parts[1]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[3:7]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(gpus: int):
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(0)
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def make_scene(size: int):
+    from fluidisim_b200 import scenes
+    return scenes.box_basin(size)
+
+
+def run_reference(args):
+    """The reference arm: the CPU oracle (a restatement of the reference's Rust projection, whose own
+    toolchain is absent here) on the host cores, same scene, metric and unit."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from fluidisim_b200 import scenes
+    from oracle import oracle as O
+    O.build()
+    threads = O.max_threads()
+    O.set_threads(threads)
+    s = make_scene(args.size)
+    scale, k1 = scenes.projection_scalars(s)
+    v = O.OracleVolume(s["nx"], s["ny"], s["nz"], s["dx"], s["rho"], s["g"], bottom=s["bottom"], solid=s["solid"])
+    v.enable_multigrid()
+    v.set_free_surface(s["eta"], s["rest"])
+    times, rep = [], None
+    for step in range(args.warmup + args.steps):
+        v.set_velocity(s["u"], s["v"], s["w"])
+        v.set_free_surface(s["eta"], s["rest"])
+        t0 = time.perf_counter()
+        rep = v.project_mobile(scale, k1, 4000)
+        dt = time.perf_counter() - t0
+        if step >= args.warmup:
+            times.append(dt)
+    ms = 1e3 * sum(times) / len(times)
+    value = 1e3 / ms
+    out = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "projections/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded box_basin scene)",
+        "config": {"workload": f"box_basin {args.size}^3 multigrid-PCG projection (reference recipe)",
+                   "cells": s["nx"] * s["ny"] * s["nz"], "solver": "mgpcg", "iterations": rep["iterations"],
+                   "rel_residual": rep["residual"], "parallelism": "host threads"},
+        "cpu_baseline": {"value": value, "unit": "projections/s", "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} projections of the {args.size}^3 scene after {args.warmup} warm-up"},
+        "e2e": {"value": value, "unit": "projections/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+def cpu_baseline_sample(size: int, budget_s: float = 20.0):
+    """The oracle (OpenMP on every host core) timed on a bounded sample of the same workload."""
+    from fluidisim_b200 import scenes
+    from oracle import oracle as O
+    O.build()
+    threads = O.max_threads()
+    O.set_threads(threads)
+    s = make_scene(size)
+    scale, k1 = scenes.projection_scalars(s)
+    v = O.OracleVolume(s["nx"], s["ny"], s["nz"], s["dx"], s["rho"], s["g"], bottom=s["bottom"], solid=s["solid"])
+    v.enable_multigrid()
+    times = []
+    t_start = time.perf_counter()
+    while not times or (time.perf_counter() - t_start < budget_s and len(times) < 5):
+        v.set_velocity(s["u"], s["v"], s["w"])
+        v.set_free_surface(s["eta"], s["rest"])
+        t0 = time.perf_counter()
+        v.project_mobile(scale, k1, 4000)
+        times.append(time.perf_counter() - t0)
+    ms = 1e3 * sum(times) / len(times)
+    return {"value": 1e3 / ms, "unit": "projections/s", "cores": threads, "kind": "port",
+            "sample": f"{len(times)} full {size}^3 projections (same scene), oracle with OpenMP"}
+
+
+def run_b200(args):
+    import numpy as np
+    import torch
+
+    from fluidisim_b200 import build as B
+    from fluidisim_b200 import scenes
+    from fluidisim_b200.delta3d import REDUCE_F64, Volume3
+
+    rank, world, local = dist_setup(args.gpus)
+    B.build()
+    s = make_scene(args.size)
+    scale, k1 = scenes.projection_scalars(s)
+    stream = torch.cuda.Stream()
+    vol = Volume3.configure_with_solid(s["nx"], s["ny"], s["nz"], s["dx"], s["rho"], s["g"], s["bottom"], s["solid"])
+    vol.set_options(reduction=REDUCE_F64, use_graphs=1)
+    vol.set_stream(stream.cuda_stream)
+    vol.enable_multigrid()
+    vol.set_free_surface(s["eta"], s["rest"])
+    # inputs resident in HBM
+    du = torch.from_numpy(s["u"]).cuda()
+    dv = torch.from_numpy(s["v"]).cuda()
+    dw = torch.from_numpy(s["w"]).cuda()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+
+    def step():
+        vol.set_velocity_device(du.data_ptr(), dv.data_ptr(), dw.data_ptr())
+        vol.reset_pressure()
+        return vol.project_mobile3(scale, k1, 4000)
+
+    rep = None
+    for _ in range(args.warmup):
+        rep = step()
+    torch.cuda.synchronize()
+    barrier(world)
+    launches0 = vol.kernel_launches()
+    evs = []
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize()
+        barrier(world)
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            rep = step()
+            b.record(stream)
+            evs.append((a, b))
+        torch.cuda.synchronize()
+        barrier(world)
+    launches = vol.kernel_launches() - launches0
+    ms_total = sum(a.elapsed_time(b) for a, b in evs)
+    ms_total = max_over_ranks(ms_total, world)
+    ms_per_step = ms_total / args.steps
+    value = world * args.steps / (ms_total * 1e-3)
+
+    # e2e through the host-buffer ABI
+    pin = lambda a: torch.from_numpy(a).pin_memory()  # noqa: E731
+    hu, hv, hw = pin(s["u"]), pin(s["v"]), pin(s["w"])
+    ou = torch.empty(vol.nu, dtype=torch.float32).pin_memory()
+    ov = torch.empty(vol.nv, dtype=torch.float32).pin_memory()
+    ow = torch.empty(vol.nw, dtype=torch.float32).pin_memory()
+    op = torch.empty(vol.cells, dtype=torch.float32).pin_memory()
+    import ctypes as C
+    L = vol._L
+    fp = lambda t: C.cast(C.c_void_p(t.data_ptr()), C.POINTER(C.c_float))  # noqa: E731
+
+    def e2e_step():
+        e = L.fd3_set_velocity(vol._h, fp(hu), vol.nu, fp(hv), vol.nv, fp(hw), vol.nw)
+        assert e == 0, e
+        vol.reset_pressure()
+        r = vol.project_mobile3(scale, k1, 4000)
+        e = L.fd3_get_velocity(vol._h, fp(ou), vol.nu, fp(ov), vol.nv, fp(ow), vol.nw)
+        assert e == 0, e
+        e = L.fd3_get_pressure(vol._h, fp(op), vol.cells)
+        assert e == 0, e
+        return r
+
+    for _ in range(2):
+        e2e_step()
+    torch.cuda.synchronize()
+    barrier(world)
+    e2e_ms = []
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        e2e_step()
+        b.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms.append(a.elapsed_time(b))
+    e2e_total = max_over_ranks(sum(e2e_ms), world)
+    e2e_value = world * args.steps / (e2e_total * 1e-3)
+    h2d = 4 * (vol.nu + vol.nv + vol.nw)
+    d2h = 4 * (vol.nu + vol.nv + vol.nw + vol.cells)
+
+    # per-kernel timing: an instrumented replay of the same steps right after the timed region
+    vol.set_options(use_graphs=0)
+    vol.profile(True)
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        step()
+    torch.cuda.synchronize()
+    prof = vol.profile_entries()
+    vol.profile(False)
+    vol.set_options(use_graphs=1)
+    total_prof = sum(ms for _, _, ms in prof)
+    known = [(n, c, ms) for n, c, ms in prof if n in BYTES_PER_CELL]
+    top = max(known, key=lambda e: e[2])
+    name, count, ms = top
+    cells = s["nx"] * s["ny"] * s["nz"]
+    alg_bytes = BYTES_PER_CELL[name] * cells
+    avg_ms = ms / count
+    peak, peak_kind = peaks()
+    achieved = alg_bytes / (avg_ms * 1e-3) / 1e9
+    ncu_traffic = None
+    traffic_file = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(traffic_file):
+        try:
+            with open(traffic_file) as f:
+                ncu_traffic = json.load(f).get(name)
+        except Exception:
+            ncu_traffic = None
+
+    if rank == 0:
+        cpu = cpu_baseline_sample(args.size) if (world == 1 and not args.no_cpu) else None
+        out = {
+            "impl": "b200", "metric": METRIC, "value": value, "unit": "projections/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded box_basin scene)",
+            "config": {"workload": f"box_basin {args.size}^3 multigrid-PCG projection (reference V-cycle recipe)",
+                       "cells": cells, "solver": "mgpcg", "reduction": "f64", "iterations": rep.iterations,
+                       "rel_residual": rep.residual, "divergence_plain": rep.divergence_plain,
+                       "l2": "flushed between steps (256 MiB write outside the timed events)",
+                       "parallelism": f"replicas x{world}"},
+            "roofline": {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": peak_kind,
+                         "traffic": ncu_traffic, "alg_bytes_per_launch": alg_bytes,
+                         "avg_launch_ms": avg_ms, "launches": count,
+                         "share_of_step": ms / total_prof if total_prof else None},
+            "kernels": {n: {"launches": c, "ms": round(m, 4)} for n, c, m in sorted(prof, key=lambda e: -e[2])[:12]},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "projections/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches,
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(out), flush=True)
+    vol.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--size", type=int, default=128)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

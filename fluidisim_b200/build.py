@@ -1,0 +1,58 @@
+"""Build the CUDA library of the delta projection, in-tree, for sm_100a.
+
+    python -m fluidisim_b200.build
+
+writes fluidisim_b200/libfluidisim_delta3d.so.  --fmad=false keeps every f32 expression
+uncontracted, as the reference's Rust code is, so the kernels reproduce its arithmetic.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+LIB = os.path.join(HERE, "libfluidisim_delta3d.so")
+SOURCES = [os.path.join(HERE, "csrc", "fd3_volume.cu")]
+DEPS = SOURCES + [os.path.join(HERE, "csrc", f) for f in ("fd3_kernels.cuh", "fd3_cut.cuh")] + [
+    os.path.join(ROOT, "include", "fluidisim_delta3d.h")]
+
+NVCC_FLAGS = [
+    "-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-Xptxas=-v",
+    "-gencode", "arch=compute_100a,code=sm_100a",
+    "-Xcompiler", "-fPIC", "-shared",
+]
+
+
+def nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", "nvcc"):
+        if cand and (os.path.isabs(cand) and os.path.exists(cand) or not os.path.isabs(cand)):
+            return cand
+    return "nvcc"
+
+
+def stale() -> bool:
+    if not os.path.exists(LIB):
+        return True
+    t = os.path.getmtime(LIB)
+    return any(os.path.getmtime(d) > t for d in DEPS if os.path.exists(d))
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    if not force and not stale():
+        return LIB
+    cmd = [nvcc(), *NVCC_FLAGS, "-o", LIB + ".tmp", *SOURCES]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        sys.stderr.write(res.stdout + res.stderr)
+        raise RuntimeError("nvcc failed building libfluidisim_delta3d.so")
+    if verbose:
+        sys.stderr.write(res.stderr)
+    os.replace(LIB + ".tmp", LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose=True)
+    print(LIB)

@@ -1,0 +1,1011 @@
+// Device code of the delta (δ) MAC-grid pressure projection for sm_100a.
+//
+// Every per-cell and per-face operation evaluates the same f32 expressions, in the same order, as
+// the reference (paths relative to code/water-core/src/); the library is compiled with
+// --fmad=false so no multiply-add is contracted, as in Rust.  Hence, with the ordered f32
+// reduction mode, a projection reproduces the reference bit for bit.
+//
+// Layout in HBM: the reference's own (delta3d.rs:187-206).  Cells x-fastest, one f32 per cell
+// per field; u/v/w faces in their own arrays; columns (eta, roundoff) x-fastest.  The operator is
+// matrix-free, as `apply_mobile3` (delta3d_mobile.rs:190-213): each row is rebuilt from the
+// column heights, the fluid fractions and the face apertures, so an SpMV reads x plus the
+// geometry (nothing for a flat bottom) instead of stored coefficients.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace fd3 {
+
+constexpr int TPB = 256;            // threads per block of the per-cell kernels
+constexpr int CHUNK = 64;           // the reference's reduction grain (delta3d.rs:867)
+constexpr int CHUNKS_PER_BLOCK = TPB / CHUNK;
+constexpr float SURFACE_THETA_MIN = 1e-3f;        // delta_mobile.rs:14
+constexpr float PROJECTION_VELOCITY_FLOOR = 1e-4f; // delta3d.rs:41
+constexpr float OMEGA = 6.f / 7.f;                // delta3d_multigrid.rs:28
+
+enum Mode { RED_F64 = 0, RED_ORD = 1 };
+
+// Fine-level geometry, passed by value to every fine kernel.
+struct Geo {
+  int nx, ny, nz, n;
+  int cut;                // 0: flat bottom (every aperture 1, nothing solid)
+  float dx, inv, rho_g, rest;
+  const float* eta;       // column heights
+  const float* rof;       // column roundoff (compensated sum)
+  const float* frac;      // fluid fraction per cell (cut only)
+  const float* ou;        // apertures (cut only)
+  const float* ov;
+  const float* ow;
+};
+
+// A coarse level (Level3, delta3d_multigrid.rs:37-52).
+struct Lev {
+  int nx, ny, nz, n;
+  float inv;
+  float* ou; float* ov; float* ow;
+  float* kind; float* diag;
+  float* x; float* x2; float* r; float* t;
+};
+
+// Device-resident scalars of one projection.  Reduced values are held in double; in ordered
+// mode they are exact f32 values and the algebra is done in f32.
+struct Scalars {
+  double b2, rr, rz, dq, rn, zn, actual;
+  double tolb2;            // tol*b2 (f32 product in ordered mode)
+  double phys;             // physical_target (delta3d_mobile.rs:566-567)
+  float alpha, beta;       // applied step lengths
+  int active;              // the inner PCG loop is running
+  int status;              // 0, or 2 (NotFinite)
+  int brk;                 // dq <= 0 stopped the loop
+  unsigned it, max_iters;
+  int any_nonzero;         // ordered-mode norm2 guard (delta3d.rs:871-875)
+  float fmax[4];           // max-reductions (divergence all/plain, |u| max, backward error)
+  unsigned long long hash; // fingerprint of p
+};
+
+// Reduction scratch: per-block f64 partials, or per-64-chunk f32 partials.
+struct Red {
+  double* p64;
+  float* p32;
+};
+
+// ------------------------------------------------------------------------------------------------
+// Geometry predicates (delta3d_mobile.rs:92-124)
+
+__device__ __forceinline__ bool solid3(const Geo& g, int c) { return g.cut && __ldg(g.frac + c) == 0.f; }
+
+__device__ __forceinline__ bool wet3(const Geo& g, int i, int j, int k) {
+  int c = (k * g.ny + j) * g.nx + i;
+  if (solid3(g, c)) return false;
+  return ((float)k + 0.5f) * g.dx < __ldg(g.eta + j * g.nx + i);
+}
+
+__device__ __forceinline__ float open3(const Geo& g, int axis, int f) {
+  if (!g.cut) return 1.f;
+  return __ldg((axis == 0 ? g.ou : (axis == 1 ? g.ov : g.ow)) + f);
+}
+
+__device__ __forceinline__ int fu(const Geo& g, int i, int j, int k) { return (k * g.ny + j) * (g.nx + 1) + i; }
+__device__ __forceinline__ int fv(const Geo& g, int i, int j, int k) { return (k * (g.ny + 1) + j) * g.nx + i; }
+__device__ __forceinline__ int fw(const Geo& g, int i, int j, int k) { return (k * g.ny + j) * g.nx + i; }
+
+// ghost_up3 (delta3d_mobile.rs:126-134)
+__device__ __forceinline__ void ghost_up3(const Geo& g, int i, int j, int k, float& it, float& value) {
+  int col = j * g.nx + i;
+  float h = __ldg(g.eta + col);
+  float theta = fmaxf((h - ((float)k + 0.5f) * g.dx) / g.dx, SURFACE_THETA_MIN);
+  value = g.rho_g * ((h - g.rest) - __ldg(g.rof + col));
+  it = 1.f / theta;
+}
+
+// ghost_side3 (delta3d_mobile.rs:136-147)
+__device__ __forceinline__ void ghost_side3(const Geo& g, int i, int j, int k, int x, int y, float& it, float& value) {
+  float zc = ((float)k + 0.5f) * g.dx;
+  float h = __ldg(g.eta + j * g.nx + i);
+  float theta = fmaxf((h - zc) / (h - __ldg(g.eta + y * g.nx + x)), SURFACE_THETA_MIN);
+  value = g.rho_g * (zc - g.rest);
+  it = 1.f / theta;
+}
+
+struct RowE { int n; float a, it, val; };  // n < 0: no fluid neighbour (a wall, a ghost or nothing)
+
+// mobile_row (delta3d_mobile.rs:152-188): order x-, x+, y-, y+, z-, z+.
+__device__ __forceinline__ void mobile_row(const Geo& g, int i, int j, int k, RowE row[6]) {
+#pragma unroll
+  for (int f = 0; f < 6; ++f) row[f] = RowE{-1, 0.f, 0.f, 0.f};
+  const int nxny = g.nx * g.ny;
+  const int c = (k * g.ny + j) * g.nx + i;
+#pragma unroll
+  for (int f = 0; f < 4; ++f) {
+    bool ok; int x, y; float a;
+    if (f == 0) { ok = i > 0; x = i - 1; y = j; a = ok ? open3(g, 0, fu(g, i, j, k)) : 0.f; }
+    else if (f == 1) { ok = i + 1 < g.nx; x = i + 1; y = j; a = ok ? open3(g, 0, fu(g, i + 1, j, k)) : 0.f; }
+    else if (f == 2) { ok = j > 0; x = i; y = j - 1; a = ok ? open3(g, 1, fv(g, i, j, k)) : 0.f; }
+    else { ok = j + 1 < g.ny; x = i; y = j + 1; a = ok ? open3(g, 1, fv(g, i, j + 1, k)) : 0.f; }
+    if (!ok) continue;
+    int cn = (k * g.ny + y) * g.nx + x;
+    if (a == 0.f || solid3(g, cn)) continue;
+    if (wet3(g, x, y, k)) row[f] = RowE{cn, a, 0.f, 0.f};
+    else { float it, b; ghost_side3(g, i, j, k, x, y, it, b); row[f] = RowE{-1, a, it, b}; }
+  }
+  float down = open3(g, 2, fw(g, i, j, k));
+  if (k > 0 && down > 0.f && !solid3(g, c - nxny)) row[4] = RowE{c - nxny, down, 0.f, 0.f};
+  float up = open3(g, 2, fw(g, i, j, k + 1));
+  if (up > 0.f) {
+    if (k + 1 < g.nz && wet3(g, i, j, k + 1)) row[5] = RowE{c + nxny, up, 0.f, 0.f};
+    else { float it, b; ghost_up3(g, i, j, k, it, b); row[5] = RowE{-1, up, it, b}; }
+  }
+}
+
+// One row of apply_mobile3 (delta3d_mobile.rs:197-209) at a wet cell.
+__device__ __forceinline__ float apply_row(const Geo& g, int i, int j, int k, int c, const float* __restrict__ p) {
+  RowE row[6];
+  mobile_row(g, i, j, k, row);
+  float pc = p[c];
+  float acc = 0.f;
+#pragma unroll
+  for (int f = 0; f < 6; ++f) {
+    if (row[f].n >= 0) acc += row[f].a * (pc - p[row[f].n]);
+    else if (row[f].a > 0.f) acc += row[f].a * pc * row[f].it;
+  }
+  return acc * g.inv;
+}
+
+__device__ __forceinline__ void cell_ijk(const Geo& g, int c, int& i, int& j, int& k) {
+  i = c % g.nx;
+  int t = c / g.nx;
+  j = t % g.ny;
+  k = t / g.ny;
+}
+
+// ------------------------------------------------------------------------------------------------
+// Block reductions.  F64: f64 tree per block -> Red.p64[block].  ORD: the reference's order: each
+// 64-cell chunk summed serially in f32 from +0 (delta3d.rs:864-866) -> Red.p32[chunk]; the chunks
+// are merged serially by k_finish.
+
+template <int MODE> struct Acc;
+template <> struct Acc<RED_F64> {
+  typedef double T;
+  static __device__ __forceinline__ double prod(float a, float b) { return (double)a * (double)b; }
+  static __device__ __forceinline__ double prod3(float a, float b, float c) { return (double)a * (double)b * (double)c; }
+};
+template <> struct Acc<RED_ORD> {
+  typedef float T;
+  static __device__ __forceinline__ float prod(float a, float b) { return a * b; }
+  static __device__ __forceinline__ float prod3(float a, float b, float c) { return a * b * c; }
+};
+
+template <int MODE>
+__device__ __forceinline__ void block_reduce(typename Acc<MODE>::T v, int c, int n, Red red) {
+  if (MODE == RED_F64) {
+    __shared__ double sw[TPB / 32];
+    double s = (c < n) ? (double)v : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) sw[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+#pragma unroll
+      for (int w = 0; w < TPB / 32; ++w) t += sw[w];
+      red.p64[blockIdx.x] = t;
+    }
+  } else {
+    __shared__ float sv[TPB];
+    sv[threadIdx.x] = (float)v;
+    __syncthreads();
+    if (threadIdx.x < CHUNKS_PER_BLOCK) {
+      int q = blockIdx.x * CHUNKS_PER_BLOCK + threadIdx.x;
+      int start = q * CHUNK;
+      if (start < n) {
+        int cnt = min(CHUNK, n - start);
+        float acc = 0.f;
+        for (int e = 0; e < cnt; ++e) acc += sv[threadIdx.x * CHUNK + e];
+        red.p32[q] = acc;
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ void flag_nonzero(bool nz, Scalars* S) {
+  if (__syncthreads_or(nz) && threadIdx.x == 0) atomicOr(&S->any_nonzero, 1);
+}
+
+// ------------------------------------------------------------------------------------------------
+// Assembly
+
+// divergence / divergence_cut (delta3d.rs:747-763, 806-855), a solid at rest.
+__global__ void k_divergence(Geo g, const float* __restrict__ u, const float* __restrict__ v,
+                             const float* __restrict__ w, float* __restrict__ out) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= g.n) return;
+  int i, j, k; cell_ijk(g, c, i, j, k);
+  if (g.cut) {
+    if (__ldg(g.frac + c) == 0.f) { out[c] = 0.f; return; }
+    float fl = __ldg(g.ou + fu(g, i, j, k)) * u[fu(g, i, j, k)];
+    float fr = __ldg(g.ou + fu(g, i + 1, j, k)) * u[fu(g, i + 1, j, k)];
+    float ff = __ldg(g.ov + fv(g, i, j, k)) * v[fv(g, i, j, k)];
+    float fk = __ldg(g.ov + fv(g, i, j + 1, k)) * v[fv(g, i, j + 1, k)];
+    float fb = __ldg(g.ow + fw(g, i, j, k)) * w[fw(g, i, j, k)];
+    float ft = __ldg(g.ow + fw(g, i, j, k + 1)) * w[fw(g, i, j, k + 1)];
+    out[c] = ((fr - fl + ft - fb) + (fk - ff)) / g.dx;
+  } else {
+    float fl = u[fu(g, i, j, k)], fr = u[fu(g, i + 1, j, k)];
+    float ff = v[fv(g, i, j, k)], fk = v[fv(g, i, j + 1, k)];
+    float fb = w[fw(g, i, j, k)], ft = w[fw(g, i, j, k + 1)];
+    out[c] = ((fr - fl + ft - fb) + (fk - ff)) / g.dx;
+  }
+}
+
+// rhs_mobile3 (delta3d_mobile.rs:215-241) fused with the b.b reduction of norm2.
+template <int MODE>
+__global__ void k_rhs_mobile(Geo g, float scale, float* __restrict__ rhs, float* __restrict__ prec, Red red,
+                             Scalars* S, int reduce) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  float b = 0.f;
+  if (c < g.n) {
+    int i, j, k; cell_ijk(g, c, i, j, k);
+    if (!wet3(g, i, j, k)) { rhs[c] = 0.f; prec[c] = 0.f; }
+    else {
+      RowE row[6]; mobile_row(g, i, j, k, row);
+      b = scale * rhs[c];
+      float diag = 0.f;
+#pragma unroll
+      for (int f = 0; f < 6; ++f) {
+        if (row[f].n >= 0) diag += row[f].a;
+        else if (row[f].a > 0.f) {
+          diag += row[f].a * row[f].it;
+          b += row[f].a * row[f].val * row[f].it * g.inv;
+        }
+      }
+      rhs[c] = b;
+      prec[c] = diag > 0.f ? 1.f / (diag * g.inv) : 0.f;
+    }
+  }
+  if (reduce) {
+    block_reduce<MODE>(Acc<MODE>::prod(b, b), c, g.n, red);
+    flag_nonzero(c < g.n && b != 0.f, S);
+  }
+}
+
+// p = 0 on dry cells (delta3d_mobile.rs:485-494).
+__global__ void k_zero_dry(Geo g, float* __restrict__ p) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= g.n) return;
+  int i, j, k; cell_ijk(g, c, i, j, k);
+  if (!wet3(g, i, j, k)) p[c] = 0.f;
+}
+
+// out = A x (apply_mobile3).
+__global__ void k_apply(Geo g, const float* __restrict__ x, float* __restrict__ out) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= g.n) return;
+  int i, j, k; cell_ijk(g, c, i, j, k);
+  out[c] = wet3(g, i, j, k) ? apply_row(g, i, j, k, c, x) : 0.f;
+}
+
+// res = rhs - A p, with res.res (delta3d_mobile.rs:496-501, 547-553).
+template <int MODE>
+__global__ void k_residual(Geo g, const float* __restrict__ p, const float* __restrict__ rhs, float* __restrict__ res,
+                           Red red, Scalars* S) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  float r = 0.f;
+  if (c < g.n) {
+    int i, j, k; cell_ijk(g, c, i, j, k);
+    float ap = wet3(g, i, j, k) ? apply_row(g, i, j, k, c, p) : 0.f;
+    r = rhs[c] - ap;
+    res[c] = r;
+  }
+  block_reduce<MODE>(Acc<MODE>::prod(r, r), c, g.n, red);
+  flag_nonzero(c < g.n && r != 0.f, S);
+}
+
+// q = A d with d.q (delta3d_mobile.rs:523-528).
+template <int MODE>
+__global__ void k_apply_dot(Geo g, const float* __restrict__ d, float* __restrict__ q, Red red, const Scalars* S) {
+  if (!S->active) return;
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  float dqv = 0.f, dc = 0.f;
+  if (c < g.n) {
+    int i, j, k; cell_ijk(g, c, i, j, k);
+    dqv = wet3(g, i, j, k) ? apply_row(g, i, j, k, c, d) : 0.f;
+    q[c] = dqv;
+    dc = d[c];
+  }
+  block_reduce<MODE>(Acc<MODE>::prod(dc, dqv), c, g.n, red);
+}
+
+// p += alpha d, r -= alpha q, with r.r (delta3d_mobile.rs:532-536).
+template <int MODE>
+__global__ void k_update(int n, float* __restrict__ p, float* __restrict__ r, const float* __restrict__ d,
+                         const float* __restrict__ q, Red red, Scalars* S) {
+  if (!S->active) return;
+  const float alpha = S->alpha;
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  float rn = 0.f;
+  if (c < n) {
+    p[c] += alpha * d[c];
+    rn = r[c] - alpha * q[c];
+    r[c] = rn;
+  }
+  block_reduce<MODE>(Acc<MODE>::prod(rn, rn), c, n, red);
+  flag_nonzero(c < n && rn != 0.f, S);
+}
+
+// a.b over cells (dot, delta3d.rs:860-869); gate = 1 skips when the loop is not active.
+template <int MODE>
+__global__ void k_dot(int n, const float* __restrict__ a, const float* __restrict__ b, Red red, const Scalars* S, int gate) {
+  if (gate && !S->active) return;
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  float x = 0.f, y = 0.f;
+  if (c < n) { x = a[c]; y = b[c]; }
+  block_reduce<MODE>(Acc<MODE>::prod(x, y), c, n, red);
+}
+
+// res.prec.res (dot_prec3, delta3d_mobile.rs:447-461).
+template <int MODE>
+__global__ void k_dot_prec(int n, const float* __restrict__ r, const float* __restrict__ prec, Red red, const Scalars* S,
+                           int gate) {
+  if (gate && !S->active) return;
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  float x = 0.f, m = 0.f;
+  if (c < n) { x = r[c]; m = prec[c]; }
+  block_reduce<MODE>(Acc<MODE>::prod3(x, m, x), c, n, red);
+}
+
+// dir = z + beta dir, z = prec res (prime_mobile3, delta3d_mobile.rs:435-445).  use_beta = 0 is
+// the `beta == 0` branch (dir = z).
+__global__ void k_jacobi_dir(int n, const float* __restrict__ prec, const float* __restrict__ r, float* __restrict__ d,
+                             const Scalars* S, int gate, int use_beta) {
+  if (gate && !S->active) return;
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  float beta = use_beta ? S->beta : 0.f;
+  float z = prec[c] * r[c];
+  d[c] = beta == 0.f ? z : z + beta * d[c];
+}
+
+// dir = z + beta dir (direction_multigrid3, delta3d_multigrid.rs:460-465); use_beta = 0 is the
+// `beta == 0` branch of prime_multigrid3 (dir = z).
+__global__ void k_mg_dir(int n, const float* __restrict__ z, float* __restrict__ d, const Scalars* S, int gate,
+                         int use_beta) {
+  if (gate && !S->active) return;
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  if (!use_beta) d[c] = z[c];
+  else d[c] = z[c] + S->beta * d[c];
+}
+
+// ------------------------------------------------------------------------------------------------
+// Fine level of the V-cycle (v_cycle3, delta3d_multigrid.rs:393-429).  The fine operator is
+// apply_mobile3 itself; the smoother is damped Jacobi with the inverse diagonal `prec`.
+
+// First pre-sweep from z = 0: A z = 0, so z = 0 + w prec (r - 0).
+__global__ void k_fine_sweep0(int n, const float* __restrict__ prec, const float* __restrict__ r, float* __restrict__ z,
+                              const Scalars* S, int gate) {
+  if (gate && !S->active) return;
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  float m = prec[c];
+  z[c] = m > 0.f ? 0.f + OMEGA * m * (r[c] - 0.f) : 0.f;
+}
+
+// zout = zin + w prec (r - A zin) where prec > 0.
+__global__ void k_fine_sweep(Geo g, const float* __restrict__ prec, const float* __restrict__ r,
+                             const float* __restrict__ zin, float* __restrict__ zout, const Scalars* S, int gate) {
+  if (gate && !S->active) return;
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= g.n) return;
+  float m = prec[c];
+  float zc = zin[c];
+  if (m > 0.f) {
+    int i, j, k; cell_ijk(g, c, i, j, k);
+    float t = apply_row(g, i, j, k, c, zin);  // prec > 0 implies wet
+    zc += OMEGA * m * (r[c] - t);
+  }
+  zout[c] = zc;
+}
+
+// Coarse r = mean of the 8 children of (r - A z) (restrict3, delta3d_multigrid.rs:258-272).
+__global__ void k_fine_restrict(Geo g, const float* __restrict__ r, const float* __restrict__ z, Lev L,
+                                const Scalars* S, int gate) {
+  if (gate && !S->active) return;
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= L.n) return;
+  int ci = q % L.nx, t = q / L.nx, cj = t % L.ny, ck = t / L.ny;
+  float s = 0.f;
+#pragma unroll
+  for (int e = 0; e < 8; ++e) {
+    int i = 2 * ci + (e & 1), j = 2 * cj + ((e >> 1) & 1), k = 2 * ck + (e >> 2);
+    int c = (k * g.ny + j) * g.nx + i;
+    float az = wet3(g, i, j, k) ? apply_row(g, i, j, k, c, z) : 0.f;
+    s += r[c] - az;
+  }
+  L.r[q] = 0.125f * s;
+}
+
+// z += parent x (prolong_add3), then z = 0 where prec == 0 (delta3d_multigrid.rs:412-418).
+__global__ void k_fine_prolong(Geo g, const float* __restrict__ prec, float* __restrict__ z, Lev L, const Scalars* S,
+                               int gate) {
+  if (gate && !S->active) return;
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= g.n) return;
+  int i, j, k; cell_ijk(g, c, i, j, k);
+  float v = z[c] + L.x[((k >> 1) * L.ny + (j >> 1)) * L.nx + (i >> 1)];
+  z[c] = prec[c] == 0.f ? 0.f : v;
+}
+
+// ------------------------------------------------------------------------------------------------
+// Coarse levels (row_sums, smooth3, restrict3, prolong_add3, coarse_cycle3;
+// delta3d_multigrid.rs:216-332).
+
+// One row of row_sums with p given (kind > 0 at c).
+__device__ __forceinline__ float level_row(const Lev& L, int i, int j, int k, int c, const float* __restrict__ p) {
+  const float pc = p[c];
+  float acc = 0.f;
+  const int nxny = L.nx * L.ny;
+  auto face = [&](float a, bool has, int m, bool top) {
+    if (a == 0.f) return;
+    if (has) {
+      float km = L.kind[m];
+      if (km > 0.f) acc += a * (pc - p[m]);
+      else if (km < 0.f) acc += 2.f * a * pc;
+    } else if (top) {
+      acc += 2.f * a * pc;
+    }
+  };
+  face(L.ou[(k * L.ny + j) * (L.nx + 1) + i], i > 0, c - 1, false);
+  face(L.ou[(k * L.ny + j) * (L.nx + 1) + i + 1], i + 1 < L.nx, c + 1, false);
+  face(L.ov[(k * (L.ny + 1) + j) * L.nx + i], j > 0, c - L.nx, false);
+  face(L.ov[(k * (L.ny + 1) + j + 1) * L.nx + i], j + 1 < L.ny, c + L.nx, false);
+  face(L.ow[(k * L.ny + j) * L.nx + i], k > 0, c - nxny, false);
+  face(L.ow[((k + 1) * L.ny + j) * L.nx + i], k + 1 < L.nz, c + nxny, true);
+  return acc * L.inv;
+}
+
+// The diagonal: row_sums with p absent (delta3d_multigrid.rs:205, 236-241).
+__global__ void k_level_diag(Lev L) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= L.n) return;
+  int i = c % L.nx, t = c / L.nx, j = t % L.ny, k = t / L.ny;
+  if (L.kind[c] <= 0.f) { L.diag[c] = 0.f; return; }
+  float acc = 0.f;
+  const int nxny = L.nx * L.ny;
+  auto face = [&](float a, bool has, int m, bool top) {
+    if (a == 0.f) return;
+    if (has) {
+      float km = L.kind[m];
+      if (km > 0.f) acc += a;
+      else if (km < 0.f) acc += 2.f * a * 1.f;
+    } else if (top) {
+      acc += 2.f * a * 1.f;
+    }
+  };
+  face(L.ou[(k * L.ny + j) * (L.nx + 1) + i], i > 0, c - 1, false);
+  face(L.ou[(k * L.ny + j) * (L.nx + 1) + i + 1], i + 1 < L.nx, c + 1, false);
+  face(L.ov[(k * (L.ny + 1) + j) * L.nx + i], j > 0, c - L.nx, false);
+  face(L.ov[(k * (L.ny + 1) + j + 1) * L.nx + i], j + 1 < L.ny, c + L.nx, false);
+  face(L.ow[(k * L.ny + j) * L.nx + i], k > 0, c - nxny, false);
+  face(L.ow[((k + 1) * L.ny + j) * L.nx + i], k + 1 < L.nz, c + nxny, true);
+  L.diag[c] = acc * L.inv;
+}
+
+// Damped Jacobi sweep (smooth3): xout = xin + w (r - L xin) / diag where diag > 0.  zero_in = 1
+// is the first sweep after `x.fill(0)`: L 0 = +0 exactly, so xout = 0 + w (r - 0) / diag.
+__global__ void k_level_sweep(Lev L, const float* __restrict__ xin, float* __restrict__ xout, int zero_in,
+                              const Scalars* S, int gate) {
+  if (gate && !S->active) return;
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= L.n) return;
+  float dg = L.diag[c];
+  if (zero_in) {
+    xout[c] = dg > 0.f ? 0.f + OMEGA * (L.r[c] - 0.f) / dg : 0.f;
+    return;
+  }
+  float xc = xin[c];
+  if (dg > 0.f) {
+    int i = c % L.nx, t = c / L.nx, j = t % L.ny, k = t / L.ny;
+    float tv = level_row(L, i, j, k, c, xin);  // diag > 0 implies kind > 0
+    xc += OMEGA * (L.r[c] - tv) / dg;
+  }
+  xout[c] = xc;
+}
+
+// Coarse r of level C = mean over 8 children of (r - L x) on level F.
+__global__ void k_level_restrict(Lev F, Lev C, const Scalars* S, int gate) {
+  if (gate && !S->active) return;
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= C.n) return;
+  int ci = q % C.nx, t = q / C.nx, cj = t % C.ny, ck = t / C.ny;
+  float s = 0.f;
+#pragma unroll
+  for (int e = 0; e < 8; ++e) {
+    int i = 2 * ci + (e & 1), j = 2 * cj + ((e >> 1) & 1), k = 2 * ck + (e >> 2);
+    int c = (k * F.ny + j) * F.nx + i;
+    float lx = F.kind[c] > 0.f ? level_row(F, i, j, k, c, F.x) : 0.f;
+    s += F.r[c] - lx;
+  }
+  C.r[q] = 0.125f * s;
+}
+
+// F.x += parent C.x (prolong_add3 between coarse levels).
+__global__ void k_level_prolong(Lev F, Lev C, const Scalars* S, int gate) {
+  if (gate && !S->active) return;
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= F.n) return;
+  int i = c % F.nx, t = c / F.nx, j = t % F.ny, k = t / F.ny;
+  F.x[c] += C.x[((k >> 1) * C.ny + (j >> 1)) * C.nx + (i >> 1)];
+}
+
+// ------------------------------------------------------------------------------------------------
+// coarsen3 (delta3d_multigrid.rs:141-206) and fine_kind3 (:357-367)
+
+__global__ void k_coarsen_kind_fine(Geo g, Lev C) {
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= C.n) return;
+  int ci = q % C.nx, t = q / C.nx, cj = t % C.ny, ck = t / C.ny;
+  bool active = false, air = false;
+#pragma unroll
+  for (int e = 0; e < 8; ++e) {
+    int i = 2 * ci + (e & 1), j = 2 * cj + ((e >> 1) & 1), k = 2 * ck + (e >> 2);
+    int c = (k * g.ny + j) * g.nx + i;
+    float v = wet3(g, i, j, k) ? 1.f : (solid3(g, c) ? 0.f : -1.f);
+    if (v > 0.f) active = true;
+    else if (v < 0.f) air = true;
+  }
+  C.kind[q] = active ? 1.f : (air ? -1.f : 0.f);
+}
+
+__global__ void k_coarsen_kind_level(Lev F, Lev C) {
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= C.n) return;
+  int ci = q % C.nx, t = q / C.nx, cj = t % C.ny, ck = t / C.ny;
+  bool active = false, air = false;
+#pragma unroll
+  for (int e = 0; e < 8; ++e) {
+    int i = 2 * ci + (e & 1), j = 2 * cj + ((e >> 1) & 1), k = 2 * ck + (e >> 2);
+    float v = F.kind[(k * F.ny + j) * F.nx + i];
+    if (v > 0.f) active = true;
+    else if (v < 0.f) air = true;
+  }
+  C.kind[q] = active ? 1.f : (air ? -1.f : 0.f);
+}
+
+// Coarse apertures: mean of the 4 fine faces a coarse face covers.  `fo*` are the fine apertures
+// (nullptr: a flat fine level, every aperture 1).  fnx/fny are the fine dimensions.
+__global__ void k_coarsen_open(int fnx, int fny, const float* __restrict__ fou, const float* __restrict__ fov,
+                               const float* __restrict__ fow, Lev C) {
+  int cx = C.nx, cy = C.ny, cz = C.nz;
+  int nu = (cx + 1) * cy * cz, nv = cx * (cy + 1) * cz, nw = cx * cy * (cz + 1);
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < nu) {
+    int i = q % (cx + 1), t = q / (cx + 1), j = t % cy, k = t / cy;
+    float s = 0.f;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      int dj = e & 1, dk = e >> 1;
+      s += fou ? fou[((2 * k + dk) * fny + 2 * j + dj) * (fnx + 1) + 2 * i] : 1.f;
+    }
+    C.ou[q] = 0.25f * s;
+    return;
+  }
+  q -= nu;
+  if (q < nv) {
+    int i = q % cx, t = q / cx, j = t % (cy + 1), k = t / (cy + 1);
+    float s = 0.f;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      int di = e & 1, dk = e >> 1;
+      s += fov ? fov[((2 * k + dk) * (fny + 1) + 2 * j) * fnx + 2 * i + di] : 1.f;
+    }
+    C.ov[q] = 0.25f * s;
+    return;
+  }
+  q -= nv;
+  if (q < nw) {
+    int i = q % cx, t = q / cx, j = t % cy, k = t / cy;
+    float s = 0.f;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      int di = e & 1, dj = e >> 1;
+      s += fow ? fow[((2 * k) * fny + 2 * j + dj) * fnx + 2 * i + di] : 1.f;
+    }
+    C.ow[q] = 0.25f * s;
+  }
+}
+
+// ------------------------------------------------------------------------------------------------
+// Correction and diagnostics
+
+// correct_mobile3 (delta3d_mobile.rs:284-343): u = us - change on every u face (axis 0), v face
+// (axis 1); untouched faces copy the prediction.
+__global__ void k_correct_uv(Geo g, float k1, const float* __restrict__ p, const float* __restrict__ us,
+                             const float* __restrict__ vs, float* __restrict__ u, float* __restrict__ v) {
+  int nu = (g.nx + 1) * g.ny * g.nz, nv = g.nx * (g.ny + 1) * g.nz;
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  int axis, f, i, j, k;
+  if (q < nu) { axis = 0; f = q; i = f % (g.nx + 1); int t = f / (g.nx + 1); j = t % g.ny; k = t / g.ny; }
+  else if (q < nu + nv) { axis = 1; f = q - nu; i = f % g.nx; int t = f / g.nx; j = t % (g.ny + 1); k = t / (g.ny + 1); }
+  else return;
+  float val = axis == 0 ? us[f] : vs[f];
+  bool interior = axis == 0 ? (i > 0 && i < g.nx) : (j > 0 && j < g.ny);
+  if (interior) {
+    int x = axis == 0 ? i - 1 : i, y = axis == 0 ? j : j - 1;
+    int l = (k * g.ny + y) * g.nx + x, r = (k * g.ny + j) * g.nx + i;
+    if (!(open3(g, axis, f) == 0.f || solid3(g, l) || solid3(g, r))) {
+      bool wl = wet3(g, x, y, k), wr = wet3(g, i, j, k);
+      if (wl || wr) {
+        float change;
+        if (wl && wr) change = k1 * (p[r] - p[l]) / g.dx;
+        else if (wl) { float a, b; ghost_side3(g, x, y, k, i, j, a, b); change = k1 * (b - p[l]) * a / g.dx; }
+        else { float a, b; ghost_side3(g, i, j, k, x, y, a, b); change = k1 * (p[r] - b) * a / g.dx; }
+        val -= change;
+      }
+    }
+  }
+  if (axis == 0) u[f] = val; else v[f] = val;
+}
+
+__global__ void k_correct_w(Geo g, float k1, const float* __restrict__ p, const float* __restrict__ ws,
+                            float* __restrict__ w) {
+  int nw = g.nx * g.ny * (g.nz + 1);
+  int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= nw) return;
+  int i = f % g.nx, t = f / g.nx, j = t % g.ny, k = t / g.ny;
+  float val = ws[f];
+  if (k >= 1 && open3(g, 2, f) != 0.f && wet3(g, i, j, k - 1)) {
+    int below = ((k - 1) * g.ny + j) * g.nx + i;
+    if (k < g.nz && wet3(g, i, j, k)) val -= k1 * (p[below + g.nx * g.ny] - p[below]) / g.dx;
+    else { float a, b; ghost_up3(g, i, j, k - 1, a, b); val -= k1 * (b - p[below]) * a / g.dx; }
+  }
+  w[f] = val;
+}
+
+// Order-independent float max of non-negative values (NaN-free inputs compare as their bits).
+__device__ __forceinline__ void atomic_fmax_nonneg(float* addr, float v) {
+  if (!(v > 0.f)) return;  // +0 initial value; NaN is ignored, as Rust's f32::max does
+  atomicMax(reinterpret_cast<int*>(addr), __float_as_int(v));
+}
+
+// divergence_mobile3 (delta3d_mobile.rs:398-433): max |div u| over wet rows (all) and over rows
+// without a surface ghost (plain).  S->fmax[0] = all, [1] = plain.
+__global__ void k_div_metric(Geo g, const float* __restrict__ u, const float* __restrict__ v,
+                             const float* __restrict__ w, Scalars* S) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  float all = 0.f, plain = 0.f;
+  if (c < g.n) {
+    int i, j, k; cell_ijk(g, c, i, j, k);
+    if (wet3(g, i, j, k)) {
+      float dv;
+      if (g.cut) {
+        float fl = __ldg(g.ou + fu(g, i, j, k)) * u[fu(g, i, j, k)];
+        float fr = __ldg(g.ou + fu(g, i + 1, j, k)) * u[fu(g, i + 1, j, k)];
+        float ff = __ldg(g.ov + fv(g, i, j, k)) * v[fv(g, i, j, k)];
+        float fk = __ldg(g.ov + fv(g, i, j + 1, k)) * v[fv(g, i, j + 1, k)];
+        float fb = __ldg(g.ow + fw(g, i, j, k)) * w[fw(g, i, j, k)];
+        float ft = __ldg(g.ow + fw(g, i, j, k + 1)) * w[fw(g, i, j, k + 1)];
+        dv = ((fr - fl + ft - fb) + (fk - ff)) / g.dx;
+      } else {
+        float fl = u[fu(g, i, j, k)], fr = u[fu(g, i + 1, j, k)];
+        float ff = v[fv(g, i, j, k)], fk = v[fv(g, i, j + 1, k)];
+        float fb = w[fw(g, i, j, k)], ft = w[fw(g, i, j, k + 1)];
+        dv = ((fr - fl + ft - fb) + (fk - ff)) / g.dx;
+      }
+      float d = fabsf(dv);
+      all = d;
+      RowE row[6]; mobile_row(g, i, j, k, row);
+      bool ghost = false;
+#pragma unroll
+      for (int f = 0; f < 6; ++f) ghost = ghost || (row[f].n < 0 && row[f].a > 0.f);
+      if (!ghost) plain = d;
+    }
+  }
+  // warp max then one atomic per warp
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    all = fmaxf(all, __shfl_down_sync(0xffffffffu, all, o));
+    plain = fmaxf(plain, __shfl_down_sync(0xffffffffu, plain, o));
+  }
+  if ((threadIdx.x & 31) == 0) { atomic_fmax_nonneg(&S->fmax[0], all); atomic_fmax_nonneg(&S->fmax[1], plain); }
+}
+
+// max |x| over an array into S->fmax[slot].
+__global__ void k_maxabs(int n, const float* __restrict__ x, Scalars* S, int slot) {
+  float m = 0.f;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) m = fmaxf(m, fabsf(x[q]));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_down_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomic_fmax_nonneg(&S->fmax[slot], m);
+}
+
+// backward_error_mobile3 (delta3d_mobile.rs:243-271) into S->fmax[3].
+__global__ void k_backward_error(Geo g, const float* __restrict__ p, const float* __restrict__ rhs,
+                                 const float* __restrict__ res, Scalars* S) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  float worst = 0.f;
+  if (c < g.n) {
+    int i, j, k; cell_ijk(g, c, i, j, k);
+    if (wet3(g, i, j, k)) {
+      RowE row[6]; mobile_row(g, i, j, k, row);
+      float pc = fabsf(p[c]);
+      float acc = 0.f;
+#pragma unroll
+      for (int f = 0; f < 6; ++f) {
+        if (row[f].n >= 0) acc += row[f].a * (pc + fabsf(p[row[f].n]));
+        else if (row[f].a > 0.f) acc += row[f].a * pc * row[f].it;
+      }
+      float scale = fabsf(rhs[c]) + acc * g.inv;
+      if (scale > 0.f) worst = fabsf(res[c]) / scale;
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) worst = fmaxf(worst, __shfl_down_sync(0xffffffffu, worst, o));
+  if ((threadIdx.x & 31) == 0) atomic_fmax_nonneg(&S->fmax[3], worst);
+}
+
+// Fingerprint of the exact bits of p for cycle detection (the role of fingerprint,
+// delta3d.rs:1360-1369).  The reference hashes the bytes serially (FNV-1a); a serial chain does
+// not map to a GPU, so each element's bits are mixed with its index (SplitMix64 finaliser) and the
+// mixes are summed mod 2^64: a function of the exact bits of p, independent of the launch shape.
+__device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+__global__ void k_hash(int n, const float* __restrict__ p, Scalars* S) {
+  unsigned long long h = 0;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x)
+    h += mix64(((unsigned long long)(unsigned)__float_as_int(p[q]) << 32 | (unsigned)q) + 0x9E3779B97F4A7C15ull);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) h += __shfl_down_sync(0xffffffffu, h, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(&S->hash, h);
+}
+
+// ------------------------------------------------------------------------------------------------
+// Finishing a reduction, then the scalar algebra of the PCG step that consumes it.
+
+enum FinOp {
+  FIN_B2 = 0,      // b2 = |rhs|^2 (norm2 checks)
+  FIN_RR0 = 1,     // rr = |res|^2 initial (norm2 checks)
+  FIN_DQ = 2,      // dq; alpha = rz/dq or stop (delta3d_mobile.rs:528-531)
+  FIN_RN = 3,      // rn = |r|^2 (norm2 checks); decides whether the loop continues
+  FIN_RZ_ITER = 4, // zn; beta = zn/rz; rz = zn; rr = rn; it++ (delta3d_mobile.rs:538-545)
+  FIN_RZ_PRIME = 5,// rz of a fresh direction (prime_*: delta3d_mobile.rs:517, 587)
+  FIN_ACTUAL = 6   // true residual |b - A p|^2 (norm2 checks)
+};
+
+__device__ __forceinline__ bool loop_continues(const Scalars* S, double rn, unsigned it_next, int ord) {
+  bool above = ord ? ((float)rn > (float)S->tolb2 || (float)rn > (float)S->phys) : (rn > S->tolb2 || rn > S->phys);
+  return above && it_next < S->max_iters;
+}
+
+template <int MODE>
+__global__ void k_finish(Red red, int nparts, Scalars* S, int op, int gate) {
+  if (gate && !S->active) return;
+  double val;
+  if (MODE == RED_F64) {
+    __shared__ double sm[1024];
+    double s = 0.0;
+    for (int q = threadIdx.x; q < nparts; q += blockDim.x) s += red.p64[q];
+    sm[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+      if ((int)threadIdx.x < w) sm[threadIdx.x] += sm[threadIdx.x + w];
+      __syncthreads();
+    }
+    val = sm[0];
+  } else {
+    // serial in-order merge in f32 (host_impl.rs:75-92, merge of delta3d.rs:867)
+    __shared__ float seg[8192];
+    float acc = 0.f;
+    for (int base = 0; base < nparts; base += 8192) {
+      int cnt = min(8192, nparts - base);
+      for (int q = threadIdx.x; q < cnt; q += blockDim.x) seg[q] = red.p32[base + q];
+      __syncthreads();
+      if (threadIdx.x == 0)
+        for (int q = 0; q < cnt; ++q) acc = acc + seg[q];
+      __syncthreads();
+    }
+    val = (double)acc;
+  }
+  if (threadIdx.x != 0) return;
+  const int ord = MODE == RED_ORD;
+  const bool finite = isfinite(val);
+  const bool zero_but_nonzero = ord && val == 0.0 && S->any_nonzero;  // norm2 guard
+  switch (op) {
+    case FIN_B2:
+      S->b2 = val;
+      if (!finite || zero_but_nonzero) S->status = 2;
+      break;
+    case FIN_RR0:
+    case FIN_ACTUAL:
+      if (op == FIN_RR0) S->rr = val; else S->actual = val;
+      if (!finite || zero_but_nonzero) S->status = 2;
+      break;
+    case FIN_DQ:
+      S->dq = val;
+      if (!(val > 0.0)) { S->active = 0; S->brk = 1; }
+      else S->alpha = ord ? (float)S->rz / (float)val : (float)(S->rz / val);
+      break;
+    case FIN_RN: {
+      S->rn = val;
+      if (!finite || zero_but_nonzero) { S->status = 2; S->active = 0; break; }
+      if (!loop_continues(S, val, S->it + 1, ord)) {
+        S->rr = val;
+        S->it += 1;
+        S->active = 0;
+      }
+      break;
+    }
+    case FIN_RZ_ITER: {
+      if (!finite) { S->status = 2; S->active = 0; break; }
+      S->zn = val;
+      if (ord) S->beta = (float)val / (float)S->rz;
+      else S->beta = (float)(val / S->rz);
+      S->rz = val;
+      S->rr = S->rn;
+      S->it += 1;
+      break;
+    }
+    case FIN_RZ_PRIME:
+      if (!finite) S->status = 2;
+      S->rz = val;
+      break;
+  }
+  S->any_nonzero = 0;
+}
+
+
+// ------------------------------------------------------------------------------------------------
+// The rest of the mobile step (delta3d_mobile.rs:615-813)
+
+// advect_mobile3 (delta3d_mobile.rs:615-732): centred MAC advection of every open interior face
+// into us/vs/ws; every other face copies the current velocity.
+__global__ void k_advect(Geo g, float dt, const float* __restrict__ u, const float* __restrict__ v,
+                         const float* __restrict__ w, float* __restrict__ us, float* __restrict__ vs,
+                         float* __restrict__ ws) {
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int nu = (nx + 1) * ny * nz, nv = nx * (ny + 1) * nz, nw = nx * ny * (nz + 1);
+  const float h = 0.5f / g.dx;
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < nu + nv) {
+    const int axis = q < nu ? 0 : 1;
+    const int f = axis == 0 ? q : q - nu;
+    int i, j, k;
+    if (axis == 0) { i = f % (nx + 1); int t = f / (nx + 1); j = t % ny; k = t / ny; }
+    else { i = f % nx; int t = f / nx; j = t % (ny + 1); k = t / (ny + 1); }
+    const int a = axis == 0 ? i : j, b = axis == 0 ? j : i;
+    const int na = axis == 0 ? nx : ny, nb = axis == 0 ? ny : nx;
+    float cur = axis == 0 ? u[f] : v[f];
+    if (a >= 1 && a < na && open3(g, axis, f) != 0.f) {
+      auto val = [&](int A, int B, int K) { return axis == 0 ? u[fu(g, A, B, K)] : v[fv(g, B, A, K)]; };
+      auto vertical = [&](int A, int B, int K) { return axis == 0 ? w[fw(g, A, B, K)] : w[fw(g, B, A, K)]; };
+      auto transverse = [&](int A, int B, int K) { return axis == 0 ? v[fv(g, A, B, K)] : u[fu(g, B, A, K)]; };
+      float uc = val(a, b, k);
+      float ux = (val(a + 1, b, k) - val(a - 1, b, k)) * h;
+      float upv = k + 1 < nz ? val(a, b, k + 1) : uc;
+      float dn = k > 0 ? val(a, b, k - 1) : uc;
+      float uz = (upv - dn) * h;
+      float wc = 0.25f * (vertical(a - 1, b, k) + vertical(a, b, k) + vertical(a - 1, b, k + 1) + vertical(a, b, k + 1));
+      float rt = b + 1 < nb ? val(a, b + 1, k) : uc;
+      float lf = b > 0 ? val(a, b - 1, k) : uc;
+      float uy = (rt - lf) * h;
+      float vc = 0.25f * (transverse(a - 1, b, k) + transverse(a, b, k) + transverse(a - 1, b + 1, k) + transverse(a, b + 1, k));
+      cur = uc - dt * (uc * ux + wc * uz + vc * uy);
+    }
+    if (axis == 0) us[f] = cur; else vs[f] = cur;
+    return;
+  }
+  q -= nu + nv;
+  if (q >= nw) return;
+  const int f = q;
+  const int i = f % nx, t = f / nx, j = t % ny, k = t / ny;
+  float cur = w[f];
+  if (k >= 1 && k < nz && open3(g, 2, f) != 0.f) {
+    float wc = w[f];
+    float rt = i + 1 < nx ? w[fw(g, i + 1, j, k)] : wc;
+    float lf = i > 0 ? w[fw(g, i - 1, j, k)] : wc;
+    float wx = (rt - lf) * h;
+    float wz = (w[fw(g, i, j, k + 1)] - w[fw(g, i, j, k - 1)]) * h;
+    float uc = 0.25f * (u[fu(g, i, j, k - 1)] + u[fu(g, i + 1, j, k - 1)] + u[fu(g, i, j, k)] + u[fu(g, i + 1, j, k)]);
+    float bk = j + 1 < ny ? w[fw(g, i, j + 1, k)] : wc;
+    float fr = j > 0 ? w[fw(g, i, j - 1, k)] : wc;
+    float wy = (bk - fr) * h;
+    float vc = 0.25f * (v[fv(g, i, j, k - 1)] + v[fv(g, i, j + 1, k - 1)] + v[fv(g, i, j, k)] + v[fv(g, i, j + 1, k)]);
+    cur = wc - dt * (uc * wx + wc * wz + vc * wy);
+  }
+  ws[f] = cur;
+}
+
+// extrapolate_mobile3 (delta3d_mobile.rs:345-394): one thread per column and axis walks up the
+// column and copies the last solved face into the unsolved open faces above it.
+__global__ void k_extrapolate(Geo g, float* __restrict__ u, float* __restrict__ v, float* __restrict__ w) {
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= 3 * g.nx * g.ny) return;
+  const int axis = q / (g.nx * g.ny);
+  const int col = q % (g.nx * g.ny);
+  const int i = col % g.nx, j = col / g.nx;
+  if ((axis == 0 && i == 0) || (axis == 1 && j == 0)) return;
+  float* field = axis == 0 ? u : (axis == 1 ? v : w);
+  bool has_last = false;
+  float last = 0.f;
+  const int start = axis == 2 ? 1 : 0, end = axis == 2 ? g.nz + 1 : g.nz;
+  for (int k = start; k < end; ++k) {
+    int f;
+    bool solved;
+    if (axis == 0) {
+      f = fu(g, i, j, k);
+      solved = open3(g, 0, f) > 0.f && !solid3(g, (k * g.ny + j) * g.nx + i - 1) && !solid3(g, (k * g.ny + j) * g.nx + i) &&
+               (wet3(g, i - 1, j, k) || wet3(g, i, j, k));
+    } else if (axis == 1) {
+      f = fv(g, i, j, k);
+      solved = open3(g, 1, f) > 0.f && !solid3(g, (k * g.ny + j - 1) * g.nx + i) && !solid3(g, (k * g.ny + j) * g.nx + i) &&
+               (wet3(g, i, j - 1, k) || wet3(g, i, j, k));
+    } else {
+      f = fw(g, i, j, k);
+      solved = open3(g, 2, f) > 0.f && wet3(g, i, j, k - 1);
+    }
+    if (open3(g, axis, f) == 0.f) continue;
+    if (solved) { last = field[f]; has_last = true; }
+    else if (has_last) field[f] = last;
+  }
+}
+
+// transport_mobile3 (delta3d_mobile.rs:734-782), fluxes: wet column flux through every interior
+// lateral face, read from eta^n.  Boundary entries stay zero (the walls).
+__global__ void k_transport_flux(Geo g, const float* __restrict__ u, const float* __restrict__ v,
+                                 float* __restrict__ flux_x, float* __restrict__ flux_y) {
+  const int nfx = (g.nx + 1) * g.ny, nfy = g.nx * (g.ny + 1);
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nfx + nfy) return;
+  const int axis = q < nfx ? 0 : 1;
+  int i, j;
+  if (axis == 0) { i = q % (g.nx + 1); j = q / (g.nx + 1); }
+  else { int r = q - nfx; i = r % g.nx; j = r / g.nx; }
+  float qf = 0.f;
+  bool interior = axis == 0 ? (i >= 1 && i < g.nx) : (j >= 1 && j < g.ny);
+  if (interior) {
+    int x = axis == 0 ? i - 1 : i, y = axis == 0 ? j : j - 1;
+    float surface = 0.5f * (g.eta[y * g.nx + x] + g.eta[j * g.nx + i]);
+    for (int k = 0; k < g.nz; ++k) {
+      float wet = (surface - (float)k * g.dx) / g.dx;
+      wet = wet < 0.f ? 0.f : (wet > 1.f ? 1.f : wet);
+      if (wet == 0.f) break;
+      float uu, a;
+      if (axis == 0) { int f = fu(g, i, j, k); uu = u[f]; a = open3(g, 0, f); }
+      else { int f = fv(g, i, j, k); uu = v[f]; a = open3(g, 1, f); }
+      qf += a * uu * g.dx * wet;
+    }
+  }
+  if (axis == 0) flux_x[q] = qf; else flux_y[q - nfx] = qf;
+}
+
+// transport_mobile3, heights: compensated f32 sum per column (delta3d_mobile.rs:770-781).
+__global__ void k_transport_eta(Geo g, float transport, const float* __restrict__ flux_x,
+                                const float* __restrict__ flux_y, float* __restrict__ eta, float* __restrict__ rof) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= g.nx * g.ny) return;
+  int i = c % g.nx, j = c / g.nx;
+  float x = flux_x[j * (g.nx + 1) + i + 1] - flux_x[j * (g.nx + 1) + i];
+  float y = flux_y[(j + 1) * g.nx + i] - flux_y[j * g.nx + i];
+  float increment = -transport * (x + y) - rof[c];
+  float height = eta[c] + increment;
+  rof[c] = (height - eta[c]) - increment;
+  eta[c] = height;
+}
+
+// mobile_in_bounds (delta3d_mobile.rs:801-813): sets *flag when a column leaves its bounds.
+__global__ void k_in_bounds(Geo g, const float* __restrict__ floor, int* flag) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  bool bad = false;
+  if (c < g.nx * g.ny) {
+    float top = (float)(g.nz - 1) * g.dx;
+    float e = g.eta[c];
+    float fl = g.cut ? floor[c] + 2.f * g.dx : 2.f * g.dx;
+    bad = !(e >= fl && e <= top);
+  }
+  if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(flag, 1);
+}
+
+}  // namespace fd3

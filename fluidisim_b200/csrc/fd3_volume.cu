@@ -1,0 +1,1115 @@
+// Host driver and C ABI of the delta (δ) pressure projection on B200.
+//
+// The driver mirrors water-core's `Volume3` (code/water-core/src/delta3d.rs, delta3d_mobile.rs,
+// delta3d_multigrid.rs): the same entry points, error codes and atomic refusals.  All arithmetic
+// on fields runs in the kernels of fd3_kernels.cuh / fd3_cut.cuh; the host only sequences launches
+// and reads back a few scalars (the reference's outer acceptance loop, delta3d_mobile.rs:513-588).
+// Scalars of the inner PCG loop (alpha, beta, the loop condition) live on the device, so an
+// iteration is a fixed launch sequence that can be replayed from a CUDA graph.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstddef>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <new>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../../include/fluidisim_delta3d.h"
+#include "fd3_cut.cuh"
+#include "fd3_kernels.cuh"
+
+using namespace fd3;
+
+namespace {
+
+thread_local std::string g_last_cuda_error;
+
+int cuda_fail(cudaError_t e, const char* what, int line) {
+  char buf[512];
+  snprintf(buf, sizeof buf, "%s (line %d): %s", what, line, cudaGetErrorString(e));
+  g_last_cuda_error = buf;
+  return e == cudaErrorMemoryAllocation ? FD3_ERR_OUT_OF_MEMORY : FD3_ERR_CUDA;
+}
+
+#define CK(call)                                                   \
+  do {                                                             \
+    cudaError_t e_ = (call);                                       \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call, __LINE__); \
+  } while (0)
+
+#define TRY(expr)        \
+  do {                   \
+    int s_ = (expr);     \
+    if (s_) return s_;   \
+  } while (0)
+
+inline int blocks_for(long long n) { return (int)((n + TPB - 1) / TPB); }
+
+// PROJECTION_DIVERGENCE_TOLERANCE (delta_projection.rs:192)
+constexpr double kDivTol = 1e-5;
+// gamma_8 and gamma_10 of u = 2^-24 (delta_projection.rs:200-203, delta3d.rs:69-72)
+const float kRoundoff2D = 8.0f * (1.0f / 16777216.0f) / (1.0f - 8.0f * (1.0f / 16777216.0f));
+const float kRoundoff3D = 10.0f * (1.0f / 16777216.0f) / (1.0f - 10.0f * (1.0f / 16777216.0f));
+
+}  // namespace
+
+struct fd3_volume {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaStream_t own_stream = nullptr;  // created at configure; capturable (not the legacy stream)
+  int nx = 0, ny = 0, nz = 0, n = 0, nu = 0, nv = 0, nw = 0, ncol = 0;
+  float dx = 0, rho = 0, g = 0, rest = 0, z0 = 0;
+  bool cut = false;
+  // geometry (cut only)
+  float *frac = nullptr, *ou = nullptr, *ov = nullptr, *ow = nullptr, *floor_ = nullptr;
+  // state and work fields (delta3d.rs:102-184)
+  float *eta = nullptr, *rof = nullptr, *u = nullptr, *v = nullptr, *w = nullptr;
+  float *us = nullptr, *vs = nullptr, *ws = nullptr, *p = nullptr, *rhs = nullptr, *res = nullptr;
+  float *dir = nullptr, *tmp = nullptr, *prec = nullptr;
+  float *sv_u = nullptr, *sv_v = nullptr, *sv_w = nullptr, *sv_p = nullptr, *sv_eta = nullptr, *sv_rof = nullptr;
+  float *flux_x = nullptr, *flux_y = nullptr;
+  // multigrid
+  bool has_mg = false;
+  float *z = nullptr, *z2 = nullptr;
+  std::vector<Lev> levels;
+  // reductions and scalars
+  double* p64 = nullptr;
+  float* p32 = nullptr;
+  Scalars* dS = nullptr;
+  Scalars* hS = nullptr;  // pinned
+  int* dflag = nullptr;
+  int* hflag = nullptr;   // pinned
+  fd3_options opt{};
+  bool has_refused = false;
+  fd3_report refused{};
+  unsigned long long launches = 0;
+  std::vector<void*> allocations;
+  // opt-in per-kernel timing: events around every launch, collected at each synchronisation
+  bool prof = false;
+  std::vector<cudaEvent_t> ev_pool;
+  size_t ev_next = 0;
+  struct Pending { const char* name; cudaEvent_t a, b; };
+  std::vector<Pending> pending;
+  std::vector<std::string> prof_names;
+  std::vector<unsigned long long> prof_count;
+  std::vector<double> prof_ms;
+  // CUDA graph of one PCG iteration
+  cudaGraphExec_t iter_exec = nullptr;
+  int iter_exec_mode = -1;
+  unsigned long long iter_nodes = 0;
+
+  Geo geo() const {
+    Geo G;
+    G.nx = nx; G.ny = ny; G.nz = nz; G.n = n;
+    G.cut = cut ? 1 : 0;
+    G.dx = dx;
+    G.inv = 1.f / (dx * dx);
+    G.rho_g = rho * g;
+    G.rest = rest;
+    G.eta = eta; G.rof = rof;
+    G.frac = frac; G.ou = ou; G.ov = ov; G.ow = ow;
+    return G;
+  }
+  bool ord() const { return opt.reduction == FD3_REDUCE_ORDERED_F32; }
+  Red red() const { return Red{p64, p32}; }
+};
+
+namespace {
+
+int dalloc(fd3_volume* V, float** ptr, size_t count) {
+  void* q = nullptr;
+  CK(cudaMalloc(&q, count * sizeof(float) + 16));
+  CK(cudaMemsetAsync(q, 0, count * sizeof(float) + 16, V->stream));
+  V->allocations.push_back(q);
+  *ptr = (float*)q;
+  return FD3_OK;
+}
+
+void release(fd3_volume* V) {
+  if (V->stream) cudaStreamSynchronize(V->stream);
+  if (V->iter_exec) cudaGraphExecDestroy(V->iter_exec);
+  for (cudaEvent_t e : V->ev_pool) cudaEventDestroy(e);
+  for (void* q : V->allocations) cudaFree(q);
+  if (V->hS) cudaFreeHost(V->hS);
+  if (V->hflag) cudaFreeHost(V->hflag);
+  if (V->own_stream) cudaStreamDestroy(V->own_stream);
+}
+
+cudaEvent_t next_event(fd3_volume* V) {
+  if (V->ev_next == V->ev_pool.size()) {
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    V->ev_pool.push_back(e);
+  }
+  return V->ev_pool[V->ev_next++];
+}
+
+// Every kernel launch of the library goes through here: grid x block on the handle's stream,
+// counted, and bracketed by events when profiling is on.
+template <class K, class... A>
+void launch_grid(fd3_volume* V, const char* name, int grid, int block, K kernel, A... args) {
+  cudaEvent_t a = nullptr, b = nullptr;
+  if (V->prof) { a = next_event(V); cudaEventRecord(a, V->stream); }
+  kernel<<<grid, block, 0, V->stream>>>(args...);
+  if (V->prof) { b = next_event(V); cudaEventRecord(b, V->stream); V->pending.push_back({name, a, b}); }
+  V->launches++;
+}
+#define LAUNCH(V, KERNEL, N, ...) launch_grid((V), #KERNEL, blocks_for(N), TPB, KERNEL, __VA_ARGS__)
+#define LAUNCH_G(V, KERNEL, GRID, BLOCK, ...) launch_grid((V), #KERNEL, (GRID), (BLOCK), KERNEL, __VA_ARGS__)
+
+void prof_collect(fd3_volume* V) {
+  for (auto& r : V->pending) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, r.a, r.b);
+    size_t q = 0;
+    while (q < V->prof_names.size() && V->prof_names[q] != r.name) ++q;
+    if (q == V->prof_names.size()) { V->prof_names.emplace_back(r.name); V->prof_count.push_back(0); V->prof_ms.push_back(0.0); }
+    V->prof_count[q] += 1;
+    V->prof_ms[q] += ms;
+  }
+  V->pending.clear();
+  V->ev_next = 0;
+}
+
+int sync(fd3_volume* V) {
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(V->stream));
+  if (V->prof) prof_collect(V);
+  return FD3_OK;
+}
+
+int pull(fd3_volume* V) {
+  CK(cudaMemcpyAsync(V->hS, V->dS, sizeof(Scalars), cudaMemcpyDeviceToHost, V->stream));
+  return sync(V);
+}
+
+// Number of partials a reduction over n elements leaves.
+int nparts(const fd3_volume* V, int n) { return V->ord() ? (n + CHUNK - 1) / CHUNK : blocks_for(n); }
+
+void finish(fd3_volume* V, int n, int op, int gate) {
+  if (V->ord()) launch_grid(V, "k_finish", 1, 256, k_finish<RED_ORD>, V->red(), nparts(V, n), V->dS, op, gate);
+  else launch_grid(V, "k_finish", 1, 1024, k_finish<RED_F64>, V->red(), nparts(V, n), V->dS, op, gate);
+}
+
+#define DISPATCH(V, KERNEL, N, ...)                                                               \
+  do {                                                                                           \
+    if ((V)->ord()) launch_grid((V), #KERNEL, blocks_for(N), TPB, KERNEL<RED_ORD>, __VA_ARGS__);   \
+    else launch_grid((V), #KERNEL, blocks_for(N), TPB, KERNEL<RED_F64>, __VA_ARGS__);              \
+  } while (0)
+
+// ------------------------------------------------------------------------------------ multigrid
+// prepare_multigrid3 (delta3d_multigrid.rs:370-387): coarse geometry follows the surface.
+void prepare_multigrid(fd3_volume* V) {
+  if (!V->has_mg || V->levels.empty()) return;
+  Geo G = V->geo();
+  for (size_t l = 0; l < V->levels.size(); ++l) {
+    Lev& C = V->levels[l];
+    long long nfaces = (long long)(C.nx + 1) * C.ny * C.nz + (long long)C.nx * (C.ny + 1) * C.nz +
+                       (long long)C.nx * C.ny * (C.nz + 1);
+    if (l == 0) {
+      LAUNCH(V, k_coarsen_kind_fine, C.n, G, C);
+      LAUNCH(V, k_coarsen_open, nfaces, V->nx, V->ny, (const float*)V->ou, (const float*)V->ov, (const float*)V->ow, C);
+    } else {
+      Lev& F = V->levels[l - 1];
+      LAUNCH(V, k_coarsen_kind_level, C.n, F, C);
+      LAUNCH(V, k_coarsen_open, nfaces, F.nx, F.ny, (const float*)F.ou, (const float*)F.ov, (const float*)F.ow, C);
+    }
+    LAUNCH(V, k_level_diag, C.n, C);
+  }
+}
+
+// coarse_cycle3 (delta3d_multigrid.rs:303-332); levels[0].r already restricted.
+void coarse_cycle(fd3_volume* V, int gate) {
+  std::vector<Lev>& Ls = V->levels;
+  size_t last = Ls.size() - 1;
+  for (size_t l = 0; l <= last; ++l) {
+    Lev& L = Ls[l];
+    int sweeps = l == last ? 8 : 2;  // COARSE_SWEEPS_3D, PRE_SWEEPS_3D
+    for (int s = 0; s < sweeps; ++s) {
+      const float* in = (s % 2 == 0) ? L.x : L.x2;
+      float* out = (s % 2 == 0) ? L.x2 : L.x;
+      LAUNCH(V, k_level_sweep, L.n, L, in, out, s == 0 ? 1 : 0, (const Scalars*)V->dS, gate);
+    }
+    if (l < last) LAUNCH(V, k_level_restrict, Ls[l + 1].n, L, Ls[l + 1], (const Scalars*)V->dS, gate);
+  }
+  for (size_t l = last; l-- > 0;) {
+    Lev& L = Ls[l];
+    LAUNCH(V, k_level_prolong, L.n, L, Ls[l + 1], (const Scalars*)V->dS, gate);
+    for (int s = 0; s < 2; ++s) {  // POST_SWEEPS_3D
+      const float* in = (s % 2 == 0) ? L.x : L.x2;
+      float* out = (s % 2 == 0) ? L.x2 : L.x;
+      LAUNCH(V, k_level_sweep, L.n, L, in, out, 0, (const Scalars*)V->dS, gate);
+    }
+  }
+}
+
+// v_cycle3 (delta3d_multigrid.rs:393-429): z = M^-1 res, result in V->z.
+void vcycle(fd3_volume* V, int gate) {
+  Geo G = V->geo();
+  const Scalars* S = V->dS;
+  LAUNCH(V, k_fine_sweep0, V->n, V->n, (const float*)V->prec, (const float*)V->res, V->z2, S, gate);
+  LAUNCH(V, k_fine_sweep, V->n, G, (const float*)V->prec, (const float*)V->res, (const float*)V->z2, V->z, S, gate);
+  if (!V->levels.empty()) {
+    LAUNCH(V, k_fine_restrict, V->levels[0].n, G, (const float*)V->res, (const float*)V->z, V->levels[0], S, gate);
+    coarse_cycle(V, gate);
+    LAUNCH(V, k_fine_prolong, V->n, G, (const float*)V->prec, V->z, V->levels[0], S, gate);
+  }
+  LAUNCH(V, k_fine_sweep, V->n, G, (const float*)V->prec, (const float*)V->res, (const float*)V->z, V->z2, S, gate);
+  LAUNCH(V, k_fine_sweep, V->n, G, (const float*)V->prec, (const float*)V->res, (const float*)V->z2, V->z, S, gate);
+}
+
+// prime_multigrid3 / prime_mobile3 with beta = 0: a fresh direction and rz.
+void prime(fd3_volume* V) {
+  if (V->has_mg) {
+    vcycle(V, 0);
+    DISPATCH(V, k_dot, V->n, V->n, (const float*)V->res, (const float*)V->z, V->red(), (const Scalars*)V->dS, 0);
+    finish(V, V->n, FIN_RZ_PRIME, 0);
+    LAUNCH(V, k_mg_dir, V->n, V->n, (const float*)V->z, V->dir, (const Scalars*)V->dS, 0, 0);
+  } else {
+    LAUNCH(V, k_jacobi_dir, V->n, V->n, (const float*)V->prec, (const float*)V->res, V->dir, (const Scalars*)V->dS, 0, 0);
+    DISPATCH(V, k_dot_prec, V->n, V->n, (const float*)V->res, (const float*)V->prec, V->red(), (const Scalars*)V->dS, 0);
+    finish(V, V->n, FIN_RZ_PRIME, 0);
+  }
+}
+
+// One inner PCG iteration (delta3d_mobile.rs:515-545), every kernel gated on S->active.
+void iteration(fd3_volume* V) {
+  Geo G = V->geo();
+  DISPATCH(V, k_apply_dot, V->n, G, (const float*)V->dir, V->tmp, V->red(), (const Scalars*)V->dS);
+  finish(V, V->n, FIN_DQ, 1);
+  DISPATCH(V, k_update, V->n, V->n, V->p, V->res, (const float*)V->dir, (const float*)V->tmp, V->red(), V->dS);
+  finish(V, V->n, FIN_RN, 1);
+  if (V->has_mg) {
+    vcycle(V, 1);
+    DISPATCH(V, k_dot, V->n, V->n, (const float*)V->res, (const float*)V->z, V->red(), (const Scalars*)V->dS, 1);
+    finish(V, V->n, FIN_RZ_ITER, 1);
+    LAUNCH(V, k_mg_dir, V->n, V->n, (const float*)V->z, V->dir, (const Scalars*)V->dS, 1, 1);
+  } else {
+    DISPATCH(V, k_dot_prec, V->n, V->n, (const float*)V->res, (const float*)V->prec, V->red(), (const Scalars*)V->dS, 1);
+    finish(V, V->n, FIN_RZ_ITER, 1);
+    LAUNCH(V, k_jacobi_dir, V->n, V->n, (const float*)V->prec, (const float*)V->res, V->dir, (const Scalars*)V->dS, 1, 1);
+  }
+}
+
+// Run the inner loop until S->active drops; each iteration replayed from a CUDA graph when enabled.
+int run_inner(fd3_volume* V) {
+  const bool graphs = V->opt.use_graphs && !V->prof;
+  if (graphs) {
+    int mode = (V->ord() ? 1 : 0) | (V->has_mg ? 2 : 0);
+    if (!V->iter_exec || V->iter_exec_mode != mode) {
+      if (V->iter_exec) { cudaGraphExecDestroy(V->iter_exec); V->iter_exec = nullptr; }
+      cudaGraph_t graph;
+      CK(cudaStreamBeginCapture(V->stream, cudaStreamCaptureModeThreadLocal));
+      unsigned long long before = V->launches;
+      iteration(V);
+      cudaError_t e = cudaStreamEndCapture(V->stream, &graph);
+      V->iter_nodes = V->launches - before;
+      V->launches = before;
+      if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture", __LINE__);
+      e = cudaGraphInstantiate(&V->iter_exec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate", __LINE__);
+      V->iter_exec_mode = mode;
+    }
+  }
+  // The device clears S->active within max_iters iterations (FIN_RN); the host bound is a guard.
+  for (unsigned guard = 0;; ++guard) {
+    if (guard > V->hS->max_iters + 2u) return FD3_ERR_CUDA;
+    if (graphs) {
+      CK(cudaGraphLaunch(V->iter_exec, V->stream));
+      V->launches += V->iter_nodes;
+    } else {
+      iteration(V);
+    }
+    TRY(pull(V));
+    if (!V->hS->active) break;
+  }
+  return FD3_OK;
+}
+
+// Max-reductions and the fingerprint (fmax slots and hash are reset before each use).
+__global__ void k_reset_diag(Scalars* S, int mask) {
+  if (mask & 1) { S->fmax[0] = 0.f; S->fmax[1] = 0.f; S->fmax[2] = 0.f; }
+  if (mask & 2) S->fmax[3] = 0.f;
+  if (mask & 4) S->hash = 0ull;
+}
+
+int divergence_metric(fd3_volume* V, double* all_out, double* plain_out) {
+  Geo G = V->geo();
+  LAUNCH_G(V, k_reset_diag, 1, 1, V->dS, 1);
+  LAUNCH(V, k_div_metric, V->n, G, (const float*)V->u, (const float*)V->v, (const float*)V->w, V->dS);
+  LAUNCH_G(V, k_maxabs, 592, TPB, V->nu, (const float*)V->u, V->dS, 2);
+  LAUNCH_G(V, k_maxabs, 592, TPB, V->nv, (const float*)V->v, V->dS, 2);
+  LAUNCH_G(V, k_maxabs, 592, TPB, V->nw, (const float*)V->w, V->dS, 2);
+  TRY(pull(V));
+  float all = V->hS->fmax[0], plain = V->hS->fmax[1], mx = V->hS->fmax[2];
+  // delta3d_mobile.rs:426-432
+  float echelle = std::fmax(mx, PROJECTION_VELOCITY_FLOOR);
+  float ratio = mx > 0.f ? V->dx / echelle : 0.f;
+  *all_out = (double)(all * ratio);
+  *plain_out = (double)(plain * ratio);
+  return FD3_OK;
+}
+
+int backward_error(fd3_volume* V, float* out) {
+  LAUNCH_G(V, k_reset_diag, 1, 1, V->dS, 2);
+  LAUNCH(V, k_backward_error, V->n, V->geo(), (const float*)V->p, (const float*)V->rhs, (const float*)V->res, V->dS);
+  TRY(pull(V));
+  *out = V->hS->fmax[3];
+  return FD3_OK;
+}
+
+int fingerprint(fd3_volume* V, unsigned long long* out) {
+  LAUNCH_G(V, k_reset_diag, 1, 1, V->dS, 4);
+  LAUNCH_G(V, k_hash, 592, TPB, V->n, (const float*)V->p, V->dS);
+  TRY(pull(V));
+  *out = V->hS->hash;
+  return FD3_OK;
+}
+
+void correct(fd3_volume* V, float k1) {
+  Geo G = V->geo();
+  LAUNCH(V, k_correct_uv, (long long)V->nu + V->nv, G, k1, (const float*)V->p, (const float*)V->us, (const float*)V->vs, V->u, V->v);
+  LAUNCH(V, k_correct_w, V->nw, G, k1, (const float*)V->p, (const float*)V->ws, V->w);
+}
+
+// Loop start: the host's view of the loop state is written to the device before the inner loop.
+__global__ void k_loop_start(Scalars* S, double rr, double tolb2, double phys, unsigned it, unsigned max_iters) {
+  S->rr = rr;
+  S->tolb2 = tolb2;
+  S->phys = phys;
+  S->it = it;
+  S->max_iters = max_iters;
+  S->brk = 0;
+  S->active = 1;
+}
+
+__global__ void k_reset_scalars(Scalars* S) {
+  Scalars z;
+  memset(&z, 0, sizeof z);
+  *S = z;
+}
+
+// project_mobile3 (delta3d_mobile.rs:465-609).
+int project_mobile3(fd3_volume* V, float scale, float k1, uint32_t max_iters, fd3_report* rep) {
+  const bool ord = V->ord();
+  Geo G = V->geo();
+  LAUNCH_G(V, k_reset_scalars, 1, 1, V->dS);
+  LAUNCH(V, k_divergence, V->n, G, (const float*)V->us, (const float*)V->vs, (const float*)V->ws, V->rhs);
+  DISPATCH(V, k_rhs_mobile, V->n, G, scale, V->rhs, V->prec, V->red(), V->dS, 1);
+  finish(V, V->n, FIN_B2, 0);
+  if (V->has_mg) prepare_multigrid(V);
+  LAUNCH(V, k_zero_dry, V->n, G, V->p);
+  DISPATCH(V, k_residual, V->n, G, (const float*)V->p, (const float*)V->rhs, V->res, V->red(), V->dS);
+  finish(V, V->n, FIN_RR0, 0);
+  TRY(pull(V));
+  if (V->hS->status) return V->hS->status;
+  const double b2 = V->hS->b2;
+  double rr = V->hS->rr;
+  // tol = 1e-12_f32 (delta3d_mobile.rs:507); tol*b2 in f32 in the reference's arithmetic
+  const double tolb2 = ord ? (double)(1e-12f * (float)b2) : 1e-12 * b2;
+  bool primed = false;
+  uint32_t it = 0;
+  bool floor_stop = false;
+  double phys = std::numeric_limits<double>::infinity();
+  bool has_checkpoint = false;
+  unsigned long long checkpoint = 0;
+  uint32_t power = 1, since = 0;
+  double actual_rr = 0;
+  bool settled = false;
+  double settled_d[2] = {0, 0};
+  auto above = [&](double r) {
+    if (ord) return (float)r > (float)tolb2 || (float)r > (float)phys;
+    return r > tolb2 || r > phys;
+  };
+  for (;;) {
+    uint32_t before = it;
+    if (b2 > 0 && above(rr) && it < max_iters) {
+      if (!primed) {
+        prime(V);
+        primed = true;
+      }
+      LAUNCH_G(V, k_loop_start, 1, 1, V->dS, rr, tolb2, phys, it, max_iters);
+      V->hS->max_iters = max_iters;
+      TRY(run_inner(V));
+      if (V->hS->status) return V->hS->status;
+      it = V->hS->it;
+      rr = V->hS->rr;
+    }
+    // the true residual decides (delta3d_mobile.rs:547-553)
+    DISPATCH(V, k_residual, V->n, G, (const float*)V->p, (const float*)V->rhs, V->res, V->red(), V->dS);
+    finish(V, V->n, FIN_ACTUAL, 0);
+    TRY(pull(V));
+    if (V->hS->status) return V->hS->status;
+    double actual = V->hS->actual;
+    bool exhausted = it >= max_iters || it == before;
+    bool has_measured = false;
+    double measured[2] = {0, 0};
+    bool converged = ord ? (float)actual <= (float)tolb2 : actual <= tolb2;
+    if (converged) {
+      if (exhausted) { actual_rr = actual; break; }
+      correct(V, k1);
+      double all, plain;
+      TRY(divergence_metric(V, &all, &plain));
+      if (plain <= kDivTol) { actual_rr = actual; settled = true; settled_d[0] = all; settled_d[1] = plain; break; }
+      has_measured = true; measured[0] = all; measured[1] = plain;
+      if (ord) {
+        float ratio = (float)(kDivTol / plain);
+        phys = (double)((float)actual * ratio * ratio);
+      } else {
+        double ratio = kDivTol / plain;
+        phys = actual * ratio * ratio;
+      }
+    } else if (exhausted) {
+      actual_rr = actual;
+      break;
+    }
+    float be;
+    TRY(backward_error(V, &be));
+    if (be <= (V->ny == 1 ? kRoundoff2D : kRoundoff3D)) {
+      floor_stop = true; actual_rr = actual;
+      if (has_measured) { settled = true; settled_d[0] = measured[0]; settled_d[1] = measured[1]; }
+      break;
+    }
+    unsigned long long state;
+    TRY(fingerprint(V, &state));
+    if (has_checkpoint && checkpoint == state) {
+      floor_stop = true; actual_rr = actual;
+      if (has_measured) { settled = true; settled_d[0] = measured[0]; settled_d[1] = measured[1]; }
+      break;
+    }
+    since += 1;
+    if (since == power) {
+      has_checkpoint = true; checkpoint = state;
+      power = power > 0x7fffffffu ? 0xffffffffu : power * 2;
+      since = 0;
+    }
+    rr = actual;
+    prime(V);
+    TRY(pull(V));
+    if (V->hS->status) return V->hS->status;
+  }
+  double residual;
+  if (ord) residual = b2 > 0 ? (double)std::sqrt((float)actual_rr / (float)b2) : 0.0;
+  else residual = b2 > 0 ? std::sqrt(actual_rr / b2) : 0.0;
+  double div_all, div_plain;
+  if (settled) { div_all = settled_d[0]; div_plain = settled_d[1]; }
+  else {
+    correct(V, k1);
+    TRY(divergence_metric(V, &div_all, &div_plain));
+  }
+  bool conv = ord ? (float)actual_rr <= (float)tolb2 : actual_rr <= tolb2;
+  bool accepted = (conv || floor_stop) && div_plain <= kDivTol;
+  float be;
+  TRY(backward_error(V, &be));
+  memset(rep, 0, sizeof *rep);
+  rep->refinements = 0;
+  rep->iterations = it;
+  rep->degraded = (b2 > 0 && !accepted) ? 1 : 0;
+  rep->residual = residual;
+  rep->divergence = div_all;
+  rep->floor = floor_stop ? 1 : 0;
+  rep->backward_error = (double)be;
+  rep->divergence_plain = div_plain;
+  return FD3_OK;
+}
+
+// ---------------------------------------------------------------------------- input validation
+__global__ void k_check_finite(long long n, const float* __restrict__ x, int* flag) {
+  bool bad = false;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+    bad |= !isfinite(x[q]);
+  if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(flag, 1);
+}
+
+// close_walls (delta3d.rs:666-690): walls, bottom, and faces the cut closes have no velocity.
+__global__ void k_close_walls(Geo g, float* __restrict__ u, float* __restrict__ v, float* __restrict__ w) {
+  int nu = (g.nx + 1) * g.ny * g.nz, nv = g.nx * (g.ny + 1) * g.nz, nw = g.nx * g.ny * (g.nz + 1);
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < nu) {
+    int i = q % (g.nx + 1);
+    if (i == 0 || i == g.nx || (g.cut && g.ou[q] == 0.f)) u[q] = 0.f;
+    return;
+  }
+  q -= nu;
+  if (q < nv) {
+    int j = (q / g.nx) % (g.ny + 1);
+    if (j == 0 || j == g.ny || (g.cut && g.ov[q] == 0.f)) v[q] = 0.f;
+    return;
+  }
+  q -= nv;
+  if (q < nw) {
+    int k = q / (g.nx * g.ny);
+    if (k == 0 || (g.cut && g.ow[q] == 0.f)) w[q] = 0.f;
+  }
+}
+
+int check_finite_device(fd3_volume* V, const float* x, long long n, bool* ok) {
+  CK(cudaMemsetAsync(V->dflag, 0, sizeof(int), V->stream));
+  LAUNCH_G(V, k_check_finite, 592, TPB, n, x, V->dflag);
+  CK(cudaMemcpyAsync(V->hflag, V->dflag, sizeof(int), cudaMemcpyDeviceToHost, V->stream));
+  TRY(sync(V));
+  *ok = *V->hflag == 0;
+  return FD3_OK;
+}
+
+// ------------------------------------------------------------------------------------ configure
+int alloc_state(fd3_volume* V) {
+  TRY(dalloc(V, &V->eta, V->ncol)); TRY(dalloc(V, &V->rof, V->ncol));
+  TRY(dalloc(V, &V->u, V->nu)); TRY(dalloc(V, &V->v, V->nv)); TRY(dalloc(V, &V->w, V->nw));
+  TRY(dalloc(V, &V->us, V->nu)); TRY(dalloc(V, &V->vs, V->nv)); TRY(dalloc(V, &V->ws, V->nw));
+  TRY(dalloc(V, &V->p, V->n)); TRY(dalloc(V, &V->rhs, V->n)); TRY(dalloc(V, &V->res, V->n));
+  TRY(dalloc(V, &V->dir, V->n)); TRY(dalloc(V, &V->tmp, V->n)); TRY(dalloc(V, &V->prec, V->n));
+  TRY(dalloc(V, &V->sv_u, V->nu)); TRY(dalloc(V, &V->sv_v, V->nv)); TRY(dalloc(V, &V->sv_w, V->nw));
+  TRY(dalloc(V, &V->sv_p, V->n)); TRY(dalloc(V, &V->sv_eta, V->ncol)); TRY(dalloc(V, &V->sv_rof, V->ncol));
+  TRY(dalloc(V, &V->flux_x, (size_t)(V->nx + 1) * V->ny)); TRY(dalloc(V, &V->flux_y, (size_t)V->nx * (V->ny + 1)));
+  float* q;
+  TRY(dalloc(V, &q, (size_t)blocks_for(V->n) * 2 + 64)); V->p64 = (double*)q;
+  TRY(dalloc(V, &V->p32, (size_t)(V->n + CHUNK - 1) / CHUNK + 64));
+  TRY(dalloc(V, &q, sizeof(Scalars) / sizeof(float) + 16)); V->dS = (Scalars*)q;
+  TRY(dalloc(V, &q, 16)); V->dflag = (int*)q;
+  CK(cudaMallocHost((void**)&V->hS, sizeof(Scalars)));
+  CK(cudaMallocHost((void**)&V->hflag, sizeof(int)));
+  memset(V->hS, 0, sizeof(Scalars));
+  // eta = z0 everywhere (delta3d.rs:255)
+  std::vector<float> z0(V->ncol, V->z0);
+  CK(cudaMemcpyAsync(V->eta, z0.data(), V->ncol * sizeof(float), cudaMemcpyHostToDevice, V->stream));
+  CK(cudaMemcpyAsync(V->sv_eta, z0.data(), V->ncol * sizeof(float), cudaMemcpyHostToDevice, V->stream));
+  return sync(V);
+}
+
+int configure(const fd3_domain* dom, float rho, float g_eff, fd3_volume** out) {
+  if (!dom || !out) return FD3_ERR_INVALID_ARGUMENT;
+  uint64_t nx = dom->nx, ny = dom->ny, nz = dom->nz;
+  float dx = dom->dx;
+  // delta3d.rs:212-243
+  if (nx == 0 || ny == 0 || nz == 0 || !std::isfinite(dx) || dx <= 0.f) return FD3_ERR_DOMAIN;
+  if (!std::isfinite(rho) || rho <= 0.f || !std::isfinite(g_eff)) return FD3_ERR_NOT_FINITE;
+  // Index arithmetic on the device is 32-bit: every array must hold fewer than 2^31 entries.
+  const uint64_t lim = (1ull << 31) - 1;
+  if (nx > lim || ny > lim || nz > lim) return FD3_ERR_DOMAIN;
+  unsigned __int128 cells = (unsigned __int128)nx * ny * nz;
+  unsigned __int128 nw = (unsigned __int128)nx * ny * (nz + 1);
+  unsigned __int128 nu = (unsigned __int128)(nx + 1) * ny * nz;
+  unsigned __int128 nv = (unsigned __int128)nx * (ny + 1) * nz;
+  if (cells > lim || nw > lim || nu > lim || nv > lim) return FD3_ERR_DOMAIN;
+  float z0 = (float)nz * dx;
+  if (!(std::isfinite(z0) && std::isfinite((float)nx * dx) && std::isfinite((float)ny * dx))) return FD3_ERR_DOMAIN;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return FD3_ERR_NO_DEVICE;
+  fd3_volume* V = new (std::nothrow) fd3_volume();
+  if (!V) return FD3_ERR_OUT_OF_MEMORY;
+  cudaGetDevice(&V->device);
+  if (cudaStreamCreateWithFlags(&V->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete V;
+    return cuda_fail(cudaGetLastError(), "cudaStreamCreateWithFlags", __LINE__);
+  }
+  V->stream = V->own_stream;
+  V->nx = (int)nx; V->ny = (int)ny; V->nz = (int)nz;
+  V->n = (int)cells; V->nu = (int)nu; V->nv = (int)nv; V->nw = (int)nw; V->ncol = (int)(nx * ny);
+  V->dx = dx; V->rho = rho; V->g = g_eff; V->z0 = z0; V->rest = z0;
+  V->opt.reduction = FD3_REDUCE_F64;
+  V->opt.mg_max_levels = 0;
+  V->opt.use_graphs = 1;
+  int e = alloc_state(V);
+  if (e) { release(V); delete V; return e; }
+  *out = V;
+  return FD3_OK;
+}
+
+int build_bottom_cut(fd3_volume* V, const float* bottom) {
+  TRY(dalloc(V, &V->frac, V->n)); TRY(dalloc(V, &V->ou, V->nu)); TRY(dalloc(V, &V->ov, V->nv));
+  TRY(dalloc(V, &V->ow, V->nw)); TRY(dalloc(V, &V->floor_, V->ncol));
+  float *dbottom, *corner;
+  TRY(dalloc(V, &dbottom, V->ncol));
+  TRY(dalloc(V, &corner, (size_t)(V->nx + 1) * (V->ny + 1)));
+  CK(cudaMemcpyAsync(dbottom, bottom, V->ncol * sizeof(float), cudaMemcpyHostToDevice, V->stream));
+  LAUNCH(V, k_corners, (long long)(V->nx + 1) * (V->ny + 1), V->nx, V->ny, (const float*)dbottom, corner);
+  CutGeo C{V->nx, V->ny, V->nz, V->dx, corner, V->frac, V->ou, V->ov, V->ow, V->floor_};
+  LAUNCH(V, k_cut_frac, V->n, C);
+  LAUNCH(V, k_cut_faces, (long long)V->nu + V->nv + V->nw, C);
+  LAUNCH(V, k_seal_isolated, V->n, C);
+  LAUNCH(V, k_floor, V->ncol, C);
+  V->cut = true;
+  return sync(V);
+}
+
+int validate_bottom(const fd3_domain* dom, const float* bottom, size_t len) {
+  uint64_t cols;
+  if (__builtin_mul_overflow(dom->nx, dom->ny, &cols)) return FD3_ERR_DOMAIN;
+  if (len != cols) return FD3_ERR_SHAPE;
+  if (!bottom && len) return FD3_ERR_INVALID_ARGUMENT;
+  float z0 = (float)dom->nz * dom->dx;
+  for (size_t q = 0; q < len; ++q)
+    if (!std::isfinite(bottom[q]) || bottom[q] < 0.f || bottom[q] >= z0) return FD3_ERR_NOT_FINITE;
+  return FD3_OK;
+}
+
+
+int in_bounds(fd3_volume* V, bool* ok) {
+  CK(cudaMemsetAsync(V->dflag, 0, sizeof(int), V->stream));
+  LAUNCH(V, k_in_bounds, V->ncol, V->geo(), (const float*)V->floor_, V->dflag);
+  CK(cudaMemcpyAsync(V->hflag, V->dflag, sizeof(int), cudaMemcpyDeviceToHost, V->stream));
+  TRY(sync(V));
+  *ok = *V->hflag == 0;
+  return FD3_OK;
+}
+
+int save_state(fd3_volume* V) {
+  CK(cudaMemcpyAsync(V->sv_u, V->u, (size_t)V->nu * 4, cudaMemcpyDeviceToDevice, V->stream));
+  CK(cudaMemcpyAsync(V->sv_v, V->v, (size_t)V->nv * 4, cudaMemcpyDeviceToDevice, V->stream));
+  CK(cudaMemcpyAsync(V->sv_w, V->w, (size_t)V->nw * 4, cudaMemcpyDeviceToDevice, V->stream));
+  CK(cudaMemcpyAsync(V->sv_p, V->p, (size_t)V->n * 4, cudaMemcpyDeviceToDevice, V->stream));
+  CK(cudaMemcpyAsync(V->sv_eta, V->eta, (size_t)V->ncol * 4, cudaMemcpyDeviceToDevice, V->stream));
+  CK(cudaMemcpyAsync(V->sv_rof, V->rof, (size_t)V->ncol * 4, cudaMemcpyDeviceToDevice, V->stream));
+  return FD3_OK;
+}
+
+void restore_state(fd3_volume* V) {
+  cudaMemcpyAsync(V->u, V->sv_u, (size_t)V->nu * 4, cudaMemcpyDeviceToDevice, V->stream);
+  cudaMemcpyAsync(V->v, V->sv_v, (size_t)V->nv * 4, cudaMemcpyDeviceToDevice, V->stream);
+  cudaMemcpyAsync(V->w, V->sv_w, (size_t)V->nw * 4, cudaMemcpyDeviceToDevice, V->stream);
+  cudaMemcpyAsync(V->p, V->sv_p, (size_t)V->n * 4, cudaMemcpyDeviceToDevice, V->stream);
+  cudaMemcpyAsync(V->eta, V->sv_eta, (size_t)V->ncol * 4, cudaMemcpyDeviceToDevice, V->stream);
+  cudaMemcpyAsync(V->rof, V->sv_rof, (size_t)V->ncol * 4, cudaMemcpyDeviceToDevice, V->stream);
+  cudaStreamSynchronize(V->stream);
+}
+
+// The body of step_surface_mobile after the saves (delta3d_mobile.rs:857-911).
+int step_body(fd3_volume* V, float scale, float correction, float transport, float advection, uint32_t max_iters,
+              fd3_report* rep) {
+  Geo G = V->geo();
+  LAUNCH(V, k_advect, (long long)V->nu + V->nv + V->nw, G, advection, (const float*)V->u, (const float*)V->v,
+         (const float*)V->w, V->us, V->vs, V->ws);
+  TRY(project_mobile3(V, scale, correction, max_iters, rep));
+  if (rep->degraded) {
+    V->has_refused = true;
+    V->refused = *rep;
+    return FD3_ERR_CONVERGENCE;
+  }
+  LAUNCH(V, k_extrapolate, 3LL * V->ncol, G, V->u, V->v, V->w);
+  LAUNCH(V, k_transport_flux, (long long)(V->nx + 1) * V->ny + (long long)V->nx * (V->ny + 1), G, (const float*)V->u,
+         (const float*)V->v, V->flux_x, V->flux_y);
+  LAUNCH(V, k_transport_eta, V->ncol, G, transport, (const float*)V->flux_x, (const float*)V->flux_y, V->eta, V->rof);
+  // every field finite (delta3d_mobile.rs:885-906)
+  struct { const float* x; long long n; } fields[] = {
+      {V->u, V->nu}, {V->v, V->nv}, {V->w, V->nw}, {V->p, V->n}, {V->eta, V->ncol}, {V->rof, V->ncol},
+      {V->us, V->nu}, {V->vs, V->nv}, {V->ws, V->nw}, {V->rhs, V->n}, {V->res, V->n}, {V->dir, V->n},
+      {V->tmp, V->n}, {V->prec, V->n}};
+  CK(cudaMemsetAsync(V->dflag, 0, sizeof(int), V->stream));
+  for (auto& f : fields) {
+    LAUNCH_G(V, k_check_finite, 592, TPB, f.n, f.x, V->dflag);
+  }
+  CK(cudaMemcpyAsync(V->hflag, V->dflag, sizeof(int), cudaMemcpyDeviceToHost, V->stream));
+  TRY(sync(V));
+  if (*V->hflag) return FD3_ERR_NOT_FINITE;
+  if (!std::isfinite(rep->residual) || !std::isfinite(rep->divergence)) return FD3_ERR_NOT_FINITE;
+  bool ok;
+  TRY(in_bounds(V, &ok));
+  if (!ok) return FD3_ERR_DOMAIN;
+  return FD3_OK;
+}
+
+// step_surface_mobile (delta3d_mobile.rs:819-927).
+int step_surface_mobile(fd3_volume* V, uint64_t duration_us, uint32_t max_iters, fd3_report* rep) {
+  if (duration_us == 0 || duration_us > (1ull << 53)) return FD3_ERR_NOT_FINITE;
+  double dt = (double)duration_us * 1e-6;
+  bool ok;
+  TRY(in_bounds(V, &ok));
+  if (V->g <= 0.f || dt * dt * (double)V->g / (double)V->dx > 1. || !ok) return FD3_ERR_DOMAIN;
+  float scale = (float)(-(double)V->rho / dt);
+  float correction = (float)(dt / (double)V->rho);
+  float transport = (float)(dt / (double)V->dx);
+  float advection = (float)dt;
+  if (!std::isfinite(scale) || !std::isfinite(correction) || correction == 0.f || !std::isfinite(transport) ||
+      transport == 0.f || !(advection > 0.f))
+    return FD3_ERR_NOT_FINITE;
+  TRY(save_state(V));
+  int e = step_body(V, scale, correction, transport, advection, max_iters, rep);
+  if (e) restore_state(V);
+  return e;
+}
+
+}  // namespace
+
+// =============================================================================== C ABI
+extern "C" {
+
+const char* fd3_version(void) { return "fluidisim_b200 delta3d 0.1 (sm_100a)"; }
+const char* fd3_last_cuda_error(void) { return g_last_cuda_error.c_str(); }
+
+int fd3_status_name(int status, char* buf, size_t len) {
+  const char* s;
+  switch (status) {
+    case FD3_OK: s = "Ok"; break;
+    case FD3_ERR_DOMAIN: s = "Domain"; break;
+    case FD3_ERR_NOT_FINITE: s = "NotFinite"; break;
+    case FD3_ERR_SHAPE: s = "Shape"; break;
+    case FD3_ERR_BUDGET: s = "Budget"; break;
+    case FD3_ERR_CLOCK: s = "Clock"; break;
+    case FD3_ERR_CONVERGENCE: s = "Convergence"; break;
+    case FD3_ERR_BACKGROUND_CONTEXT: s = "BackgroundContext"; break;
+    case FD3_ERR_NON_PLANAR: s = "NonPlanar"; break;
+    case FD3_ERR_CUDA: s = "Cuda"; break;
+    case FD3_ERR_NO_DEVICE: s = "NoDevice"; break;
+    case FD3_ERR_INVALID_ARGUMENT: s = "InvalidArgument"; break;
+    case FD3_ERR_OUT_OF_MEMORY: s = "OutOfMemory"; break;
+    default: s = "Unknown"; break;
+  }
+  if (buf && len) { strncpy(buf, s, len - 1); buf[len - 1] = 0; }
+  return FD3_OK;
+}
+
+int fd3_configure(const fd3_domain* domain, float rho, float g_eff, fd3_volume** out) {
+  return configure(domain, rho, g_eff, out);
+}
+
+// delta3d.rs:300-321
+int fd3_configure_with_bottom(const fd3_domain* domain, float rho, float g_eff, const float* bottom, size_t len,
+                              fd3_volume** out) {
+  if (!domain || !out) return FD3_ERR_INVALID_ARGUMENT;
+  TRY(validate_bottom(domain, bottom, len));
+  fd3_volume* V;
+  TRY(configure(domain, rho, g_eff, &V));
+  int e = build_bottom_cut(V, bottom);
+  if (e) { release(V); delete V; return e; }
+  *out = V;
+  return FD3_OK;
+}
+
+// delta3d.rs:327-365
+int fd3_configure_with_solid(const fd3_domain* domain, float rho, float g_eff, const float* bottom, size_t blen,
+                             const float* solid, size_t slen, fd3_volume** out) {
+  if (!domain || !out) return FD3_ERR_INVALID_ARGUMENT;
+  unsigned __int128 nodes = (unsigned __int128)(domain->nx + 1) * (domain->ny + 1) * (domain->nz + 1);
+  if (nodes > (unsigned __int128)SIZE_MAX) return FD3_ERR_DOMAIN;
+  if (slen != (size_t)nodes) return FD3_ERR_SHAPE;
+  if (!solid && slen) return FD3_ERR_INVALID_ARGUMENT;
+  for (size_t q = 0; q < slen; ++q)
+    if (!std::isfinite(solid[q])) return FD3_ERR_NOT_FINITE;
+  fd3_volume* V;
+  TRY(fd3_configure_with_bottom(domain, rho, g_eff, bottom, blen, &V));
+  auto fail = [&](int e) { release(V); delete V; return e; };
+  float* dsdf;
+  int e = dalloc(V, &dsdf, slen);
+  if (e) return fail(e);
+  if (cudaMemcpyAsync(dsdf, solid, slen * sizeof(float), cudaMemcpyHostToDevice, V->stream) != cudaSuccess)
+    return fail(cuda_fail(cudaGetLastError(), "solid upload", __LINE__));
+  SolidGeo S{V->nx, V->ny, V->nz, V->dx, dsdf, 0};
+  cudaMemsetAsync(V->dflag, 0, sizeof(int), V->stream);
+  long long all = (long long)V->n + V->nu + V->nv + V->nw;
+  LAUNCH(V, k_check_solid, all, S, (const float*)V->frac, (const float*)V->ou, (const float*)V->ov, (const float*)V->ow, V->dflag);
+  cudaMemcpyAsync(V->hflag, V->dflag, sizeof(int), cudaMemcpyDeviceToHost, V->stream);
+  if ((e = sync(V))) return fail(e);
+  if (*V->hflag) return fail(FD3_ERR_DOMAIN);
+  LAUNCH(V, k_add_solid, all, S, V->frac, V->ou, V->ov, V->ow, V->floor_);
+  CutGeo C{V->nx, V->ny, V->nz, V->dx, nullptr, V->frac, V->ou, V->ov, V->ow, V->floor_};
+  LAUNCH(V, k_seal_isolated, V->n, C);
+  if ((e = sync(V))) return fail(e);
+  *out = V;
+  return FD3_OK;
+}
+
+void fd3_destroy(fd3_volume* v) {
+  if (!v) return;
+  if (v->stream) cudaStreamSynchronize(v->stream);
+  release(v);
+  delete v;
+}
+
+int fd3_set_options(fd3_volume* v, const fd3_options* o) {
+  if (!v || !o) return FD3_ERR_INVALID_ARGUMENT;
+  if (o->reduction > 1) return FD3_ERR_DOMAIN;
+  v->opt = *o;
+  return FD3_OK;
+}
+
+int fd3_get_options(const fd3_volume* v, fd3_options* o) {
+  if (!v || !o) return FD3_ERR_INVALID_ARGUMENT;
+  *o = v->opt;
+  return FD3_OK;
+}
+
+int fd3_set_stream(fd3_volume* v, void* stream) {
+  if (!v) return FD3_ERR_INVALID_ARGUMENT;
+  TRY(sync(v));
+  v->stream = stream ? (cudaStream_t)stream : v->own_stream;
+  if (v->iter_exec) { cudaGraphExecDestroy(v->iter_exec); v->iter_exec = nullptr; }
+  return FD3_OK;
+}
+
+// delta3d_multigrid.rs:339-349: coarse levels while all dims are even and >= 4.
+int fd3_enable_multigrid(fd3_volume* V) {
+  if (!V) return FD3_ERR_INVALID_ARGUMENT;
+  if (V->has_mg) return FD3_OK;
+  TRY(dalloc(V, &V->z, V->n));
+  TRY(dalloc(V, &V->z2, V->n));
+  int x = V->nx, y = V->ny, zz = V->nz;
+  float h = V->dx;
+  while (x % 2 == 0 && y % 2 == 0 && zz % 2 == 0 && x >= 4 && y >= 4 && zz >= 4 &&
+         (V->opt.mg_max_levels == 0 || V->levels.size() < V->opt.mg_max_levels)) {
+    int cx = x / 2, cy = y / 2, cz = zz / 2;
+    h *= 2.f;
+    Lev L{};
+    L.nx = cx; L.ny = cy; L.nz = cz; L.n = cx * cy * cz;
+    L.inv = 1.f / (h * h);
+    TRY(dalloc(V, &L.ou, (size_t)(cx + 1) * cy * cz));
+    TRY(dalloc(V, &L.ov, (size_t)cx * (cy + 1) * cz));
+    TRY(dalloc(V, &L.ow, (size_t)cx * cy * (cz + 1)));
+    TRY(dalloc(V, &L.kind, L.n)); TRY(dalloc(V, &L.diag, L.n));
+    TRY(dalloc(V, &L.x, L.n)); TRY(dalloc(V, &L.x2, L.n)); TRY(dalloc(V, &L.r, L.n)); TRY(dalloc(V, &L.t, L.n));
+    V->levels.push_back(L);
+    x = cx; y = cy; zz = cz;
+  }
+  V->has_mg = true;
+  return sync(V);
+}
+
+int fd3_multigrid_levels(const fd3_volume* v) { return v && v->has_mg ? (int)v->levels.size() : -1; }
+
+// delta3d_mobile.rs:9-25
+int fd3_set_free_surface(fd3_volume* V, const float* eta, size_t len, float rest) {
+  if (!V || (!eta && len)) return FD3_ERR_INVALID_ARGUMENT;
+  if (len != (size_t)V->ncol) return FD3_ERR_SHAPE;
+  if (!std::isfinite(rest)) return FD3_ERR_NOT_FINITE;
+  for (size_t q = 0; q < len; ++q)
+    if (!std::isfinite(eta[q])) return FD3_ERR_NOT_FINITE;
+  CK(cudaMemcpyAsync(V->eta, eta, len * sizeof(float), cudaMemcpyHostToDevice, V->stream));
+  CK(cudaMemsetAsync(V->rof, 0, len * sizeof(float), V->stream));
+  CK(cudaMemsetAsync(V->p, 0, (size_t)V->n * sizeof(float), V->stream));
+  V->rest = rest;
+  return sync(V);
+}
+
+// delta3d.rs:614-628
+int fd3_set_surface(fd3_volume* V, const float* eta, size_t len) {
+  if (!V || (!eta && len)) return FD3_ERR_INVALID_ARGUMENT;
+  if (len != (size_t)V->ncol) return FD3_ERR_SHAPE;
+  for (size_t q = 0; q < len; ++q)
+    if (!std::isfinite(eta[q])) return FD3_ERR_NOT_FINITE;
+  CK(cudaMemcpyAsync(V->eta, eta, len * sizeof(float), cudaMemcpyHostToDevice, V->stream));
+  CK(cudaMemsetAsync(V->rof, 0, len * sizeof(float), V->stream));
+  return sync(V);
+}
+
+// delta3d.rs:631-645: the faces are staged in us/vs/ws, checked on the device, then published.
+static int set_velocity_staged(fd3_volume* V) {
+  bool ok1, ok2, ok3;
+  TRY(check_finite_device(V, V->us, V->nu, &ok1));
+  TRY(check_finite_device(V, V->vs, V->nv, &ok2));
+  TRY(check_finite_device(V, V->ws, V->nw, &ok3));
+  if (!(ok1 && ok2 && ok3)) return FD3_ERR_NOT_FINITE;
+  CK(cudaMemcpyAsync(V->u, V->us, (size_t)V->nu * 4, cudaMemcpyDeviceToDevice, V->stream));
+  CK(cudaMemcpyAsync(V->v, V->vs, (size_t)V->nv * 4, cudaMemcpyDeviceToDevice, V->stream));
+  CK(cudaMemcpyAsync(V->w, V->ws, (size_t)V->nw * 4, cudaMemcpyDeviceToDevice, V->stream));
+  LAUNCH(V, k_close_walls, (long long)V->nu + V->nv + V->nw, V->geo(), V->u, V->v, V->w);
+  return sync(V);
+}
+
+int fd3_set_velocity(fd3_volume* V, const float* u, size_t nu, const float* vv, size_t nv, const float* w, size_t nw) {
+  if (!V || !u || !vv || !w) return FD3_ERR_INVALID_ARGUMENT;
+  if (nu != (size_t)V->nu || nv != (size_t)V->nv || nw != (size_t)V->nw) return FD3_ERR_SHAPE;
+  CK(cudaMemcpyAsync(V->us, u, nu * 4, cudaMemcpyHostToDevice, V->stream));
+  CK(cudaMemcpyAsync(V->vs, vv, nv * 4, cudaMemcpyHostToDevice, V->stream));
+  CK(cudaMemcpyAsync(V->ws, w, nw * 4, cudaMemcpyHostToDevice, V->stream));
+  return set_velocity_staged(V);
+}
+
+int fd3_set_velocity_device(fd3_volume* V, const float* u, const float* vv, const float* w) {
+  if (!V || !u || !vv || !w) return FD3_ERR_INVALID_ARGUMENT;
+  CK(cudaMemcpyAsync(V->us, u, (size_t)V->nu * 4, cudaMemcpyDeviceToDevice, V->stream));
+  CK(cudaMemcpyAsync(V->vs, vv, (size_t)V->nv * 4, cudaMemcpyDeviceToDevice, V->stream));
+  CK(cudaMemcpyAsync(V->ws, w, (size_t)V->nw * 4, cudaMemcpyDeviceToDevice, V->stream));
+  return set_velocity_staged(V);
+}
+
+int fd3_reset_pressure(fd3_volume* V) {
+  if (!V) return FD3_ERR_INVALID_ARGUMENT;
+  CK(cudaMemsetAsync(V->p, 0, (size_t)V->n * sizeof(float), V->stream));
+  return FD3_OK;
+}
+
+// tests_delta3d.rs:392-395: us = u, then project_mobile3.  A refusal leaves u, v, w, p untouched.
+int fd3_project_mobile(fd3_volume* V, float scale, float k1, uint32_t max_iters, fd3_report* rep) {
+  if (!V || !rep) return FD3_ERR_INVALID_ARGUMENT;
+  CK(cudaMemcpyAsync(V->us, V->u, (size_t)V->nu * 4, cudaMemcpyDeviceToDevice, V->stream));
+  CK(cudaMemcpyAsync(V->vs, V->v, (size_t)V->nv * 4, cudaMemcpyDeviceToDevice, V->stream));
+  CK(cudaMemcpyAsync(V->ws, V->w, (size_t)V->nw * 4, cudaMemcpyDeviceToDevice, V->stream));
+  CK(cudaMemcpyAsync(V->sv_p, V->p, (size_t)V->n * 4, cudaMemcpyDeviceToDevice, V->stream));
+  int e = project_mobile3(V, scale, k1, max_iters, rep);
+  if (e) {
+    cudaMemcpyAsync(V->u, V->us, (size_t)V->nu * 4, cudaMemcpyDeviceToDevice, V->stream);
+    cudaMemcpyAsync(V->v, V->vs, (size_t)V->nv * 4, cudaMemcpyDeviceToDevice, V->stream);
+    cudaMemcpyAsync(V->w, V->ws, (size_t)V->nw * 4, cudaMemcpyDeviceToDevice, V->stream);
+    cudaMemcpyAsync(V->p, V->sv_p, (size_t)V->n * 4, cudaMemcpyDeviceToDevice, V->stream);
+    cudaStreamSynchronize(V->stream);
+  }
+  return e;
+}
+
+int fd3_step_surface_mobile(fd3_volume* V, uint64_t duration_us, uint32_t max_iters, fd3_report* rep) {
+  if (!V || !rep) return FD3_ERR_INVALID_ARGUMENT;
+  return step_surface_mobile(V, duration_us, max_iters, rep);
+}
+
+int fd3_last_refused_report(const fd3_volume* V, fd3_report* rep) {
+  if (!V || !rep) return FD3_ERR_INVALID_ARGUMENT;
+  if (!V->has_refused) return FD3_ERR_DOMAIN;
+  *rep = V->refused;
+  return FD3_OK;
+}
+
+static int copy_d2h(fd3_volume* V, float* dst, const float* src, size_t len, size_t want) {
+  if (!dst && len) return FD3_ERR_INVALID_ARGUMENT;
+  if (len != want) return FD3_ERR_SHAPE;
+  CK(cudaMemcpyAsync(dst, src, len * 4, cudaMemcpyDeviceToHost, V->stream));
+  return FD3_OK;
+}
+
+int fd3_get_pressure(const fd3_volume* cv, float* out, size_t len) {
+  if (!cv) return FD3_ERR_INVALID_ARGUMENT;
+  fd3_volume* V = const_cast<fd3_volume*>(cv);
+  TRY(copy_d2h(V, out, V->p, len, V->n));
+  return sync(V);
+}
+
+int fd3_get_velocity(const fd3_volume* cv, float* u, size_t nu, float* vv, size_t nv, float* w, size_t nw) {
+  if (!cv) return FD3_ERR_INVALID_ARGUMENT;
+  fd3_volume* V = const_cast<fd3_volume*>(cv);
+  TRY(copy_d2h(V, u, V->u, nu, V->nu));
+  TRY(copy_d2h(V, vv, V->v, nv, V->nv));
+  TRY(copy_d2h(V, w, V->w, nw, V->nw));
+  return sync(V);
+}
+
+int fd3_get_surface(const fd3_volume* cv, float* eta, float* roundoff, size_t len) {
+  if (!cv) return FD3_ERR_INVALID_ARGUMENT;
+  fd3_volume* V = const_cast<fd3_volume*>(cv);
+  TRY(copy_d2h(V, eta, V->eta, len, V->ncol));
+  TRY(copy_d2h(V, roundoff, V->rof, len, V->ncol));
+  return sync(V);
+}
+
+int fd3_device_fields(const fd3_volume* V, float** p, float** u, float** vv, float** w) {
+  if (!V) return FD3_ERR_INVALID_ARGUMENT;
+  if (p) *p = V->p;
+  if (u) *u = V->u;
+  if (vv) *vv = V->v;
+  if (w) *w = V->w;
+  return FD3_OK;
+}
+
+int fd3_get_geometry(const fd3_volume* cv, float* frac, float* ou, float* ov, float* ow, float* floor) {
+  if (!cv) return FD3_ERR_INVALID_ARGUMENT;
+  if (!cv->cut) return FD3_ERR_DOMAIN;
+  fd3_volume* V = const_cast<fd3_volume*>(cv);
+  TRY(copy_d2h(V, frac, V->frac, V->n, V->n));
+  TRY(copy_d2h(V, ou, V->ou, V->nu, V->nu));
+  TRY(copy_d2h(V, ov, V->ov, V->nv, V->nv));
+  TRY(copy_d2h(V, ow, V->ow, V->nw, V->nw));
+  TRY(copy_d2h(V, floor, V->floor_, V->ncol, V->ncol));
+  return sync(V);
+}
+
+__global__ void k_count_wet(Geo g, unsigned long long* count) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  bool wet = false;
+  if (c < g.n) { int i, j, k; cell_ijk(g, c, i, j, k); wet = wet3(g, i, j, k); }
+  unsigned m = __ballot_sync(0xffffffffu, wet);
+  if ((threadIdx.x & 31) == 0 && m) atomicAdd(count, (unsigned long long)__popc(m));
+}
+
+uint64_t fd3_wet_cells(const fd3_volume* cv) {
+  if (!cv) return 0;
+  fd3_volume* V = const_cast<fd3_volume*>(cv);
+  LAUNCH_G(V, k_reset_diag, 1, 1, V->dS, 4);
+  LAUNCH(V, k_count_wet, V->n, V->geo(), &V->dS->hash);
+  if (pull(V)) return 0;
+  return V->hS->hash;
+}
+
+// delta3d_mobile.rs:936-953
+int fd3_apply_pressure_operator_for_trials(fd3_volume* V, const float* p, float* out, size_t len) {
+  if (!V || !p || !out) return FD3_ERR_INVALID_ARGUMENT;
+  if (len != (size_t)V->n) return FD3_ERR_DOMAIN;
+  CK(cudaMemcpyAsync(V->tmp, p, len * 4, cudaMemcpyHostToDevice, V->stream));
+  bool ok;
+  TRY(check_finite_device(V, V->tmp, V->n, &ok));
+  if (!ok) return FD3_ERR_NOT_FINITE;
+  LAUNCH(V, k_apply, V->n, V->geo(), (const float*)V->tmp, V->dir);
+  CK(cudaMemcpyAsync(out, V->dir, len * 4, cudaMemcpyDeviceToHost, V->stream));
+  return sync(V);
+}
+
+// delta3d_mobile.rs:960-979
+int fd3_assemble_pressure_problem_for_trials(fd3_volume* V, const float* divergence, float scale, float* rhs,
+                                             float* prec, size_t len) {
+  if (!V || !divergence || !rhs || !prec) return FD3_ERR_INVALID_ARGUMENT;
+  if (len != (size_t)V->n) return FD3_ERR_DOMAIN;
+  if (!std::isfinite(scale)) return FD3_ERR_NOT_FINITE;
+  CK(cudaMemcpyAsync(V->tmp, divergence, len * 4, cudaMemcpyHostToDevice, V->stream));
+  bool ok;
+  TRY(check_finite_device(V, V->tmp, V->n, &ok));
+  if (!ok) return FD3_ERR_NOT_FINITE;
+  CK(cudaMemcpyAsync(V->rhs, V->tmp, len * 4, cudaMemcpyDeviceToDevice, V->stream));
+  DISPATCH(V, k_rhs_mobile, V->n, V->geo(), scale, V->rhs, V->prec, V->red(), V->dS, 0);
+  CK(cudaMemcpyAsync(rhs, V->rhs, len * 4, cudaMemcpyDeviceToHost, V->stream));
+  CK(cudaMemcpyAsync(prec, V->prec, len * 4, cudaMemcpyDeviceToHost, V->stream));
+  return sync(V);
+}
+
+// tests_delta3d.rs:1840-1873 set-up, then v_cycle3.
+int fd3_vcycle_for_tests(fd3_volume* V, const float* x, float* z, size_t len) {
+  if (!V || !x || !z) return FD3_ERR_INVALID_ARGUMENT;
+  if (!V->has_mg) return FD3_ERR_DOMAIN;
+  if (len != (size_t)V->n) return FD3_ERR_SHAPE;
+  CK(cudaMemsetAsync(V->rhs, 0, len * 4, V->stream));
+  DISPATCH(V, k_rhs_mobile, V->n, V->geo(), 1.f, V->rhs, V->prec, V->red(), V->dS, 0);
+  prepare_multigrid(V);
+  CK(cudaMemcpyAsync(V->res, x, len * 4, cudaMemcpyHostToDevice, V->stream));
+  vcycle(V, 0);
+  CK(cudaMemcpyAsync(z, V->z, len * 4, cudaMemcpyDeviceToHost, V->stream));
+  return sync(V);
+}
+
+int fd3_level_geometry(const fd3_volume* cv, uint32_t l, float* kind, float* diag, float* ou, float* ov, float* ow) {
+  if (!cv) return FD3_ERR_INVALID_ARGUMENT;
+  if (!cv->has_mg || l >= cv->levels.size()) return FD3_ERR_DOMAIN;
+  fd3_volume* V = const_cast<fd3_volume*>(cv);
+  const Lev& L = V->levels[l];
+  size_t nu = (size_t)(L.nx + 1) * L.ny * L.nz, nv = (size_t)L.nx * (L.ny + 1) * L.nz, nw = (size_t)L.nx * L.ny * (L.nz + 1);
+  TRY(copy_d2h(V, kind, L.kind, L.n, L.n));
+  TRY(copy_d2h(V, diag, L.diag, L.n, L.n));
+  TRY(copy_d2h(V, ou, L.ou, nu, nu));
+  TRY(copy_d2h(V, ov, L.ov, nv, nv));
+  TRY(copy_d2h(V, ow, L.ow, nw, nw));
+  return sync(V);
+}
+
+uint64_t fd3_kernel_launches(const fd3_volume* V) { return V ? V->launches : 0; }
+
+int fd3_profile(fd3_volume* V, int on) {
+  if (!V) return FD3_ERR_INVALID_ARGUMENT;
+  TRY(sync(V));
+  V->prof = on != 0;
+  V->pending.clear();
+  V->ev_next = 0;
+  if (on) { V->prof_names.clear(); V->prof_count.clear(); V->prof_ms.clear(); }
+  return FD3_OK;
+}
+
+int fd3_profile_count(const fd3_volume* V) { return V ? (int)V->prof_names.size() : 0; }
+
+int fd3_profile_entry(const fd3_volume* V, int idx, char* name, size_t len, uint64_t* launches, double* total_ms) {
+  if (!V || idx < 0 || idx >= (int)V->prof_names.size()) return FD3_ERR_INVALID_ARGUMENT;
+  if (name && len) { strncpy(name, V->prof_names[idx].c_str(), len - 1); name[len - 1] = 0; }
+  if (launches) *launches = V->prof_count[idx];
+  if (total_ms) *total_ms = V->prof_ms[idx];
+  return FD3_OK;
+}
+
+}  // extern "C"

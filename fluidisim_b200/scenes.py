@@ -57,19 +57,18 @@ class SplitMix64:
         return lo + (hi - lo) * ((self.next_u64() >> 11) * (1.0 / (1 << 53)))
 
     def normal_array(self, n: int, sigma: float) -> np.ndarray:
-        """n draws of N(0, sigma) by Box-Muller on SplitMix64 uniforms (vectorised)."""
+        """n draws of N(0, sigma) (f32) by Box-Muller on two counter-based SplitMix64 streams."""
         m = (n + 1) // 2
-        raw = np.empty(2 * m, dtype=np.uint64)
-        for q in range(2 * m):
-            raw[q] = self.next_u64()
-        u = ((raw >> np.uint64(11)).astype(np.float64) + 0.5) * (1.0 / (1 << 53))
-        r = np.sqrt(-2.0 * np.log(u[:m]))
-        t = 2.0 * np.pi * u[m:]
+        u1 = self._unit_stream(m, offset=0.5)
+        u2 = self._unit_stream(m, offset=0.0)
+        r = np.sqrt(-2.0 * np.log(u1))
+        t = 2.0 * np.pi * u2
         z = np.concatenate([r * np.cos(t), r * np.sin(t)])[:n]
         return (sigma * z).astype(np.float32)
 
-    def uniform_array(self, n: int, lo: float, hi: float) -> np.ndarray:
-        """n draws of U[lo, hi) as f32, from a fast counter-based SplitMix64 stream seeded here."""
+    def _unit_stream(self, n: int, offset: float = 0.0) -> np.ndarray:
+        """n f64 values in [0,1) (offset 0.5 shifts them into (0,1)) from a SplitMix64 counter stream
+        whose base is the next draw of this generator."""
         base = np.uint64(self.next_u64())
         idx = np.arange(n, dtype=np.uint64)
         with np.errstate(over="ignore"):
@@ -77,8 +76,11 @@ class SplitMix64:
             z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
             z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
             z = z ^ (z >> np.uint64(31))
-        x = (z >> np.uint64(11)).astype(np.float64) * (1.0 / (1 << 53))
-        return (lo + (hi - lo) * x).astype(np.float32)
+        return ((z >> np.uint64(11)).astype(np.float64) + offset) * (1.0 / (1 << 53))
+
+    def uniform_array(self, n: int, lo: float, hi: float) -> np.ndarray:
+        """n draws of U[lo, hi) as f32 from a counter-based SplitMix64 stream."""
+        return (lo + (hi - lo) * self._unit_stream(n)).astype(np.float32)
 
 
 def noise(n: int, seed: int) -> np.ndarray:
@@ -120,3 +122,121 @@ def s385_case(nx: int, bump: bool = False) -> dict:
                            for j in range(ny) for i in range(nx)], dtype=np.float32)
     return dict(nx=nx, ny=ny, nz=nz, dx=float(dx), rho=S385_RHO, g=S385_G, bottom=bottom, eta=eta,
                 rest=float(S385_LZ), dt_us=S385_DT_US)
+
+
+# ----------------------------------------------------------------------------------------------
+# Signed distances at the nodes, (nx+1)(ny+1)(nz+1) x-fastest, negative inside (delta3d.rs:322-327).
+
+def _node_grid(nx, ny, nz, dx):
+    d = float(f32(dx))
+    z, y, x = np.meshgrid(np.arange(nz + 1) * d, np.arange(ny + 1) * d, np.arange(nx + 1) * d, indexing="ij")
+    return x, y, z
+
+
+def spheres_sdf(nx, ny, nz, dx, centres, radii) -> np.ndarray:
+    """Union of spheres (centres, radii in metres), as the sphere nodes of tests_delta3d.rs:1161-1179."""
+    x, y, z = _node_grid(nx, ny, nz, dx)
+    out = np.full(x.shape, np.inf)
+    for (cx, cy, cz), r in zip(centres, radii):
+        out = np.minimum(out, np.sqrt((x - cx) ** 2 + (y - cy) ** 2 + (z - cz) ** 2) - r)
+    return out.astype(np.float32).ravel()
+
+
+def boxes_sdf(nx, ny, nz, dx, centres, halves) -> np.ndarray:
+    """Union of boxes (centre, half sizes in metres), the box distance of tests_delta3d.rs:1332-1350."""
+    x, y, z = _node_grid(nx, ny, nz, dx)
+    out = np.full(x.shape, np.inf)
+    for c, h in zip(centres, halves):
+        q = [np.abs(x - c[0]) - h[0], np.abs(y - c[1]) - h[1], np.abs(z - c[2]) - h[2]]
+        outside = np.sqrt(sum(np.maximum(a, 0.0) ** 2 for a in q))
+        inside = np.minimum(np.maximum(np.maximum(q[0], q[1]), q[2]), 0.0)
+        out = np.minimum(out, outside + inside)
+    return out.astype(np.float32).ravel()
+
+
+def face_counts(nx, ny, nz):
+    return (nx + 1) * ny * nz, nx * (ny + 1) * nz, nx * ny * (nz + 1)
+
+
+def sphere_lake(n: int = 64, seed: int = 1, dx: float = 0.1, spheres: int = 8) -> dict:
+    """Closed n^3 box, `spheres` random solid spheres (radius U[3,8] cells, clear of the walls, of the
+    lid layer and of the top two liquid layers), liquid filling the lower half, faces U[-1,1] m/s
+    (set_velocity zeroes the closed faces).  dt = 1/60 s; project with scale = -rho/dt, k1 = dt/rho."""
+    rng = SplitMix64(seed)
+    d = float(f32(dx))
+    eta_cells = n // 2
+    centres, radii = [], []
+    for _ in range(spheres):
+        r = rng.uniform(3.0, 8.0)
+        cx = rng.uniform(r + 1.0, n - r - 1.0)
+        cy = rng.uniform(r + 1.0, n - r - 1.0)
+        cz = rng.uniform(r + 1.0, eta_cells - 2.0 - r)
+        centres.append((cx * d, cy * d, cz * d))
+        radii.append(r * d)
+    sdf = spheres_sdf(n, n, n, dx, centres, radii)
+    nu, nv, nw = face_counts(n, n, n)
+    return dict(nx=n, ny=n, nz=n, dx=float(f32(dx)), rho=1025.0, g=9.81, bottom=np.zeros(n * n, np.float32),
+                solid=sdf, eta=np.full(n * n, f32(eta_cells * d), np.float32), rest=float(f32(eta_cells * d)),
+                u=rng.uniform_array(nu, -1.0, 1.0), v=rng.uniform_array(nv, -1.0, 1.0),
+                w=rng.uniform_array(nw, -1.0, 1.0), dt=1.0 / 60.0)
+
+
+def box_basin(n: int = 128, seed: int = 2, dx: float = 0.1, boxes: int = 16, noise_sigma: float = 0.5) -> dict:
+    """n^3 basin: free surface h = n/2 + sum_{k=1..6} a_k sin(kx x + ky y + phi_k) cells with a_k ~
+    U[1,4] (one height per column: the reference's vertical axis is z), `boxes` random submerged
+    solid boxes, a divergence-free background (discrete curl of a seeded smooth vector potential on
+    the cell edges) plus i.i.d. N(0, noise_sigma) m/s face noise."""
+    rng = SplitMix64(seed)
+    d = float(f32(dx))
+    i = (np.arange(n) + 0.5)
+    X, Y = np.meshgrid(i, i, indexing="xy")
+    h = np.full((n, n), 0.5 * n)
+    for _ in range(6):
+        a = rng.uniform(1.0, 4.0)
+        kx = rng.uniform(-3.0, 3.0) * 2 * np.pi / n
+        ky = rng.uniform(-3.0, 3.0) * 2 * np.pi / n
+        ph = rng.uniform(0.0, 2 * np.pi)
+        h += a * np.sin(kx * X + ky * Y + ph)
+    hmin = float(h.min())
+    eta = (h * d).astype(np.float32).ravel()
+    centres, halves = [], []
+    top_limit = hmin - 4.0
+    for _ in range(boxes):
+        hx, hy, hz = rng.uniform(2.0, 8.0), rng.uniform(2.0, 8.0), rng.uniform(2.0, 6.0)
+        cx = rng.uniform(hx + 1.0, n - hx - 1.0)
+        cy = rng.uniform(hy + 1.0, n - hy - 1.0)
+        cz = rng.uniform(hz + 1.0, max(hz + 1.5, top_limit - hz))
+        centres.append((cx * d, cy * d, cz * d))
+        halves.append((hx * d, hy * d, hz * d))
+    sdf = boxes_sdf(n, n, n, dx, centres, halves)
+    # vector potential on the edges: Ax at (i+1/2, j, k), Ay at (i, j+1/2, k), Az at (i, j, k+1/2)
+    def potential(sx, sy, sz):
+        zz, yy, xx = np.meshgrid(np.arange(n + 1) + sz, np.arange(n + 1) + sy, np.arange(n + 1) + sx, indexing="ij")
+        out = np.zeros(xx.shape)
+        for _ in range(4):
+            kx, ky, kz = (rng.uniform(0.5, 3.0) * 2 * np.pi / n for _ in range(3))
+            amp = rng.uniform(0.5, 1.5) * n * d / (2 * np.pi * 3)
+            ph = rng.uniform(0.0, 2 * np.pi)
+            out += amp * np.sin(kx * xx + ky * yy + kz * zz + ph)
+        return out
+    Ax = potential(0.5, 0.0, 0.0)
+    Ay = potential(0.0, 0.5, 0.0)
+    Az = potential(0.0, 0.0, 0.5)
+    # u(i,j,k) at x = i, y = j+1/2, z = k+1/2: dAz/dy - dAy/dz
+    u = ((Az[:n, 1:n + 1, :n + 1] - Az[:n, :n, :n + 1]) - (Ay[1:n + 1, :n, :n + 1] - Ay[:n, :n, :n + 1])) / d
+    v = ((Ax[1:n + 1, :n + 1, :n] - Ax[:n, :n + 1, :n]) - (Az[:n, :n + 1, 1:n + 1] - Az[:n, :n + 1, :n])) / d
+    w = ((Ay[:n + 1, :n, 1:n + 1] - Ay[:n + 1, :n, :n]) - (Ax[:n + 1, 1:n + 1, :n] - Ax[:n + 1, :n, :n])) / d
+    nu, nv, nw = face_counts(n, n, n)
+    u = u.astype(np.float32).ravel() + rng.normal_array(nu, noise_sigma)
+    v = v.astype(np.float32).ravel() + rng.normal_array(nv, noise_sigma)
+    w = w.astype(np.float32).ravel() + rng.normal_array(nw, noise_sigma)
+    return dict(nx=n, ny=n, nz=n, dx=float(f32(dx)), rho=1025.0, g=9.81, bottom=np.zeros(n * n, np.float32),
+                solid=sdf, eta=eta, rest=float(f32(0.5 * n * d)), u=u.astype(np.float32), v=v.astype(np.float32),
+                w=w.astype(np.float32), dt=1.0 / 60.0)
+
+
+def projection_scalars(scene: dict):
+    """(scale, k1) of a projection with the scene's dt: -rho/dt and dt/rho, rounded to f32 as
+    step_surface_mobile does (delta3d_mobile.rs:838-840)."""
+    dt, rho = scene["dt"], scene["rho"]
+    return float(f32(-rho / dt)), float(f32(dt / rho))

@@ -1,0 +1,168 @@
+/* fluidisim_delta3d.h — C ABI of the B200 delta (δ) MAC-grid pressure projection.
+ *
+ * The drop-in boundary for water-core's `Volume3` projection API.  Each entry point names the
+ * reference function it replaces (paths relative to the reference project, code/water-core/src/).
+ * Plain C types only: no CUDA, no torch.  Link against libfluidisim_delta3d.so.
+ *
+ * Conventions
+ *  - Layouts are the reference's (delta3d.rs:24-28, 187-206): cells c = (k*ny + j)*nx + i, x
+ *    fastest; u faces (nx+1)*ny*nz, v faces nx*(ny+1)*nz, w faces nx*ny*(nz+1); columns j*nx + i;
+ *    SDF nodes (nx+1)*(ny+1)*(nz+1), x fastest.
+ *  - Every entry point returns an fd3_status.  Codes 1..8 are the reference's `Error`
+ *    (delta_projection.rs:133-150) in declaration order; codes >= 100 are device-side failures.
+ *  - Refusals are atomic, as in the reference: on any error the published fields (u, v, w, p,
+ *    eta and its roundoff) keep their previous bits.
+ *  - All device memory is allocated by fd3_configure* and fd3_enable_multigrid; projections and
+ *    steps allocate nothing (the reference's I-06 after `seal()`).
+ *  - One CUDA stream per handle (fd3_set_stream); calls on one handle are not thread-safe, as
+ *    `&mut self` in the reference.
+ */
+#ifndef FLUIDISIM_DELTA3D_H
+#define FLUIDISIM_DELTA3D_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum fd3_status {
+  FD3_OK = 0,
+  FD3_ERR_DOMAIN = 1,             /* Error::Domain */
+  FD3_ERR_NOT_FINITE = 2,         /* Error::NotFinite */
+  FD3_ERR_SHAPE = 3,              /* Error::Shape */
+  FD3_ERR_BUDGET = 4,             /* Error::Budget (never raised here) */
+  FD3_ERR_CLOCK = 5,              /* Error::Clock (never raised here) */
+  FD3_ERR_CONVERGENCE = 6,        /* Error::Convergence */
+  FD3_ERR_BACKGROUND_CONTEXT = 7, /* Error::BackgroundContext (never raised here) */
+  FD3_ERR_NON_PLANAR = 8,         /* Error::NonPlanar (never raised here) */
+  FD3_ERR_CUDA = 100,             /* a CUDA runtime call failed; fd3_last_cuda_error() says which */
+  FD3_ERR_NO_DEVICE = 101,        /* no CUDA device */
+  FD3_ERR_INVALID_ARGUMENT = 102, /* null handle or pointer */
+  FD3_ERR_OUT_OF_MEMORY = 103     /* device allocation failed at configure/enable time */
+} fd3_status;
+
+/* Domain3 (delta3d.rs:44-63): cubic cells of side dx; the lid is z0 = nz*dx. */
+typedef struct fd3_domain {
+  uint64_t nx, ny, nz;
+  float dx;
+} fd3_domain;
+
+/* Report (delta_projection.rs:164-189). */
+typedef struct fd3_report {
+  uint32_t refinements;
+  uint32_t iterations;
+  uint8_t degraded;
+  uint8_t floor;
+  uint8_t pad[6];
+  double residual;
+  double divergence;
+  double backward_error;
+  double divergence_plain;
+} fd3_report;
+
+/* Arithmetic of the global reductions (dot products, norms).
+ *  FD3_REDUCE_F64          FP64 accumulation, FP64 alpha/beta and residual tests (default).
+ *  FD3_REDUCE_ORDERED_F32  the reference's own order and precision (host.rs:60-72,
+ *                          delta3d.rs:860-876): f32 sums of 64-element chunks merged in index
+ *                          order in f32.  With it the whole projection reproduces the reference
+ *                          bit for bit; the in-order merge is serial, so it is a parity mode. */
+typedef enum fd3_reduction { FD3_REDUCE_F64 = 0, FD3_REDUCE_ORDERED_F32 = 1 } fd3_reduction;
+
+typedef struct fd3_options {
+  uint32_t reduction;     /* fd3_reduction */
+  uint32_t mg_max_levels; /* coarse levels kept by fd3_enable_multigrid; 0 = every level the
+                             reference's coarsening rule allows (delta3d_multigrid.rs:73-88) */
+  uint32_t use_graphs;    /* 1 = replay the PCG iteration from a captured CUDA graph */
+  uint32_t reserved[5];
+} fd3_options;
+
+typedef struct fd3_volume fd3_volume;
+
+/* Library and device. */
+const char* fd3_version(void);
+const char* fd3_last_cuda_error(void);
+int fd3_status_name(int status, char* buf, size_t len);
+
+/* Volume3::configure (delta3d.rs:210): flat bottom, lateral walls, open lid. */
+int fd3_configure(const fd3_domain* domain, float rho, float g_eff, fd3_volume** out);
+/* Volume3::configure_with_bottom (delta3d.rs:300): bottom heights at column centres (nx*ny). */
+int fd3_configure_with_bottom(const fd3_domain* domain, float rho, float g_eff, const float* bottom,
+                              size_t bottom_len, fd3_volume** out);
+/* Volume3::configure_with_solid (delta3d.rs:327): plus a solid given by its signed distance at
+ * the nodes (negative inside), cut exactly by 24 tetrahedra per cell (delta3d_cut.rs:429). */
+int fd3_configure_with_solid(const fd3_domain* domain, float rho, float g_eff, const float* bottom,
+                             size_t bottom_len, const float* solid, size_t solid_len, fd3_volume** out);
+void fd3_destroy(fd3_volume* v);
+
+/* Solver options; call before fd3_enable_multigrid for mg_max_levels to apply. */
+int fd3_set_options(fd3_volume* v, const fd3_options* options);
+int fd3_get_options(const fd3_volume* v, fd3_options* options);
+/* The CUDA stream (a cudaStream_t) every call of this handle is ordered on; NULL = the handle's
+ * own non-blocking stream, created at configure (the legacy default stream cannot be captured). */
+int fd3_set_stream(fd3_volume* v, void* stream);
+
+/* Volume3::enable_multigrid (delta3d_multigrid.rs:339): the V-cycle preconditioner. */
+int fd3_enable_multigrid(fd3_volume* v);
+/* Volume3::multigrid_levels (delta3d_multigrid.rs:353); -1 when not enabled. */
+int fd3_multigrid_levels(const fd3_volume* v);
+
+/* Volume3::set_free_surface (delta3d_mobile.rs:9): eta per column and the rest level; p = 0. */
+int fd3_set_free_surface(fd3_volume* v, const float* eta, size_t len, float rest);
+/* Volume3::set_surface (delta3d.rs:614). */
+int fd3_set_surface(fd3_volume* v, const float* eta, size_t len);
+/* Volume3::set_velocity (delta3d.rs:631): closes walls and closed faces (close_walls, :666). */
+int fd3_set_velocity(fd3_volume* v, const float* u, size_t nu, const float* vv, size_t nv,
+                     const float* w, size_t nw);
+/* The same with device pointers (inputs already resident in HBM). */
+int fd3_set_velocity_device(fd3_volume* v, const float* d_u, const float* d_v, const float* d_w);
+/* Zero the pressure (the state set_free_surface leaves), e.g. to repeat a first projection. */
+int fd3_reset_pressure(fd3_volume* v);
+
+/* project_mobile3 (delta3d_mobile.rs:465) of the current velocity field: us = u, then the
+ * projection with `scale` (-rho/dt) and `k1` (dt/rho), as tests_delta3d.rs:389-400 does. */
+int fd3_project_mobile(fd3_volume* v, float scale, float k1, uint32_t max_iters, fd3_report* report);
+/* Volume3::step_surface_mobile (delta3d_mobile.rs:819): advect, project, extrapolate, transport. */
+int fd3_step_surface_mobile(fd3_volume* v, uint64_t duration_us, uint32_t max_iters, fd3_report* report);
+/* Volume3::last_refused_report (delta3d_mobile.rs:982); FD3_ERR_DOMAIN when none. */
+int fd3_last_refused_report(const fd3_volume* v, fd3_report* report);
+
+/* Accessors (delta3d.rs:647-661) into caller buffers. */
+int fd3_get_pressure(const fd3_volume* v, float* out, size_t len);
+int fd3_get_velocity(const fd3_volume* v, float* u, size_t nu, float* vv, size_t nv, float* w, size_t nw);
+int fd3_get_surface(const fd3_volume* v, float* eta, float* roundoff, size_t len);
+/* Device pointers of the published fields (p, u, v, w), valid until fd3_destroy. */
+int fd3_device_fields(const fd3_volume* v, float** p, float** u, float** vv, float** w);
+/* Cut geometry (delta3d.rs:595-602): frac, open_u/v/w, floor.  FD3_ERR_DOMAIN on a flat bottom. */
+int fd3_get_geometry(const fd3_volume* v, float* frac, float* open_u, float* open_v, float* open_w, float* floor);
+uint64_t fd3_wet_cells(const fd3_volume* v);
+
+/* Volume3::apply_pressure_operator_for_trials (delta3d_mobile.rs:936). */
+int fd3_apply_pressure_operator_for_trials(fd3_volume* v, const float* p, float* out, size_t len);
+/* Volume3::assemble_pressure_problem_for_trials (delta3d_mobile.rs:960). */
+int fd3_assemble_pressure_problem_for_trials(fd3_volume* v, const float* divergence, float scale,
+                                             float* rhs, float* prec, size_t len);
+/* v_cycle3 (delta3d_multigrid.rs:393) on `x`, set up as tests_delta3d.rs:1840-1873 does
+ * (rhs = 0, rhs_mobile3(1), prepare_multigrid3, res = x).  Writes z = M^-1 x. */
+int fd3_vcycle_for_tests(fd3_volume* v, const float* x, float* z, size_t len);
+/* Coarse level l after prepare_multigrid3: kind, diag, open_u/v/w (Level3, delta3d_multigrid.rs:37). */
+int fd3_level_geometry(const fd3_volume* v, uint32_t l, float* kind, float* diag, float* open_u,
+                       float* open_v, float* open_w);
+
+/* Kernel launches issued by this handle since creation (for launch accounting).  No reference
+ * counterpart: instrumentation of this library. */
+uint64_t fd3_kernel_launches(const fd3_volume* v);
+/* Per-kernel timing (no reference counterpart): with on = 1, every launch of this handle is
+ * bracketed by CUDA events on its stream and the durations are summed per kernel name at each
+ * synchronisation; CUDA-graph replay is bypassed meanwhile.  on = 0 stops it. */
+int fd3_profile(fd3_volume* v, int on);
+int fd3_profile_count(const fd3_volume* v);
+int fd3_profile_entry(const fd3_volume* v, int index, char* name, size_t name_len, uint64_t* launches,
+                      double* total_ms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FLUIDISIM_DELTA3D_H */

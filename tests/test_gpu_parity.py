@@ -1,0 +1,200 @@
+"""Parity of the sm_100a projection with the oracle, through the C ABI (needs a GPU).
+
+With the ordered f32 reduction (the reference's own order, delta3d.rs:860-876) every field the
+reference publishes must be bit-identical to the oracle's; with the default f64 reductions the
+projection must reach the reference's acceptance (relative residual <= 1e-6, plain divergence
+<= 1e-5) and its pressure must match the oracle's to 1e-5 relative in L-infinity.
+"""
+import numpy as np
+import pytest
+
+from fluidisim_b200 import scenes
+from fluidisim_b200.delta3d import REDUCE_F64, REDUCE_ORDERED_F32, Delta3dError, Volume3
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+P_TOL = 1e-5  # pressure L-inf difference, relative to L-inf of the oracle's pressure
+
+
+def bits(a):
+    return np.ascontiguousarray(a, dtype=np.float32).view(np.uint32)
+
+
+def assert_bits(a, b, what):
+    a, b = bits(a), bits(b)
+    bad = np.nonzero(a != b)[0]
+    assert bad.size == 0, f"{what}: {bad.size} differ, first at {bad[:5]}"
+
+
+def pair(nx, ny, nz, dx, rho=1025.0, g=9.81, bottom=None, solid=None, mg=False, reduction=REDUCE_ORDERED_F32,
+         max_levels=0):
+    o = O.OracleVolume(nx, ny, nz, dx, rho, g, bottom=bottom, solid=solid)
+    if solid is not None:
+        d = Volume3.configure_with_solid(nx, ny, nz, dx, rho, g, bottom, solid)
+    elif bottom is not None:
+        d = Volume3.configure_with_bottom(nx, ny, nz, dx, rho, g, bottom)
+    else:
+        d = Volume3.configure(nx, ny, nz, dx, rho, g)
+    d.set_options(reduction=reduction, mg_max_levels=max_levels)
+    if mg:
+        o.enable_multigrid(max_levels)
+        d.enable_multigrid()
+    return o, d
+
+
+def s385_pair(nx, bump, mg=True, reduction=REDUCE_ORDERED_F32):
+    s = scenes.s385_case(nx, bump)
+    o, d = pair(s["nx"], s["ny"], s["nz"], s["dx"], s["rho"], s["g"], bottom=s["bottom"], mg=mg, reduction=reduction)
+    o.set_free_surface(s["eta"], s["rest"])
+    d.set_free_surface(s["eta"], s["rest"])
+    return o, d, s
+
+
+def lake_pair(n=32, mg=True, reduction=REDUCE_ORDERED_F32, seed=1):
+    s = scenes.sphere_lake(n, seed=seed, spheres=4)
+    o, d = pair(s["nx"], s["ny"], s["nz"], s["dx"], s["rho"], s["g"], bottom=s["bottom"], solid=s["solid"], mg=mg,
+                reduction=reduction)
+    for v in (o, d):
+        v.set_free_surface(s["eta"], s["rest"])
+        v.set_velocity(s["u"], s["v"], s["w"])
+    return o, d, s
+
+
+# ------------------------------------------------------------------------------------ geometry
+def test_bottom_cut_geometry_is_bit_identical():
+    o, d, s = s385_pair(32, True)
+    for a, b, name in zip(o.geometry(), d.geometry(), ["frac", "open_u", "open_v", "open_w", "floor"]):
+        assert_bits(a, b, name)
+
+
+def test_solid_cut_geometry_is_bit_identical():
+    o, d, s = lake_pair(32)
+    for a, b, name in zip(o.geometry(), d.geometry(), ["frac", "open_u", "open_v", "open_w", "floor"]):
+        assert_bits(a, b, name)
+    frac = d.geometry()[0]
+    assert np.any((frac > 0) & (frac < 1)), "the spheres cut no cell"
+
+
+def test_a_solid_in_the_lid_layer_is_refused():
+    n = 8
+    sdf = scenes.spheres_sdf(n, n, n, 0.25, [(1.0, 1.0, 1.9)], [0.3])
+    with pytest.raises(Delta3dError) as e:
+        Volume3.configure_with_solid(n, n, n, 0.25, 1025.0, 9.81, np.zeros(n * n, np.float32), sdf)
+    assert e.value.kind == "Domain"
+    with pytest.raises(O.OracleError):
+        O.OracleVolume(n, n, n, 0.25, bottom=np.zeros(n * n, np.float32), solid=sdf)
+
+
+# ------------------------------------------------------------------------------------ operator
+@pytest.mark.parametrize("case", ["flat", "bump", "lake"])
+def test_operator_and_assembly_are_bit_identical(case):
+    if case == "lake":
+        o, d, s = lake_pair(32)
+    else:
+        o, d, s = s385_pair(32, case == "bump")
+    x = scenes.noise(d.cells, 7) * np.float32(300.0)
+    assert_bits(o.apply_pressure_operator_for_trials(x), d.apply_pressure_operator_for_trials(x), "A x")
+    div = scenes.noise(d.cells, 9)
+    ro, po = o.assemble_pressure_problem_for_trials(div, -61500.0)
+    rd, pd = d.assemble_pressure_problem_for_trials(div, -61500.0)
+    assert_bits(ro, rd, "rhs")
+    assert_bits(po, pd, "prec")
+
+
+@pytest.mark.parametrize("case", ["flat", "bump", "lake"])
+def test_vcycle_is_bit_identical(case):
+    if case == "lake":
+        o, d, s = lake_pair(32)
+    else:
+        o, d, s = s385_pair(32, case == "bump")
+    x = scenes.noise(d.cells, 11)
+    assert_bits(o.vcycle_for_tests(x), d.vcycle_for_tests(x), "z = M^-1 x")
+    for l in range(d.multigrid_levels()):
+        a = O.OracleVolume  # noqa: F841  (level geometry compared through the V-cycle output)
+
+
+# ------------------------------------------------------------------------------------ projection
+def _compare_projection(o, d, ro, rd, exact):
+    if exact:
+        assert ro == rd.as_dict(), (ro, rd)
+        assert_bits(o.pressure(), d.pressure(), "p")
+        for a, b, name in zip(o.velocity(), d.velocity(), "uvw"):
+            assert_bits(a, b, name)
+    else:
+        assert not rd.degraded
+        assert rd.residual <= 1e-6 and rd.divergence_plain <= 1e-5
+        assert abs(rd.iterations - ro["iterations"]) <= 1
+        po, pd = o.pressure(), d.pressure()
+        scale = np.max(np.abs(po))
+        assert np.max(np.abs(po - pd)) <= P_TOL * scale, np.max(np.abs(po - pd)) / scale
+
+
+@pytest.mark.parametrize("reduction", [REDUCE_ORDERED_F32, REDUCE_F64])
+@pytest.mark.parametrize("bump", [False, True])
+@pytest.mark.parametrize("nx", [32, 64])
+def test_s385_first_step_matches_the_oracle(nx, bump, reduction):
+    o, d, s = s385_pair(nx, bump, reduction=reduction)
+    ro = o.step_surface_mobile(s["dt_us"], 20000)
+    rd = d.step_surface_mobile(s["dt_us"], 20000)
+    assert rd.iterations == {32: 9, 64: 10}[nx] or reduction == REDUCE_F64
+    _compare_projection(o, d, ro, rd, reduction == REDUCE_ORDERED_F32)
+    if reduction == REDUCE_ORDERED_F32:
+        for a, b in zip(o.surface(), d.surface_and_roundoff()):
+            assert_bits(a, b, "eta/roundoff")
+
+
+@pytest.mark.parametrize("reduction", [REDUCE_ORDERED_F32, REDUCE_F64])
+@pytest.mark.parametrize("mg", [True, False])
+def test_sphere_lake_projection_matches_the_oracle(mg, reduction):
+    o, d, s = lake_pair(32, mg=mg, reduction=reduction)
+    scale, k1 = scenes.projection_scalars(s)
+    ro = o.project_mobile(scale, k1, 4000)
+    rd = d.project_mobile3(scale, k1, 4000)
+    _compare_projection(o, d, ro, rd, reduction == REDUCE_ORDERED_F32)
+
+
+def test_ten_warm_steps_stay_bit_identical():
+    o, d, s = s385_pair(32, True)
+    for _ in range(10):
+        ro = o.step_surface_mobile(s["dt_us"], 20000)
+        rd = d.step_surface_mobile(s["dt_us"], 20000)
+        assert ro == rd.as_dict()
+    assert_bits(o.pressure(), d.pressure(), "p")
+    for a, b in zip(o.surface(), d.surface_and_roundoff()):
+        assert_bits(a, b, "eta/roundoff")
+
+
+def test_rest_projects_to_exact_zero():
+    o, d = pair(6, 4, 5, 0.5, mg=True)
+    d.set_free_surface(np.full(24, 2.0, np.float32), 2.0)
+    r = d.project_mobile3(-1025.0 / 0.002, 0.002 / 1025.0, 100)
+    assert (r.iterations, r.degraded, r.residual, r.divergence) == (0, False, 0.0, 0.0)
+    assert not np.any(bits(d.pressure()))
+    assert not any(np.any(bits(x)) for x in d.velocity())
+
+
+# ------------------------------------------------------------------------------------ refusals
+def test_refusals_leave_the_published_fields_untouched():
+    o, d, s = s385_pair(32, False)
+    d.step_surface_mobile(s["dt_us"], 20000)
+    before = [d.pressure().copy(), *[x.copy() for x in d.velocity()]]
+    with pytest.raises(Delta3dError) as e:
+        d.set_velocity(np.zeros(3, np.float32), np.zeros(d.nv), np.zeros(d.nw))
+    assert e.value.kind == "Shape"
+    u = np.zeros(d.nu, np.float32)
+    u[5] = np.inf
+    with pytest.raises(Delta3dError) as e:
+        d.set_velocity(u, np.zeros(d.nv), np.zeros(d.nw))
+    assert e.value.kind == "NotFinite"
+    # a cap of one iteration cannot converge: Convergence, and nothing published changes
+    with pytest.raises(Delta3dError) as e:
+        d.step_surface_mobile(s["dt_us"], 1)
+    assert e.value.kind == "Convergence"
+    assert d.last_refused_report() is not None and d.last_refused_report().degraded
+    after = [d.pressure(), *d.velocity()]
+    for a, b in zip(before, after):
+        assert_bits(a, b, "published field")
+    with pytest.raises(Delta3dError) as e:
+        Volume3.configure(0, 4, 4, 0.25)
+    assert e.value.kind == "Domain"
