@@ -31,22 +31,25 @@ sys.path.insert(0, ROOT)
 
 METRIC = "128³ projections/s at rel. residual 1e-6: learned-FCG vs plain MGPCG, 1 B200"
 
-# Algorithmic bytes per cell of each fine-level kernel (f32 fields, cut geometry): every distinct
-# array a pass must touch, counted once (stencil neighbours are not re-counted).  Geometry = the
-# fluid fraction (4 B) and the three face apertures (12 B) the matrix-free rows read; the column
-# heights are per column and negligible.
+# Algorithmic bytes per cell of each fine-level kernel (f32 fields): every distinct array a pass
+# must touch, counted once (stencil neighbours are not re-counted).  The hot kernels read the
+# 2-byte row code of the projection; apertures are read only at cut faces and column heights
+# only at ghost faces (both negligible in bulk).  Set-up kernels read the full geometry: the
+# fluid fraction (4 B) and three face apertures (12 B).
 GEOM = 16
 BYTES_PER_CELL = {
-    "k_fine_sweep": 4 + 4 + 4 + 4 + GEOM,      # prec, r, z in, z out
-    "k_fine_sweep0": 4 + 4 + 4,                # prec, r, z out
-    "k_fine_restrict": 4 + 4 + GEOM + 0.5,     # r, z, geometry, coarse r (1/8 cell)
-    "k_fine_prolong": 4 + 4 + 4 + 0.5,         # z in/out, prec, coarse x
-    "k_apply_dot": 4 + 4 + GEOM,               # d, q, geometry
-    "k_update": 4 * 6,                         # p, r read+write; d, q
-    "k_dot": 8,
-    "k_mg_dir": 12,
-    "k_residual": 4 * 3 + GEOM,                # p, rhs, res
-    "k_rhs_mobile": 4 * 3 + GEOM,
+    "k_dir_apply_dot": 2 + 4 + 4 + 4 + 4,      # code, z, d in, d out, q
+    "k_update_rn": 4 * 6,                      # p, r read+write; d, q
+    "k_fine_pre": 2 + 4 + 4 + 4,               # code, prec, r, z out
+    "k_fine_restrict_c": 2 + 4 + 4 + 0.5,      # code, r, z, coarse r (1/8 cell)
+    "k_fine_post1": 2 + 4 + 4 + 4 + 0.5 + 4,   # code, prec, r, z in, coarse x, z out
+    "k_fine_post2_rz": 2 + 4 + 4 + 4 + 4,      # code, prec, r, z in, z out
+    "k_apply_dot_c": 2 + 4 + 4,                # code, d, q
+    "k_dot_prec_fin": 8,
+    "k_jacobi_dir": 12,
+    "k_residual_c": 2 + 4 * 3,                 # code, p, rhs, res
+    "k_rhs_b2": 4 * 3 + GEOM,                  # rhs read+write, prec, geometry
+    "k_row_codes": GEOM + 2,
     "k_divergence": 4 * 3 + 4 + GEOM,          # three face families in, rhs out
 }
 

@@ -1,0 +1,574 @@
+// The hot path of the MG-PCG iteration on sm_100a: fused passes over the fine level, fused coarse
+// sweeps, a single-CTA solve of the small coarse levels, and reductions finished by the last block.
+//
+// Every fusion recomputes, at each stencil point, the value the unfused sequence would have
+// stored (the same f32 expression in the same order), so a fused iteration is bit-identical to
+// the reference's sequence of passes (delta3d_mobile.rs:515-545, delta3d_multigrid.rs:393-465).
+#pragma once
+
+#include "fd3_kernels.cuh"
+
+namespace fd3 {
+
+// ------------------------------------------------------------------------------------------------
+// Row codes.  The mobile row (delta3d_mobile.rs:152-188) depends on the surface, which is frozen
+// during a projection, so its structure is encoded once per projection in 16 bits:
+//   bit 0        wet
+//   bits 1+2f    face f (x-, x+, y-, y+, z-, z+): 0 nothing, 1 fluid neighbour, 2 surface ghost
+//   bit 13       every live face has aperture 1 (no aperture load needed)
+// A hot stencil then reads 2 bytes instead of rebuilding the row from the fractions, the
+// apertures and six wet tests.  Apertures of cut faces and ghost coefficients are recomputed with
+// the reference's own expressions, so an encoded row evaluates to the same bits.
+constexpr unsigned RC_WET = 1u;
+constexpr unsigned RC_UNIT = 1u << 13;
+
+__device__ __forceinline__ unsigned face_state(unsigned code, int f) { return (code >> (1 + 2 * f)) & 3u; }
+
+__global__ void k_row_codes(Geo g, unsigned short* __restrict__ codes) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= g.n) return;
+  int i, j, k; cell_ijk(g, c, i, j, k);
+  unsigned code = 0;
+  if (wet3(g, i, j, k)) {
+    RowE row[6]; mobile_row(g, i, j, k, row);
+    code = RC_WET;
+    bool unit = true;
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+      unsigned st = row[f].n >= 0 ? 1u : (row[f].a > 0.f ? 2u : 0u);
+      code |= st << (1 + 2 * f);
+      if (st && row[f].a != 1.f) unit = false;
+    }
+    if (unit) code |= RC_UNIT;
+  }
+  codes[c] = (unsigned short)code;
+}
+
+// 1/max(theta, 1e-3) of ghost_side3 and ghost_up3 (delta3d_mobile.rs:126-147).
+__device__ __forceinline__ float ghost_it_side(const Geo& g, int i, int j, int k, int x, int y) {
+  float zc = ((float)k + 0.5f) * g.dx;
+  float h = __ldg(g.eta + j * g.nx + i);
+  float theta = fmaxf((h - zc) / (h - __ldg(g.eta + y * g.nx + x)), SURFACE_THETA_MIN);
+  return 1.f / theta;
+}
+__device__ __forceinline__ float ghost_it_up(const Geo& g, int i, int j, int k) {
+  float h = __ldg(g.eta + j * g.nx + i);
+  float theta = fmaxf((h - ((float)k + 0.5f) * g.dx) / g.dx, SURFACE_THETA_MIN);
+  return 1.f / theta;
+}
+
+// One row of apply_mobile3 from its code; P(n) yields the operand at cell n (a load, or a value
+// recomputed on the fly by a fused kernel).
+template <class P>
+__device__ __forceinline__ float apply_code(const Geo& g, unsigned code, int i, int j, int k, int c, P p) {
+  const float pc = p(c);
+  const bool unit = code & RC_UNIT;
+  const int nxny = g.nx * g.ny;
+  float acc = 0.f;
+  unsigned st = face_state(code, 0);
+  if (st) {
+    float a = unit ? 1.f : open3(g, 0, fu(g, i, j, k));
+    if (st == 1) acc += a * (pc - p(c - 1)); else acc += a * pc * ghost_it_side(g, i, j, k, i - 1, j);
+  }
+  st = face_state(code, 1);
+  if (st) {
+    float a = unit ? 1.f : open3(g, 0, fu(g, i + 1, j, k));
+    if (st == 1) acc += a * (pc - p(c + 1)); else acc += a * pc * ghost_it_side(g, i, j, k, i + 1, j);
+  }
+  st = face_state(code, 2);
+  if (st) {
+    float a = unit ? 1.f : open3(g, 1, fv(g, i, j, k));
+    if (st == 1) acc += a * (pc - p(c - g.nx)); else acc += a * pc * ghost_it_side(g, i, j, k, i, j - 1);
+  }
+  st = face_state(code, 3);
+  if (st) {
+    float a = unit ? 1.f : open3(g, 1, fv(g, i, j + 1, k));
+    if (st == 1) acc += a * (pc - p(c + g.nx)); else acc += a * pc * ghost_it_side(g, i, j, k, i, j + 1);
+  }
+  st = face_state(code, 4);  // the face below is never a ghost
+  if (st) {
+    float a = unit ? 1.f : open3(g, 2, fw(g, i, j, k));
+    acc += a * (pc - p(c - nxny));
+  }
+  st = face_state(code, 5);
+  if (st) {
+    float a = unit ? 1.f : open3(g, 2, fw(g, i, j, k + 1));
+    if (st == 1) acc += a * (pc - p(c + nxny)); else acc += a * pc * ghost_it_up(g, i, j, k);
+  }
+  return acc * g.inv;
+}
+
+struct Load {
+  const float* __restrict__ x;
+  __device__ __forceinline__ float operator()(int n) const { return x[n]; }
+};
+
+// ------------------------------------------------------------------------------------------------
+// Reductions finished in the kernel that produces them: each block leaves its partial(s), the last
+// block to arrive (a counter) merges them in a fixed order and applies the PCG scalar step.
+
+template <int MODE>
+__device__ void finish_block(Red red, int nparts, Scalars* S, int op);
+
+__device__ __forceinline__ void apply_op(Scalars* S, double val, int op, int ord) {
+  const bool finite = isfinite(val);
+  const bool zero_but_nonzero = ord && val == 0.0 && S->any_nonzero;
+  switch (op) {
+    case FIN_B2:
+      S->b2 = val;
+      if (!finite || zero_but_nonzero) S->status = 2;
+      break;
+    case FIN_RR0:
+    case FIN_ACTUAL:
+      if (op == FIN_RR0) S->rr = val; else S->actual = val;
+      if (!finite || zero_but_nonzero) S->status = 2;
+      break;
+    case FIN_DQ:
+      S->dq = val;
+      if (!(val > 0.0)) { S->active = 0; S->brk = 1; }
+      else S->alpha = ord ? (float)S->rz / (float)val : (float)(S->rz / val);
+      break;
+    case FIN_RN:
+      S->rn = val;
+      if (!finite || zero_but_nonzero) { S->status = 2; S->active = 0; break; }
+      if (!loop_continues(S, val, S->it + 1, ord)) { S->rr = val; S->it += 1; S->active = 0; }
+      break;
+    case FIN_RZ_ITER:
+      if (!finite) { S->status = 2; S->active = 0; break; }
+      S->zn = val;
+      S->beta = ord ? (float)val / (float)S->rz : (float)(val / S->rz);
+      S->rz = val;
+      S->rr = S->rn;
+      S->it += 1;
+      S->dir_mode = 1;
+      break;
+    case FIN_RZ_PRIME:
+      if (!finite) S->status = 2;
+      S->rz = val;
+      S->dir_mode = 0;
+      break;
+  }
+  S->any_nonzero = 0;
+}
+
+template <>
+__device__ void finish_block<RED_F64>(Red red, int nparts, Scalars* S, int op) {
+  __shared__ double sm[TPB];
+  double s = 0.0;
+  for (int q = threadIdx.x; q < nparts; q += blockDim.x) s += __ldcg(red.p64 + q);
+  sm[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) sm[threadIdx.x] += sm[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) apply_op(S, sm[0], op, 0);
+}
+
+template <>
+__device__ void finish_block<RED_ORD>(Red red, int nparts, Scalars* S, int op) {
+  if (threadIdx.x != 0) return;
+  // serial in-order merge in f32 (host_impl.rs:75-92, merge of delta3d.rs:867)
+  float acc = 0.f;
+  int q = 0;
+  for (; q + 8 <= nparts; q += 8) {
+    float v[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) v[e] = __ldcg(red.p32 + q + e);
+#pragma unroll
+    for (int e = 0; e < 8; ++e) acc = acc + v[e];
+  }
+  for (; q < nparts; ++q) acc = acc + __ldcg(red.p32 + q);
+  apply_op(S, (double)acc, op, 1);
+}
+
+template <int MODE>
+__device__ __forceinline__ void reduce_finish(typename Acc<MODE>::T v, int c, int n, Red red, Scalars* S, int op) {
+  block_reduce<MODE>(v, c, n, red);
+  __shared__ bool last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(red.count, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  const int nparts = MODE == RED_ORD ? (n + CHUNK - 1) / CHUNK : (int)gridDim.x;
+  finish_block<MODE>(red, nparts, S, op);
+  if (threadIdx.x == 0) *red.count = 0u;
+}
+
+// ------------------------------------------------------------------------------------------------
+// The PCG step (delta3d_mobile.rs:523-545) with the multigrid preconditioner.
+
+// d = z (S->dir_mode 0, after a prime) or d = z + beta d (1, direction_multigrid3), written to
+// dout; q = A d; d.q; alpha = rz/dq or a stop (FIN_DQ).  d is recomputed at each stencil point.
+template <int MODE>
+__global__ void __launch_bounds__(TPB) k_dir_apply_dot(Geo g, const unsigned short* __restrict__ codes,
+                                                       const float* __restrict__ z, const float* __restrict__ din,
+                                                       float* __restrict__ dout, float* __restrict__ q, Red red,
+                                                       Scalars* S) {
+  if (!S->active) return;
+  const int mode = S->dir_mode;
+  const float beta = S->beta;
+  auto D = [&](int n) { return mode ? z[n] + beta * din[n] : z[n]; };
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  float dc = 0.f, qc = 0.f;
+  if (c < g.n) {
+    dc = D(c);
+    unsigned code = codes[c];
+    if (code & RC_WET) { int i, j, k; cell_ijk(g, c, i, j, k); qc = apply_code(g, code, i, j, k, c, D); }
+    dout[c] = dc;
+    q[c] = qc;
+  }
+  reduce_finish<MODE>(Acc<MODE>::prod(dc, qc), c, g.n, red, S, FIN_DQ);
+}
+
+// p += alpha d, r -= alpha q, with r.r (FIN_RN decides whether the loop continues).
+template <int MODE>
+__global__ void __launch_bounds__(TPB) k_update_rn(int n, float* __restrict__ p, float* __restrict__ r,
+                                                   const float* __restrict__ d, const float* __restrict__ q, Red red,
+                                                   Scalars* S) {
+  if (!S->active) return;
+  const float alpha = S->alpha;
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  float rn = 0.f;
+  if (c < n) {
+    p[c] += alpha * d[c];
+    rn = r[c] - alpha * q[c];
+    r[c] = rn;
+  }
+  if (__syncthreads_or(c < n && rn != 0.f) && threadIdx.x == 0) atomicOr(&S->any_nonzero, 1);
+  reduce_finish<MODE>(Acc<MODE>::prod(rn, rn), c, n, red, S, FIN_RN);
+}
+
+// The two pre-sweeps from z = 0 (v_cycle3, delta3d_multigrid.rs:398-405): z1 = w prec r is
+// recomputed at each stencil point, z2 = z1 + w prec (r - A z1) is written.
+__global__ void __launch_bounds__(TPB) k_fine_pre(Geo g, const unsigned short* __restrict__ codes,
+                                                  const float* __restrict__ prec, const float* __restrict__ r,
+                                                  float* __restrict__ z2, const Scalars* S, int gate) {
+  if (gate && !S->active) return;
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= g.n) return;
+  auto Z1 = [&](int n) {
+    float m = prec[n];
+    return m > 0.f ? 0.f + OMEGA * m * (r[n] - 0.f) : 0.f;
+  };
+  float m = prec[c];
+  float zc = Z1(c);
+  if (m > 0.f) {
+    int i, j, k; cell_ijk(g, c, i, j, k);
+    zc += OMEGA * m * (r[c] - apply_code(g, (unsigned)codes[c], i, j, k, c, Z1));
+  }
+  z2[c] = zc;
+}
+
+// Coarse r = mean over the 8 children of (r - A z) (restrict3).
+__global__ void __launch_bounds__(TPB) k_fine_restrict_c(Geo g, const unsigned short* __restrict__ codes,
+                                                         const float* __restrict__ r, const float* __restrict__ z,
+                                                         Lev L, const Scalars* S, int gate) {
+  if (gate && !S->active) return;
+  int qi = blockIdx.x * blockDim.x + threadIdx.x;
+  if (qi >= L.n) return;
+  int ci = qi % L.nx, t = qi / L.nx, cj = t % L.ny, ck = t / L.ny;
+  Load Z{z};
+  float s = 0.f;
+#pragma unroll
+  for (int e = 0; e < 8; ++e) {
+    int i = 2 * ci + (e & 1), j = 2 * cj + ((e >> 1) & 1), k = 2 * ck + (e >> 2);
+    int c = (k * g.ny + j) * g.nx + i;
+    unsigned code = codes[c];
+    float az = (code & RC_WET) ? apply_code(g, code, i, j, k, c, Z) : 0.f;
+    s += r[c] - az;
+  }
+  L.r[qi] = 0.125f * s;
+}
+
+// Prolongation (z += parent x; z = 0 where prec == 0) fused with the first post-sweep; without
+// coarse levels (prolong = 0) the plain third sweep.
+__global__ void __launch_bounds__(TPB) k_fine_post1(Geo g, const unsigned short* __restrict__ codes,
+                                                    const float* __restrict__ prec, const float* __restrict__ r,
+                                                    const float* __restrict__ zin, Lev L, int prolong,
+                                                    float* __restrict__ zout, const Scalars* S, int gate) {
+  if (gate && !S->active) return;
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= g.n) return;
+  const int nx = g.nx;
+  auto ZP = [&](int n) {
+    if (!prolong) return zin[n];
+    int i = n % nx, t = n / nx, j = t % g.ny, k = t / g.ny;
+    float v = zin[n] + L.x[((k >> 1) * L.ny + (j >> 1)) * L.nx + (i >> 1)];
+    return prec[n] == 0.f ? 0.f : v;
+  };
+  float m = prec[c];
+  float zc = ZP(c);
+  if (m > 0.f) {
+    int i, j, k; cell_ijk(g, c, i, j, k);
+    zc += OMEGA * m * (r[c] - apply_code(g, (unsigned)codes[c], i, j, k, c, ZP));
+  }
+  zout[c] = zc;
+}
+
+// The last post-sweep fused with res.z (prime: FIN_RZ_PRIME; iteration: FIN_RZ_ITER).
+template <int MODE>
+__global__ void __launch_bounds__(TPB) k_fine_post2_rz(Geo g, const unsigned short* __restrict__ codes,
+                                                       const float* __restrict__ prec, const float* __restrict__ r,
+                                                       const float* __restrict__ zin, float* __restrict__ zout,
+                                                       Red red, Scalars* S, int gate, int op) {
+  if (gate && !S->active) return;
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  float rc = 0.f, zc = 0.f;
+  if (c < g.n) {
+    Load Z{zin};
+    float m = prec[c];
+    rc = r[c];
+    zc = zin[c];
+    if (m > 0.f) {
+      int i, j, k; cell_ijk(g, c, i, j, k);
+      zc += OMEGA * m * (rc - apply_code(g, (unsigned)codes[c], i, j, k, c, Z));
+    }
+    zout[c] = zc;
+  }
+  reduce_finish<MODE>(Acc<MODE>::prod(rc, zc), c, g.n, red, S, op);
+}
+
+// ------------------------------------------------------------------------------------------------
+// Jacobi-preconditioned step (the reference's default without enable_multigrid).
+
+template <int MODE>
+__global__ void __launch_bounds__(TPB) k_apply_dot_c(Geo g, const unsigned short* __restrict__ codes,
+                                                     const float* __restrict__ d, float* __restrict__ q, Red red,
+                                                     Scalars* S) {
+  if (!S->active) return;
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  float dc = 0.f, qc = 0.f;
+  if (c < g.n) {
+    dc = d[c];
+    unsigned code = codes[c];
+    if (code & RC_WET) { int i, j, k; cell_ijk(g, c, i, j, k); qc = apply_code(g, code, i, j, k, c, Load{d}); }
+    q[c] = qc;
+  }
+  reduce_finish<MODE>(Acc<MODE>::prod(dc, qc), c, g.n, red, S, FIN_DQ);
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(TPB) k_dot_prec_fin(int n, const float* __restrict__ r, const float* __restrict__ prec,
+                                                      Red red, Scalars* S, int gate, int op) {
+  if (gate && !S->active) return;
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  float x = 0.f, m = 0.f;
+  if (c < n) { x = r[c]; m = prec[c]; }
+  reduce_finish<MODE>(Acc<MODE>::prod3(x, m, x), c, n, red, S, op);
+}
+
+// ------------------------------------------------------------------------------------------------
+// Coarse levels.  level_row with an operand functor.
+template <class P>
+__device__ __forceinline__ float level_row_f(const Lev& L, int i, int j, int k, int c, P p) {
+  const float pc = p(c);
+  float acc = 0.f;
+  const int nxny = L.nx * L.ny;
+  auto face = [&](float a, bool has, int m, bool top) {
+    if (a == 0.f) return;
+    if (has) {
+      float km = L.kind[m];
+      if (km > 0.f) acc += a * (pc - p(m));
+      else if (km < 0.f) acc += 2.f * a * pc;
+    } else if (top) {
+      acc += 2.f * a * pc;
+    }
+  };
+  face(L.ou[(k * L.ny + j) * (L.nx + 1) + i], i > 0, c - 1, false);
+  face(L.ou[(k * L.ny + j) * (L.nx + 1) + i + 1], i + 1 < L.nx, c + 1, false);
+  face(L.ov[(k * (L.ny + 1) + j) * L.nx + i], j > 0, c - L.nx, false);
+  face(L.ov[(k * (L.ny + 1) + j + 1) * L.nx + i], j + 1 < L.ny, c + L.nx, false);
+  face(L.ow[(k * L.ny + j) * L.nx + i], k > 0, c - nxny, false);
+  face(L.ow[((k + 1) * L.ny + j) * L.nx + i], k + 1 < L.nz, c + nxny, true);
+  return acc * L.inv;
+}
+
+// x0 = 0 + w (r - 0)/diag (first sweep), recomputed per stencil point.
+__device__ __forceinline__ float level_x1(const Lev& L, int n) {
+  float dg = L.diag[n];
+  return dg > 0.f ? 0.f + OMEGA * (L.r[n] - 0.f) / dg : 0.f;
+}
+
+// The two pre-sweeps of a coarse level from x = 0, written to L.x (smooth3 twice after fill(0)).
+__global__ void __launch_bounds__(TPB) k_level_pre(Lev L, const Scalars* S, int gate) {
+  if (gate && !S->active) return;
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= L.n) return;
+  auto X1 = [&](int n) { return level_x1(L, n); };
+  float dg = L.diag[c];
+  float xc = X1(c);
+  if (dg > 0.f) {
+    int i = c % L.nx, t = c / L.nx, j = t % L.ny, k = t / L.ny;
+    xc += OMEGA * (L.r[c] - level_row_f(L, i, j, k, c, X1)) / dg;
+  }
+  L.x[c] = xc;
+}
+
+// Prolongation from C (x += parent) fused with the first post-sweep, L.x -> L.x2.
+__global__ void __launch_bounds__(TPB) k_level_post1(Lev L, Lev C, const Scalars* S, int gate) {
+  if (gate && !S->active) return;
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= L.n) return;
+  auto XP = [&](int n) {
+    int i = n % L.nx, t = n / L.nx, j = t % L.ny, k = t / L.ny;
+    return L.x[n] + C.x[((k >> 1) * C.ny + (j >> 1)) * C.nx + (i >> 1)];
+  };
+  float dg = L.diag[c];
+  float xc = XP(c);
+  if (dg > 0.f) {
+    int i = c % L.nx, t = c / L.nx, j = t % L.ny, k = t / L.ny;
+    xc += OMEGA * (L.r[c] - level_row_f(L, i, j, k, c, XP)) / dg;
+  }
+  L.x2[c] = xc;
+}
+
+// The second post-sweep, L.x2 -> L.x.
+__global__ void __launch_bounds__(TPB) k_level_post2(Lev L, const Scalars* S, int gate) {
+  if (gate && !S->active) return;
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= L.n) return;
+  Load X{L.x2};
+  float dg = L.diag[c];
+  float xc = L.x2[c];
+  if (dg > 0.f) {
+    int i = c % L.nx, t = c / L.nx, j = t % L.ny, k = t / L.ny;
+    xc += OMEGA * (L.r[c] - level_row_f(L, i, j, k, c, X)) / dg;
+  }
+  L.x[c] = xc;
+}
+
+// All levels from `first` to `last` in one CTA (coarse_cycle3 restricted to them): each phase is a
+// block-strided loop, phases are separated by __syncthreads (global writes of a block are visible
+// to the block after the barrier).  levels[first].r is already restricted; leaves levels[first].x.
+constexpr int TAIL_THREADS = 1024;
+
+__device__ __forceinline__ void tail_sweep(const Lev& L, const float* xin, float* xout, bool zero_in) {
+  for (int c = threadIdx.x; c < L.n; c += blockDim.x) {
+    float dg = L.diag[c];
+    if (zero_in) { xout[c] = dg > 0.f ? 0.f + OMEGA * (L.r[c] - 0.f) / dg : 0.f; continue; }
+    float xc = xin[c];
+    if (dg > 0.f) {
+      int i = c % L.nx, t = c / L.nx, j = t % L.ny, k = t / L.ny;
+      xc += OMEGA * (L.r[c] - level_row_f(L, i, j, k, c, Load{xin})) / dg;
+    }
+    xout[c] = xc;
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(TAIL_THREADS) k_coarse_tail(const Lev* __restrict__ T, int first, int last,
+                                                              const Scalars* S, int gate) {
+  if (gate && !S->active) return;
+  for (int l = first; l <= last; ++l) {
+    const Lev L = T[l];
+    const int sweeps = l == last ? 8 : 2;  // COARSE_SWEEPS_3D, PRE_SWEEPS_3D
+    for (int s = 0; s < sweeps; ++s)
+      tail_sweep(L, (s % 2 == 0) ? L.x : L.x2, (s % 2 == 0) ? L.x2 : L.x, s == 0);
+    if (l < last) {
+      const Lev C = T[l + 1];
+      for (int q = threadIdx.x; q < C.n; q += blockDim.x) {
+        int ci = q % C.nx, t = q / C.nx, cj = t % C.ny, ck = t / C.ny;
+        float s = 0.f;
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+          int i = 2 * ci + (e & 1), j = 2 * cj + ((e >> 1) & 1), k = 2 * ck + (e >> 2);
+          int c = (k * L.ny + j) * L.nx + i;
+          float lx = L.kind[c] > 0.f ? level_row_f(L, i, j, k, c, Load{L.x}) : 0.f;
+          s += L.r[c] - lx;
+        }
+        C.r[q] = 0.125f * s;
+      }
+      __syncthreads();
+    }
+  }
+  for (int l = last - 1; l >= first; --l) {
+    const Lev L = T[l];
+    const Lev C = T[l + 1];
+    for (int c = threadIdx.x; c < L.n; c += blockDim.x) {
+      int i = c % L.nx, t = c / L.nx, j = t % L.ny, k = t / L.ny;
+      L.x[c] += C.x[((k >> 1) * C.ny + (j >> 1)) * C.nx + (i >> 1)];
+    }
+    __syncthreads();
+    tail_sweep(L, L.x, L.x2, false);
+    tail_sweep(L, L.x2, L.x, false);
+  }
+}
+
+// ------------------------------------------------------------------------------------------------
+// The WHILE node of the inner loop repeats its body (two iterations) while this sets 1.  Each
+// iteration that runs advances S->it, so the loop ends within max_iters iterations; as a guard
+// independent of that logic, the body never runs more than max_iters + 2 times (status 100).
+__global__ void k_loop_cond(cudaGraphConditionalHandle handle, Scalars* S) {
+  unsigned runs = ++S->body_runs;
+  bool go = S->active != 0;
+  if (go && runs > S->max_iters + 2u) { S->active = 0; S->status = 100; go = false; }
+  cudaGraphSetConditional(handle, go ? 1u : 0u);
+}
+
+// ------------------------------------------------------------------------------------------------
+// Set-up reductions with the in-kernel finish.
+
+// rhs_mobile3 (delta3d_mobile.rs:215-241) with b.b (FIN_B2) when `reduce`.
+template <int MODE>
+__global__ void __launch_bounds__(TPB) k_rhs_b2(Geo g, float scale, float* __restrict__ rhs, float* __restrict__ prec,
+                                                Red red, Scalars* S, int reduce) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  float b = 0.f;
+  if (c < g.n) {
+    int i, j, k; cell_ijk(g, c, i, j, k);
+    if (!wet3(g, i, j, k)) { rhs[c] = 0.f; prec[c] = 0.f; }
+    else {
+      RowE row[6]; mobile_row(g, i, j, k, row);
+      b = scale * rhs[c];
+      float diag = 0.f;
+#pragma unroll
+      for (int f = 0; f < 6; ++f) {
+        if (row[f].n >= 0) diag += row[f].a;
+        else if (row[f].a > 0.f) {
+          diag += row[f].a * row[f].it;
+          b += row[f].a * row[f].val * row[f].it * g.inv;
+        }
+      }
+      rhs[c] = b;
+      prec[c] = diag > 0.f ? 1.f / (diag * g.inv) : 0.f;
+    }
+  }
+  if (!reduce) return;
+  if (__syncthreads_or(c < g.n && b != 0.f) && threadIdx.x == 0) atomicOr(&S->any_nonzero, 1);
+  reduce_finish<MODE>(Acc<MODE>::prod(b, b), c, g.n, red, S, FIN_B2);
+}
+
+// res = rhs - A p with res.res (FIN_RR0 or FIN_ACTUAL), from the row codes.
+template <int MODE>
+__global__ void __launch_bounds__(TPB) k_residual_c(Geo g, const unsigned short* __restrict__ codes,
+                                                    const float* __restrict__ p, const float* __restrict__ rhs,
+                                                    float* __restrict__ res, Red red, Scalars* S, int op) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  float r = 0.f;
+  if (c < g.n) {
+    unsigned code = codes[c];
+    float ap = 0.f;
+    if (code & RC_WET) { int i, j, k; cell_ijk(g, c, i, j, k); ap = apply_code(g, code, i, j, k, c, Load{p}); }
+    r = rhs[c] - ap;
+    res[c] = r;
+  }
+  if (__syncthreads_or(c < g.n && r != 0.f) && threadIdx.x == 0) atomicOr(&S->any_nonzero, 1);
+  reduce_finish<MODE>(Acc<MODE>::prod(r, r), c, g.n, red, S, op);
+}
+
+// Loop start: the host's view of the loop state; a pending NotFinite keeps the loop closed.
+__global__ void k_loop_start(Scalars* S, double rr, double tolb2, double phys, unsigned it, unsigned max_iters) {
+  S->rr = rr;
+  S->tolb2 = tolb2;
+  S->phys = phys;
+  S->it = it;
+  S->max_iters = max_iters;
+  S->brk = 0;
+  S->body_runs = 0;
+  S->active = S->status ? 0 : 1;
+}
+
+}  // namespace fd3

@@ -62,12 +62,15 @@ struct Scalars {
   int any_nonzero;         // ordered-mode norm2 guard (delta3d.rs:871-875)
   float fmax[4];           // max-reductions (divergence all/plain, |u| max, backward error)
   unsigned long long hash; // fingerprint of p
+  int dir_mode;            // next direction: 0 d = z (after a prime), 1 d = z + beta d
+  unsigned body_runs;      // executions of the device loop body since the loop started
 };
 
 // Reduction scratch: per-block f64 partials, or per-64-chunk f32 partials.
 struct Red {
   double* p64;
   float* p32;
+  unsigned* count;         // blocks done, for the last-block finish (reset by that block)
 };
 
 // ------------------------------------------------------------------------------------------------
@@ -238,37 +241,6 @@ __global__ void k_divergence(Geo g, const float* __restrict__ u, const float* __
   }
 }
 
-// rhs_mobile3 (delta3d_mobile.rs:215-241) fused with the b.b reduction of norm2.
-template <int MODE>
-__global__ void k_rhs_mobile(Geo g, float scale, float* __restrict__ rhs, float* __restrict__ prec, Red red,
-                             Scalars* S, int reduce) {
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
-  float b = 0.f;
-  if (c < g.n) {
-    int i, j, k; cell_ijk(g, c, i, j, k);
-    if (!wet3(g, i, j, k)) { rhs[c] = 0.f; prec[c] = 0.f; }
-    else {
-      RowE row[6]; mobile_row(g, i, j, k, row);
-      b = scale * rhs[c];
-      float diag = 0.f;
-#pragma unroll
-      for (int f = 0; f < 6; ++f) {
-        if (row[f].n >= 0) diag += row[f].a;
-        else if (row[f].a > 0.f) {
-          diag += row[f].a * row[f].it;
-          b += row[f].a * row[f].val * row[f].it * g.inv;
-        }
-      }
-      rhs[c] = b;
-      prec[c] = diag > 0.f ? 1.f / (diag * g.inv) : 0.f;
-    }
-  }
-  if (reduce) {
-    block_reduce<MODE>(Acc<MODE>::prod(b, b), c, g.n, red);
-    flag_nonzero(c < g.n && b != 0.f, S);
-  }
-}
-
 // p = 0 on dry cells (delta3d_mobile.rs:485-494).
 __global__ void k_zero_dry(Geo g, float* __restrict__ p) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -285,75 +257,6 @@ __global__ void k_apply(Geo g, const float* __restrict__ x, float* __restrict__ 
   out[c] = wet3(g, i, j, k) ? apply_row(g, i, j, k, c, x) : 0.f;
 }
 
-// res = rhs - A p, with res.res (delta3d_mobile.rs:496-501, 547-553).
-template <int MODE>
-__global__ void k_residual(Geo g, const float* __restrict__ p, const float* __restrict__ rhs, float* __restrict__ res,
-                           Red red, Scalars* S) {
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
-  float r = 0.f;
-  if (c < g.n) {
-    int i, j, k; cell_ijk(g, c, i, j, k);
-    float ap = wet3(g, i, j, k) ? apply_row(g, i, j, k, c, p) : 0.f;
-    r = rhs[c] - ap;
-    res[c] = r;
-  }
-  block_reduce<MODE>(Acc<MODE>::prod(r, r), c, g.n, red);
-  flag_nonzero(c < g.n && r != 0.f, S);
-}
-
-// q = A d with d.q (delta3d_mobile.rs:523-528).
-template <int MODE>
-__global__ void k_apply_dot(Geo g, const float* __restrict__ d, float* __restrict__ q, Red red, const Scalars* S) {
-  if (!S->active) return;
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
-  float dqv = 0.f, dc = 0.f;
-  if (c < g.n) {
-    int i, j, k; cell_ijk(g, c, i, j, k);
-    dqv = wet3(g, i, j, k) ? apply_row(g, i, j, k, c, d) : 0.f;
-    q[c] = dqv;
-    dc = d[c];
-  }
-  block_reduce<MODE>(Acc<MODE>::prod(dc, dqv), c, g.n, red);
-}
-
-// p += alpha d, r -= alpha q, with r.r (delta3d_mobile.rs:532-536).
-template <int MODE>
-__global__ void k_update(int n, float* __restrict__ p, float* __restrict__ r, const float* __restrict__ d,
-                         const float* __restrict__ q, Red red, Scalars* S) {
-  if (!S->active) return;
-  const float alpha = S->alpha;
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
-  float rn = 0.f;
-  if (c < n) {
-    p[c] += alpha * d[c];
-    rn = r[c] - alpha * q[c];
-    r[c] = rn;
-  }
-  block_reduce<MODE>(Acc<MODE>::prod(rn, rn), c, n, red);
-  flag_nonzero(c < n && rn != 0.f, S);
-}
-
-// a.b over cells (dot, delta3d.rs:860-869); gate = 1 skips when the loop is not active.
-template <int MODE>
-__global__ void k_dot(int n, const float* __restrict__ a, const float* __restrict__ b, Red red, const Scalars* S, int gate) {
-  if (gate && !S->active) return;
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
-  float x = 0.f, y = 0.f;
-  if (c < n) { x = a[c]; y = b[c]; }
-  block_reduce<MODE>(Acc<MODE>::prod(x, y), c, n, red);
-}
-
-// res.prec.res (dot_prec3, delta3d_mobile.rs:447-461).
-template <int MODE>
-__global__ void k_dot_prec(int n, const float* __restrict__ r, const float* __restrict__ prec, Red red, const Scalars* S,
-                           int gate) {
-  if (gate && !S->active) return;
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
-  float x = 0.f, m = 0.f;
-  if (c < n) { x = r[c]; m = prec[c]; }
-  block_reduce<MODE>(Acc<MODE>::prod3(x, m, x), c, n, red);
-}
-
 // dir = z + beta dir, z = prec res (prime_mobile3, delta3d_mobile.rs:435-445).  use_beta = 0 is
 // the `beta == 0` branch (dir = z).
 __global__ void k_jacobi_dir(int n, const float* __restrict__ prec, const float* __restrict__ r, float* __restrict__ d,
@@ -364,76 +267,6 @@ __global__ void k_jacobi_dir(int n, const float* __restrict__ prec, const float*
   float beta = use_beta ? S->beta : 0.f;
   float z = prec[c] * r[c];
   d[c] = beta == 0.f ? z : z + beta * d[c];
-}
-
-// dir = z + beta dir (direction_multigrid3, delta3d_multigrid.rs:460-465); use_beta = 0 is the
-// `beta == 0` branch of prime_multigrid3 (dir = z).
-__global__ void k_mg_dir(int n, const float* __restrict__ z, float* __restrict__ d, const Scalars* S, int gate,
-                         int use_beta) {
-  if (gate && !S->active) return;
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= n) return;
-  if (!use_beta) d[c] = z[c];
-  else d[c] = z[c] + S->beta * d[c];
-}
-
-// ------------------------------------------------------------------------------------------------
-// Fine level of the V-cycle (v_cycle3, delta3d_multigrid.rs:393-429).  The fine operator is
-// apply_mobile3 itself; the smoother is damped Jacobi with the inverse diagonal `prec`.
-
-// First pre-sweep from z = 0: A z = 0, so z = 0 + w prec (r - 0).
-__global__ void k_fine_sweep0(int n, const float* __restrict__ prec, const float* __restrict__ r, float* __restrict__ z,
-                              const Scalars* S, int gate) {
-  if (gate && !S->active) return;
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= n) return;
-  float m = prec[c];
-  z[c] = m > 0.f ? 0.f + OMEGA * m * (r[c] - 0.f) : 0.f;
-}
-
-// zout = zin + w prec (r - A zin) where prec > 0.
-__global__ void k_fine_sweep(Geo g, const float* __restrict__ prec, const float* __restrict__ r,
-                             const float* __restrict__ zin, float* __restrict__ zout, const Scalars* S, int gate) {
-  if (gate && !S->active) return;
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= g.n) return;
-  float m = prec[c];
-  float zc = zin[c];
-  if (m > 0.f) {
-    int i, j, k; cell_ijk(g, c, i, j, k);
-    float t = apply_row(g, i, j, k, c, zin);  // prec > 0 implies wet
-    zc += OMEGA * m * (r[c] - t);
-  }
-  zout[c] = zc;
-}
-
-// Coarse r = mean of the 8 children of (r - A z) (restrict3, delta3d_multigrid.rs:258-272).
-__global__ void k_fine_restrict(Geo g, const float* __restrict__ r, const float* __restrict__ z, Lev L,
-                                const Scalars* S, int gate) {
-  if (gate && !S->active) return;
-  int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= L.n) return;
-  int ci = q % L.nx, t = q / L.nx, cj = t % L.ny, ck = t / L.ny;
-  float s = 0.f;
-#pragma unroll
-  for (int e = 0; e < 8; ++e) {
-    int i = 2 * ci + (e & 1), j = 2 * cj + ((e >> 1) & 1), k = 2 * ck + (e >> 2);
-    int c = (k * g.ny + j) * g.nx + i;
-    float az = wet3(g, i, j, k) ? apply_row(g, i, j, k, c, z) : 0.f;
-    s += r[c] - az;
-  }
-  L.r[q] = 0.125f * s;
-}
-
-// z += parent x (prolong_add3), then z = 0 where prec == 0 (delta3d_multigrid.rs:412-418).
-__global__ void k_fine_prolong(Geo g, const float* __restrict__ prec, float* __restrict__ z, Lev L, const Scalars* S,
-                               int gate) {
-  if (gate && !S->active) return;
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= g.n) return;
-  int i, j, k; cell_ijk(g, c, i, j, k);
-  float v = z[c] + L.x[((k >> 1) * L.ny + (j >> 1)) * L.nx + (i >> 1)];
-  z[c] = prec[c] == 0.f ? 0.f : v;
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -527,15 +360,6 @@ __global__ void k_level_restrict(Lev F, Lev C, const Scalars* S, int gate) {
     s += F.r[c] - lx;
   }
   C.r[q] = 0.125f * s;
-}
-
-// F.x += parent C.x (prolong_add3 between coarse levels).
-__global__ void k_level_prolong(Lev F, Lev C, const Scalars* S, int gate) {
-  if (gate && !S->active) return;
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= F.n) return;
-  int i = c % F.nx, t = c / F.nx, j = t % F.ny, k = t / F.ny;
-  F.x[c] += C.x[((k >> 1) * C.ny + (j >> 1)) * C.nx + (i >> 1)];
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -779,83 +603,6 @@ __device__ __forceinline__ bool loop_continues(const Scalars* S, double rn, unsi
   bool above = ord ? ((float)rn > (float)S->tolb2 || (float)rn > (float)S->phys) : (rn > S->tolb2 || rn > S->phys);
   return above && it_next < S->max_iters;
 }
-
-template <int MODE>
-__global__ void k_finish(Red red, int nparts, Scalars* S, int op, int gate) {
-  if (gate && !S->active) return;
-  double val;
-  if (MODE == RED_F64) {
-    __shared__ double sm[1024];
-    double s = 0.0;
-    for (int q = threadIdx.x; q < nparts; q += blockDim.x) s += red.p64[q];
-    sm[threadIdx.x] = s;
-    __syncthreads();
-    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-      if ((int)threadIdx.x < w) sm[threadIdx.x] += sm[threadIdx.x + w];
-      __syncthreads();
-    }
-    val = sm[0];
-  } else {
-    // serial in-order merge in f32 (host_impl.rs:75-92, merge of delta3d.rs:867)
-    __shared__ float seg[8192];
-    float acc = 0.f;
-    for (int base = 0; base < nparts; base += 8192) {
-      int cnt = min(8192, nparts - base);
-      for (int q = threadIdx.x; q < cnt; q += blockDim.x) seg[q] = red.p32[base + q];
-      __syncthreads();
-      if (threadIdx.x == 0)
-        for (int q = 0; q < cnt; ++q) acc = acc + seg[q];
-      __syncthreads();
-    }
-    val = (double)acc;
-  }
-  if (threadIdx.x != 0) return;
-  const int ord = MODE == RED_ORD;
-  const bool finite = isfinite(val);
-  const bool zero_but_nonzero = ord && val == 0.0 && S->any_nonzero;  // norm2 guard
-  switch (op) {
-    case FIN_B2:
-      S->b2 = val;
-      if (!finite || zero_but_nonzero) S->status = 2;
-      break;
-    case FIN_RR0:
-    case FIN_ACTUAL:
-      if (op == FIN_RR0) S->rr = val; else S->actual = val;
-      if (!finite || zero_but_nonzero) S->status = 2;
-      break;
-    case FIN_DQ:
-      S->dq = val;
-      if (!(val > 0.0)) { S->active = 0; S->brk = 1; }
-      else S->alpha = ord ? (float)S->rz / (float)val : (float)(S->rz / val);
-      break;
-    case FIN_RN: {
-      S->rn = val;
-      if (!finite || zero_but_nonzero) { S->status = 2; S->active = 0; break; }
-      if (!loop_continues(S, val, S->it + 1, ord)) {
-        S->rr = val;
-        S->it += 1;
-        S->active = 0;
-      }
-      break;
-    }
-    case FIN_RZ_ITER: {
-      if (!finite) { S->status = 2; S->active = 0; break; }
-      S->zn = val;
-      if (ord) S->beta = (float)val / (float)S->rz;
-      else S->beta = (float)(val / S->rz);
-      S->rz = val;
-      S->rr = S->rn;
-      S->it += 1;
-      break;
-    }
-    case FIN_RZ_PRIME:
-      if (!finite) S->status = 2;
-      S->rz = val;
-      break;
-  }
-  S->any_nonzero = 0;
-}
-
 
 // ------------------------------------------------------------------------------------------------
 // The rest of the mobile step (delta3d_mobile.rs:615-813)

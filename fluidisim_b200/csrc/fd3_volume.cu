@@ -20,7 +20,7 @@
 
 #include "../../include/fluidisim_delta3d.h"
 #include "fd3_cut.cuh"
-#include "fd3_kernels.cuh"
+#include "fd3_fast.cuh"
 
 using namespace fd3;
 
@@ -49,6 +49,9 @@ int cuda_fail(cudaError_t e, const char* what, int line) {
 
 inline int blocks_for(long long n) { return (int)((n + TPB - 1) / TPB); }
 
+// Coarse levels of at most this many cells are solved together by one CTA (k_coarse_tail).
+constexpr int TAIL_MAX_CELLS = 4096;
+
 // PROJECTION_DIVERGENCE_TOLERANCE (delta_projection.rs:192)
 constexpr double kDivTol = 1e-5;
 // gamma_8 and gamma_10 of u = 2^-24 (delta_projection.rs:200-203, delta3d.rs:69-72)
@@ -69,16 +72,20 @@ struct fd3_volume {
   // state and work fields (delta3d.rs:102-184)
   float *eta = nullptr, *rof = nullptr, *u = nullptr, *v = nullptr, *w = nullptr;
   float *us = nullptr, *vs = nullptr, *ws = nullptr, *p = nullptr, *rhs = nullptr, *res = nullptr;
-  float *dir = nullptr, *tmp = nullptr, *prec = nullptr;
+  float *dir = nullptr, *dir2 = nullptr, *tmp = nullptr, *prec = nullptr;
+  unsigned short* codes = nullptr;  // row codes of the current projection
   float *sv_u = nullptr, *sv_v = nullptr, *sv_w = nullptr, *sv_p = nullptr, *sv_eta = nullptr, *sv_rof = nullptr;
   float *flux_x = nullptr, *flux_y = nullptr;
   // multigrid
   bool has_mg = false;
   float *z = nullptr, *z2 = nullptr;
   std::vector<Lev> levels;
+  Lev* dlev = nullptr;   // the level table in device memory (for the single-CTA coarse tail)
+  int tail_first = 0;    // first level small enough for the single-CTA tail
   // reductions and scalars
   double* p64 = nullptr;
   float* p32 = nullptr;
+  unsigned* count = nullptr;
   Scalars* dS = nullptr;
   Scalars* hS = nullptr;  // pinned
   int* dflag = nullptr;
@@ -97,10 +104,11 @@ struct fd3_volume {
   std::vector<std::string> prof_names;
   std::vector<unsigned long long> prof_count;
   std::vector<double> prof_ms;
-  // CUDA graph of one PCG iteration
-  cudaGraphExec_t iter_exec = nullptr;
-  int iter_exec_mode = -1;
-  unsigned long long iter_nodes = 0;
+  // the inner loop as a CUDA graph with a WHILE node
+  cudaGraphExec_t loop_exec = nullptr;
+  int loop_mode = -1;
+  cudaStream_t loop_stream = nullptr;
+  unsigned long long body_nodes = 0;
 
   Geo geo() const {
     Geo G;
@@ -115,7 +123,7 @@ struct fd3_volume {
     return G;
   }
   bool ord() const { return opt.reduction == FD3_REDUCE_ORDERED_F32; }
-  Red red() const { return Red{p64, p32}; }
+  Red red() const { return Red{p64, p32, count}; }
 };
 
 namespace {
@@ -131,7 +139,7 @@ int dalloc(fd3_volume* V, float** ptr, size_t count) {
 
 void release(fd3_volume* V) {
   if (V->stream) cudaStreamSynchronize(V->stream);
-  if (V->iter_exec) cudaGraphExecDestroy(V->iter_exec);
+  if (V->loop_exec) cudaGraphExecDestroy(V->loop_exec);
   for (cudaEvent_t e : V->ev_pool) cudaEventDestroy(e);
   for (void* q : V->allocations) cudaFree(q);
   if (V->hS) cudaFreeHost(V->hS);
@@ -187,14 +195,6 @@ int pull(fd3_volume* V) {
   return sync(V);
 }
 
-// Number of partials a reduction over n elements leaves.
-int nparts(const fd3_volume* V, int n) { return V->ord() ? (n + CHUNK - 1) / CHUNK : blocks_for(n); }
-
-void finish(fd3_volume* V, int n, int op, int gate) {
-  if (V->ord()) launch_grid(V, "k_finish", 1, 256, k_finish<RED_ORD>, V->red(), nparts(V, n), V->dS, op, gate);
-  else launch_grid(V, "k_finish", 1, 1024, k_finish<RED_F64>, V->red(), nparts(V, n), V->dS, op, gate);
-}
-
 #define DISPATCH(V, KERNEL, N, ...)                                                               \
   do {                                                                                           \
     if ((V)->ord()) launch_grid((V), #KERNEL, blocks_for(N), TPB, KERNEL<RED_ORD>, __VA_ARGS__);   \
@@ -222,109 +222,136 @@ void prepare_multigrid(fd3_volume* V) {
   }
 }
 
-// coarse_cycle3 (delta3d_multigrid.rs:303-332); levels[0].r already restricted.
+// coarse_cycle3 (delta3d_multigrid.rs:303-332); levels[0].r already restricted.  Levels from
+// V->tail_first on are solved by one CTA; the larger ones by grid-wide fused kernels.
 void coarse_cycle(fd3_volume* V, int gate) {
   std::vector<Lev>& Ls = V->levels;
-  size_t last = Ls.size() - 1;
-  for (size_t l = 0; l <= last; ++l) {
+  const int last = (int)Ls.size() - 1;
+  const int first_tail = V->tail_first;
+  const Scalars* S = V->dS;
+  for (int l = 0; l < first_tail && l <= last; ++l) {
     Lev& L = Ls[l];
-    int sweeps = l == last ? 8 : 2;  // COARSE_SWEEPS_3D, PRE_SWEEPS_3D
-    for (int s = 0; s < sweeps; ++s) {
-      const float* in = (s % 2 == 0) ? L.x : L.x2;
-      float* out = (s % 2 == 0) ? L.x2 : L.x;
-      LAUNCH(V, k_level_sweep, L.n, L, in, out, s == 0 ? 1 : 0, (const Scalars*)V->dS, gate);
+    if (l == last) {  // a large coarsest level: its 8 sweeps one by one
+      for (int s = 0; s < 8; ++s)
+        LAUNCH(V, k_level_sweep, L.n, L, (const float*)((s % 2 == 0) ? L.x : L.x2), (s % 2 == 0) ? L.x2 : L.x,
+               s == 0 ? 1 : 0, S, gate);
+    } else {
+      LAUNCH(V, k_level_pre, L.n, L, S, gate);
+      LAUNCH(V, k_level_restrict, Ls[l + 1].n, L, Ls[l + 1], S, gate);
     }
-    if (l < last) LAUNCH(V, k_level_restrict, Ls[l + 1].n, L, Ls[l + 1], (const Scalars*)V->dS, gate);
   }
-  for (size_t l = last; l-- > 0;) {
-    Lev& L = Ls[l];
-    LAUNCH(V, k_level_prolong, L.n, L, Ls[l + 1], (const Scalars*)V->dS, gate);
-    for (int s = 0; s < 2; ++s) {  // POST_SWEEPS_3D
-      const float* in = (s % 2 == 0) ? L.x : L.x2;
-      float* out = (s % 2 == 0) ? L.x2 : L.x;
-      LAUNCH(V, k_level_sweep, L.n, L, in, out, 0, (const Scalars*)V->dS, gate);
-    }
+  if (first_tail <= last) LAUNCH_G(V, k_coarse_tail, 1, TAIL_THREADS, (const Lev*)V->dlev, first_tail, last, S, gate);
+  for (int l = std::min(first_tail, last) - 1; l >= 0; --l) {
+    LAUNCH(V, k_level_post1, Ls[l].n, Ls[l], Ls[l + 1], S, gate);
+    LAUNCH(V, k_level_post2, Ls[l].n, Ls[l], S, gate);
   }
 }
 
-// v_cycle3 (delta3d_multigrid.rs:393-429): z = M^-1 res, result in V->z.
-void vcycle(fd3_volume* V, int gate) {
+// v_cycle3 (delta3d_multigrid.rs:393-429) with res.z at its end (op FIN_RZ_PRIME or FIN_RZ_ITER);
+// z = M^-1 res is left in V->z.
+void vcycle(fd3_volume* V, int gate, int op) {
   Geo G = V->geo();
   const Scalars* S = V->dS;
-  LAUNCH(V, k_fine_sweep0, V->n, V->n, (const float*)V->prec, (const float*)V->res, V->z2, S, gate);
-  LAUNCH(V, k_fine_sweep, V->n, G, (const float*)V->prec, (const float*)V->res, (const float*)V->z2, V->z, S, gate);
-  if (!V->levels.empty()) {
-    LAUNCH(V, k_fine_restrict, V->levels[0].n, G, (const float*)V->res, (const float*)V->z, V->levels[0], S, gate);
+  const bool levels = !V->levels.empty();
+  Lev L0 = levels ? V->levels[0] : Lev{};
+  LAUNCH(V, k_fine_pre, V->n, G, (const unsigned short*)V->codes, (const float*)V->prec, (const float*)V->res, V->z, S, gate);
+  if (levels) {
+    LAUNCH(V, k_fine_restrict_c, L0.n, G, (const unsigned short*)V->codes, (const float*)V->res, (const float*)V->z, L0,
+           S, gate);
     coarse_cycle(V, gate);
-    LAUNCH(V, k_fine_prolong, V->n, G, (const float*)V->prec, V->z, V->levels[0], S, gate);
   }
-  LAUNCH(V, k_fine_sweep, V->n, G, (const float*)V->prec, (const float*)V->res, (const float*)V->z, V->z2, S, gate);
-  LAUNCH(V, k_fine_sweep, V->n, G, (const float*)V->prec, (const float*)V->res, (const float*)V->z2, V->z, S, gate);
+  LAUNCH(V, k_fine_post1, V->n, G, (const unsigned short*)V->codes, (const float*)V->prec, (const float*)V->res,
+         (const float*)V->z, L0, levels ? 1 : 0, V->z2, S, gate);
+  DISPATCH(V, k_fine_post2_rz, V->n, G, (const unsigned short*)V->codes, (const float*)V->prec, (const float*)V->res,
+           (const float*)V->z2, V->z, V->red(), V->dS, gate, op);
 }
 
-// prime_multigrid3 / prime_mobile3 with beta = 0: a fresh direction and rz.
+// prime_multigrid3 / prime_mobile3 with beta = 0 (delta3d_mobile.rs:517, 587): rz of a fresh
+// direction; with the multigrid the direction itself is formed by the next k_dir_apply_dot.
 void prime(fd3_volume* V) {
   if (V->has_mg) {
-    vcycle(V, 0);
-    DISPATCH(V, k_dot, V->n, V->n, (const float*)V->res, (const float*)V->z, V->red(), (const Scalars*)V->dS, 0);
-    finish(V, V->n, FIN_RZ_PRIME, 0);
-    LAUNCH(V, k_mg_dir, V->n, V->n, (const float*)V->z, V->dir, (const Scalars*)V->dS, 0, 0);
+    vcycle(V, 0, FIN_RZ_PRIME);
   } else {
     LAUNCH(V, k_jacobi_dir, V->n, V->n, (const float*)V->prec, (const float*)V->res, V->dir, (const Scalars*)V->dS, 0, 0);
-    DISPATCH(V, k_dot_prec, V->n, V->n, (const float*)V->res, (const float*)V->prec, V->red(), (const Scalars*)V->dS, 0);
-    finish(V, V->n, FIN_RZ_PRIME, 0);
+    DISPATCH(V, k_dot_prec_fin, V->n, V->n, (const float*)V->res, (const float*)V->prec, V->red(), V->dS, 0,
+             (int)FIN_RZ_PRIME);
   }
 }
 
-// One inner PCG iteration (delta3d_mobile.rs:515-545), every kernel gated on S->active.
-void iteration(fd3_volume* V) {
+// One inner PCG iteration (delta3d_mobile.rs:515-545), every kernel gated on S->active.  With the
+// multigrid, the direction alternates between dir and dir2 (parity) because it is recomputed at
+// the stencil points of the operator.
+void iteration(fd3_volume* V, int parity) {
   Geo G = V->geo();
-  DISPATCH(V, k_apply_dot, V->n, G, (const float*)V->dir, V->tmp, V->red(), (const Scalars*)V->dS);
-  finish(V, V->n, FIN_DQ, 1);
-  DISPATCH(V, k_update, V->n, V->n, V->p, V->res, (const float*)V->dir, (const float*)V->tmp, V->red(), V->dS);
-  finish(V, V->n, FIN_RN, 1);
   if (V->has_mg) {
-    vcycle(V, 1);
-    DISPATCH(V, k_dot, V->n, V->n, (const float*)V->res, (const float*)V->z, V->red(), (const Scalars*)V->dS, 1);
-    finish(V, V->n, FIN_RZ_ITER, 1);
-    LAUNCH(V, k_mg_dir, V->n, V->n, (const float*)V->z, V->dir, (const Scalars*)V->dS, 1, 1);
+    float* din = parity ? V->dir2 : V->dir;
+    float* dout = parity ? V->dir : V->dir2;
+    DISPATCH(V, k_dir_apply_dot, V->n, G, (const unsigned short*)V->codes, (const float*)V->z, (const float*)din, dout,
+             V->tmp, V->red(), V->dS);
+    DISPATCH(V, k_update_rn, V->n, V->n, V->p, V->res, (const float*)dout, (const float*)V->tmp, V->red(), V->dS);
+    vcycle(V, 1, FIN_RZ_ITER);
   } else {
-    DISPATCH(V, k_dot_prec, V->n, V->n, (const float*)V->res, (const float*)V->prec, V->red(), (const Scalars*)V->dS, 1);
-    finish(V, V->n, FIN_RZ_ITER, 1);
+    DISPATCH(V, k_apply_dot_c, V->n, G, (const unsigned short*)V->codes, (const float*)V->dir, V->tmp, V->red(), V->dS);
+    DISPATCH(V, k_update_rn, V->n, V->n, V->p, V->res, (const float*)V->dir, (const float*)V->tmp, V->red(), V->dS);
+    DISPATCH(V, k_dot_prec_fin, V->n, V->n, (const float*)V->res, (const float*)V->prec, V->red(), V->dS, 1,
+             (int)FIN_RZ_ITER);
     LAUNCH(V, k_jacobi_dir, V->n, V->n, (const float*)V->prec, (const float*)V->res, V->dir, (const Scalars*)V->dS, 1, 1);
   }
 }
 
-// Run the inner loop until S->active drops; each iteration replayed from a CUDA graph when enabled.
-int run_inner(fd3_volume* V) {
+// The inner loop as one CUDA graph: a WHILE node whose body is two iterations and the condition
+// kernel, so the whole loop runs on the device without a host round trip per iteration.
+int build_loop_graph(fd3_volume* V) {
+  if (V->loop_exec) { cudaGraphExecDestroy(V->loop_exec); V->loop_exec = nullptr; }
+  cudaGraph_t graph;
+  CK(cudaGraphCreate(&graph, 0));
+  cudaGraphConditionalHandle handle;
+  cudaError_t e = cudaGraphConditionalHandleCreate(&handle, graph, 1, cudaGraphCondAssignDefault);
+  if (e != cudaSuccess) { cudaGraphDestroy(graph); return cuda_fail(e, "cudaGraphConditionalHandleCreate", __LINE__); }
+  cudaGraphNodeParams params{};
+  params.type = cudaGraphNodeTypeConditional;
+  params.conditional.handle = handle;
+  params.conditional.type = cudaGraphCondTypeWhile;
+  params.conditional.size = 1;
+  cudaGraphNode_t node;
+  e = cudaGraphAddNode(&node, graph, nullptr, 0, &params);
+  if (e != cudaSuccess) { cudaGraphDestroy(graph); return cuda_fail(e, "cudaGraphAddNode(while)", __LINE__); }
+  cudaGraph_t body = params.conditional.phGraph_out[0];
+  e = cudaStreamBeginCaptureToGraph(V->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) { cudaGraphDestroy(graph); return cuda_fail(e, "cudaStreamBeginCaptureToGraph", __LINE__); }
+  unsigned long long before = V->launches;
+  iteration(V, 0);
+  iteration(V, 1);
+  LAUNCH_G(V, k_loop_cond, 1, 1, handle, V->dS);
+  cudaGraph_t captured = body;
+  e = cudaStreamEndCapture(V->stream, &captured);
+  V->body_nodes = V->launches - before;
+  V->launches = before;
+  if (e != cudaSuccess) { cudaGraphDestroy(graph); return cuda_fail(e, "cudaStreamEndCapture", __LINE__); }
+  e = cudaGraphInstantiate(&V->loop_exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate(loop)", __LINE__);
+  V->loop_mode = (V->ord() ? 1 : 0) | (V->has_mg ? 2 : 0);
+  V->loop_stream = V->stream;
+  return FD3_OK;
+}
+
+// Run the inner loop until S->active drops.
+int run_inner(fd3_volume* V, uint32_t it_before) {
   const bool graphs = V->opt.use_graphs && !V->prof;
   if (graphs) {
     int mode = (V->ord() ? 1 : 0) | (V->has_mg ? 2 : 0);
-    if (!V->iter_exec || V->iter_exec_mode != mode) {
-      if (V->iter_exec) { cudaGraphExecDestroy(V->iter_exec); V->iter_exec = nullptr; }
-      cudaGraph_t graph;
-      CK(cudaStreamBeginCapture(V->stream, cudaStreamCaptureModeThreadLocal));
-      unsigned long long before = V->launches;
-      iteration(V);
-      cudaError_t e = cudaStreamEndCapture(V->stream, &graph);
-      V->iter_nodes = V->launches - before;
-      V->launches = before;
-      if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture", __LINE__);
-      e = cudaGraphInstantiate(&V->iter_exec, graph, 0);
-      cudaGraphDestroy(graph);
-      if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate", __LINE__);
-      V->iter_exec_mode = mode;
-    }
+    if (!V->loop_exec || V->loop_mode != mode || V->loop_stream != V->stream) TRY(build_loop_graph(V));
+    CK(cudaGraphLaunch(V->loop_exec, V->stream));
+    TRY(pull(V));
+    unsigned ran = V->hS->it > it_before ? V->hS->it - it_before : 1;
+    V->launches += (unsigned long long)((ran + 1) / 2) * V->body_nodes;
+    return FD3_OK;
   }
   // The device clears S->active within max_iters iterations (FIN_RN); the host bound is a guard.
   for (unsigned guard = 0;; ++guard) {
     if (guard > V->hS->max_iters + 2u) return FD3_ERR_CUDA;
-    if (graphs) {
-      CK(cudaGraphLaunch(V->iter_exec, V->stream));
-      V->launches += V->iter_nodes;
-    } else {
-      iteration(V);
-    }
+    iteration(V, guard & 1);
     TRY(pull(V));
     if (!V->hS->active) break;
   }
@@ -338,54 +365,44 @@ __global__ void k_reset_diag(Scalars* S, int mask) {
   if (mask & 4) S->hash = 0ull;
 }
 
-int divergence_metric(fd3_volume* V, double* all_out, double* plain_out) {
-  Geo G = V->geo();
-  LAUNCH_G(V, k_reset_diag, 1, 1, V->dS, 1);
-  LAUNCH(V, k_div_metric, V->n, G, (const float*)V->u, (const float*)V->v, (const float*)V->w, V->dS);
-  LAUNCH_G(V, k_maxabs, 592, TPB, V->nu, (const float*)V->u, V->dS, 2);
-  LAUNCH_G(V, k_maxabs, 592, TPB, V->nv, (const float*)V->v, V->dS, 2);
-  LAUNCH_G(V, k_maxabs, 592, TPB, V->nw, (const float*)V->w, V->dS, 2);
-  TRY(pull(V));
-  float all = V->hS->fmax[0], plain = V->hS->fmax[1], mx = V->hS->fmax[2];
-  // delta3d_mobile.rs:426-432
-  float echelle = std::fmax(mx, PROJECTION_VELOCITY_FLOOR);
-  float ratio = mx > 0.f ? V->dx / echelle : 0.f;
-  *all_out = (double)(all * ratio);
-  *plain_out = (double)(plain * ratio);
-  return FD3_OK;
-}
-
-int backward_error(fd3_volume* V, float* out) {
-  LAUNCH_G(V, k_reset_diag, 1, 1, V->dS, 2);
-  LAUNCH(V, k_backward_error, V->n, V->geo(), (const float*)V->p, (const float*)V->rhs, (const float*)V->res, V->dS);
-  TRY(pull(V));
-  *out = V->hS->fmax[3];
-  return FD3_OK;
-}
-
-int fingerprint(fd3_volume* V, unsigned long long* out) {
-  LAUNCH_G(V, k_reset_diag, 1, 1, V->dS, 4);
-  LAUNCH_G(V, k_hash, 592, TPB, V->n, (const float*)V->p, V->dS);
-  TRY(pull(V));
-  *out = V->hS->hash;
-  return FD3_OK;
-}
-
 void correct(fd3_volume* V, float k1) {
   Geo G = V->geo();
   LAUNCH(V, k_correct_uv, (long long)V->nu + V->nv, G, k1, (const float*)V->p, (const float*)V->us, (const float*)V->vs, V->u, V->v);
   LAUNCH(V, k_correct_w, V->nw, G, k1, (const float*)V->p, (const float*)V->ws, V->w);
 }
 
-// Loop start: the host's view of the loop state is written to the device before the inner loop.
-__global__ void k_loop_start(Scalars* S, double rr, double tolb2, double phys, unsigned it, unsigned max_iters) {
-  S->rr = rr;
-  S->tolb2 = tolb2;
-  S->phys = phys;
-  S->it = it;
-  S->max_iters = max_iters;
-  S->brk = 0;
-  S->active = 1;
+// The checks that end or restart the outer loop (delta3d_mobile.rs:547-585), launched together:
+// the true residual, the corrected field and its divergence metric (delta3d_mobile.rs:398-433),
+// the backward error (:243-271) and the fingerprint of p.  Correcting before knowing whether the
+// solve is accepted is harmless: us is untouched and every exit corrects from it again or restores
+// u.  One synchronisation.
+struct Checks { double actual, all, plain; float be; unsigned long long hash; int status; };
+
+int outer_checks(fd3_volume* V, float k1, Checks* out) {
+  Geo G = V->geo();
+  DISPATCH(V, k_residual_c, V->n, G, (const unsigned short*)V->codes, (const float*)V->p, (const float*)V->rhs, V->res,
+           V->red(), V->dS, (int)FIN_ACTUAL);
+  correct(V, k1);
+  LAUNCH_G(V, k_reset_diag, 1, 1, V->dS, 7);
+  LAUNCH(V, k_div_metric, V->n, G, (const float*)V->u, (const float*)V->v, (const float*)V->w, V->dS);
+  LAUNCH_G(V, k_maxabs, 592, TPB, V->nu, (const float*)V->u, V->dS, 2);
+  LAUNCH_G(V, k_maxabs, 592, TPB, V->nv, (const float*)V->v, V->dS, 2);
+  LAUNCH_G(V, k_maxabs, 592, TPB, V->nw, (const float*)V->w, V->dS, 2);
+  LAUNCH(V, k_backward_error, V->n, G, (const float*)V->p, (const float*)V->rhs, (const float*)V->res, V->dS);
+  LAUNCH_G(V, k_hash, 592, TPB, V->n, (const float*)V->p, V->dS);
+  TRY(pull(V));
+  const Scalars* S = V->hS;
+  // delta3d_mobile.rs:426-432
+  float all = S->fmax[0], plain = S->fmax[1], mx = S->fmax[2];
+  float echelle = std::fmax(mx, PROJECTION_VELOCITY_FLOOR);
+  float ratio = mx > 0.f ? V->dx / echelle : 0.f;
+  out->actual = S->actual;
+  out->all = (double)(all * ratio);
+  out->plain = (double)(plain * ratio);
+  out->be = S->fmax[3];
+  out->hash = S->hash;
+  out->status = S->status;
+  return FD3_OK;
 }
 
 __global__ void k_reset_scalars(Scalars* S) {
@@ -400,12 +417,12 @@ int project_mobile3(fd3_volume* V, float scale, float k1, uint32_t max_iters, fd
   Geo G = V->geo();
   LAUNCH_G(V, k_reset_scalars, 1, 1, V->dS);
   LAUNCH(V, k_divergence, V->n, G, (const float*)V->us, (const float*)V->vs, (const float*)V->ws, V->rhs);
-  DISPATCH(V, k_rhs_mobile, V->n, G, scale, V->rhs, V->prec, V->red(), V->dS, 1);
-  finish(V, V->n, FIN_B2, 0);
+  DISPATCH(V, k_rhs_b2, V->n, G, scale, V->rhs, V->prec, V->red(), V->dS, 1);
+  LAUNCH(V, k_row_codes, V->n, G, V->codes);
   if (V->has_mg) prepare_multigrid(V);
   LAUNCH(V, k_zero_dry, V->n, G, V->p);
-  DISPATCH(V, k_residual, V->n, G, (const float*)V->p, (const float*)V->rhs, V->res, V->red(), V->dS);
-  finish(V, V->n, FIN_RR0, 0);
+  DISPATCH(V, k_residual_c, V->n, G, (const unsigned short*)V->codes, (const float*)V->p, (const float*)V->rhs, V->res,
+           V->red(), V->dS, (int)FIN_RR0);
   TRY(pull(V));
   if (V->hS->status) return V->hS->status;
   const double b2 = V->hS->b2;
@@ -422,6 +439,7 @@ int project_mobile3(fd3_volume* V, float scale, float k1, uint32_t max_iters, fd
   double actual_rr = 0;
   bool settled = false;
   double settled_d[2] = {0, 0};
+  Checks ck{};
   auto above = [&](double r) {
     if (ord) return (float)r > (float)tolb2 || (float)r > (float)phys;
     return r > tolb2 || r > phys;
@@ -435,77 +453,60 @@ int project_mobile3(fd3_volume* V, float scale, float k1, uint32_t max_iters, fd
       }
       LAUNCH_G(V, k_loop_start, 1, 1, V->dS, rr, tolb2, phys, it, max_iters);
       V->hS->max_iters = max_iters;
-      TRY(run_inner(V));
+      TRY(run_inner(V, it));
       if (V->hS->status) return V->hS->status;
       it = V->hS->it;
       rr = V->hS->rr;
     }
-    // the true residual decides (delta3d_mobile.rs:547-553)
-    DISPATCH(V, k_residual, V->n, G, (const float*)V->p, (const float*)V->rhs, V->res, V->red(), V->dS);
-    finish(V, V->n, FIN_ACTUAL, 0);
-    TRY(pull(V));
-    if (V->hS->status) return V->hS->status;
-    double actual = V->hS->actual;
+    TRY(outer_checks(V, k1, &ck));
+    if (ck.status) return ck.status;
+    const double actual = ck.actual;
     bool exhausted = it >= max_iters || it == before;
     bool has_measured = false;
     double measured[2] = {0, 0};
     bool converged = ord ? (float)actual <= (float)tolb2 : actual <= tolb2;
     if (converged) {
       if (exhausted) { actual_rr = actual; break; }
-      correct(V, k1);
-      double all, plain;
-      TRY(divergence_metric(V, &all, &plain));
-      if (plain <= kDivTol) { actual_rr = actual; settled = true; settled_d[0] = all; settled_d[1] = plain; break; }
-      has_measured = true; measured[0] = all; measured[1] = plain;
+      if (ck.plain <= kDivTol) { actual_rr = actual; settled = true; settled_d[0] = ck.all; settled_d[1] = ck.plain; break; }
+      has_measured = true; measured[0] = ck.all; measured[1] = ck.plain;
       if (ord) {
-        float ratio = (float)(kDivTol / plain);
+        float ratio = (float)(kDivTol / ck.plain);
         phys = (double)((float)actual * ratio * ratio);
       } else {
-        double ratio = kDivTol / plain;
+        double ratio = kDivTol / ck.plain;
         phys = actual * ratio * ratio;
       }
     } else if (exhausted) {
       actual_rr = actual;
       break;
     }
-    float be;
-    TRY(backward_error(V, &be));
-    if (be <= (V->ny == 1 ? kRoundoff2D : kRoundoff3D)) {
+    if (ck.be <= (V->ny == 1 ? kRoundoff2D : kRoundoff3D)) {
       floor_stop = true; actual_rr = actual;
       if (has_measured) { settled = true; settled_d[0] = measured[0]; settled_d[1] = measured[1]; }
       break;
     }
-    unsigned long long state;
-    TRY(fingerprint(V, &state));
-    if (has_checkpoint && checkpoint == state) {
+    if (has_checkpoint && checkpoint == ck.hash) {
       floor_stop = true; actual_rr = actual;
       if (has_measured) { settled = true; settled_d[0] = measured[0]; settled_d[1] = measured[1]; }
       break;
     }
     since += 1;
     if (since == power) {
-      has_checkpoint = true; checkpoint = state;
+      has_checkpoint = true; checkpoint = ck.hash;
       power = power > 0x7fffffffu ? 0xffffffffu : power * 2;
       since = 0;
     }
     rr = actual;
     prime(V);
-    TRY(pull(V));
-    if (V->hS->status) return V->hS->status;
   }
   double residual;
   if (ord) residual = b2 > 0 ? (double)std::sqrt((float)actual_rr / (float)b2) : 0.0;
   else residual = b2 > 0 ? std::sqrt(actual_rr / b2) : 0.0;
-  double div_all, div_plain;
-  if (settled) { div_all = settled_d[0]; div_plain = settled_d[1]; }
-  else {
-    correct(V, k1);
-    TRY(divergence_metric(V, &div_all, &div_plain));
-  }
+  // The last checks ran on the final p: their correction and metrics are the reference's tail
+  // (delta3d_mobile.rs:592-598).
+  double div_all = settled ? settled_d[0] : ck.all, div_plain = settled ? settled_d[1] : ck.plain;
   bool conv = ord ? (float)actual_rr <= (float)tolb2 : actual_rr <= tolb2;
   bool accepted = (conv || floor_stop) && div_plain <= kDivTol;
-  float be;
-  TRY(backward_error(V, &be));
   memset(rep, 0, sizeof *rep);
   rep->refinements = 0;
   rep->iterations = it;
@@ -513,7 +514,7 @@ int project_mobile3(fd3_volume* V, float scale, float k1, uint32_t max_iters, fd
   rep->residual = residual;
   rep->divergence = div_all;
   rep->floor = floor_stop ? 1 : 0;
-  rep->backward_error = (double)be;
+  rep->backward_error = (double)ck.be;
   rep->divergence_plain = div_plain;
   return FD3_OK;
 }
@@ -563,7 +564,11 @@ int alloc_state(fd3_volume* V) {
   TRY(dalloc(V, &V->u, V->nu)); TRY(dalloc(V, &V->v, V->nv)); TRY(dalloc(V, &V->w, V->nw));
   TRY(dalloc(V, &V->us, V->nu)); TRY(dalloc(V, &V->vs, V->nv)); TRY(dalloc(V, &V->ws, V->nw));
   TRY(dalloc(V, &V->p, V->n)); TRY(dalloc(V, &V->rhs, V->n)); TRY(dalloc(V, &V->res, V->n));
-  TRY(dalloc(V, &V->dir, V->n)); TRY(dalloc(V, &V->tmp, V->n)); TRY(dalloc(V, &V->prec, V->n));
+  TRY(dalloc(V, &V->dir, V->n)); TRY(dalloc(V, &V->dir2, V->n)); TRY(dalloc(V, &V->tmp, V->n));
+  TRY(dalloc(V, &V->prec, V->n));
+  float* cq;
+  TRY(dalloc(V, &cq, (size_t)(V->n + 1) / 2)); V->codes = (unsigned short*)cq;
+  TRY(dalloc(V, &cq, 4)); V->count = (unsigned*)cq;
   TRY(dalloc(V, &V->sv_u, V->nu)); TRY(dalloc(V, &V->sv_v, V->nv)); TRY(dalloc(V, &V->sv_w, V->nw));
   TRY(dalloc(V, &V->sv_p, V->n)); TRY(dalloc(V, &V->sv_eta, V->ncol)); TRY(dalloc(V, &V->sv_rof, V->ncol));
   TRY(dalloc(V, &V->flux_x, (size_t)(V->nx + 1) * V->ny)); TRY(dalloc(V, &V->flux_y, (size_t)V->nx * (V->ny + 1)));
@@ -838,7 +843,7 @@ int fd3_set_stream(fd3_volume* v, void* stream) {
   if (!v) return FD3_ERR_INVALID_ARGUMENT;
   TRY(sync(v));
   v->stream = stream ? (cudaStream_t)stream : v->own_stream;
-  if (v->iter_exec) { cudaGraphExecDestroy(v->iter_exec); v->iter_exec = nullptr; }
+  if (v->loop_exec) { cudaGraphExecDestroy(v->loop_exec); v->loop_exec = nullptr; }
   return FD3_OK;
 }
 
@@ -864,6 +869,14 @@ int fd3_enable_multigrid(fd3_volume* V) {
     TRY(dalloc(V, &L.x, L.n)); TRY(dalloc(V, &L.x2, L.n)); TRY(dalloc(V, &L.r, L.n)); TRY(dalloc(V, &L.t, L.n));
     V->levels.push_back(L);
     x = cx; y = cy; zz = cz;
+  }
+  V->tail_first = (int)V->levels.size();
+  while (V->tail_first > 0 && V->levels[V->tail_first - 1].n <= TAIL_MAX_CELLS) --V->tail_first;
+  if (!V->levels.empty()) {
+    float* q;
+    TRY(dalloc(V, &q, (V->levels.size() * sizeof(Lev) + 3) / 4));
+    V->dlev = (Lev*)q;
+    CK(cudaMemcpyAsync(V->dlev, V->levels.data(), V->levels.size() * sizeof(Lev), cudaMemcpyHostToDevice, V->stream));
   }
   V->has_mg = true;
   return sync(V);
@@ -1056,7 +1069,7 @@ int fd3_assemble_pressure_problem_for_trials(fd3_volume* V, const float* diverge
   TRY(check_finite_device(V, V->tmp, V->n, &ok));
   if (!ok) return FD3_ERR_NOT_FINITE;
   CK(cudaMemcpyAsync(V->rhs, V->tmp, len * 4, cudaMemcpyDeviceToDevice, V->stream));
-  DISPATCH(V, k_rhs_mobile, V->n, V->geo(), scale, V->rhs, V->prec, V->red(), V->dS, 0);
+  DISPATCH(V, k_rhs_b2, V->n, V->geo(), scale, V->rhs, V->prec, V->red(), V->dS, 0);
   CK(cudaMemcpyAsync(rhs, V->rhs, len * 4, cudaMemcpyDeviceToHost, V->stream));
   CK(cudaMemcpyAsync(prec, V->prec, len * 4, cudaMemcpyDeviceToHost, V->stream));
   return sync(V);
@@ -1068,10 +1081,11 @@ int fd3_vcycle_for_tests(fd3_volume* V, const float* x, float* z, size_t len) {
   if (!V->has_mg) return FD3_ERR_DOMAIN;
   if (len != (size_t)V->n) return FD3_ERR_SHAPE;
   CK(cudaMemsetAsync(V->rhs, 0, len * 4, V->stream));
-  DISPATCH(V, k_rhs_mobile, V->n, V->geo(), 1.f, V->rhs, V->prec, V->red(), V->dS, 0);
+  DISPATCH(V, k_rhs_b2, V->n, V->geo(), 1.f, V->rhs, V->prec, V->red(), V->dS, 0);
+  LAUNCH(V, k_row_codes, V->n, V->geo(), V->codes);
   prepare_multigrid(V);
   CK(cudaMemcpyAsync(V->res, x, len * 4, cudaMemcpyHostToDevice, V->stream));
-  vcycle(V, 0);
+  vcycle(V, 0, FIN_RZ_PRIME);
   CK(cudaMemcpyAsync(z, V->z, len * 4, cudaMemcpyDeviceToHost, V->stream));
   return sync(V);
 }
