@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstring>
 #include <limits>
+#include <mutex>
 #include <new>
 #include <string>
 #include <utility>
@@ -1127,3 +1128,135 @@ int fd3_profile_entry(const fd3_volume* V, int idx, char* name, size_t len, uint
 }
 
 }  // extern "C"
+
+// =============================================================================== no-alloc entry
+// fd3_assemble_pressure_problem_noalloc: the assembly of the pressure problem (rhs_mobile3 with
+// the norm of its right-hand side) for callers that may not allocate device memory at call time,
+// e.g. a host whose memory arena is sealed after set-up (no allocation after `seal()`), or a
+// real-time loop in which a cudaMalloc would stall the frame.  It allocates nothing: its scratch
+// (per-block partial sums, the completion counter, the finiteness flag) is the file-scope array
+// below, which every GPU that loads this library holds until the process exits.
+namespace {
+
+constexpr int kNoAllocMaxCells = 4194304;                      // largest volume accepted (cells)
+constexpr int kNoAllocMaxBlocks = kNoAllocMaxCells / TPB;       // 16384 partial sums
+constexpr size_t kNoAllocScratchBytes = (size_t)kNoAllocMaxBlocks * sizeof(double) + 256;
+
+// Layout: [0, 8*kNoAllocMaxBlocks) partials (f64) | counter (u32) | flag (i32) | sum (f64).
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+struct NoAllocScratch {
+  double* partials;
+  unsigned* counter;
+  int* flag;
+  double* sum;
+};
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+void* g_noalloc_addr[kMaxDevices] = {};
+
+// The device address of g_noalloc_scratch on the current device, looked up once per device (in
+// host code the symbol is only a host-side stand-in, not a device address).
+int noalloc_scratch(NoAllocScratch* out) {
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) return FD3_ERR_NO_DEVICE;
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_addr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) return cuda_fail(e != cudaSuccess ? e : cudaErrorInvalidSymbol, "cudaGetSymbolAddress", __LINE__);
+    g_noalloc_addr[dev] = p;
+  }
+  unsigned char* base = (unsigned char*)g_noalloc_addr[dev];
+  out->partials = (double*)base;
+  out->counter = (unsigned*)(base + (size_t)kNoAllocMaxBlocks * sizeof(double));
+  out->flag = (int*)(base + (size_t)kNoAllocMaxBlocks * sizeof(double) + 8);
+  out->sum = (double*)(base + (size_t)kNoAllocMaxBlocks * sizeof(double) + 16);
+  return FD3_OK;
+}
+
+// rhs_mobile3 (delta3d_mobile.rs:215-241) of a caller's divergence field into the caller's rhs and
+// prec, with |rhs|^2 in f64: block partials in the scratch, the last block sums them in a fixed
+// order.  The divergence is checked finite on the way (flag).
+__global__ void __launch_bounds__(TPB) k_assemble_noalloc(Geo g, float scale, const float* __restrict__ div,
+                                                          float* __restrict__ rhs, float* __restrict__ prec,
+                                                          NoAllocScratch sc) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  float b = 0.f;
+  bool bad = false;
+  if (c < g.n) {
+    float dv = div[c];
+    bad = !isfinite(dv);
+    int i, j, k; cell_ijk(g, c, i, j, k);
+    if (!wet3(g, i, j, k)) { rhs[c] = 0.f; prec[c] = 0.f; }
+    else {
+      RowE row[6]; mobile_row(g, i, j, k, row);
+      b = scale * dv;
+      float diag = 0.f;
+#pragma unroll
+      for (int f = 0; f < 6; ++f) {
+        if (row[f].n >= 0) diag += row[f].a;
+        else if (row[f].a > 0.f) {
+          diag += row[f].a * row[f].it;
+          b += row[f].a * row[f].val * row[f].it * g.inv;
+        }
+      }
+      rhs[c] = b;
+      prec[c] = diag > 0.f ? 1.f / (diag * g.inv) : 0.f;
+    }
+  }
+  if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(sc.flag, 1);
+  __shared__ double sw[TPB / 32];
+  double s = (double)b * (double)b;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) sw[threadIdx.x >> 5] = s;
+  __syncthreads();
+  __shared__ bool last;
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+#pragma unroll
+    for (int w = 0; w < TPB / 32; ++w) t += sw[w];
+    sc.partials[blockIdx.x] = t;
+    __threadfence();
+    last = atomicAdd(sc.counter, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  __shared__ double sm[TPB];
+  double t = 0.0;
+  for (int q = threadIdx.x; q < (int)gridDim.x; q += blockDim.x) t += __ldcg(sc.partials + q);
+  sm[threadIdx.x] = t;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) sm[threadIdx.x] += sm[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) { *sc.sum = sm[0]; *sc.counter = 0u; }
+}
+
+}  // namespace
+
+extern "C" int fd3_assemble_pressure_problem_noalloc(fd3_volume* V, const float* d_divergence, float scale,
+                                                     float* d_rhs, float* d_prec, size_t len, double* rhs_norm2) {
+  if (!V || !d_divergence || !d_rhs || !d_prec || !rhs_norm2) return FD3_ERR_INVALID_ARGUMENT;
+  if (len != (size_t)V->n) return FD3_ERR_DOMAIN;
+  if (len > (size_t)kNoAllocMaxCells) return FD3_ERR_SCRATCH_LIMIT;
+  if (!std::isfinite(scale)) return FD3_ERR_NOT_FINITE;
+  NoAllocScratch sc;
+  TRY(noalloc_scratch(&sc));
+  // the counter, the flag and the sum start at zero on every call (the array keeps the last call's
+  // contents); the partials are all overwritten
+  CK(cudaMemsetAsync(sc.counter, 0, 24, V->stream));
+  k_assemble_noalloc<<<blocks_for(V->n), TPB, 0, V->stream>>>(V->geo(), scale, d_divergence, d_rhs, d_prec, sc);
+  CK(cudaGetLastError());
+  int flag = 0;
+  CK(cudaMemcpyAsync(&flag, sc.flag, sizeof(int), cudaMemcpyDeviceToHost, V->stream));
+  CK(cudaMemcpyAsync(rhs_norm2, sc.sum, sizeof(double), cudaMemcpyDeviceToHost, V->stream));
+  CK(cudaStreamSynchronize(V->stream));
+  V->launches++;
+  return flag ? FD3_ERR_NOT_FINITE : FD3_OK;
+}

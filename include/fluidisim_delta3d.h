@@ -40,7 +40,8 @@ typedef enum fd3_status {
   FD3_ERR_CUDA = 100,             /* a CUDA runtime call failed; fd3_last_cuda_error() says which */
   FD3_ERR_NO_DEVICE = 101,        /* no CUDA device */
   FD3_ERR_INVALID_ARGUMENT = 102, /* null handle or pointer */
-  FD3_ERR_OUT_OF_MEMORY = 103     /* device allocation failed at configure/enable time */
+  FD3_ERR_OUT_OF_MEMORY = 103,    /* device allocation failed at configure/enable time */
+  FD3_ERR_SCRATCH_LIMIT = 104     /* the volume exceeds the static scratch of a no-alloc entry point */
 } fd3_status;
 
 /* Domain3 (delta3d.rs:44-63): cubic cells of side dx; the lid is z0 = nz*dx. */
@@ -143,6 +144,23 @@ int fd3_apply_pressure_operator_for_trials(fd3_volume* v, const float* p, float*
 /* Volume3::assemble_pressure_problem_for_trials (delta3d_mobile.rs:960). */
 int fd3_assemble_pressure_problem_for_trials(fd3_volume* v, const float* divergence, float scale,
                                              float* rhs, float* prec, size_t len);
+/* The pressure-problem assembly for callers that cannot allocate device memory when they call:
+ * e.g. a host whose memory arena is sealed once set up (the reference's own rule: nothing is
+ * allocated after `seal()`), or a real-time loop where a cudaMalloc would stall the frame.
+ * No counterpart in the reference (its trial hook above allocates nothing either, but this
+ * library's version stages through the volume's work buffers).  Device pointers in and out:
+ * d_divergence (len cells) -> d_rhs and d_prec, as rhs_mobile3 (delta3d_mobile.rs:215-241)
+ * computes them, plus |rhs|^2 in f64 written to *rhs_norm2 (host).  The volume's own buffers
+ * are not touched.
+ * It allocates nothing: its scratch is a static device array of 128 KiB + 256 B in this library
+ * (held on every GPU that loads it until exit), so volumes above 4,194,304 cells are refused with
+ * FD3_ERR_SCRATCH_LIMIT.  The first call on a device looks the scratch's device address up
+ * (cudaGetSymbolAddress) and should come before any stream capture.  All calls share the one
+ * scratch array: calls that overlap on the GPU (other streams, other threads) race; each call
+ * clears the parts that must start at zero.  A non-finite divergence gives FD3_ERR_NOT_FINITE
+ * (the outputs are then written anyway). */
+int fd3_assemble_pressure_problem_noalloc(fd3_volume* v, const float* d_divergence, float scale, float* d_rhs,
+                                          float* d_prec, size_t len, double* rhs_norm2);
 /* v_cycle3 (delta3d_multigrid.rs:393) on `x`, set up as tests_delta3d.rs:1840-1873 does
  * (rhs = 0, rhs_mobile3(1), prepare_multigrid3, res = x).  Writes z = M^-1 x. */
 int fd3_vcycle_for_tests(fd3_volume* v, const float* x, float* z, size_t len);
