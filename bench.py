@@ -235,7 +235,7 @@ def run_b200(args):
     scale, k1 = scenes.projection_scalars(s)
     stream = torch.cuda.Stream()
     vol = Volume3.configure_with_solid(s["nx"], s["ny"], s["nz"], s["dx"], s["rho"], s["g"], s["bottom"], s["solid"])
-    vol.set_options(reduction=REDUCE_F64, use_graphs=1)
+    vol.set_options(reduction=REDUCE_F64, use_graphs=args.graphs)
     vol.set_stream(stream.cuda_stream)
     vol.enable_multigrid()
     vol.set_free_surface(s["eta"], s["rest"])
@@ -328,7 +328,7 @@ def run_b200(args):
     torch.cuda.synchronize()
     prof = vol.profile_entries()
     vol.profile(False)
-    vol.set_options(use_graphs=1)
+    vol.set_options(use_graphs=args.graphs)
     total_prof = sum(ms for _, _, ms in prof)
     known = [(n, c, ms) for n, c, ms in prof if n in BYTES_PER_CELL]
     top = max(known, key=lambda e: e[2])
@@ -384,6 +384,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--size", type=int, default=128)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    ap.add_argument("--graphs", type=int, default=1,
+                    help="1: the inner loop as a CUDA graph with a WHILE node; 0: host-driven (for ncu launch lists)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":

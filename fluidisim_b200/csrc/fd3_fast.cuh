@@ -59,12 +59,24 @@ __device__ __forceinline__ float ghost_it_up(const Geo& g, int i, int j, int k) 
 
 // One row of apply_mobile3 from its code; P(n) yields the operand at cell n (a load, or a value
 // recomputed on the fly by a fused kernel).
+// The code of a wet cell whose six faces are open (aperture 1) onto fluid neighbours: the bulk.
+constexpr unsigned RC_INTERIOR = RC_WET | RC_UNIT | (1u << 1) | (1u << 3) | (1u << 5) | (1u << 7) | (1u << 9) | (1u << 11);
+
 template <class P>
 __device__ __forceinline__ float apply_code(const Geo& g, unsigned code, int i, int j, int k, int c, P p) {
   const float pc = p(c);
   const bool unit = code & RC_UNIT;
   const int nxny = g.nx * g.ny;
   float acc = 0.f;
+  if (code == RC_INTERIOR) {  // a = 1 on every face: the same sum without the decoding
+    acc += pc - p(c - 1);
+    acc += pc - p(c + 1);
+    acc += pc - p(c - g.nx);
+    acc += pc - p(c + g.nx);
+    acc += pc - p(c - nxny);
+    acc += pc - p(c + nxny);
+    return acc * g.inv;
+  }
   unsigned st = face_state(code, 0);
   if (st) {
     float a = unit ? 1.f : open3(g, 0, fu(g, i, j, k));
@@ -386,6 +398,74 @@ __device__ __forceinline__ float level_row_f(const Lev& L, int i, int j, int k, 
   return acc * L.inv;
 }
 
+// Row codes of a coarse level (row_sums, delta3d_multigrid.rs:216-255), once per projection after
+// coarsen3: bit 0 active (kind > 0); per face 0 nothing, 1 active neighbour (a (pc - p_m)),
+// 2 Dirichlet (an air neighbour or the top of the domain: 2 a pc); bit 13 every live aperture is 1.
+__global__ void k_level_codes(Lev L) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= L.n) return;
+  unsigned code = 0;
+  if (L.kind[c] > 0.f) {
+    int i = c % L.nx, t = c / L.nx, j = t % L.ny, k = t / L.ny;
+    const int nxny = L.nx * L.ny;
+    code = RC_WET;
+    bool unit = true;
+    auto face = [&](int f, float a, bool has, int m, bool top) {
+      unsigned st = 0;
+      if (a != 0.f) {
+        if (has) {
+          float km = L.kind[m];
+          st = km > 0.f ? 1u : (km < 0.f ? 2u : 0u);
+        } else if (top) {
+          st = 2u;
+        }
+      }
+      code |= st << (1 + 2 * f);
+      if (st && a != 1.f) unit = false;
+    };
+    face(0, L.ou[(k * L.ny + j) * (L.nx + 1) + i], i > 0, c - 1, false);
+    face(1, L.ou[(k * L.ny + j) * (L.nx + 1) + i + 1], i + 1 < L.nx, c + 1, false);
+    face(2, L.ov[(k * (L.ny + 1) + j) * L.nx + i], j > 0, c - L.nx, false);
+    face(3, L.ov[(k * (L.ny + 1) + j + 1) * L.nx + i], j + 1 < L.ny, c + L.nx, false);
+    face(4, L.ow[(k * L.ny + j) * L.nx + i], k > 0, c - nxny, false);
+    face(5, L.ow[((k + 1) * L.ny + j) * L.nx + i], k + 1 < L.nz, c + nxny, true);
+    if (unit) code |= RC_UNIT;
+  }
+  L.code[c] = (unsigned short)code;
+}
+
+// One row of row_sums (with p) from its code: the same terms, in the same order, as level_row_f.
+template <class P>
+__device__ __forceinline__ float level_row_code(const Lev& L, unsigned code, int i, int j, int k, int c, P p) {
+  const float pc = p(c);
+  const int nxny = L.nx * L.ny;
+  float acc = 0.f;
+  if (code == RC_INTERIOR) {
+    acc += pc - p(c - 1);
+    acc += pc - p(c + 1);
+    acc += pc - p(c - L.nx);
+    acc += pc - p(c + L.nx);
+    acc += pc - p(c - nxny);
+    acc += pc - p(c + nxny);
+    return acc * L.inv;
+  }
+  const bool unit = code & RC_UNIT;
+  auto face = [&](int f, const float* ap, int fi, int m) {
+    unsigned st = face_state(code, f);
+    if (!st) return;
+    float a = unit ? 1.f : ap[fi];
+    if (st == 1) acc += a * (pc - p(m));
+    else acc += 2.f * a * pc;
+  };
+  face(0, L.ou, (k * L.ny + j) * (L.nx + 1) + i, c - 1);
+  face(1, L.ou, (k * L.ny + j) * (L.nx + 1) + i + 1, c + 1);
+  face(2, L.ov, (k * (L.ny + 1) + j) * L.nx + i, c - L.nx);
+  face(3, L.ov, (k * (L.ny + 1) + j + 1) * L.nx + i, c + L.nx);
+  face(4, L.ow, (k * L.ny + j) * L.nx + i, c - nxny);
+  face(5, L.ow, ((k + 1) * L.ny + j) * L.nx + i, c + nxny);
+  return acc * L.inv;
+}
+
 // x0 = 0 + w (r - 0)/diag (first sweep), recomputed per stencil point.
 __device__ __forceinline__ float level_x1(const Lev& L, int n) {
   float dg = L.diag[n];
@@ -402,9 +482,38 @@ __global__ void __launch_bounds__(TPB) k_level_pre(Lev L, const Scalars* S, int 
   float xc = X1(c);
   if (dg > 0.f) {
     int i = c % L.nx, t = c / L.nx, j = t % L.ny, k = t / L.ny;
-    xc += OMEGA * (L.r[c] - level_row_f(L, i, j, k, c, X1)) / dg;
+    xc += OMEGA * (L.r[c] - level_row_code(L, L.code[c], i, j, k, c, X1)) / dg;
   }
   L.x[c] = xc;
+}
+
+// t = r - L x on every cell of a coarse level (0 on inactive rows), the restriction's operand.
+__global__ void __launch_bounds__(TPB) k_level_resid(Lev L, const Scalars* S, int gate) {
+  if (gate && !S->active) return;
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= L.n) return;
+  unsigned code = L.code[c];
+  float lx = 0.f;
+  if (code & RC_WET) {
+    int i = c % L.nx, t = c / L.nx, j = t % L.ny, k = t / L.ny;
+    lx = level_row_code(L, code, i, j, k, c, Load{L.x});
+  }
+  L.t[c] = L.r[c] - lx;
+}
+
+// C.r = mean of the 8 children of F.t, in the reference's CHILDREN order (restrict3).
+__global__ void __launch_bounds__(TPB) k_level_sum8(Lev F, Lev C, const Scalars* S, int gate) {
+  if (gate && !S->active) return;
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= C.n) return;
+  int ci = q % C.nx, t = q / C.nx, cj = t % C.ny, ck = t / C.ny;
+  float s = 0.f;
+#pragma unroll
+  for (int e = 0; e < 8; ++e) {
+    int i = 2 * ci + (e & 1), j = 2 * cj + ((e >> 1) & 1), k = 2 * ck + (e >> 2);
+    s += F.t[(k * F.ny + j) * F.nx + i];
+  }
+  C.r[q] = 0.125f * s;
 }
 
 // Prolongation from C (x += parent) fused with the first post-sweep, L.x -> L.x2.
@@ -420,7 +529,7 @@ __global__ void __launch_bounds__(TPB) k_level_post1(Lev L, Lev C, const Scalars
   float xc = XP(c);
   if (dg > 0.f) {
     int i = c % L.nx, t = c / L.nx, j = t % L.ny, k = t / L.ny;
-    xc += OMEGA * (L.r[c] - level_row_f(L, i, j, k, c, XP)) / dg;
+    xc += OMEGA * (L.r[c] - level_row_code(L, L.code[c], i, j, k, c, XP)) / dg;
   }
   L.x2[c] = xc;
 }
@@ -430,14 +539,29 @@ __global__ void __launch_bounds__(TPB) k_level_post2(Lev L, const Scalars* S, in
   if (gate && !S->active) return;
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= L.n) return;
-  Load X{L.x2};
   float dg = L.diag[c];
   float xc = L.x2[c];
   if (dg > 0.f) {
     int i = c % L.nx, t = c / L.nx, j = t % L.ny, k = t / L.ny;
-    xc += OMEGA * (L.r[c] - level_row_f(L, i, j, k, c, X)) / dg;
+    xc += OMEGA * (L.r[c] - level_row_code(L, L.code[c], i, j, k, c, Load{L.x2})) / dg;
   }
   L.x[c] = xc;
+}
+
+// One damped Jacobi sweep from codes (a large coarsest level's 8 sweeps); zero_in: from x = 0.
+__global__ void __launch_bounds__(TPB) k_level_sweep_c(Lev L, const float* __restrict__ xin, float* __restrict__ xout,
+                                                       int zero_in, const Scalars* S, int gate) {
+  if (gate && !S->active) return;
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= L.n) return;
+  float dg = L.diag[c];
+  if (zero_in) { xout[c] = dg > 0.f ? 0.f + OMEGA * (L.r[c] - 0.f) / dg : 0.f; return; }
+  float xc = xin[c];
+  if (dg > 0.f) {
+    int i = c % L.nx, t = c / L.nx, j = t % L.ny, k = t / L.ny;
+    xc += OMEGA * (L.r[c] - level_row_code(L, L.code[c], i, j, k, c, Load{xin})) / dg;
+  }
+  xout[c] = xc;
 }
 
 // All levels from `first` to `last` in one CTA (coarse_cycle3 restricted to them): each phase is a
@@ -459,16 +583,15 @@ __device__ __forceinline__ void tail_sweep(const Lev& L, const float* xin, float
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(TAIL_THREADS) k_coarse_tail(const Lev* __restrict__ T, int first, int last,
-                                                              const Scalars* S, int gate) {
-  if (gate && !S->active) return;
+// coarse_cycle3 (delta3d_multigrid.rs:303-332) over levels first..last of Ls, in one block.
+__device__ __forceinline__ void tail_run(const Lev* Ls, int first, int last) {
   for (int l = first; l <= last; ++l) {
-    const Lev L = T[l];
+    const Lev L = Ls[l];
     const int sweeps = l == last ? 8 : 2;  // COARSE_SWEEPS_3D, PRE_SWEEPS_3D
     for (int s = 0; s < sweeps; ++s)
       tail_sweep(L, (s % 2 == 0) ? L.x : L.x2, (s % 2 == 0) ? L.x2 : L.x, s == 0);
     if (l < last) {
-      const Lev C = T[l + 1];
+      const Lev C = Ls[l + 1];
       for (int q = threadIdx.x; q < C.n; q += blockDim.x) {
         int ci = q % C.nx, t = q / C.nx, cj = t % C.ny, ck = t / C.ny;
         float s = 0.f;
@@ -485,8 +608,8 @@ __global__ void __launch_bounds__(TAIL_THREADS) k_coarse_tail(const Lev* __restr
     }
   }
   for (int l = last - 1; l >= first; --l) {
-    const Lev L = T[l];
-    const Lev C = T[l + 1];
+    const Lev L = Ls[l];
+    const Lev C = Ls[l + 1];
     for (int c = threadIdx.x; c < L.n; c += blockDim.x) {
       int i = c % L.nx, t = c / L.nx, j = t % L.ny, k = t / L.ny;
       L.x[c] += C.x[((k >> 1) * C.ny + (j >> 1)) * C.nx + (i >> 1)];
@@ -495,6 +618,65 @@ __global__ void __launch_bounds__(TAIL_THREADS) k_coarse_tail(const Lev* __restr
     tail_sweep(L, L.x, L.x2, false);
     tail_sweep(L, L.x2, L.x, false);
   }
+}
+
+// The levels in global memory (fallback when they do not fit in shared memory).
+__global__ void __launch_bounds__(TAIL_THREADS) k_coarse_tail(const Lev* __restrict__ T, int first, int last,
+                                                              const Scalars* S, int gate) {
+  if (gate && !S->active) return;
+  tail_run(T, first, last);
+}
+
+// Floats of shared memory a level takes in the shared-memory tail: five cell arrays and three face
+// arrays, each rounded up to a multiple of four floats (16 bytes), as k_coarse_tail_smem carves them.
+__host__ __device__ inline int round4(int c) { return (c + 3) & ~3; }
+__host__ __device__ inline int tail_level_floats(int nx, int ny, int nz) {
+  const int n = nx * ny * nz;
+  return 5 * round4(n) + round4((nx + 1) * ny * nz) + round4(nx * (ny + 1) * nz) + round4(nx * ny * (nz + 1));
+}
+
+// The same with every level copied into dynamic shared memory first: geometry (kind, diag,
+// apertures) of all tail levels and the restricted r of the first; only the first level's x goes
+// back to global memory (the level above prolongates from it).
+constexpr int MAX_TAIL_LEVELS = 12;
+__global__ void __launch_bounds__(TAIL_THREADS) k_coarse_tail_smem(const Lev* __restrict__ T, int first, int last,
+                                                                   const Scalars* S, int gate) {
+  if (gate && !S->active) return;
+  extern __shared__ float4 tail_smem4[];
+  float* sm = reinterpret_cast<float*>(tail_smem4);
+  __shared__ Lev Ls[MAX_TAIL_LEVELS];
+  if (threadIdx.x == 0) {
+    int off = 0;
+    for (int l = first; l <= last; ++l) {
+      Lev L = T[l];
+      const int n = L.n;
+      const int nu = (L.nx + 1) * L.ny * L.nz, nv = L.nx * (L.ny + 1) * L.nz, nw = L.nx * L.ny * (L.nz + 1);
+      auto take = [&](int cnt) { float* p = sm + off; off += round4(cnt); return p; };
+      Lev M = L;
+      M.kind = take(n); M.diag = take(n); M.r = take(n); M.x = take(n); M.x2 = take(n);
+      M.ou = take(nu); M.ov = take(nv); M.ow = take(nw);
+      Ls[l - first] = M;
+    }
+  }
+  __syncthreads();
+  for (int l = first; l <= last; ++l) {
+    const Lev G = T[l];
+    const Lev M = Ls[l - first];
+    const int nu = (G.nx + 1) * G.ny * G.nz, nv = G.nx * (G.ny + 1) * G.nz, nw = G.nx * G.ny * (G.nz + 1);
+    for (int q = threadIdx.x; q < G.n; q += blockDim.x) {
+      M.kind[q] = G.kind[q];
+      M.diag[q] = G.diag[q];
+      if (l == first) M.r[q] = G.r[q];
+    }
+    for (int q = threadIdx.x; q < nu; q += blockDim.x) M.ou[q] = G.ou[q];
+    for (int q = threadIdx.x; q < nv; q += blockDim.x) M.ov[q] = G.ov[q];
+    for (int q = threadIdx.x; q < nw; q += blockDim.x) M.ow[q] = G.ow[q];
+  }
+  __syncthreads();
+  tail_run(Ls, 0, last - first);
+  const Lev G = T[first];
+  const Lev M = Ls[0];
+  for (int q = threadIdx.x; q < G.n; q += blockDim.x) G.x[q] = M.x[q];
 }
 
 // ------------------------------------------------------------------------------------------------

@@ -46,6 +46,7 @@ struct Lev {
   float* ou; float* ov; float* ow;
   float* kind; float* diag;
   float* x; float* x2; float* r; float* t;
+  unsigned short* code;   // row codes of the level (k_level_codes)
 };
 
 // Device-resident scalars of one projection.  Reduced values are held in double; in ordered

@@ -8,6 +8,7 @@
 // iteration is a fixed launch sequence that can be replayed from a CUDA graph.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstddef>
 #include <cstdio>
@@ -21,7 +22,7 @@
 
 #include "../../include/fluidisim_delta3d.h"
 #include "fd3_cut.cuh"
-#include "fd3_fast.cuh"
+#include "fd3_zmarch.cuh"
 
 using namespace fd3;
 
@@ -51,7 +52,7 @@ int cuda_fail(cudaError_t e, const char* what, int line) {
 inline int blocks_for(long long n) { return (int)((n + TPB - 1) / TPB); }
 
 // Coarse levels of at most this many cells are solved together by one CTA (k_coarse_tail).
-constexpr int TAIL_MAX_CELLS = 4096;
+constexpr int TAIL_MAX_CELLS = 512;
 
 // PROJECTION_DIVERGENCE_TOLERANCE (delta_projection.rs:192)
 constexpr double kDivTol = 1e-5;
@@ -83,8 +84,10 @@ struct fd3_volume {
   std::vector<Lev> levels;
   Lev* dlev = nullptr;   // the level table in device memory (for the single-CTA coarse tail)
   int tail_first = 0;    // first level small enough for the single-CTA tail
+  size_t tail_smem_bytes = 0;  // dynamic shared memory of the shared-memory tail (0: global tail)
   // reductions and scalars
   double* p64 = nullptr;
+  int p64_cap = 0;  // f64 partial slots
   float* p32 = nullptr;
   unsigned* count = nullptr;
   Scalars* dS = nullptr;
@@ -124,6 +127,7 @@ struct fd3_volume {
     return G;
   }
   bool ord() const { return opt.reduction == FD3_REDUCE_ORDERED_F32; }
+  bool blocked() const { return !ord() && opt.kernels == 0; }
   Red red() const { return Red{p64, p32, count}; }
 };
 
@@ -168,6 +172,16 @@ void launch_grid(fd3_volume* V, const char* name, int grid, int block, K kernel,
   V->launches++;
 }
 #define LAUNCH(V, KERNEL, N, ...) launch_grid((V), #KERNEL, blocks_for(N), TPB, KERNEL, __VA_ARGS__)
+
+// The same with dynamic shared memory.
+template <class K, class... A>
+void launch_grid_smem(fd3_volume* V, const char* name, int grid, int block, size_t smem, K kernel, A... args) {
+  cudaEvent_t a = nullptr, b = nullptr;
+  if (V->prof) { a = next_event(V); cudaEventRecord(a, V->stream); }
+  kernel<<<grid, block, smem, V->stream>>>(args...);
+  if (V->prof) { b = next_event(V); cudaEventRecord(b, V->stream); V->pending.push_back({name, a, b}); }
+  V->launches++;
+}
 #define LAUNCH_G(V, KERNEL, GRID, BLOCK, ...) launch_grid((V), #KERNEL, (GRID), (BLOCK), KERNEL, __VA_ARGS__)
 
 void prof_collect(fd3_volume* V) {
@@ -196,6 +210,9 @@ int pull(fd3_volume* V) {
   return sync(V);
 }
 
+// Grid of the grid-stride update: no more blocks than groups of four cells need.
+inline int update_blocks(int n) { return std::min(UPDATE_BLOCKS, std::max(1, blocks_for((n + 3) / 4))); }
+
 #define DISPATCH(V, KERNEL, N, ...)                                                               \
   do {                                                                                           \
     if ((V)->ord()) launch_grid((V), #KERNEL, blocks_for(N), TPB, KERNEL<RED_ORD>, __VA_ARGS__);   \
@@ -220,6 +237,7 @@ void prepare_multigrid(fd3_volume* V) {
       LAUNCH(V, k_coarsen_open, nfaces, F.nx, F.ny, (const float*)F.ou, (const float*)F.ov, (const float*)F.ow, C);
     }
     LAUNCH(V, k_level_diag, C.n, C);
+    LAUNCH(V, k_level_codes, C.n, C);
   }
 }
 
@@ -234,14 +252,21 @@ void coarse_cycle(fd3_volume* V, int gate) {
     Lev& L = Ls[l];
     if (l == last) {  // a large coarsest level: its 8 sweeps one by one
       for (int s = 0; s < 8; ++s)
-        LAUNCH(V, k_level_sweep, L.n, L, (const float*)((s % 2 == 0) ? L.x : L.x2), (s % 2 == 0) ? L.x2 : L.x,
+        LAUNCH(V, k_level_sweep_c, L.n, L, (const float*)((s % 2 == 0) ? L.x : L.x2), (s % 2 == 0) ? L.x2 : L.x,
                s == 0 ? 1 : 0, S, gate);
     } else {
       LAUNCH(V, k_level_pre, L.n, L, S, gate);
-      LAUNCH(V, k_level_restrict, Ls[l + 1].n, L, Ls[l + 1], S, gate);
+      LAUNCH(V, k_level_resid, L.n, L, S, gate);
+      LAUNCH(V, k_level_sum8, Ls[l + 1].n, L, Ls[l + 1], S, gate);
     }
   }
-  if (first_tail <= last) LAUNCH_G(V, k_coarse_tail, 1, TAIL_THREADS, (const Lev*)V->dlev, first_tail, last, S, gate);
+  if (first_tail <= last) {
+    if (V->tail_smem_bytes > 0)
+      launch_grid_smem(V, "k_coarse_tail_smem", 1, TAIL_THREADS, V->tail_smem_bytes, k_coarse_tail_smem,
+                       (const Lev*)V->dlev, first_tail, last, S, gate);
+    else
+      LAUNCH_G(V, k_coarse_tail, 1, TAIL_THREADS, (const Lev*)V->dlev, first_tail, last, S, gate);
+  }
   for (int l = std::min(first_tail, last) - 1; l >= 0; --l) {
     LAUNCH(V, k_level_post1, Ls[l].n, Ls[l], Ls[l + 1], S, gate);
     LAUNCH(V, k_level_post2, Ls[l].n, Ls[l], S, gate);
@@ -255,16 +280,29 @@ void vcycle(fd3_volume* V, int gate, int op) {
   const Scalars* S = V->dS;
   const bool levels = !V->levels.empty();
   Lev L0 = levels ? V->levels[0] : Lev{};
-  LAUNCH(V, k_fine_pre, V->n, G, (const unsigned short*)V->codes, (const float*)V->prec, (const float*)V->res, V->z, S, gate);
+  const unsigned short* codes = V->codes;
+  if (V->blocked()) {  // 2.5-D blocked kernels (f64 reductions)
+    const int zb = zblocks(V->nx, V->ny, V->nz);
+    LAUNCH_G(V, kz_fine_pre, zb, ZT, G, codes, (const float*)V->prec, (const float*)V->res, V->z, S, gate);
+    if (levels) {
+      LAUNCH_G(V, kz_fine_restrict, zb, ZT, G, codes, (const float*)V->res, (const float*)V->z, L0, S, gate);
+      coarse_cycle(V, gate);
+    }
+    LAUNCH_G(V, kz_fine_post1, zb, ZT, G, codes, (const float*)V->prec, (const float*)V->res, (const float*)V->z, L0,
+             levels ? 1 : 0, V->z2, S, gate);
+    LAUNCH_G(V, kz_fine_post2_rz, zb, ZT, G, codes, (const float*)V->prec, (const float*)V->res, (const float*)V->z2,
+             V->z, V->red(), V->dS, gate, op);
+    return;
+  }
+  LAUNCH(V, k_fine_pre, V->n, G, codes, (const float*)V->prec, (const float*)V->res, V->z, S, gate);
   if (levels) {
-    LAUNCH(V, k_fine_restrict_c, L0.n, G, (const unsigned short*)V->codes, (const float*)V->res, (const float*)V->z, L0,
-           S, gate);
+    LAUNCH(V, k_fine_restrict_c, L0.n, G, codes, (const float*)V->res, (const float*)V->z, L0, S, gate);
     coarse_cycle(V, gate);
   }
-  LAUNCH(V, k_fine_post1, V->n, G, (const unsigned short*)V->codes, (const float*)V->prec, (const float*)V->res,
-         (const float*)V->z, L0, levels ? 1 : 0, V->z2, S, gate);
-  DISPATCH(V, k_fine_post2_rz, V->n, G, (const unsigned short*)V->codes, (const float*)V->prec, (const float*)V->res,
-           (const float*)V->z2, V->z, V->red(), V->dS, gate, op);
+  LAUNCH(V, k_fine_post1, V->n, G, codes, (const float*)V->prec, (const float*)V->res, (const float*)V->z, L0,
+         levels ? 1 : 0, V->z2, S, gate);
+  DISPATCH(V, k_fine_post2_rz, V->n, G, codes, (const float*)V->prec, (const float*)V->res, (const float*)V->z2, V->z,
+           V->red(), V->dS, gate, op);
 }
 
 // prime_multigrid3 / prime_mobile3 with beta = 0 (delta3d_mobile.rs:517, 587): rz of a fresh
@@ -287,9 +325,16 @@ void iteration(fd3_volume* V, int parity) {
   if (V->has_mg) {
     float* din = parity ? V->dir2 : V->dir;
     float* dout = parity ? V->dir : V->dir2;
-    DISPATCH(V, k_dir_apply_dot, V->n, G, (const unsigned short*)V->codes, (const float*)V->z, (const float*)din, dout,
-             V->tmp, V->red(), V->dS);
-    DISPATCH(V, k_update_rn, V->n, V->n, V->p, V->res, (const float*)dout, (const float*)V->tmp, V->red(), V->dS);
+    if (V->blocked()) {
+      LAUNCH_G(V, kz_dir_apply_dot, zblocks(V->nx, V->ny, V->nz), ZT, G, (const unsigned short*)V->codes,
+               (const float*)V->z, (const float*)din, dout, V->tmp, V->red(), V->dS);
+      LAUNCH_G(V, kv_update_rn, update_blocks(V->n), TPB, V->n, V->p, V->res, (const float*)dout,
+               (const float*)V->tmp, V->red(), V->dS);
+    } else {
+      DISPATCH(V, k_dir_apply_dot, V->n, G, (const unsigned short*)V->codes, (const float*)V->z, (const float*)din, dout,
+               V->tmp, V->red(), V->dS);
+      DISPATCH(V, k_update_rn, V->n, V->n, V->p, V->res, (const float*)dout, (const float*)V->tmp, V->red(), V->dS);
+    }
     vcycle(V, 1, FIN_RZ_ITER);
   } else {
     DISPATCH(V, k_apply_dot_c, V->n, G, (const unsigned short*)V->codes, (const float*)V->dir, V->tmp, V->red(), V->dS);
@@ -332,7 +377,7 @@ int build_loop_graph(fd3_volume* V) {
   e = cudaGraphInstantiate(&V->loop_exec, graph, 0);
   cudaGraphDestroy(graph);
   if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate(loop)", __LINE__);
-  V->loop_mode = (V->ord() ? 1 : 0) | (V->has_mg ? 2 : 0);
+  V->loop_mode = (V->ord() ? 1 : 0) | (V->has_mg ? 2 : 0) | (V->blocked() ? 4 : 0);
   V->loop_stream = V->stream;
   return FD3_OK;
 }
@@ -341,7 +386,7 @@ int build_loop_graph(fd3_volume* V) {
 int run_inner(fd3_volume* V, uint32_t it_before) {
   const bool graphs = V->opt.use_graphs && !V->prof;
   if (graphs) {
-    int mode = (V->ord() ? 1 : 0) | (V->has_mg ? 2 : 0);
+    int mode = (V->ord() ? 1 : 0) | (V->has_mg ? 2 : 0) | (V->blocked() ? 4 : 0);
     if (!V->loop_exec || V->loop_mode != mode || V->loop_stream != V->stream) TRY(build_loop_graph(V));
     CK(cudaGraphLaunch(V->loop_exec, V->stream));
     TRY(pull(V));
@@ -574,7 +619,10 @@ int alloc_state(fd3_volume* V) {
   TRY(dalloc(V, &V->sv_p, V->n)); TRY(dalloc(V, &V->sv_eta, V->ncol)); TRY(dalloc(V, &V->sv_rof, V->ncol));
   TRY(dalloc(V, &V->flux_x, (size_t)(V->nx + 1) * V->ny)); TRY(dalloc(V, &V->flux_y, (size_t)V->nx * (V->ny + 1)));
   float* q;
-  TRY(dalloc(V, &q, (size_t)blocks_for(V->n) * 2 + 64)); V->p64 = (double*)q;
+  // one f64 partial per block of the largest reduction launch: linear (one cell per thread),
+  // 2.5-D blocked, or the grid-stride update
+  V->p64_cap = std::max(std::max(blocks_for(V->n), zblocks(V->nx, V->ny, V->nz)), UPDATE_BLOCKS);
+  TRY(dalloc(V, &q, (size_t)V->p64_cap * 2 + 64)); V->p64 = (double*)q;
   TRY(dalloc(V, &V->p32, (size_t)(V->n + CHUNK - 1) / CHUNK + 64));
   TRY(dalloc(V, &q, sizeof(Scalars) / sizeof(float) + 16)); V->dS = (Scalars*)q;
   TRY(dalloc(V, &q, 16)); V->dflag = (int*)q;
@@ -829,7 +877,7 @@ void fd3_destroy(fd3_volume* v) {
 
 int fd3_set_options(fd3_volume* v, const fd3_options* o) {
   if (!v || !o) return FD3_ERR_INVALID_ARGUMENT;
-  if (o->reduction > 1) return FD3_ERR_DOMAIN;
+  if (o->reduction > 1 || o->kernels > 1) return FD3_ERR_DOMAIN;
   v->opt = *o;
   return FD3_OK;
 }
@@ -868,11 +916,24 @@ int fd3_enable_multigrid(fd3_volume* V) {
     TRY(dalloc(V, &L.ow, (size_t)cx * cy * (cz + 1)));
     TRY(dalloc(V, &L.kind, L.n)); TRY(dalloc(V, &L.diag, L.n));
     TRY(dalloc(V, &L.x, L.n)); TRY(dalloc(V, &L.x2, L.n)); TRY(dalloc(V, &L.r, L.n)); TRY(dalloc(V, &L.t, L.n));
+    float* cq;
+    TRY(dalloc(V, &cq, (size_t)(L.n + 1) / 2)); L.code = (unsigned short*)cq;
     V->levels.push_back(L);
     x = cx; y = cy; zz = cz;
   }
   V->tail_first = (int)V->levels.size();
   while (V->tail_first > 0 && V->levels[V->tail_first - 1].n <= TAIL_MAX_CELLS) --V->tail_first;
+  // shared-memory tail when every tail level fits (at most 200 KiB of the 227 KiB per block)
+  V->tail_smem_bytes = 0;
+  if (V->tail_first < (int)V->levels.size() && (int)V->levels.size() - V->tail_first <= MAX_TAIL_LEVELS) {
+    size_t floats = 0;
+    for (size_t l = V->tail_first; l < V->levels.size(); ++l)
+      floats += tail_level_floats(V->levels[l].nx, V->levels[l].ny, V->levels[l].nz);
+    if (floats * sizeof(float) <= 200 * 1024) {
+      V->tail_smem_bytes = floats * sizeof(float);
+      CK(cudaFuncSetAttribute(k_coarse_tail_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)V->tail_smem_bytes));
+    }
+  }
   if (!V->levels.empty()) {
     float* q;
     TRY(dalloc(V, &q, (V->levels.size() * sizeof(Lev) + 3) / 4));

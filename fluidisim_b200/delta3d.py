@@ -48,7 +48,7 @@ class _Report(C.Structure):
 
 class _Options(C.Structure):
     _fields_ = [("reduction", C.c_uint32), ("mg_max_levels", C.c_uint32), ("use_graphs", C.c_uint32),
-                ("reserved", C.c_uint32 * 5)]
+                ("kernels", C.c_uint32), ("reserved", C.c_uint32 * 4)]
 
 
 @dataclass
@@ -191,7 +191,7 @@ class Volume3:
             raise Delta3dError(e, where, self._L.fd3_last_cuda_error().decode() if e >= 100 else "")
 
     # ---- options
-    def set_options(self, reduction=None, mg_max_levels=None, use_graphs=None):
+    def set_options(self, reduction=None, mg_max_levels=None, use_graphs=None, kernels=None):
         o = _Options()
         self._check(self._L.fd3_get_options(self._h, C.byref(o)), "get_options")
         if reduction is not None:
@@ -200,6 +200,8 @@ class Volume3:
             o.mg_max_levels = int(mg_max_levels)
         if use_graphs is not None:
             o.use_graphs = int(use_graphs)
+        if kernels is not None:
+            o.kernels = int(kernels)
         self._check(self._L.fd3_set_options(self._h, C.byref(o)), "set_options")
 
     def set_stream(self, stream_ptr: int):

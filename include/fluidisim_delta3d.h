@@ -75,8 +75,10 @@ typedef struct fd3_options {
   uint32_t reduction;     /* fd3_reduction */
   uint32_t mg_max_levels; /* coarse levels kept by fd3_enable_multigrid; 0 = every level the
                              reference's coarsening rule allows (delta3d_multigrid.rs:73-88) */
-  uint32_t use_graphs;    /* 1 = replay the PCG iteration from a captured CUDA graph */
-  uint32_t reserved[5];
+  uint32_t use_graphs;    /* 1 = run the inner PCG loop as a CUDA graph with a WHILE node */
+  uint32_t kernels;       /* fine-level kernels in f64 mode: 0 = 2.5-D blocked (default), 1 = one cell
+                             per thread (the family the ordered mode always uses) */
+  uint32_t reserved[4];
 } fd3_options;
 
 typedef struct fd3_volume fd3_volume;
