@@ -25,6 +25,7 @@ constexpr unsigned RC_UNIT = 1u << 13;
 __device__ __forceinline__ unsigned face_state(unsigned code, int f) { return (code >> (1 + 2 * f)) & 3u; }
 
 __global__ void k_row_codes(Geo g, unsigned short* __restrict__ codes) {
+  KSTART();
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= g.n) return;
   int i, j, k; cell_ijk(g, c, i, j, k);
@@ -219,6 +220,7 @@ __global__ void __launch_bounds__(TPB) k_dir_apply_dot(Geo g, const unsigned sho
                                                        const float* __restrict__ z, const float* __restrict__ din,
                                                        float* __restrict__ dout, float* __restrict__ q, Red red,
                                                        Scalars* S) {
+  KSTART();
   if (!S->active) return;
   const int mode = S->dir_mode;
   const float beta = S->beta;
@@ -240,6 +242,7 @@ template <int MODE>
 __global__ void __launch_bounds__(TPB) k_update_rn(int n, float* __restrict__ p, float* __restrict__ r,
                                                    const float* __restrict__ d, const float* __restrict__ q, Red red,
                                                    Scalars* S) {
+  KSTART();
   if (!S->active) return;
   const float alpha = S->alpha;
   int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -258,6 +261,7 @@ __global__ void __launch_bounds__(TPB) k_update_rn(int n, float* __restrict__ p,
 __global__ void __launch_bounds__(TPB) k_fine_pre(Geo g, const unsigned short* __restrict__ codes,
                                                   const float* __restrict__ prec, const float* __restrict__ r,
                                                   float* __restrict__ z2, const Scalars* S, int gate) {
+  KSTART();
   if (gate && !S->active) return;
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= g.n) return;
@@ -278,6 +282,7 @@ __global__ void __launch_bounds__(TPB) k_fine_pre(Geo g, const unsigned short* _
 __global__ void __launch_bounds__(TPB) k_fine_restrict_c(Geo g, const unsigned short* __restrict__ codes,
                                                          const float* __restrict__ r, const float* __restrict__ z,
                                                          Lev L, const Scalars* S, int gate) {
+  KSTART();
   if (gate && !S->active) return;
   int qi = blockIdx.x * blockDim.x + threadIdx.x;
   if (qi >= L.n) return;
@@ -301,6 +306,7 @@ __global__ void __launch_bounds__(TPB) k_fine_post1(Geo g, const unsigned short*
                                                     const float* __restrict__ prec, const float* __restrict__ r,
                                                     const float* __restrict__ zin, Lev L, int prolong,
                                                     float* __restrict__ zout, const Scalars* S, int gate) {
+  KSTART();
   if (gate && !S->active) return;
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= g.n) return;
@@ -326,6 +332,7 @@ __global__ void __launch_bounds__(TPB) k_fine_post2_rz(Geo g, const unsigned sho
                                                        const float* __restrict__ prec, const float* __restrict__ r,
                                                        const float* __restrict__ zin, float* __restrict__ zout,
                                                        Red red, Scalars* S, int gate, int op) {
+  KSTART();
   if (gate && !S->active) return;
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   float rc = 0.f, zc = 0.f;
@@ -350,6 +357,7 @@ template <int MODE>
 __global__ void __launch_bounds__(TPB) k_apply_dot_c(Geo g, const unsigned short* __restrict__ codes,
                                                      const float* __restrict__ d, float* __restrict__ q, Red red,
                                                      Scalars* S) {
+  KSTART();
   if (!S->active) return;
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   float dc = 0.f, qc = 0.f;
@@ -365,6 +373,7 @@ __global__ void __launch_bounds__(TPB) k_apply_dot_c(Geo g, const unsigned short
 template <int MODE>
 __global__ void __launch_bounds__(TPB) k_dot_prec_fin(int n, const float* __restrict__ r, const float* __restrict__ prec,
                                                       Red red, Scalars* S, int gate, int op) {
+  KSTART();
   if (gate && !S->active) return;
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   float x = 0.f, m = 0.f;
@@ -402,6 +411,7 @@ __device__ __forceinline__ float level_row_f(const Lev& L, int i, int j, int k, 
 // coarsen3: bit 0 active (kind > 0); per face 0 nothing, 1 active neighbour (a (pc - p_m)),
 // 2 Dirichlet (an air neighbour or the top of the domain: 2 a pc); bit 13 every live aperture is 1.
 __global__ void k_level_codes(Lev L) {
+  KSTART();
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= L.n) return;
   unsigned code = 0;
@@ -474,6 +484,7 @@ __device__ __forceinline__ float level_x1(const Lev& L, int n) {
 
 // The two pre-sweeps of a coarse level from x = 0, written to L.x (smooth3 twice after fill(0)).
 __global__ void __launch_bounds__(TPB) k_level_pre(Lev L, const Scalars* S, int gate) {
+  KSTART();
   if (gate && !S->active) return;
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= L.n) return;
@@ -489,6 +500,7 @@ __global__ void __launch_bounds__(TPB) k_level_pre(Lev L, const Scalars* S, int 
 
 // t = r - L x on every cell of a coarse level (0 on inactive rows), the restriction's operand.
 __global__ void __launch_bounds__(TPB) k_level_resid(Lev L, const Scalars* S, int gate) {
+  KSTART();
   if (gate && !S->active) return;
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= L.n) return;
@@ -503,6 +515,7 @@ __global__ void __launch_bounds__(TPB) k_level_resid(Lev L, const Scalars* S, in
 
 // C.r = mean of the 8 children of F.t, in the reference's CHILDREN order (restrict3).
 __global__ void __launch_bounds__(TPB) k_level_sum8(Lev F, Lev C, const Scalars* S, int gate) {
+  KSTART();
   if (gate && !S->active) return;
   int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= C.n) return;
@@ -518,6 +531,7 @@ __global__ void __launch_bounds__(TPB) k_level_sum8(Lev F, Lev C, const Scalars*
 
 // Prolongation from C (x += parent) fused with the first post-sweep, L.x -> L.x2.
 __global__ void __launch_bounds__(TPB) k_level_post1(Lev L, Lev C, const Scalars* S, int gate) {
+  KSTART();
   if (gate && !S->active) return;
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= L.n) return;
@@ -536,6 +550,7 @@ __global__ void __launch_bounds__(TPB) k_level_post1(Lev L, Lev C, const Scalars
 
 // The second post-sweep, L.x2 -> L.x.
 __global__ void __launch_bounds__(TPB) k_level_post2(Lev L, const Scalars* S, int gate) {
+  KSTART();
   if (gate && !S->active) return;
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= L.n) return;
@@ -551,6 +566,7 @@ __global__ void __launch_bounds__(TPB) k_level_post2(Lev L, const Scalars* S, in
 // One damped Jacobi sweep from codes (a large coarsest level's 8 sweeps); zero_in: from x = 0.
 __global__ void __launch_bounds__(TPB) k_level_sweep_c(Lev L, const float* __restrict__ xin, float* __restrict__ xout,
                                                        int zero_in, const Scalars* S, int gate) {
+  KSTART();
   if (gate && !S->active) return;
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= L.n) return;
@@ -623,6 +639,7 @@ __device__ __forceinline__ void tail_run(const Lev* Ls, int first, int last) {
 // The levels in global memory (fallback when they do not fit in shared memory).
 __global__ void __launch_bounds__(TAIL_THREADS) k_coarse_tail(const Lev* __restrict__ T, int first, int last,
                                                               const Scalars* S, int gate) {
+  KSTART();
   if (gate && !S->active) return;
   tail_run(T, first, last);
 }
@@ -641,6 +658,7 @@ __host__ __device__ inline int tail_level_floats(int nx, int ny, int nz) {
 constexpr int MAX_TAIL_LEVELS = 12;
 __global__ void __launch_bounds__(TAIL_THREADS) k_coarse_tail_smem(const Lev* __restrict__ T, int first, int last,
                                                                    const Scalars* S, int gate) {
+  KSTART();
   if (gate && !S->active) return;
   extern __shared__ float4 tail_smem4[];
   float* sm = reinterpret_cast<float*>(tail_smem4);
@@ -679,11 +697,157 @@ __global__ void __launch_bounds__(TAIL_THREADS) k_coarse_tail_smem(const Lev* __
   for (int q = threadIdx.x; q < G.n; q += blockDim.x) G.x[q] = M.x[q];
 }
 
+// The coarse tail with one cell per thread.  Every tail level has at most TAIL_REG_THREADS cells;
+// thread c owns cell c of the level being worked on and keeps its row (code, apertures, diagonal,
+// right-hand side, x) in registers, so a sweep is six shared-memory reads, the row, one write and
+// one barrier.  The phases and their arithmetic are those of coarse_cycle3
+// (delta3d_multigrid.rs:303-332): 2 pre-sweeps, residual, 8-child mean, ..., 8 sweeps on the
+// coarsest level, then prolongation and 2 post-sweeps per level on the way up.
+constexpr int TAIL_REG_THREADS = 512;
+constexpr int TAIL_REG_LEVELS = 5;  // 40 KiB of static shared memory
+
+struct TailRow {
+  unsigned code;
+  float a[6];
+  int m[6];
+  float diag, r;
+  bool own;
+};
+
+__device__ __forceinline__ TailRow tail_row(const Lev& L, int c, float r) {
+  TailRow w;
+  w.own = c < L.n;
+  w.code = 0;
+  w.diag = 0.f;
+  w.r = r;
+#pragma unroll
+  for (int f = 0; f < 6; ++f) { w.a[f] = 0.f; w.m[f] = 0; }
+  if (!w.own) return w;
+  w.code = L.code[c];
+  w.diag = L.diag[c];
+  const int i = c % L.nx, t = c / L.nx, j = t % L.ny, k = t / L.ny, nxny = L.nx * L.ny;
+  const bool unit = w.code & RC_UNIT;
+  const int fi[6] = {(k * L.ny + j) * (L.nx + 1) + i, (k * L.ny + j) * (L.nx + 1) + i + 1,
+                     (k * (L.ny + 1) + j) * L.nx + i, (k * (L.ny + 1) + j + 1) * L.nx + i,
+                     (k * L.ny + j) * L.nx + i, ((k + 1) * L.ny + j) * L.nx + i};
+  const int mm[6] = {c - 1, c + 1, c - L.nx, c + L.nx, c - nxny, c + nxny};
+#pragma unroll
+  for (int f = 0; f < 6; ++f) {
+    const unsigned st = face_state(w.code, f);
+    if (st) {
+      const float* ap = f < 2 ? L.ou : (f < 4 ? L.ov : L.ow);
+      w.a[f] = unit ? 1.f : ap[fi[f]];
+      w.m[f] = st == 1 ? mm[f] : c;
+    } else {
+      w.m[f] = c;
+    }
+  }
+  return w;
+}
+
+// row_sums at the owned cell, the neighbours' values read from X (shared memory).
+__device__ __forceinline__ float tail_rowsum(const TailRow& w, float pc, const float* X, float inv) {
+  float acc = 0.f;
+#pragma unroll
+  for (int f = 0; f < 6; ++f) {
+    const unsigned st = face_state(w.code, f);
+    if (st == 1) acc += w.a[f] * (pc - X[w.m[f]]);
+    else if (st == 2) acc += 2.f * w.a[f] * pc;
+  }
+  return acc * inv;
+}
+
+__global__ void __launch_bounds__(TAIL_REG_THREADS) k_coarse_tail_reg(const Lev* __restrict__ T, int first, int last,
+                                                                     const Scalars* S, int gate) {
+  KSTART();
+  if (gate && !S->active) return;
+  // per level: XA, XB (sweep ping-pong), XF (final x of the level), R (right-hand side), TT (residual)
+  __shared__ float XA[TAIL_REG_LEVELS][TAIL_REG_THREADS];
+  __shared__ float XB[TAIL_REG_LEVELS][TAIL_REG_THREADS];
+  __shared__ float XF[TAIL_REG_LEVELS][TAIL_REG_THREADS];
+  __shared__ float R[TAIL_REG_LEVELS][TAIL_REG_THREADS];
+  const int c = threadIdx.x;
+  const int nl = last - first + 1;
+  {
+    const Lev L0 = T[first];
+    if (c < L0.n) R[0][c] = L0.r[c];
+  }
+  __syncthreads();
+  // descent
+  for (int l = 0; l < nl; ++l) {
+    const Lev L = T[first + l];
+    const TailRow w = tail_row(L, c, c < L.n ? R[l][c] : 0.f);
+    const int sweeps = l == nl - 1 ? 8 : 2;  // COARSE_SWEEPS_3D, PRE_SWEEPS_3D
+    float x = 0.f;
+    for (int s = 0; s < sweeps; ++s) {
+      float* out = (s & 1) ? XB[l] : XA[l];
+      const float* in = (s & 1) ? XA[l] : XB[l];
+      float xn = x;
+      if (w.own) {
+        if (s == 0) xn = w.diag > 0.f ? 0.f + OMEGA * (w.r - 0.f) / w.diag : 0.f;
+        else if (w.diag > 0.f) xn = x + OMEGA * (w.r - tail_rowsum(w, x, in, L.inv)) / w.diag;
+        out[c] = xn;
+      }
+      __syncthreads();
+      x = xn;
+    }
+    if (w.own) XF[l][c] = x;
+    if (l < nl - 1) {
+      // residual t = r - L x (0 on inactive rows), then the 8-child mean into the next level
+      const float* xs = ((sweeps - 1) & 1) ? XB[l] : XA[l];
+      float tv = 0.f;
+      if (w.own) tv = w.r - ((w.code & RC_WET) ? tail_rowsum(w, x, xs, L.inv) : 0.f);
+      __syncthreads();
+      if (w.own) XA[l][c] = tv;
+      __syncthreads();
+      const Lev C = T[first + l + 1];
+      if (c < C.n) {
+        int ci = c % C.nx, t = c / C.nx, cj = t % C.ny, ck = t / C.ny;
+        float sum = 0.f;
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+          int i = 2 * ci + (e & 1), j = 2 * cj + ((e >> 1) & 1), k = 2 * ck + (e >> 2);
+          sum += XA[l][(k * L.ny + j) * L.nx + i];
+        }
+        R[l + 1][c] = 0.125f * sum;
+      }
+      __syncthreads();
+    }
+  }
+  // ascent
+  for (int l = nl - 2; l >= 0; --l) {
+    const Lev L = T[first + l];
+    const Lev C = T[first + l + 1];
+    const TailRow w = tail_row(L, c, c < L.n ? R[l][c] : 0.f);
+    float x = 0.f;
+    if (w.own) {
+      int i = c % L.nx, t = c / L.nx, j = t % L.ny, k = t / L.ny;
+      x = XF[l][c] + XF[l + 1][((k >> 1) * C.ny + (j >> 1)) * C.nx + (i >> 1)];
+      XB[l][c] = x;
+    }
+    __syncthreads();
+    for (int s = 0; s < 2; ++s) {  // POST_SWEEPS_3D
+      float* out = (s & 1) ? XB[l] : XA[l];
+      const float* in = (s & 1) ? XA[l] : XB[l];
+      float xn = x;
+      if (w.own && w.diag > 0.f) xn = x + OMEGA * (w.r - tail_rowsum(w, x, in, L.inv)) / w.diag;
+      if (w.own) out[c] = xn;
+      __syncthreads();
+      x = xn;
+    }
+    if (w.own) XF[l][c] = x;
+    __syncthreads();
+  }
+  const Lev L0 = T[first];
+  if (c < L0.n) L0.x[c] = XF[0][c];
+}
+
 // ------------------------------------------------------------------------------------------------
 // The WHILE node of the inner loop repeats its body (two iterations) while this sets 1.  Each
 // iteration that runs advances S->it, so the loop ends within max_iters iterations; as a guard
 // independent of that logic, the body never runs more than max_iters + 2 times (status 100).
 __global__ void k_loop_cond(cudaGraphConditionalHandle handle, Scalars* S) {
+  KSTART();
   unsigned runs = ++S->body_runs;
   bool go = S->active != 0;
   if (go && runs > S->max_iters + 2u) { S->active = 0; S->status = 100; go = false; }
@@ -697,6 +861,7 @@ __global__ void k_loop_cond(cudaGraphConditionalHandle handle, Scalars* S) {
 template <int MODE>
 __global__ void __launch_bounds__(TPB) k_rhs_b2(Geo g, float scale, float* __restrict__ rhs, float* __restrict__ prec,
                                                 Red red, Scalars* S, int reduce) {
+  KSTART();
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   float b = 0.f;
   if (c < g.n) {
@@ -728,6 +893,7 @@ template <int MODE>
 __global__ void __launch_bounds__(TPB) k_residual_c(Geo g, const unsigned short* __restrict__ codes,
                                                     const float* __restrict__ p, const float* __restrict__ rhs,
                                                     float* __restrict__ res, Red red, Scalars* S, int op) {
+  KSTART();
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   float r = 0.f;
   if (c < g.n) {
@@ -743,6 +909,7 @@ __global__ void __launch_bounds__(TPB) k_residual_c(Geo g, const unsigned short*
 
 // Loop start: the host's view of the loop state; a pending NotFinite keeps the loop closed.
 __global__ void k_loop_start(Scalars* S, double rr, double tolb2, double phys, unsigned it, unsigned max_iters) {
+  KSTART();
   S->rr = rr;
   S->tolb2 = tolb2;
   S->phys = phys;

@@ -26,6 +26,17 @@ constexpr float OMEGA = 6.f / 7.f;                // delta3d_multigrid.rs:28
 
 enum Mode { RED_F64 = 0, RED_ORD = 1 };
 
+// Programmatic dependent launch (sm_90+): every kernel of the library is launched so that its CTAs
+// may be scheduled while the previous kernel on the stream is still running.  KSTART, the first
+// statement of every kernel, waits until that previous grid has completed and its memory is
+// visible (griddepcontrol.wait; a no-op when launched without the attribute), then lets the next
+// kernel start scheduling (griddepcontrol.launch_dependents).  Nothing is read before the wait.
+#define KSTART()                                              \
+  do {                                                        \
+    asm volatile("griddepcontrol.wait;" ::: "memory");        \
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); \
+  } while (0)
+
 // Fine-level geometry, passed by value to every fine kernel.
 struct Geo {
   int nx, ny, nz, n;
@@ -222,6 +233,7 @@ __device__ __forceinline__ void flag_nonzero(bool nz, Scalars* S) {
 // divergence / divergence_cut (delta3d.rs:747-763, 806-855), a solid at rest.
 __global__ void k_divergence(Geo g, const float* __restrict__ u, const float* __restrict__ v,
                              const float* __restrict__ w, float* __restrict__ out) {
+  KSTART();
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= g.n) return;
   int i, j, k; cell_ijk(g, c, i, j, k);
@@ -244,6 +256,7 @@ __global__ void k_divergence(Geo g, const float* __restrict__ u, const float* __
 
 // p = 0 on dry cells (delta3d_mobile.rs:485-494).
 __global__ void k_zero_dry(Geo g, float* __restrict__ p) {
+  KSTART();
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= g.n) return;
   int i, j, k; cell_ijk(g, c, i, j, k);
@@ -252,6 +265,7 @@ __global__ void k_zero_dry(Geo g, float* __restrict__ p) {
 
 // out = A x (apply_mobile3).
 __global__ void k_apply(Geo g, const float* __restrict__ x, float* __restrict__ out) {
+  KSTART();
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= g.n) return;
   int i, j, k; cell_ijk(g, c, i, j, k);
@@ -262,6 +276,7 @@ __global__ void k_apply(Geo g, const float* __restrict__ x, float* __restrict__ 
 // the `beta == 0` branch (dir = z).
 __global__ void k_jacobi_dir(int n, const float* __restrict__ prec, const float* __restrict__ r, float* __restrict__ d,
                              const Scalars* S, int gate, int use_beta) {
+  KSTART();
   if (gate && !S->active) return;
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= n) return;
@@ -300,6 +315,7 @@ __device__ __forceinline__ float level_row(const Lev& L, int i, int j, int k, in
 
 // The diagonal: row_sums with p absent (delta3d_multigrid.rs:205, 236-241).
 __global__ void k_level_diag(Lev L) {
+  KSTART();
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= L.n) return;
   int i = c % L.nx, t = c / L.nx, j = t % L.ny, k = t / L.ny;
@@ -329,6 +345,7 @@ __global__ void k_level_diag(Lev L) {
 // is the first sweep after `x.fill(0)`: L 0 = +0 exactly, so xout = 0 + w (r - 0) / diag.
 __global__ void k_level_sweep(Lev L, const float* __restrict__ xin, float* __restrict__ xout, int zero_in,
                               const Scalars* S, int gate) {
+  KSTART();
   if (gate && !S->active) return;
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= L.n) return;
@@ -348,6 +365,7 @@ __global__ void k_level_sweep(Lev L, const float* __restrict__ xin, float* __res
 
 // Coarse r of level C = mean over 8 children of (r - L x) on level F.
 __global__ void k_level_restrict(Lev F, Lev C, const Scalars* S, int gate) {
+  KSTART();
   if (gate && !S->active) return;
   int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= C.n) return;
@@ -367,6 +385,7 @@ __global__ void k_level_restrict(Lev F, Lev C, const Scalars* S, int gate) {
 // coarsen3 (delta3d_multigrid.rs:141-206) and fine_kind3 (:357-367)
 
 __global__ void k_coarsen_kind_fine(Geo g, Lev C) {
+  KSTART();
   int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= C.n) return;
   int ci = q % C.nx, t = q / C.nx, cj = t % C.ny, ck = t / C.ny;
@@ -383,6 +402,7 @@ __global__ void k_coarsen_kind_fine(Geo g, Lev C) {
 }
 
 __global__ void k_coarsen_kind_level(Lev F, Lev C) {
+  KSTART();
   int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= C.n) return;
   int ci = q % C.nx, t = q / C.nx, cj = t % C.ny, ck = t / C.ny;
@@ -401,6 +421,7 @@ __global__ void k_coarsen_kind_level(Lev F, Lev C) {
 // (nullptr: a flat fine level, every aperture 1).  fnx/fny are the fine dimensions.
 __global__ void k_coarsen_open(int fnx, int fny, const float* __restrict__ fou, const float* __restrict__ fov,
                                const float* __restrict__ fow, Lev C) {
+  KSTART();
   int cx = C.nx, cy = C.ny, cz = C.nz;
   int nu = (cx + 1) * cy * cz, nv = cx * (cy + 1) * cz, nw = cx * cy * (cz + 1);
   int q = blockIdx.x * blockDim.x + threadIdx.x;
@@ -447,6 +468,7 @@ __global__ void k_coarsen_open(int fnx, int fny, const float* __restrict__ fou, 
 // (axis 1); untouched faces copy the prediction.
 __global__ void k_correct_uv(Geo g, float k1, const float* __restrict__ p, const float* __restrict__ us,
                              const float* __restrict__ vs, float* __restrict__ u, float* __restrict__ v) {
+  KSTART();
   int nu = (g.nx + 1) * g.ny * g.nz, nv = g.nx * (g.ny + 1) * g.nz;
   int q = blockIdx.x * blockDim.x + threadIdx.x;
   int axis, f, i, j, k;
@@ -474,6 +496,7 @@ __global__ void k_correct_uv(Geo g, float k1, const float* __restrict__ p, const
 
 __global__ void k_correct_w(Geo g, float k1, const float* __restrict__ p, const float* __restrict__ ws,
                             float* __restrict__ w) {
+  KSTART();
   int nw = g.nx * g.ny * (g.nz + 1);
   int f = blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= nw) return;
@@ -497,6 +520,7 @@ __device__ __forceinline__ void atomic_fmax_nonneg(float* addr, float v) {
 // without a surface ghost (plain).  S->fmax[0] = all, [1] = plain.
 __global__ void k_div_metric(Geo g, const float* __restrict__ u, const float* __restrict__ v,
                              const float* __restrict__ w, Scalars* S) {
+  KSTART();
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   float all = 0.f, plain = 0.f;
   if (c < g.n) {
@@ -537,6 +561,7 @@ __global__ void k_div_metric(Geo g, const float* __restrict__ u, const float* __
 
 // max |x| over an array into S->fmax[slot].
 __global__ void k_maxabs(int n, const float* __restrict__ x, Scalars* S, int slot) {
+  KSTART();
   float m = 0.f;
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) m = fmaxf(m, fabsf(x[q]));
 #pragma unroll
@@ -547,6 +572,7 @@ __global__ void k_maxabs(int n, const float* __restrict__ x, Scalars* S, int slo
 // backward_error_mobile3 (delta3d_mobile.rs:243-271) into S->fmax[3].
 __global__ void k_backward_error(Geo g, const float* __restrict__ p, const float* __restrict__ rhs,
                                  const float* __restrict__ res, Scalars* S) {
+  KSTART();
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   float worst = 0.f;
   if (c < g.n) {
@@ -579,6 +605,7 @@ __device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
   return z ^ (z >> 31);
 }
 __global__ void k_hash(int n, const float* __restrict__ p, Scalars* S) {
+  KSTART();
   unsigned long long h = 0;
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x)
     h += mix64(((unsigned long long)(unsigned)__float_as_int(p[q]) << 32 | (unsigned)q) + 0x9E3779B97F4A7C15ull);
@@ -613,6 +640,7 @@ __device__ __forceinline__ bool loop_continues(const Scalars* S, double rn, unsi
 __global__ void k_advect(Geo g, float dt, const float* __restrict__ u, const float* __restrict__ v,
                          const float* __restrict__ w, float* __restrict__ us, float* __restrict__ vs,
                          float* __restrict__ ws) {
+  KSTART();
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const int nu = (nx + 1) * ny * nz, nv = nx * (ny + 1) * nz, nw = nx * ny * (nz + 1);
   const float h = 0.5f / g.dx;
@@ -669,6 +697,7 @@ __global__ void k_advect(Geo g, float dt, const float* __restrict__ u, const flo
 // extrapolate_mobile3 (delta3d_mobile.rs:345-394): one thread per column and axis walks up the
 // column and copies the last solved face into the unsolved open faces above it.
 __global__ void k_extrapolate(Geo g, float* __restrict__ u, float* __restrict__ v, float* __restrict__ w) {
+  KSTART();
   int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= 3 * g.nx * g.ny) return;
   const int axis = q / (g.nx * g.ny);
@@ -704,6 +733,7 @@ __global__ void k_extrapolate(Geo g, float* __restrict__ u, float* __restrict__ 
 // lateral face, read from eta^n.  Boundary entries stay zero (the walls).
 __global__ void k_transport_flux(Geo g, const float* __restrict__ u, const float* __restrict__ v,
                                  float* __restrict__ flux_x, float* __restrict__ flux_y) {
+  KSTART();
   const int nfx = (g.nx + 1) * g.ny, nfy = g.nx * (g.ny + 1);
   int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= nfx + nfy) return;
@@ -732,6 +762,7 @@ __global__ void k_transport_flux(Geo g, const float* __restrict__ u, const float
 // transport_mobile3, heights: compensated f32 sum per column (delta3d_mobile.rs:770-781).
 __global__ void k_transport_eta(Geo g, float transport, const float* __restrict__ flux_x,
                                 const float* __restrict__ flux_y, float* __restrict__ eta, float* __restrict__ rof) {
+  KSTART();
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= g.nx * g.ny) return;
   int i = c % g.nx, j = c / g.nx;
@@ -745,6 +776,7 @@ __global__ void k_transport_eta(Geo g, float transport, const float* __restrict_
 
 // mobile_in_bounds (delta3d_mobile.rs:801-813): sets *flag when a column leaves its bounds.
 __global__ void k_in_bounds(Geo g, const float* __restrict__ floor, int* flag) {
+  KSTART();
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   bool bad = false;
   if (c < g.nx * g.ny) {

@@ -85,6 +85,7 @@ struct fd3_volume {
   Lev* dlev = nullptr;   // the level table in device memory (for the single-CTA coarse tail)
   int tail_first = 0;    // first level small enough for the single-CTA tail
   size_t tail_smem_bytes = 0;  // dynamic shared memory of the shared-memory tail (0: global tail)
+  bool tail_reg = false;       // every tail level fits one cell per thread of k_coarse_tail_reg
   // reductions and scalars
   double* p64 = nullptr;
   int p64_cap = 0;  // f64 partial slots
@@ -163,11 +164,27 @@ cudaEvent_t next_event(fd3_volume* V) {
 
 // Every kernel launch of the library goes through here: grid x block on the handle's stream,
 // counted, and bracketed by events when profiling is on.
+// Launch with the programmatic-stream-serialization attribute (see KSTART in fd3_kernels.cuh).
+template <class... P, class... A>
+void launch_pdl(fd3_volume* V, int grid, int block, size_t smem, void (*kernel)(P...), A... args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = V->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = V->opt.no_overlap ? 0 : 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, kernel, ((P)args)...);
+}
+
 template <class K, class... A>
 void launch_grid(fd3_volume* V, const char* name, int grid, int block, K kernel, A... args) {
   cudaEvent_t a = nullptr, b = nullptr;
   if (V->prof) { a = next_event(V); cudaEventRecord(a, V->stream); }
-  kernel<<<grid, block, 0, V->stream>>>(args...);
+  launch_pdl(V, grid, block, 0, kernel, args...);
   if (V->prof) { b = next_event(V); cudaEventRecord(b, V->stream); V->pending.push_back({name, a, b}); }
   V->launches++;
 }
@@ -178,7 +195,7 @@ template <class K, class... A>
 void launch_grid_smem(fd3_volume* V, const char* name, int grid, int block, size_t smem, K kernel, A... args) {
   cudaEvent_t a = nullptr, b = nullptr;
   if (V->prof) { a = next_event(V); cudaEventRecord(a, V->stream); }
-  kernel<<<grid, block, smem, V->stream>>>(args...);
+  launch_pdl(V, grid, block, smem, kernel, args...);
   if (V->prof) { b = next_event(V); cudaEventRecord(b, V->stream); V->pending.push_back({name, a, b}); }
   V->launches++;
 }
@@ -261,7 +278,9 @@ void coarse_cycle(fd3_volume* V, int gate) {
     }
   }
   if (first_tail <= last) {
-    if (V->tail_smem_bytes > 0)
+    if (V->tail_reg)
+      LAUNCH_G(V, k_coarse_tail_reg, 1, TAIL_REG_THREADS, (const Lev*)V->dlev, first_tail, last, S, gate);
+    else if (V->tail_smem_bytes > 0)
       launch_grid_smem(V, "k_coarse_tail_smem", 1, TAIL_THREADS, V->tail_smem_bytes, k_coarse_tail_smem,
                        (const Lev*)V->dlev, first_tail, last, S, gate);
     else
@@ -283,15 +302,26 @@ void vcycle(fd3_volume* V, int gate, int op) {
   const unsigned short* codes = V->codes;
   if (V->blocked()) {  // 2.5-D blocked kernels (f64 reductions)
     const int zb = zblocks(V->nx, V->ny, V->nz);
-    LAUNCH_G(V, kz_fine_pre, zb, ZT, G, codes, (const float*)V->prec, (const float*)V->res, V->z, S, gate);
+    const bool full = zfull(V->nx, V->ny, V->nz);
+    if (full) LAUNCH_G(V, kz_fine_pre<true>, zb, ZT, G, codes, (const float*)V->prec, (const float*)V->res, V->z, S, gate);
+    else LAUNCH_G(V, kz_fine_pre<false>, zb, ZT, G, codes, (const float*)V->prec, (const float*)V->res, V->z, S, gate);
     if (levels) {
-      LAUNCH_G(V, kz_fine_restrict, zb, ZT, G, codes, (const float*)V->res, (const float*)V->z, L0, S, gate);
+      if (full) LAUNCH_G(V, kz_fine_restrict<true>, zb, ZT, G, codes, (const float*)V->res, (const float*)V->z, L0, S, gate);
+      else LAUNCH_G(V, kz_fine_restrict<false>, zb, ZT, G, codes, (const float*)V->res, (const float*)V->z, L0, S, gate);
       coarse_cycle(V, gate);
     }
-    LAUNCH_G(V, kz_fine_post1, zb, ZT, G, codes, (const float*)V->prec, (const float*)V->res, (const float*)V->z, L0,
-             levels ? 1 : 0, V->z2, S, gate);
-    LAUNCH_G(V, kz_fine_post2_rz, zb, ZT, G, codes, (const float*)V->prec, (const float*)V->res, (const float*)V->z2,
-             V->z, V->red(), V->dS, gate, op);
+    if (full)
+      LAUNCH_G(V, kz_fine_post1<true>, zb, ZT, G, codes, (const float*)V->prec, (const float*)V->res, (const float*)V->z,
+               L0, levels ? 1 : 0, V->z2, S, gate);
+    else
+      LAUNCH_G(V, kz_fine_post1<false>, zb, ZT, G, codes, (const float*)V->prec, (const float*)V->res, (const float*)V->z,
+               L0, levels ? 1 : 0, V->z2, S, gate);
+    if (full)
+      LAUNCH_G(V, kz_fine_post2_rz<true>, zb, ZT, G, codes, (const float*)V->prec, (const float*)V->res,
+               (const float*)V->z2, V->z, V->red(), V->dS, gate, op);
+    else
+      LAUNCH_G(V, kz_fine_post2_rz<false>, zb, ZT, G, codes, (const float*)V->prec, (const float*)V->res,
+               (const float*)V->z2, V->z, V->red(), V->dS, gate, op);
     return;
   }
   LAUNCH(V, k_fine_pre, V->n, G, codes, (const float*)V->prec, (const float*)V->res, V->z, S, gate);
@@ -326,8 +356,12 @@ void iteration(fd3_volume* V, int parity) {
     float* din = parity ? V->dir2 : V->dir;
     float* dout = parity ? V->dir : V->dir2;
     if (V->blocked()) {
-      LAUNCH_G(V, kz_dir_apply_dot, zblocks(V->nx, V->ny, V->nz), ZT, G, (const unsigned short*)V->codes,
-               (const float*)V->z, (const float*)din, dout, V->tmp, V->red(), V->dS);
+      if (zfull(V->nx, V->ny, V->nz))
+        LAUNCH_G(V, kz_dir_apply_dot<true>, zblocks(V->nx, V->ny, V->nz), ZT, G, (const unsigned short*)V->codes,
+                 (const float*)V->z, (const float*)din, dout, V->tmp, V->red(), V->dS);
+      else
+        LAUNCH_G(V, kz_dir_apply_dot<false>, zblocks(V->nx, V->ny, V->nz), ZT, G, (const unsigned short*)V->codes,
+                 (const float*)V->z, (const float*)din, dout, V->tmp, V->red(), V->dS);
       LAUNCH_G(V, kv_update_rn, update_blocks(V->n), TPB, V->n, V->p, V->res, (const float*)dout,
                (const float*)V->tmp, V->red(), V->dS);
     } else {
@@ -377,7 +411,7 @@ int build_loop_graph(fd3_volume* V) {
   e = cudaGraphInstantiate(&V->loop_exec, graph, 0);
   cudaGraphDestroy(graph);
   if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate(loop)", __LINE__);
-  V->loop_mode = (V->ord() ? 1 : 0) | (V->has_mg ? 2 : 0) | (V->blocked() ? 4 : 0);
+  V->loop_mode = (V->ord() ? 1 : 0) | (V->has_mg ? 2 : 0) | (V->blocked() ? 4 : 0) | (V->opt.no_overlap ? 8 : 0);
   V->loop_stream = V->stream;
   return FD3_OK;
 }
@@ -386,7 +420,7 @@ int build_loop_graph(fd3_volume* V) {
 int run_inner(fd3_volume* V, uint32_t it_before) {
   const bool graphs = V->opt.use_graphs && !V->prof;
   if (graphs) {
-    int mode = (V->ord() ? 1 : 0) | (V->has_mg ? 2 : 0) | (V->blocked() ? 4 : 0);
+    int mode = (V->ord() ? 1 : 0) | (V->has_mg ? 2 : 0) | (V->blocked() ? 4 : 0) | (V->opt.no_overlap ? 8 : 0);
     if (!V->loop_exec || V->loop_mode != mode || V->loop_stream != V->stream) TRY(build_loop_graph(V));
     CK(cudaGraphLaunch(V->loop_exec, V->stream));
     TRY(pull(V));
@@ -877,7 +911,7 @@ void fd3_destroy(fd3_volume* v) {
 
 int fd3_set_options(fd3_volume* v, const fd3_options* o) {
   if (!v || !o) return FD3_ERR_INVALID_ARGUMENT;
-  if (o->reduction > 1 || o->kernels > 1) return FD3_ERR_DOMAIN;
+  if (o->reduction > 1 || o->kernels > 1 || o->no_overlap > 1) return FD3_ERR_DOMAIN;
   v->opt = *o;
   return FD3_OK;
 }
@@ -923,6 +957,8 @@ int fd3_enable_multigrid(fd3_volume* V) {
   }
   V->tail_first = (int)V->levels.size();
   while (V->tail_first > 0 && V->levels[V->tail_first - 1].n <= TAIL_MAX_CELLS) --V->tail_first;
+  V->tail_reg = (int)V->levels.size() - V->tail_first <= TAIL_REG_LEVELS;
+  for (size_t l = V->tail_first; l < V->levels.size(); ++l) V->tail_reg = V->tail_reg && V->levels[l].n <= TAIL_REG_THREADS;
   // shared-memory tail when every tail level fits (at most 200 KiB of the 227 KiB per block)
   V->tail_smem_bytes = 0;
   if (V->tail_first < (int)V->levels.size() && (int)V->levels.size() - V->tail_first <= MAX_TAIL_LEVELS) {

@@ -13,7 +13,13 @@
 
 namespace fd3 {
 
-constexpr int ZX = 32, ZY = 8, ZK = 8, ZT = ZX * ZY;
+#ifndef FD3_ZK
+#define FD3_ZK 8
+#endif
+#ifndef FD3_ZMINB
+#define FD3_ZMINB 4
+#endif
+constexpr int ZX = 32, ZY = 8, ZK = FD3_ZK, ZT = ZX * ZY;
 
 // apply_code with the six neighbour values given (only fluid-neighbour faces read them).
 __device__ __forceinline__ float apply_code_nb(const Geo& g, unsigned code, int i, int j, int k, float pc,
@@ -154,6 +160,80 @@ __device__ __forceinline__ void zmarch(const Geo& g, const unsigned short* __res
   }
 }
 
+// The same march for full tiles (nx % ZX == 0, ny % ZY == 0, nz % ZK == 0): every thread owns a
+// cell in every layer, so the per-cell bounds tests go, and the ZK-layer loop is unrolled so the
+// register window rotates for free.  Halo threads on the domain boundary still read nothing.
+template <class L, class E, class A = NoAfter>
+__device__ __forceinline__ void zmarch_full(const Geo& g, const unsigned short* __restrict__ codes, const L& ld, E epi,
+                                            A after = A()) {
+  typedef typename L::Raw Raw;
+  typedef typename L::Halo Halo;
+  __shared__ float s[ZY + 2][ZX + 2];
+  const int tx = threadIdx.x % ZX, ty = threadIdx.x / ZX;
+  const ZTile t = ztile(g);
+  const int nxny = g.nx * g.ny;
+  const int base = t.j * g.nx + t.i;
+  const int hxi = tx == 0 ? t.i - 1 : (tx == ZX - 1 ? t.i + 1 : -1);
+  const int hyj = ty == 0 ? t.j - 1 : (ty == ZY - 1 ? t.j + 1 : -1);
+  const bool hx_on = hxi >= 0 && hxi < g.nx;
+  const bool hy_on = hyj >= 0 && hyj < g.ny;
+  const int hx_off = hxi - t.i;          // -1 or +1 (when hx_on)
+  const int hy_off = (hyj - t.j) * g.nx;  // -nx or +nx (when hy_on)
+  const int hxs = tx == 0 ? 0 : ZX + 1;
+  const int hys = ty == 0 ? 0 : ZY + 1;
+  const bool last_chunk = t.k0 + ZK >= g.nz;
+
+  float pprev = 0.f;
+  if (t.k0 > 0) pprev = ld.pv(ld.full(t.i, t.j, t.k0 - 1, base + (t.k0 - 1) * nxny));
+  Raw rc = ld.full(t.i, t.j, t.k0, base + t.k0 * nxny);
+  Raw rn = ld.full(t.i, t.j, t.k0 + 1, base + (t.k0 + 1) * nxny);  // ZK >= 2 and nz % ZK == 0
+  Halo hx = hx_on ? ld.halo(hxi, t.j, t.k0, base + hx_off + t.k0 * nxny) : Halo();
+  Halo hy = hy_on ? ld.halo(t.i, hyj, t.k0, base + hy_off + t.k0 * nxny) : Halo();
+  unsigned code = codes[base + t.k0 * nxny];
+#pragma unroll
+  for (int kk = 0; kk < ZK; ++kk) {
+    const int k = t.k0 + kk;
+    const int c = base + k * nxny;
+    Raw rnn;
+    if (kk + 2 < ZK || (!last_chunk && kk + 2 == ZK)) rnn = ld.full(t.i, t.j, k + 2, c + 2 * nxny);
+    Halo hx2, hy2;
+    unsigned code2 = 0;
+    if (kk + 1 < ZK) {
+      if (hx_on) hx2 = ld.halo(hxi, t.j, k + 1, c + nxny + hx_off);
+      if (hy_on) hy2 = ld.halo(t.i, hyj, k + 1, c + nxny + hy_off);
+      code2 = codes[c + nxny];
+    }
+    const float pc = ld.pv(rc);
+    const float pn = (kk + 1 < ZK || !last_chunk) ? ld.pv(rn) : 0.f;
+    s[ty + 1][tx + 1] = pc;
+    if (hxi >= 0) s[ty + 1][hxs] = hx_on ? ld.hv(hx) : 0.f;
+    if (hyj >= 0) s[hys][tx + 1] = hy_on ? ld.hv(hy) : 0.f;
+    __syncthreads();
+    float ax = 0.f;
+    if (code & RC_WET)
+      ax = apply_code_nb(g, code, t.i, t.j, k, pc, s[ty + 1][tx], s[ty + 1][tx + 2], s[ty][tx + 1], s[ty + 2][tx + 1],
+                         pprev, pn);
+    epi(c, rc, pc, ax);
+    __syncthreads();
+    after(k);
+    pprev = pc;
+    rc = rn;
+    rn = rnn;
+    hx = hx2;
+    hy = hy2;
+    code = code2;
+  }
+}
+
+inline bool zfull(int nx, int ny, int nz) { return nx % ZX == 0 && ny % ZY == 0 && nz % ZK == 0; }
+
+// Full tiles or not, chosen by the kernel's FULL template parameter.
+#define ZMARCH(...)                      \
+  do {                                   \
+    if (FULL) zmarch_full(__VA_ARGS__);  \
+    else zmarch(__VA_ARGS__);            \
+  } while (0)
+
 // Loaders.
 struct LdLoad {  // operand = x
   const float* __restrict__ x;
@@ -240,14 +320,16 @@ __device__ __forceinline__ void zreduce_finish(double v, Red red, Scalars* S, in
 }
 
 // d = z (+ beta d); q = A d; d.q; alpha (FIN_DQ).
-__global__ void __launch_bounds__(ZT) kz_dir_apply_dot(Geo g, const unsigned short* __restrict__ codes,
+template <bool FULL>
+__global__ void __launch_bounds__(ZT, FD3_ZMINB) kz_dir_apply_dot(Geo g, const unsigned short* __restrict__ codes,
                                                        const float* __restrict__ z, const float* __restrict__ din,
                                                        float* __restrict__ dout, float* __restrict__ q, Red red,
                                                        Scalars* S) {
+  KSTART();
   if (!S->active) return;
   LdDir ld{z, din, S->dir_mode, S->beta};
   double acc = 0.0;
-  zmarch(g, codes, ld, [&](int c, const LdDir::Raw&, float pc, float ax) {
+  ZMARCH(g, codes, ld, [&](int c, const LdDir::Raw&, float pc, float ax) {
     dout[c] = pc;
     q[c] = ax;
     acc += (double)pc * (double)ax;
@@ -256,12 +338,14 @@ __global__ void __launch_bounds__(ZT) kz_dir_apply_dot(Geo g, const unsigned sho
 }
 
 // The two pre-sweeps from z = 0.
-__global__ void __launch_bounds__(ZT) kz_fine_pre(Geo g, const unsigned short* __restrict__ codes,
+template <bool FULL>
+__global__ void __launch_bounds__(ZT, FD3_ZMINB) kz_fine_pre(Geo g, const unsigned short* __restrict__ codes,
                                                   const float* __restrict__ prec, const float* __restrict__ r,
                                                   float* __restrict__ z2, const Scalars* S, int gate) {
+  KSTART();
   if (gate && !S->active) return;
   LdZ1 ld{prec, r};
-  zmarch(g, codes, ld, [&](int c, const LdZ1::Raw& o, float pc, float ax) {
+  ZMARCH(g, codes, ld, [&](int c, const LdZ1::Raw& o, float pc, float ax) {
     float zc = pc;
     if (o.m > 0.f) zc += OMEGA * o.m * (o.r - ax);
     z2[c] = zc;
@@ -269,13 +353,15 @@ __global__ void __launch_bounds__(ZT) kz_fine_pre(Geo g, const unsigned short* _
 }
 
 // Prolongation + zeroing + first post-sweep (or the plain third sweep without coarse levels).
-__global__ void __launch_bounds__(ZT) kz_fine_post1(Geo g, const unsigned short* __restrict__ codes,
+template <bool FULL>
+__global__ void __launch_bounds__(ZT, FD3_ZMINB) kz_fine_post1(Geo g, const unsigned short* __restrict__ codes,
                                                     const float* __restrict__ prec, const float* __restrict__ r,
                                                     const float* __restrict__ zin, Lev L, int prolong,
                                                     float* __restrict__ zout, const Scalars* S, int gate) {
+  KSTART();
   if (gate && !S->active) return;
   LdProlong ld{zin, prec, r, L.x, L.nx, L.ny, prolong};
-  zmarch(g, codes, ld, [&](int c, const LdProlong::Raw& o, float pc, float ax) {
+  ZMARCH(g, codes, ld, [&](int c, const LdProlong::Raw& o, float pc, float ax) {
     float zc = pc;
     if (o.m > 0.f) zc += OMEGA * o.m * (o.r - ax);
     zout[c] = zc;
@@ -283,14 +369,16 @@ __global__ void __launch_bounds__(ZT) kz_fine_post1(Geo g, const unsigned short*
 }
 
 // Second post-sweep with r.z (FIN_RZ_PRIME or FIN_RZ_ITER).
-__global__ void __launch_bounds__(ZT) kz_fine_post2_rz(Geo g, const unsigned short* __restrict__ codes,
+template <bool FULL>
+__global__ void __launch_bounds__(ZT, FD3_ZMINB) kz_fine_post2_rz(Geo g, const unsigned short* __restrict__ codes,
                                                        const float* __restrict__ prec, const float* __restrict__ r,
                                                        const float* __restrict__ zin, float* __restrict__ zout, Red red,
                                                        Scalars* S, int gate, int op) {
+  KSTART();
   if (gate && !S->active) return;
   LdSweep ld{zin, prec, r};
   double acc = 0.0;
-  zmarch(g, codes, ld, [&](int c, const LdSweep::Raw& o, float pc, float ax) {
+  ZMARCH(g, codes, ld, [&](int c, const LdSweep::Raw& o, float pc, float ax) {
     float zc = pc;
     if (o.m > 0.f) zc += OMEGA * o.m * (o.r - ax);
     zout[c] = zc;
@@ -303,16 +391,18 @@ __global__ void __launch_bounds__(ZT) kz_fine_post2_rz(Geo g, const unsigned sho
 // two layers at a time: the even thread of each 2 x 2 column group sums its coarse cell's eight
 // children in the reference's CHILDREN order from the two layers kept in shared memory.  Needs even
 // nx, ny, nz (the coarsening rule guarantees them) and even ZX, ZY, ZK.
-__global__ void __launch_bounds__(ZT) kz_fine_restrict(Geo g, const unsigned short* __restrict__ codes,
+template <bool FULL>
+__global__ void __launch_bounds__(ZT, FD3_ZMINB) kz_fine_restrict(Geo g, const unsigned short* __restrict__ codes,
                                                        const float* __restrict__ r, const float* __restrict__ z, Lev L,
                                                        const Scalars* S, int gate) {
+  KSTART();
   if (gate && !S->active) return;
   __shared__ float tr[2][ZY][ZX];
   const int tx = threadIdx.x % ZX, ty = threadIdx.x / ZX;
   const ZTile t = ztile(g);
   const int nxny = g.nx * g.ny;
   LdLoadR ld{z, r};
-  zmarch(
+  ZMARCH(
       g, codes, ld,
       [&](int c, const LdLoadR::Raw& o, float, float ax) { tr[(c / nxny) & 1][ty][tx] = o.r - ax; },
       [&](int k) {
@@ -336,6 +426,7 @@ constexpr int UPDATE_BLOCKS = 592;
 __global__ void __launch_bounds__(TPB) kv_update_rn(int n, float* __restrict__ p, float* __restrict__ r,
                                                     const float* __restrict__ d, const float* __restrict__ q, Red red,
                                                     Scalars* S) {
+  KSTART();
   if (!S->active) return;
   const float alpha = S->alpha;
   const int stride = gridDim.x * blockDim.x;

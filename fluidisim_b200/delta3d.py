@@ -48,7 +48,7 @@ class _Report(C.Structure):
 
 class _Options(C.Structure):
     _fields_ = [("reduction", C.c_uint32), ("mg_max_levels", C.c_uint32), ("use_graphs", C.c_uint32),
-                ("kernels", C.c_uint32), ("reserved", C.c_uint32 * 4)]
+                ("kernels", C.c_uint32), ("no_overlap", C.c_uint32), ("reserved", C.c_uint32 * 3)]
 
 
 @dataclass
@@ -191,7 +191,7 @@ class Volume3:
             raise Delta3dError(e, where, self._L.fd3_last_cuda_error().decode() if e >= 100 else "")
 
     # ---- options
-    def set_options(self, reduction=None, mg_max_levels=None, use_graphs=None, kernels=None):
+    def set_options(self, reduction=None, mg_max_levels=None, use_graphs=None, kernels=None, no_overlap=None):
         o = _Options()
         self._check(self._L.fd3_get_options(self._h, C.byref(o)), "get_options")
         if reduction is not None:
@@ -202,6 +202,8 @@ class Volume3:
             o.use_graphs = int(use_graphs)
         if kernels is not None:
             o.kernels = int(kernels)
+        if no_overlap is not None:
+            o.no_overlap = int(no_overlap)
         self._check(self._L.fd3_set_options(self._h, C.byref(o)), "set_options")
 
     def set_stream(self, stream_ptr: int):

@@ -78,7 +78,10 @@ typedef struct fd3_options {
   uint32_t use_graphs;    /* 1 = run the inner PCG loop as a CUDA graph with a WHILE node */
   uint32_t kernels;       /* fine-level kernels in f64 mode: 0 = 2.5-D blocked (default), 1 = one cell
                              per thread (the family the ordered mode always uses) */
-  uint32_t reserved[4];
+  uint32_t no_overlap;    /* 1 = launch each kernel only after the previous one completes; 0 (default)
+                             = programmatic dependent launch: the next kernel is scheduled early and
+                             waits on the device (results are identical either way) */
+  uint32_t reserved[3];
 } fd3_options;
 
 typedef struct fd3_volume fd3_volume;

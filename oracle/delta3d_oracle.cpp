@@ -65,6 +65,11 @@ inline R clamp01(R x) { return x < (R)0 ? (R)0 : (x > (R)1 ? (R)1 : x); }
 
 int g_threads = 1;
 
+// Smoother of the V-cycle: 0 = the reference's damped Jacobi (delta3d_multigrid.rs:28, 290-299);
+// 1 = red-black Gauss-Seidel (omega = 1), pre-sweeps red then black, post-sweeps black then red,
+// the coarsest level's sweeps forward then backward, so the preconditioner stays symmetric.
+int g_smoother = 0;
+
 // ---------------------------------------------------------------------------------------------
 // Ordered reduction: host.rs:60-72 contract, host_impl.rs:75-92 sequential reference.  Chunks of
 // `grain` are reduced in index order inside the chunk; the chunk results are merged in increasing
@@ -639,6 +644,27 @@ void smooth3(Level3& L) {
     if (L.diag[c] > 0) L.x[c] += SMOOTH_DAMPING_3D * (L.r[c] - L.t[c]) / L.diag[c];
 }
 
+// One red-black Gauss-Seidel half sweep of a coarse level on cells of `color` ((i+j+k) & 1).
+void smooth3_rb(Level3& L, int color) {
+  size_t nx = L.nx, ny = L.ny, nz = L.nz;
+  row_sums(L, L.x.data(), L.t.data());
+  for (size_t k = 0; k < nz; ++k)
+    for (size_t j = 0; j < ny; ++j)
+      for (size_t i = 0; i < nx; ++i) {
+        if ((int)((i + j + k) & 1) != color) continue;
+        size_t c = L.c(i, j, k);
+        if (L.diag[c] > 0) L.x[c] += (L.r[c] - L.t[c]) / L.diag[c];
+      }
+}
+// `count` smoothing sweeps of a coarse level; `forward` orders each sweep red then black.
+void smooth_level(Level3& L, int count, bool forward) {
+  for (int s = 0; s < count; ++s) {
+    if (g_smoother == 0) { smooth3(L); continue; }
+    smooth3_rb(L, forward ? 0 : 1);
+    smooth3_rb(L, forward ? 1 : 0);
+  }
+}
+
 // delta3d_multigrid.rs:303-332
 void coarse_cycle3(std::vector<Level3>& levels) {
   size_t last = levels.size() - 1;
@@ -646,7 +672,8 @@ void coarse_cycle3(std::vector<Level3>& levels) {
     int sweeps = l == last ? COARSE_SWEEPS_3D : PRE_SWEEPS_3D;
     Level3& L = levels[l];
     std::fill(L.x.begin(), L.x.end(), (R)0);
-    for (int s = 0; s < sweeps; ++s) smooth3(L);
+    if (g_smoother == 0 || l < last) smooth_level(L, sweeps, true);
+    else { smooth_level(L, sweeps / 2, true); smooth_level(L, sweeps / 2, false); }
     if (l < last) {
       row_sums(L, L.x.data(), L.t.data());
       for (size_t c = 0; c < L.cells(); ++c) L.t[c] = L.r[c] - L.t[c];
@@ -656,7 +683,7 @@ void coarse_cycle3(std::vector<Level3>& levels) {
   for (size_t l = last; l-- > 0;) {
     Level3& L = levels[l];
     prolong_add3(L.nx, L.ny, L.x.data(), levels[l + 1]);
-    for (int s = 0; s < POST_SWEEPS_3D; ++s) smooth3(L);
+    smooth_level(L, POST_SWEEPS_3D, false);
   }
 }
 
@@ -1011,11 +1038,25 @@ struct Volume3 {
   void v_cycle3() {
     size_t nx = d.nx, ny = d.ny, cells = p.size();
     std::fill(mg.z.begin(), mg.z.end(), (R)0);
-    for (int s = 0; s < PRE_SWEEPS_3D; ++s) {
-      apply_mobile3(mg.z.data(), mg.t.data());
-      for (size_t q = 0; q < cells; ++q)
-        if (prec[q] > 0) mg.z[q] += SMOOTH_DAMPING_3D * prec[q] * (res[q] - mg.t[q]);
-    }
+    // one fine sweep: Jacobi (the reference) or a red-black half sweep pair in the given order
+    auto fine_sweep = [&](bool forward) {
+      if (g_smoother == 0) {
+        apply_mobile3(mg.z.data(), mg.t.data());
+        for (size_t q = 0; q < cells; ++q)
+          if (prec[q] > 0) mg.z[q] += SMOOTH_DAMPING_3D * prec[q] * (res[q] - mg.t[q]);
+        return;
+      }
+      for (int h = 0; h < 2; ++h) {
+        int color = forward ? h : 1 - h;
+        apply_mobile3(mg.z.data(), mg.t.data());
+        for (size_t q = 0; q < cells; ++q) {
+          size_t i = q % nx, j = (q / nx) % ny, k = q / (nx * ny);
+          if ((int)((i + j + k) & 1) != color) continue;
+          if (prec[q] > 0) mg.z[q] += prec[q] * (res[q] - mg.t[q]);
+        }
+      }
+    };
+    for (int s = 0; s < PRE_SWEEPS_3D; ++s) fine_sweep(true);
     if (!mg.levels.empty()) {
       apply_mobile3(mg.z.data(), mg.t.data());
       for (size_t q = 0; q < cells; ++q) mg.t[q] = res[q] - mg.t[q];
@@ -1025,11 +1066,7 @@ struct Volume3 {
       for (size_t q = 0; q < cells; ++q)
         if (prec[q] == 0) mg.z[q] = 0;
     }
-    for (int s = 0; s < POST_SWEEPS_3D; ++s) {
-      apply_mobile3(mg.z.data(), mg.t.data());
-      for (size_t q = 0; q < cells; ++q)
-        if (prec[q] > 0) mg.z[q] += SMOOTH_DAMPING_3D * prec[q] * (res[q] - mg.t[q]);
-    }
+    for (int s = 0; s < POST_SWEEPS_3D; ++s) fine_sweep(false);
   }
   // delta3d_multigrid.rs:433-465
   int prime_multigrid3(R beta, R& out) {
@@ -1403,6 +1440,7 @@ struct od3_domain { uint64_t nx, ny, nz; float dx; };
 
 int od3_real_bytes(void) { return (int)sizeof(R); }
 void od3_set_threads(int n) { g_threads = n > 0 ? n : 1; }
+void od3_set_smoother(int s) { g_smoother = s == 1 ? 1 : 0; }
 int od3_max_threads(void) {
 #ifdef _OPENMP
   return omp_get_max_threads();
