@@ -63,6 +63,17 @@ BYTES_PER_CELL = {
 }
 
 
+def merge_templates(entries):
+    """Per-kernel profile entries with template arguments dropped (kz_fine_pre<true> and
+    kz_fine_pre<false> are one kernel: full tiles and ragged tiles of the same pass)."""
+    acc = {}
+    for name, count, ms in entries:
+        base = name.split("<", 1)[0]
+        c, m = acc.get(base, (0, 0.0))
+        acc[base] = (c + count, m + ms)
+    return [(n, c, m) for n, (c, m) in acc.items()]
+
+
 def peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -74,7 +85,11 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi samples of the SM clock and throttle reasons while the timed region runs."""
+    """nvidia-smi samples of the SM clock and throttle reasons, kept only for the timed region.
+
+    The sampler starts before the warm-up (nvidia-smi needs about half a second to produce its
+    first line); `mark(True)` / `mark(False)` bracket the timed region and only lines that arrive
+    between the two marks are summarised."""
 
     FIELDS = "clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown," \
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown," \
@@ -84,11 +99,13 @@ class ClockSampler:
         self.index = index
         self.proc = None
         self.lines = []
+        self.t0 = None
+        self.t1 = None
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100",
                  "-i", str(self.index)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
@@ -98,7 +115,13 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.monotonic(), line.strip()))
+
+    def mark(self, start: bool):
+        if start:
+            self.t0 = time.monotonic()
+        else:
+            self.t1 = time.monotonic()
 
     def __exit__(self, *exc):
         if self.proc:
@@ -109,15 +132,20 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
-        sm, smax, reasons = [], [], set()
+        sm, smax, power, reasons = [], [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
+        t0 = self.t0 if self.t0 is not None else float("-inf")
+        t1 = self.t1 if self.t1 is not None else float("inf")
+        for t, line in self.lines:
+            if not (t0 <= t <= t1):
+                continue
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 7:
                 continue
             try:
                 sm.append(float(parts[0]))
                 smax.append(float(parts[1]))
+                power.append(float(parts[2]))
             except ValueError:
                 continue
             for name, val in zip(names, parts[3:7]):
@@ -126,7 +154,7 @@ class ClockSampler:
         if not sm:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "power_w_max": max(power), "samples": len(sm)}
 
 
 def dist_setup(gpus: int):
@@ -181,15 +209,22 @@ def run_reference(args):
     v = O.OracleVolume(s["nx"], s["ny"], s["nz"], s["dx"], s["rho"], s["g"], bottom=s["bottom"], solid=s["solid"])
     v.enable_multigrid()
     v.set_free_surface(s["eta"], s["rest"])
+    # A CPU projection at 128^3 takes most of a second, so the arm is bounded: at most 2 warm-up
+    # projections, then timed projections until K are done or 90 s have passed.
     times, rep = [], None
-    for step in range(args.warmup + args.steps):
+    warm = min(args.warmup, 2)
+    t_begin = None
+    for step in range(warm + args.steps):
         v.set_velocity(s["u"], s["v"], s["w"])
         v.set_free_surface(s["eta"], s["rest"])
         t0 = time.perf_counter()
         rep = v.project_mobile(scale, k1, 4000)
         dt = time.perf_counter() - t0
-        if step >= args.warmup:
+        if step >= warm:
             times.append(dt)
+            t_begin = t_begin if t_begin is not None else t0
+            if time.perf_counter() - t_begin > 90.0:
+                break
     ms = 1e3 * sum(times) / len(times)
     value = 1e3 / ms
     out = {
@@ -200,7 +235,8 @@ def run_reference(args):
                    "cells": s["nx"] * s["ny"] * s["nz"], "solver": "mgpcg", "iterations": rep["iterations"],
                    "rel_residual": rep["residual"], "parallelism": "host threads"},
         "cpu_baseline": {"value": value, "unit": "projections/s", "cores": threads, "kind": "port",
-                         "sample": f"{args.steps} projections of the {args.size}^3 scene after {args.warmup} warm-up"},
+                         "sample": f"{len(times)} timed projections of the {args.size}^3 scene after {warm} warm-up "
+                                   f"(capped at {args.steps} or 90 s)"},
         "e2e": {"value": value, "unit": "projections/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out), flush=True)
@@ -261,15 +297,20 @@ def run_b200(args):
         return vol.project_mobile3(scale, k1, 4000)
 
     rep = None
-    for _ in range(args.warmup):
-        rep = step()
-    torch.cuda.synchronize()
-    barrier(world)
-    launches0 = vol.kernel_launches()
     evs = []
     with ClockSampler(local) as clocks:
+        t_warm = time.monotonic()
+        for _ in range(args.warmup):
+            rep = step()
+        torch.cuda.synchronize()
+        while time.monotonic() - t_warm < 1.0:   # let nvidia-smi produce its first lines
+            rep = step()
+            torch.cuda.synchronize()
+        barrier(world)
+        launches0 = vol.kernel_launches()
         torch.cuda.synchronize()
         barrier(world)
+        clocks.mark(True)
         for _ in range(args.steps):
             with torch.cuda.stream(stream):
                 flush.zero_()
@@ -279,8 +320,9 @@ def run_b200(args):
             b.record(stream)
             evs.append((a, b))
         torch.cuda.synchronize()
+        clocks.mark(False)
         barrier(world)
-    launches = vol.kernel_launches() - launches0
+        launches = vol.kernel_launches() - launches0
     ms_total = sum(a.elapsed_time(b) for a, b in evs)
     ms_total = max_over_ranks(ms_total, world)
     ms_per_step = ms_total / args.steps
@@ -330,12 +372,13 @@ def run_b200(args):
     # per-kernel timing: an instrumented replay of the same steps right after the timed region
     vol.set_options(use_graphs=0)
     vol.profile(True)
-    for _ in range(args.steps):
+    prof_steps = min(args.steps, 20)
+    for _ in range(prof_steps):
         with torch.cuda.stream(stream):
             flush.zero_()
         step()
     torch.cuda.synchronize()
-    prof = vol.profile_entries()
+    prof = merge_templates(vol.profile_entries())
     vol.profile(False)
     vol.set_options(use_graphs=args.graphs)
     total_prof = sum(ms for _, _, ms in prof)
@@ -372,7 +415,8 @@ def run_b200(args):
                          "traffic": ncu_traffic, "alg_bytes_per_launch": alg_bytes,
                          "avg_launch_ms": avg_ms, "launches": count,
                          "share_of_step": ms / total_prof if total_prof else None},
-            "kernels": {n: {"launches": c, "ms": round(m, 4)} for n, c, m in sorted(prof, key=lambda e: -e[2])[:12]},
+            "kernels": {n: {"launches": c, "ms_per_step": round(m / prof_steps, 5)}
+                        for n, c, m in sorted(prof, key=lambda e: -e[2])[:14]},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "projections/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,
@@ -388,7 +432,7 @@ def run_b200(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--size", type=int, default=128)

@@ -7,6 +7,7 @@ uncontracted, as the reference's Rust code is, so the kernels reproduce its arit
 """
 from __future__ import annotations
 
+import glob
 import os
 import subprocess
 import sys
@@ -15,7 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libfluidisim_delta3d.so")
 SOURCES = [os.path.join(HERE, "csrc", "fd3_volume.cu")]
-DEPS = SOURCES + [os.path.join(HERE, "csrc", f) for f in ("fd3_kernels.cuh", "fd3_cut.cuh")] + [
+DEPS = SOURCES + sorted(glob.glob(os.path.join(HERE, "csrc", "*.cuh"))) + [
     os.path.join(ROOT, "include", "fluidisim_delta3d.h")]
 
 NVCC_FLAGS = [

@@ -698,60 +698,55 @@ __global__ void __launch_bounds__(TAIL_THREADS) k_coarse_tail_smem(const Lev* __
 }
 
 // The coarse tail with one cell per thread.  Every tail level has at most TAIL_REG_THREADS cells;
-// thread c owns cell c of the level being worked on and keeps its row (code, apertures, diagonal,
-// right-hand side, x) in registers, so a sweep is six shared-memory reads, the row, one write and
-// one barrier.  The phases and their arithmetic are those of coarse_cycle3
-// (delta3d_multigrid.rs:303-332): 2 pre-sweeps, residual, 8-child mean, ..., 8 sweeps on the
-// coarsest level, then prolongation and 2 post-sweeps per level on the way up.
+// thread c owns cell c of each level and keeps its rows (code, apertures, diagonal) for all levels
+// in registers, fetched once at the start with independent loads, so the phases below touch only
+// shared memory: a sweep is six shared-memory reads, the row, one write and one barrier.  The
+// phases and their arithmetic are those of coarse_cycle3 (delta3d_multigrid.rs:303-332): 2
+// pre-sweeps, residual, 8-child mean, ..., 8 sweeps on the coarsest level, then prolongation and 2
+// post-sweeps per level on the way up.
 constexpr int TAIL_REG_THREADS = 512;
 constexpr int TAIL_REG_LEVELS = 5;  // 40 KiB of static shared memory
 
 struct TailRow {
   unsigned code;
   float a[6];
-  int m[6];
-  float diag, r;
-  bool own;
+  float diag;
 };
 
-__device__ __forceinline__ TailRow tail_row(const Lev& L, int c, float r) {
+__device__ __forceinline__ TailRow tail_row(const Lev& L, int c) {
   TailRow w;
-  w.own = c < L.n;
   w.code = 0;
   w.diag = 0.f;
-  w.r = r;
 #pragma unroll
-  for (int f = 0; f < 6; ++f) { w.a[f] = 0.f; w.m[f] = 0; }
-  if (!w.own) return w;
+  for (int f = 0; f < 6; ++f) w.a[f] = 0.f;
+  if (c >= L.n) return w;
   w.code = L.code[c];
   w.diag = L.diag[c];
-  const int i = c % L.nx, t = c / L.nx, j = t % L.ny, k = t / L.ny, nxny = L.nx * L.ny;
+  const int i = c % L.nx, t = c / L.nx, j = t % L.ny, k = t / L.ny;
   const bool unit = w.code & RC_UNIT;
   const int fi[6] = {(k * L.ny + j) * (L.nx + 1) + i, (k * L.ny + j) * (L.nx + 1) + i + 1,
                      (k * (L.ny + 1) + j) * L.nx + i, (k * (L.ny + 1) + j + 1) * L.nx + i,
                      (k * L.ny + j) * L.nx + i, ((k + 1) * L.ny + j) * L.nx + i};
-  const int mm[6] = {c - 1, c + 1, c - L.nx, c + L.nx, c - nxny, c + nxny};
 #pragma unroll
   for (int f = 0; f < 6; ++f) {
-    const unsigned st = face_state(w.code, f);
-    if (st) {
+    if (face_state(w.code, f)) {
       const float* ap = f < 2 ? L.ou : (f < 4 ? L.ov : L.ow);
       w.a[f] = unit ? 1.f : ap[fi[f]];
-      w.m[f] = st == 1 ? mm[f] : c;
-    } else {
-      w.m[f] = c;
     }
   }
   return w;
 }
 
-// row_sums at the owned cell, the neighbours' values read from X (shared memory).
-__device__ __forceinline__ float tail_rowsum(const TailRow& w, float pc, const float* X, float inv) {
+// row_sums at cell c of a level with dims (nx, ny), the neighbours' values read from X (shared
+// memory); the terms are added in face order x-, x+, y-, y+, z-, z+.
+__device__ __forceinline__ float tail_rowsum(const TailRow& w, int c, int nx, int nxny, float pc, const float* X,
+                                             float inv) {
+  const int mm[6] = {c - 1, c + 1, c - nx, c + nx, c - nxny, c + nxny};
   float acc = 0.f;
 #pragma unroll
   for (int f = 0; f < 6; ++f) {
     const unsigned st = face_state(w.code, f);
-    if (st == 1) acc += w.a[f] * (pc - X[w.m[f]]);
+    if (st == 1) acc += w.a[f] * (pc - X[mm[f]]);
     else if (st == 2) acc += 2.f * w.a[f] * pc;
   }
   return acc * inv;
@@ -761,85 +756,102 @@ __global__ void __launch_bounds__(TAIL_REG_THREADS) k_coarse_tail_reg(const Lev*
                                                                      const Scalars* S, int gate) {
   KSTART();
   if (gate && !S->active) return;
-  // per level: XA, XB (sweep ping-pong), XF (final x of the level), R (right-hand side), TT (residual)
+  // per level: XA, XB (sweep ping-pong), XF (final x of the level), R (right-hand side)
   __shared__ float XA[TAIL_REG_LEVELS][TAIL_REG_THREADS];
   __shared__ float XB[TAIL_REG_LEVELS][TAIL_REG_THREADS];
   __shared__ float XF[TAIL_REG_LEVELS][TAIL_REG_THREADS];
   __shared__ float R[TAIL_REG_LEVELS][TAIL_REG_THREADS];
+  __shared__ Lev Ls[TAIL_REG_LEVELS];
   const int c = threadIdx.x;
   const int nl = last - first + 1;
-  {
-    const Lev L0 = T[first];
-    if (c < L0.n) R[0][c] = L0.r[c];
+  if (c < nl) Ls[c] = T[first + c];
+  __syncthreads();
+  // every row of every level, and the right-hand side of the first, in one round of loads
+  TailRow w[TAIL_REG_LEVELS];
+#pragma unroll
+  for (int l = 0; l < TAIL_REG_LEVELS; ++l) {
+    if (l < nl) w[l] = tail_row(Ls[l], c);
   }
+  if (c < Ls[0].n) R[0][c] = Ls[0].r[c];
   __syncthreads();
   // descent
-  for (int l = 0; l < nl; ++l) {
-    const Lev L = T[first + l];
-    const TailRow w = tail_row(L, c, c < L.n ? R[l][c] : 0.f);
-    const int sweeps = l == nl - 1 ? 8 : 2;  // COARSE_SWEEPS_3D, PRE_SWEEPS_3D
-    float x = 0.f;
-    for (int s = 0; s < sweeps; ++s) {
-      float* out = (s & 1) ? XB[l] : XA[l];
-      const float* in = (s & 1) ? XA[l] : XB[l];
-      float xn = x;
-      if (w.own) {
-        if (s == 0) xn = w.diag > 0.f ? 0.f + OMEGA * (w.r - 0.f) / w.diag : 0.f;
-        else if (w.diag > 0.f) xn = x + OMEGA * (w.r - tail_rowsum(w, x, in, L.inv)) / w.diag;
-        out[c] = xn;
-      }
-      __syncthreads();
-      x = xn;
-    }
-    if (w.own) XF[l][c] = x;
-    if (l < nl - 1) {
-      // residual t = r - L x (0 on inactive rows), then the 8-child mean into the next level
-      const float* xs = ((sweeps - 1) & 1) ? XB[l] : XA[l];
-      float tv = 0.f;
-      if (w.own) tv = w.r - ((w.code & RC_WET) ? tail_rowsum(w, x, xs, L.inv) : 0.f);
-      __syncthreads();
-      if (w.own) XA[l][c] = tv;
-      __syncthreads();
-      const Lev C = T[first + l + 1];
-      if (c < C.n) {
-        int ci = c % C.nx, t = c / C.nx, cj = t % C.ny, ck = t / C.ny;
-        float sum = 0.f;
 #pragma unroll
-        for (int e = 0; e < 8; ++e) {
-          int i = 2 * ci + (e & 1), j = 2 * cj + ((e >> 1) & 1), k = 2 * ck + (e >> 2);
-          sum += XA[l][(k * L.ny + j) * L.nx + i];
+  for (int l = 0; l < TAIL_REG_LEVELS; ++l) {
+    if (l < nl) {
+      const Lev& L = Ls[l];
+      const bool own = c < L.n;
+      const int nx = L.nx, nxny = L.nx * L.ny;
+      const float inv = L.inv;
+      const float r = own ? R[l][c] : 0.f;
+      const int sweeps = l == nl - 1 ? 8 : 2;  // COARSE_SWEEPS_3D, PRE_SWEEPS_3D
+      float x = 0.f;
+      for (int s = 0; s < sweeps; ++s) {
+        float* out = (s & 1) ? XB[l] : XA[l];
+        const float* in = (s & 1) ? XA[l] : XB[l];
+        float xn = x;
+        if (own) {
+          if (s == 0) xn = w[l].diag > 0.f ? 0.f + OMEGA * (r - 0.f) / w[l].diag : 0.f;
+          else if (w[l].diag > 0.f) xn = x + OMEGA * (r - tail_rowsum(w[l], c, nx, nxny, x, in, inv)) / w[l].diag;
+          out[c] = xn;
         }
-        R[l + 1][c] = 0.125f * sum;
+        __syncthreads();
+        x = xn;
       }
-      __syncthreads();
+      if (own) XF[l][c] = x;
+      if (l < nl - 1) {
+        // residual t = r - L x (0 on inactive rows), then the 8-child mean into the next level
+        const float* xs = ((sweeps - 1) & 1) ? XB[l] : XA[l];
+        float tv = 0.f;
+        if (own) tv = r - ((w[l].code & RC_WET) ? tail_rowsum(w[l], c, nx, nxny, x, xs, inv) : 0.f);
+        __syncthreads();
+        if (own) XA[l][c] = tv;
+        __syncthreads();
+        const Lev& C = Ls[l + 1];
+        if (c < C.n) {
+          int ci = c % C.nx, t = c / C.nx, cj = t % C.ny, ck = t / C.ny;
+          float sum = 0.f;
+#pragma unroll
+          for (int e = 0; e < 8; ++e) {
+            int i = 2 * ci + (e & 1), j = 2 * cj + ((e >> 1) & 1), k = 2 * ck + (e >> 2);
+            sum += XA[l][(k * L.ny + j) * L.nx + i];
+          }
+          R[l + 1][c] = 0.125f * sum;
+        }
+        __syncthreads();
+      }
     }
   }
   // ascent
-  for (int l = nl - 2; l >= 0; --l) {
-    const Lev L = T[first + l];
-    const Lev C = T[first + l + 1];
-    const TailRow w = tail_row(L, c, c < L.n ? R[l][c] : 0.f);
-    float x = 0.f;
-    if (w.own) {
-      int i = c % L.nx, t = c / L.nx, j = t % L.ny, k = t / L.ny;
-      x = XF[l][c] + XF[l + 1][((k >> 1) * C.ny + (j >> 1)) * C.nx + (i >> 1)];
-      XB[l][c] = x;
-    }
-    __syncthreads();
-    for (int s = 0; s < 2; ++s) {  // POST_SWEEPS_3D
-      float* out = (s & 1) ? XB[l] : XA[l];
-      const float* in = (s & 1) ? XA[l] : XB[l];
-      float xn = x;
-      if (w.own && w.diag > 0.f) xn = x + OMEGA * (w.r - tail_rowsum(w, x, in, L.inv)) / w.diag;
-      if (w.own) out[c] = xn;
+#pragma unroll
+  for (int l = TAIL_REG_LEVELS - 2; l >= 0; --l) {
+    if (l <= nl - 2) {
+      const Lev& L = Ls[l];
+      const Lev& C = Ls[l + 1];
+      const bool own = c < L.n;
+      const int nx = L.nx, nxny = L.nx * L.ny;
+      const float inv = L.inv;
+      const float r = own ? R[l][c] : 0.f;
+      float x = 0.f;
+      if (own) {
+        int i = c % L.nx, t = c / L.nx, j = t % L.ny, k = t / L.ny;
+        x = XF[l][c] + XF[l + 1][((k >> 1) * C.ny + (j >> 1)) * C.nx + (i >> 1)];
+        XB[l][c] = x;
+      }
       __syncthreads();
-      x = xn;
+      for (int s = 0; s < 2; ++s) {  // POST_SWEEPS_3D
+        float* out = (s & 1) ? XB[l] : XA[l];
+        const float* in = (s & 1) ? XA[l] : XB[l];
+        float xn = x;
+        if (own && w[l].diag > 0.f) xn = x + OMEGA * (r - tail_rowsum(w[l], c, nx, nxny, x, in, inv)) / w[l].diag;
+        if (own) out[c] = xn;
+        __syncthreads();
+        x = xn;
+      }
+      if (own) XF[l][c] = x;
+      __syncthreads();
     }
-    if (w.own) XF[l][c] = x;
-    __syncthreads();
   }
-  const Lev L0 = T[first];
-  if (c < L0.n) L0.x[c] = XF[0][c];
+  if (c < Ls[0].n) Ls[0].x[c] = XF[0][c];
 }
 
 // ------------------------------------------------------------------------------------------------
