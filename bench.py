@@ -391,13 +391,13 @@ def run_b200(args):
     peak, peak_kind = peaks()
     achieved = alg_bytes / (avg_ms * 1e-3) / 1e9
     ncu_traffic = None
-    traffic_file = os.path.join(ROOT, "profiles", "traffic.json")
+    traffic_file = os.path.join(ROOT, "profiles", f"traffic_box_basin_{args.size}.txt")
     if os.path.exists(traffic_file):
-        try:
-            with open(traffic_file) as f:
-                ncu_traffic = json.load(f).get(name)
-        except Exception:
-            ncu_traffic = None
+        with open(traffic_file) as f:
+            for line in f:
+                parts = line.split()
+                if len(parts) == 2 and not line.startswith("#") and parts[0] == name:
+                    ncu_traffic = float(parts[1])
 
     if rank == 0:
         cpu = cpu_baseline_sample(args.size) if (world == 1 and not args.no_cpu) else None
