@@ -106,7 +106,9 @@ __device__ __forceinline__ float apply_code(const Geo& g, unsigned code, int i, 
   st = face_state(code, 5);
   if (st) {
     float a = unit ? 1.f : open3(g, 2, fw(g, i, j, k + 1));
-    if (st == 1) acc += a * (pc - p(c + nxny)); else acc += a * pc * ghost_it_up(g, i, j, k);
+    if (st == 1) acc += a * (pc - p(c + nxny));
+    else if (g.linear) acc += 2.f * a * pc;  // the lid of apply / apply_cut (delta3d.rs:741, 797)
+    else acc += a * pc * ghost_it_up(g, i, j, k);
   }
   return acc * g.inv;
 }

@@ -41,6 +41,7 @@ enum Mode { RED_F64 = 0, RED_ORD = 1 };
 struct Geo {
   int nx, ny, nz, n;
   int cut;                // 0: flat bottom (every aperture 1, nothing solid)
+  int linear;             // 1: the linear path's rows (the only ghost is the lid, coefficient 2)
   float dx, inv, rho_g, rest;
   const float* eta;       // column heights
   const float* rof;       // column roundoff (compensated sum)

@@ -23,6 +23,7 @@
 #include "../../include/fluidisim_delta3d.h"
 #include "fd3_cut.cuh"
 #include "fd3_zmarch.cuh"
+#include "fd3_linear.cuh"
 
 using namespace fd3;
 
@@ -80,6 +81,8 @@ struct fd3_volume {
   float *flux_x = nullptr, *flux_y = nullptr;
   // multigrid
   bool has_mg = false;
+  bool linear = false;            // the current projection is the linear path's
+  bool precondition_cut = true;   // Jacobi on the linear cut path (set_precondition_cut, delta3d.rs:526)
   float *z = nullptr, *z2 = nullptr;
   std::vector<Lev> levels;
   Lev* dlev = nullptr;   // the level table in device memory (for the single-CTA coarse tail)
@@ -119,6 +122,7 @@ struct fd3_volume {
     Geo G;
     G.nx = nx; G.ny = ny; G.nz = nz; G.n = n;
     G.cut = cut ? 1 : 0;
+    G.linear = linear ? 1 : 0;
     G.dx = dx;
     G.inv = 1.f / (dx * dx);
     G.rho_g = rho * g;
@@ -129,6 +133,10 @@ struct fd3_volume {
   }
   bool ord() const { return opt.reduction == FD3_REDUCE_ORDERED_F32; }
   bool blocked() const { return !ord() && opt.kernels == 0; }
+  bool mg_on() const { return has_mg && !linear; }  // the linear path has no multigrid
+  int loop_key() const {
+    return (ord() ? 1 : 0) | (mg_on() ? 2 : 0) | (blocked() ? 4 : 0) | (opt.no_overlap ? 8 : 0) | (linear ? 16 : 0);
+  }
   Red red() const { return Red{p64, p32, count}; }
 };
 
@@ -338,7 +346,7 @@ void vcycle(fd3_volume* V, int gate, int op) {
 // prime_multigrid3 / prime_mobile3 with beta = 0 (delta3d_mobile.rs:517, 587): rz of a fresh
 // direction; with the multigrid the direction itself is formed by the next k_dir_apply_dot.
 void prime(fd3_volume* V) {
-  if (V->has_mg) {
+  if (V->mg_on()) {
     vcycle(V, 0, FIN_RZ_PRIME);
   } else {
     LAUNCH(V, k_jacobi_dir, V->n, V->n, (const float*)V->prec, (const float*)V->res, V->dir, (const Scalars*)V->dS, 0, 0);
@@ -352,7 +360,7 @@ void prime(fd3_volume* V) {
 // the stencil points of the operator.
 void iteration(fd3_volume* V, int parity) {
   Geo G = V->geo();
-  if (V->has_mg) {
+  if (V->mg_on()) {
     float* din = parity ? V->dir2 : V->dir;
     float* dout = parity ? V->dir : V->dir2;
     if (V->blocked()) {
@@ -411,7 +419,7 @@ int build_loop_graph(fd3_volume* V) {
   e = cudaGraphInstantiate(&V->loop_exec, graph, 0);
   cudaGraphDestroy(graph);
   if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate(loop)", __LINE__);
-  V->loop_mode = (V->ord() ? 1 : 0) | (V->has_mg ? 2 : 0) | (V->blocked() ? 4 : 0) | (V->opt.no_overlap ? 8 : 0);
+  V->loop_mode = V->loop_key();
   V->loop_stream = V->stream;
   return FD3_OK;
 }
@@ -420,7 +428,7 @@ int build_loop_graph(fd3_volume* V) {
 int run_inner(fd3_volume* V, uint32_t it_before) {
   const bool graphs = V->opt.use_graphs && !V->prof;
   if (graphs) {
-    int mode = (V->ord() ? 1 : 0) | (V->has_mg ? 2 : 0) | (V->blocked() ? 4 : 0) | (V->opt.no_overlap ? 8 : 0);
+    int mode = V->loop_key();
     if (!V->loop_exec || V->loop_mode != mode || V->loop_stream != V->stream) TRY(build_loop_graph(V));
     CK(cudaGraphLaunch(V->loop_exec, V->stream));
     TRY(pull(V));
@@ -462,19 +470,29 @@ int outer_checks(fd3_volume* V, float k1, Checks* out) {
   Geo G = V->geo();
   DISPATCH(V, k_residual_c, V->n, G, (const unsigned short*)V->codes, (const float*)V->p, (const float*)V->rhs, V->res,
            V->red(), V->dS, (int)FIN_ACTUAL);
-  correct(V, k1);
+  if (V->linear) {
+    LAUNCH(V, k_correct_linear_uv, (long long)V->nu + V->nv, G, k1, (const float*)V->p, (const float*)V->us,
+           (const float*)V->vs, V->u, V->v);
+    LAUNCH(V, k_correct_linear_w, V->nw, G, k1, (const float*)V->p, (const float*)V->ws, V->w);
+  } else {
+    correct(V, k1);
+  }
   LAUNCH_G(V, k_reset_diag, 1, 1, V->dS, 7);
-  LAUNCH(V, k_div_metric, V->n, G, (const float*)V->u, (const float*)V->v, (const float*)V->w, V->dS);
+  if (V->linear) LAUNCH(V, k_div_metric_linear, V->n, G, (const float*)V->u, (const float*)V->v, (const float*)V->w, V->dS);
+  else LAUNCH(V, k_div_metric, V->n, G, (const float*)V->u, (const float*)V->v, (const float*)V->w, V->dS);
   LAUNCH_G(V, k_maxabs, 592, TPB, V->nu, (const float*)V->u, V->dS, 2);
   LAUNCH_G(V, k_maxabs, 592, TPB, V->nv, (const float*)V->v, V->dS, 2);
   LAUNCH_G(V, k_maxabs, 592, TPB, V->nw, (const float*)V->w, V->dS, 2);
-  LAUNCH(V, k_backward_error, V->n, G, (const float*)V->p, (const float*)V->rhs, (const float*)V->res, V->dS);
+  if (V->linear)
+    LAUNCH(V, k_backward_error_linear, V->n, G, (const float*)V->p, (const float*)V->rhs, (const float*)V->res, V->dS);
+  else
+    LAUNCH(V, k_backward_error, V->n, G, (const float*)V->p, (const float*)V->rhs, (const float*)V->res, V->dS);
   LAUNCH_G(V, k_hash, 592, TPB, V->n, (const float*)V->p, V->dS);
   TRY(pull(V));
   const Scalars* S = V->hS;
-  // delta3d_mobile.rs:426-432
+  // delta3d_mobile.rs:426-432; the linear metric (delta3d.rs:1043-1052) has no velocity floor
   float all = S->fmax[0], plain = S->fmax[1], mx = S->fmax[2];
-  float echelle = std::fmax(mx, PROJECTION_VELOCITY_FLOOR);
+  float echelle = V->linear ? mx : std::fmax(mx, PROJECTION_VELOCITY_FLOOR);
   float ratio = mx > 0.f ? V->dx / echelle : 0.f;
   out->actual = S->actual;
   out->all = (double)(all * ratio);
@@ -491,16 +509,24 @@ __global__ void k_reset_scalars(Scalars* S) {
   *S = z;
 }
 
-// project_mobile3 (delta3d_mobile.rs:465-609).
+// project_mobile3 (delta3d_mobile.rs:465-609), or, with V->linear, project (delta3d.rs:1060-1196):
+// the same loop and outer logic on the linear rows, CG or Jacobi-PCG, from p = 0 everywhere.
 int project_mobile3(fd3_volume* V, float scale, float k1, uint32_t max_iters, fd3_report* rep) {
   const bool ord = V->ord();
   Geo G = V->geo();
   LAUNCH_G(V, k_reset_scalars, 1, 1, V->dS);
   LAUNCH(V, k_divergence, V->n, G, (const float*)V->us, (const float*)V->vs, (const float*)V->ws, V->rhs);
-  DISPATCH(V, k_rhs_b2, V->n, G, scale, V->rhs, V->prec, V->red(), V->dS, 1);
-  LAUNCH(V, k_row_codes, V->n, G, V->codes);
-  if (V->has_mg) prepare_multigrid(V);
-  LAUNCH(V, k_zero_dry, V->n, G, V->p);
+  if (V->linear) {
+    const int jacobi = V->cut && V->precondition_cut && V->ny > 1;  // delta3d.rs:1091
+    DISPATCH(V, k_rhs_linear, V->n, G, scale, jacobi, V->rhs, V->prec, V->red(), V->dS);
+    LAUNCH(V, k_row_codes_linear, V->n, G, V->codes);
+    CK(cudaMemsetAsync(V->p, 0, (size_t)V->n * sizeof(float), V->stream));
+  } else {
+    DISPATCH(V, k_rhs_b2, V->n, G, scale, V->rhs, V->prec, V->red(), V->dS, 1);
+    LAUNCH(V, k_row_codes, V->n, G, V->codes);
+    if (V->has_mg) prepare_multigrid(V);
+    LAUNCH(V, k_zero_dry, V->n, G, V->p);
+  }
   DISPATCH(V, k_residual_c, V->n, G, (const unsigned short*)V->codes, (const float*)V->p, (const float*)V->rhs, V->res,
            V->red(), V->dS, (int)FIN_RR0);
   TRY(pull(V));
@@ -560,7 +586,7 @@ int project_mobile3(fd3_volume* V, float scale, float k1, uint32_t max_iters, fd
       actual_rr = actual;
       break;
     }
-    if (ck.be <= (V->ny == 1 ? kRoundoff2D : kRoundoff3D)) {
+    if (ck.be <= (V->ny == 1 && !V->linear ? kRoundoff2D : kRoundoff3D)) {
       floor_stop = true; actual_rr = actual;
       if (has_measured) { settled = true; settled_d[0] = measured[0]; settled_d[1] = measured[1]; }
       break;
@@ -822,6 +848,61 @@ int step_surface_mobile(fd3_volume* V, uint64_t duration_us, uint32_t max_iters,
   return e;
 }
 
+// The linear path's projection of the prediction in us/vs/ws (V->linear for its duration).
+int project_linear(fd3_volume* V, float scale, float k1, uint32_t max_iters, fd3_report* rep) {
+  V->linear = true;
+  int e = project_mobile3(V, scale, k1, max_iters, rep);
+  V->linear = false;
+  return e;
+}
+
+// linear (delta3d.rs:1255-1357) after the saves, without a sponge or a graded column.
+int linear_body(fd3_volume* V, float scale, float correction, float transport, uint32_t max_iters, fd3_report* rep) {
+  if (V->cut) {  // the lid must stay fully open (delta3d.rs:1261-1268)
+    CK(cudaMemsetAsync(V->dflag, 0, sizeof(int), V->stream));
+    LAUNCH(V, k_lid_open, V->ncol, V->geo(), V->dflag);
+    CK(cudaMemcpyAsync(V->hflag, V->dflag, sizeof(int), cudaMemcpyDeviceToHost, V->stream));
+    TRY(sync(V));
+    if (*V->hflag) return FD3_ERR_DOMAIN;
+  }
+  CK(cudaMemcpyAsync(V->us, V->u, (size_t)V->nu * 4, cudaMemcpyDeviceToDevice, V->stream));
+  CK(cudaMemcpyAsync(V->vs, V->v, (size_t)V->nv * 4, cudaMemcpyDeviceToDevice, V->stream));
+  CK(cudaMemcpyAsync(V->ws, V->w, (size_t)V->nw * 4, cudaMemcpyDeviceToDevice, V->stream));
+  TRY(project_linear(V, scale, correction, max_iters, rep));
+  if (rep->degraded) return FD3_ERR_CONVERGENCE;
+  LAUNCH(V, k_linear_transport, V->ncol, V->geo(), transport, (const float*)V->u, (const float*)V->v, V->eta, V->rof);
+  // every field finite (delta3d.rs:1347-1353)
+  struct { const float* x; long long n; } fields[] = {
+      {V->u, V->nu}, {V->v, V->nv}, {V->w, V->nw}, {V->p, V->n}, {V->eta, V->ncol}, {V->rof, V->ncol},
+      {V->rhs, V->n}, {V->res, V->n}, {V->dir, V->n}, {V->tmp, V->n}};
+  CK(cudaMemsetAsync(V->dflag, 0, sizeof(int), V->stream));
+  for (auto& f : fields) {
+    LAUNCH_G(V, k_check_finite, 592, TPB, f.n, f.x, V->dflag);
+  }
+  CK(cudaMemcpyAsync(V->hflag, V->dflag, sizeof(int), cudaMemcpyDeviceToHost, V->stream));
+  TRY(sync(V));
+  if (*V->hflag) return FD3_ERR_NOT_FINITE;
+  if (!std::isfinite(rep->residual) || !std::isfinite(rep->divergence)) return FD3_ERR_NOT_FINITE;
+  return FD3_OK;
+}
+
+// step_surface_linear (delta3d.rs:1209-1253).
+int step_surface_linear(fd3_volume* V, uint64_t duration_us, uint32_t max_iters, fd3_report* rep) {
+  if (duration_us == 0 || duration_us > (1ull << 53)) return FD3_ERR_NOT_FINITE;
+  double dt = (double)duration_us * 1e-6;
+  if (V->g <= 0.f || dt * dt * (double)V->g / (double)V->dx > 1.) return FD3_ERR_DOMAIN;
+  float scale = (float)(-(double)V->rho / dt);
+  float correction = (float)(dt / (double)V->rho);
+  float transport = (float)(dt / (double)V->dx);
+  if (!std::isfinite(scale) || !std::isfinite(correction) || correction == 0.f || !std::isfinite(transport) ||
+      transport == 0.f)
+    return FD3_ERR_NOT_FINITE;
+  TRY(save_state(V));
+  int e = linear_body(V, scale, correction, transport, max_iters, rep);
+  if (e) restore_state(V);
+  return e;
+}
+
 }  // namespace
 
 // =============================================================================== C ABI
@@ -1065,6 +1146,35 @@ int fd3_project_mobile(fd3_volume* V, float scale, float k1, uint32_t max_iters,
 int fd3_step_surface_mobile(fd3_volume* V, uint64_t duration_us, uint32_t max_iters, fd3_report* rep) {
   if (!V || !rep) return FD3_ERR_INVALID_ARGUMENT;
   return step_surface_mobile(V, duration_us, max_iters, rep);
+}
+
+// tests_delta3d.rs:143-148: us = u, then project.  A refusal leaves u, v, w, p untouched.
+int fd3_project_linear(fd3_volume* V, float scale, float k1, uint32_t max_iters, fd3_report* rep) {
+  if (!V || !rep) return FD3_ERR_INVALID_ARGUMENT;
+  CK(cudaMemcpyAsync(V->us, V->u, (size_t)V->nu * 4, cudaMemcpyDeviceToDevice, V->stream));
+  CK(cudaMemcpyAsync(V->vs, V->v, (size_t)V->nv * 4, cudaMemcpyDeviceToDevice, V->stream));
+  CK(cudaMemcpyAsync(V->ws, V->w, (size_t)V->nw * 4, cudaMemcpyDeviceToDevice, V->stream));
+  CK(cudaMemcpyAsync(V->sv_p, V->p, (size_t)V->n * 4, cudaMemcpyDeviceToDevice, V->stream));
+  int e = project_linear(V, scale, k1, max_iters, rep);
+  if (e) {
+    cudaMemcpyAsync(V->u, V->us, (size_t)V->nu * 4, cudaMemcpyDeviceToDevice, V->stream);
+    cudaMemcpyAsync(V->v, V->vs, (size_t)V->nv * 4, cudaMemcpyDeviceToDevice, V->stream);
+    cudaMemcpyAsync(V->w, V->ws, (size_t)V->nw * 4, cudaMemcpyDeviceToDevice, V->stream);
+    cudaMemcpyAsync(V->p, V->sv_p, (size_t)V->n * 4, cudaMemcpyDeviceToDevice, V->stream);
+    cudaStreamSynchronize(V->stream);
+  }
+  return e;
+}
+
+int fd3_step_surface_linear(fd3_volume* V, uint64_t duration_us, uint32_t max_iters, fd3_report* rep) {
+  if (!V || !rep) return FD3_ERR_INVALID_ARGUMENT;
+  return step_surface_linear(V, duration_us, max_iters, rep);
+}
+
+int fd3_set_precondition_cut(fd3_volume* V, int on) {
+  if (!V) return FD3_ERR_INVALID_ARGUMENT;
+  V->precondition_cut = on != 0;
+  return FD3_OK;
 }
 
 int fd3_last_refused_report(const fd3_volume* V, fd3_report* rep) {

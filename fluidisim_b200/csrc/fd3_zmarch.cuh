@@ -63,7 +63,9 @@ __device__ __forceinline__ float apply_code_nb(const Geo& g, unsigned code, int 
   st = face_state(code, 5);
   if (st) {
     float a = unit ? 1.f : open3(g, 2, fw(g, i, j, k + 1));
-    if (st == 1) acc += a * (pc - zp); else acc += a * pc * ghost_it_up(g, i, j, k);
+    if (st == 1) acc += a * (pc - zp);
+    else if (g.linear) acc += 2.f * a * pc;
+    else acc += a * pc * ghost_it_up(g, i, j, k);
   }
   return acc * g.inv;
 }

@@ -105,6 +105,9 @@ def library() -> C.CDLL:
     L.fd3_project_mobile.argtypes = [vp, f32, f32, u32, C.POINTER(_Report)]
     L.fd3_step_surface_mobile.argtypes = [vp, u64, u32, C.POINTER(_Report)]
     L.fd3_last_refused_report.argtypes = [vp, C.POINTER(_Report)]
+    L.fd3_project_linear.argtypes = [vp, f32, f32, u32, C.POINTER(_Report)]
+    L.fd3_step_surface_linear.argtypes = [vp, u64, u32, C.POINTER(_Report)]
+    L.fd3_set_precondition_cut.argtypes = [vp, C.c_int]
     L.fd3_get_pressure.argtypes = [vp, fp, sz]
     L.fd3_get_velocity.argtypes = [vp, fp, sz, fp, sz, fp, sz]
     L.fd3_get_surface.argtypes = [vp, fp, fp, sz]
@@ -255,6 +258,24 @@ class Volume3:
     def last_refused_report(self):
         r = _Report()
         return None if self._L.fd3_last_refused_report(self._h, C.byref(r)) else Report._from(r)
+
+    # ---- the linear (fixed-lid) path (delta3d.rs:1060-1357)
+    def project(self, scale, k1, max_iters=4000) -> Report:
+        """project (delta3d.rs:1060) of the current velocity (us = u), as tests_delta3d.rs:143-148 does."""
+        r = _Report()
+        self._check(self._L.fd3_project_linear(self._h, np.float32(scale), np.float32(k1), int(max_iters),
+                                               C.byref(r)), "project")
+        return Report._from(r)
+
+    def step_surface_linear(self, duration_us, max_iters=4000) -> Report:
+        r = _Report()
+        self._check(self._L.fd3_step_surface_linear(self._h, int(duration_us), int(max_iters), C.byref(r)),
+                    "step_surface_linear")
+        return Report._from(r)
+
+    def set_precondition_cut(self, on: bool):
+        """set_precondition_cut (delta3d.rs:526): Jacobi on the linear path's cut bottom."""
+        self._check(self._L.fd3_set_precondition_cut(self._h, 1 if on else 0), "set_precondition_cut")
 
     # ---- outputs (delta3d.rs:647-661)
     def pressure(self) -> np.ndarray:

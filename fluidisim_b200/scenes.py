@@ -125,6 +125,86 @@ def s385_case(nx: int, bump: bool = False) -> dict:
 
 
 # ----------------------------------------------------------------------------------------------
+# The linear path's cut-bottom bench (examples/delta3d_fond_coupe.rs): 8 x 4 x 4 m, lid
+# eta = z0 + 0.01 sin(2 pi x / 8), one 2 ms step from rest; the smooth bottom of S232 (independent
+# of y) or the off-centre bump.
+
+def s324_smooth(x: np.float32, y: np.float32) -> np.float32:
+    d = f32(f32(x - f32(3.0)) / f32(1.2))
+    return f32(0.4) + f32(0.6) * expf(-f32(d * d))
+
+
+def s324_case(nx: int, bump: bool = True) -> dict:
+    """Domain nx x nx/2 x nx/2, dx = 8/nx, its bottom and its lid heights."""
+    ny = nz = nx // 2
+    dx = f32(S385_LX / f32(nx))
+    fond = s385_bump if bump else s324_smooth
+    bottom = np.array([fond(f32(f32(f32(i) + f32(0.5)) * dx), f32(f32(f32(j) + f32(0.5)) * dx))
+                       for j in range(ny) for i in range(nx)], dtype=np.float32)
+    z0 = f32(f32(nz) * dx)
+    row = np.array([z0 + S385_A * sinf(f32(f32(TAU32 * f32(f32(i) + f32(0.5))) * dx) / S385_LX)
+                    for i in range(nx)], dtype=np.float32)
+    return dict(nx=nx, ny=ny, nz=nz, dx=float(dx), rho=S385_RHO, g=S385_G, bottom=bottom, eta=np.tile(row, ny),
+                dt_us=S385_DT_US)
+
+
+def open_flux_x(ou: np.ndarray, u: np.ndarray, nx: int, ny: int, nz: int, dx: float) -> float:
+    """Open flux through x = L/2, sum of aperture * u * dx^2 in f64 (delta3d_fond_coupe.rs:83-90)."""
+    i = nx // 2
+    f = (np.arange(nz)[:, None] * ny + np.arange(ny)[None, :]) * (nx + 1) + i
+    q = 0.0
+    for ff in f.ravel():
+        q += float(ou[ff]) * float(u[ff]) * float(dx) * float(dx)
+    return q
+
+
+def oblique_wave(n: int, g: float = 9.81) -> dict:
+    """Mode (1, 1) of an 8 x 4 m tank, h = 4 m, A = 1 cm, at rest (tests_delta3d.rs:312-343)."""
+    lx, ly, h, a = 8.0, 4.0, 4.0, 0.01
+    dx = lx / n
+    nx, ny, nz = n, int(ly / dx), int(h / dx)
+    kx, ky = np.pi / lx, np.pi / ly
+    jj, ii = np.meshgrid(np.arange(ny), np.arange(nx), indexing="ij")
+    mode = np.cos(kx * (ii + 0.5) * dx) * np.cos(ky * (jj + 0.5) * dx)
+    return dict(nx=nx, ny=ny, nz=nz, dx=float(np.float32(dx)), rho=1025.0, g=float(np.float32(g)),
+                eta=(h + a * mode).astype(np.float32).ravel(), mode=mode.ravel(), h=h, a=a, kx=kx, ky=ky)
+
+
+def scheme_frequency(kx: float, ky: float, dx: float, nz: int, g: float, dt: float):
+    """Frequency of the linear scheme for mode (kx, ky) and its symplectic half-step term
+    (tests_delta3d.rs:281-310): discrete horizontal eigenvalue, vertical structure of the
+    Neumann-bottom / half-cell-Dirichlet-lid problem (Thomas), symplectic Euler."""
+    kappa2 = 4.0 / (dx * dx) * (np.sin(kx * dx / 2.0) ** 2 + np.sin(ky * dx / 2.0) ** 2)
+    a = [0.0] * nz
+    b = [0.0] * nz
+    c = [0.0] * nz
+    d = [0.0] * nz
+    for k in range(nz):
+        diag = kappa2 * dx * dx
+        if k > 0:
+            diag += 1.0
+            a[k] = -1.0
+        if k + 1 < nz:
+            diag += 1.0
+            c[k] = -1.0
+        else:
+            diag += 2.0
+            d[k] = 2.0
+        b[k] = diag
+    for k in range(1, nz):
+        m = a[k] / b[k - 1]
+        b[k] -= m * c[k - 1]
+        d[k] -= m * d[k - 1]
+    phi = [0.0] * nz
+    phi[nz - 1] = d[nz - 1] / b[nz - 1]
+    for k in range(nz - 2, -1, -1):
+        phi[k] = (d[k] - c[k] * phi[k + 1]) / b[k]
+    ws2 = g * kappa2 * sum(x * dx for x in phi)
+    big = np.arccos(1.0 - ws2 * dt * dt / 2.0) / dt
+    return big, -ws2 * dt * dt / (2.0 * np.sin(big * dt))
+
+
+# ----------------------------------------------------------------------------------------------
 # Signed distances at the nodes, (nx+1)(ny+1)(nz+1) x-fastest, negative inside (delta3d.rs:322-327).
 
 def _node_grid(nx, ny, nz, dx):

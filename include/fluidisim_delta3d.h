@@ -134,6 +134,16 @@ int fd3_step_surface_mobile(fd3_volume* v, uint64_t duration_us, uint32_t max_it
 /* Volume3::last_refused_report (delta3d_mobile.rs:982); FD3_ERR_DOMAIN when none. */
 int fd3_last_refused_report(const fd3_volume* v, fd3_report* report);
 
+/* The linear (fixed-lid) path.  project (delta3d.rs:1060) of the current velocity field: us = u,
+ * then CG (or Jacobi-PCG on a cut bottom with ny > 1) with the lid at eta - z0, as
+ * tests_delta3d.rs:143-148 does.  The multigrid, when enabled, is not used on this path. */
+int fd3_project_linear(fd3_volume* v, float scale, float k1, uint32_t max_iters, fd3_report* report);
+/* Volume3::step_surface_linear (delta3d.rs:1209): project, then the heights from the column
+ * fluxes (compensated).  Refusal is atomic, as for the mobile step. */
+int fd3_step_surface_linear(fd3_volume* v, uint64_t duration_us, uint32_t max_iters, fd3_report* report);
+/* Volume3::set_precondition_cut (delta3d.rs:526): Jacobi on the linear cut path (default on). */
+int fd3_set_precondition_cut(fd3_volume* v, int on);
+
 /* Accessors (delta3d.rs:647-661) into caller buffers. */
 int fd3_get_pressure(const fd3_volume* v, float* out, size_t len);
 int fd3_get_velocity(const fd3_volume* v, float* u, size_t nu, float* vv, size_t nv, float* w, size_t nw);

@@ -7,7 +7,8 @@
 // It restates, function by function and in the same floating-point evaluation order, the Rust
 // reference (paths relative to the reference project):
 //   code/water-core/src/delta3d.rs           Domain3, Volume3 buffers, configure*, set_*, divergence*,
-//                                             dot/norm2, fingerprint
+//                                             dot/norm2, fingerprint, the linear path (lid, apply*,
+//                                             backward_error*, correct*, project, step_surface_linear)
 //   code/water-core/src/delta3d_mobile.rs    wet3/open3/solid3, ghosts, mobile_row, apply/rhs/backward
 //                                             error/correct/extrapolate/divergence, project_mobile3,
 //                                             advect/transport, step_surface_mobile, trial hooks
@@ -1400,6 +1401,337 @@ struct Volume3 {
     if (has_cut) prec_cut();
     return e;
   }
+
+  // ------------------------------------------------------------------ the linear (fixed-lid) path
+  // delta3d.rs:697-715.  The partial-lid branch needs a lid aperture strictly between 0 and 1,
+  // which only a hull piercing the lid produces; the linear step refuses any lid that is not fully
+  // open (delta3d.rs:1261-1268), so the fully open value is the one used here.
+  R lid(size_t i, size_t j) const {
+    size_t cc = col(i, j);
+    return rho * g_eff * ((eta[cc] - d.z0()) - eta_roundoff[cc]);
+  }
+
+  // apply (delta3d.rs:721-744) and apply_cut (:771-802): Neumann walls and bottom, homogeneous
+  // Dirichlet lid half a cell above the top layer; cut rows weighted by the apertures.
+  void apply_linear(const R* pp, R* out) const {
+    size_t nx = d.nx, ny = d.ny, nz = d.nz;
+    R inv = (R)1 / (d.dx * d.dx);
+    for_cells([&](size_t i, size_t j, size_t k) {
+      size_t cc = c(i, j, k);
+      if (!has_cut) {
+        R pc = pp[cc];
+        R acc = 0;
+        if (i > 0) acc += pc - pp[cc - 1];
+        if (i + 1 < nx) acc += pc - pp[cc + 1];
+        if (j > 0) acc += pc - pp[cc - nx];
+        if (j + 1 < ny) acc += pc - pp[cc + nx];
+        if (k > 0) acc += pc - pp[cc - nx * ny];
+        if (k + 1 < nz) acc += pc - pp[cc + nx * ny]; else acc += (R)2 * pc;
+        out[cc] = acc * inv;
+        return;
+      }
+      if (g.frac[cc] == 0) { out[cc] = 0; return; }
+      R acc = 0;
+      auto face = [&](R a, bool has, size_t m, bool top) {
+        if (a == 0) return;
+        if (has) { if (g.frac[m] > 0) acc += a * (pp[cc] - pp[m]); }
+        else if (top) acc += (R)2 * a * pp[cc];
+      };
+      face(g.open_u[fu(i, j, k)], i > 0, cc - 1, false);
+      face(g.open_u[fu(i + 1, j, k)], i + 1 < nx, cc + 1, false);
+      face(g.open_v[fv(i, j, k)], j > 0, cc - nx, false);
+      face(g.open_v[fv(i, j + 1, k)], j + 1 < ny, cc + nx, false);
+      face(g.open_w[fw(i, j, k)], k > 0, cc - nx * ny, false);
+      face(g.open_w[fw(i, j, k + 1)], k + 1 < nz, cc + nx * ny, true);
+      out[cc] = acc * inv;
+    });
+  }
+
+  // The right-hand side of project (delta3d.rs:1066-1086): scale * div, the lid value entering
+  // through the top layer, zero on solid cells.
+  void rhs_linear(R scale) {
+    size_t nz = d.nz;
+    R inv = (R)1 / (d.dx * d.dx);
+    for_cells([&](size_t i, size_t j, size_t k) {
+      size_t cc = c(i, j, k);
+      R b = scale * rhs[cc];
+      if (has_cut) {
+        if (g.frac[cc] == 0) b = 0;
+        else if (k + 1 == nz) {
+          R a = g.open_w[fw(i, j, k + 1)];
+          if (a > 0) b += (R)2 * a * lid(i, j) * inv;
+        }
+      } else if (k + 1 == nz) {
+        b += (R)2 * lid(i, j) * inv;
+      }
+      rhs[cc] = b;
+    });
+  }
+
+  // backward_error (delta3d.rs:881-907) and backward_error_cut (:909-945).
+  R backward_error_linear() const {
+    size_t nx = d.nx, ny = d.ny, nz = d.nz;
+    R inv = (R)1 / (d.dx * d.dx);
+    std::vector<R> part(nz, (R)0);
+#pragma omp parallel for schedule(static) num_threads(g_threads) if (nx * ny * nz > 32768)
+    for (long long kk = 0; kk < (long long)nz; ++kk) {
+      size_t k = (size_t)kk;
+      R worst = 0;
+      for (size_t j = 0; j < ny; ++j)
+        for (size_t i = 0; i < nx; ++i) {
+          size_t cc = c(i, j, k);
+          R pc = std::fabs(p[cc]);
+          R acc = 0;
+          if (!has_cut) {
+            if (i > 0) acc += pc + std::fabs(p[cc - 1]);
+            if (i + 1 < nx) acc += pc + std::fabs(p[cc + 1]);
+            if (j > 0) acc += pc + std::fabs(p[cc - nx]);
+            if (j + 1 < ny) acc += pc + std::fabs(p[cc + nx]);
+            if (k > 0) acc += pc + std::fabs(p[cc - nx * ny]);
+            if (k + 1 < nz) acc += pc + std::fabs(p[cc + nx * ny]); else acc += pc * (R)2;
+          } else {
+            if (g.frac[cc] == 0) continue;
+            auto face = [&](R a, bool has, size_t m, bool top) {
+              if (a == 0) return;
+              if (has) { if (g.frac[m] > 0) acc += a * (pc + std::fabs(p[m])); }
+              else if (top) acc += a * pc * (R)2;
+            };
+            face(g.open_u[fu(i, j, k)], i > 0, cc - 1, false);
+            face(g.open_u[fu(i + 1, j, k)], i + 1 < nx, cc + 1, false);
+            face(g.open_v[fv(i, j, k)], j > 0, cc - nx, false);
+            face(g.open_v[fv(i, j + 1, k)], j + 1 < ny, cc + nx, false);
+            face(g.open_w[fw(i, j, k)], k > 0, cc - nx * ny, false);
+            face(g.open_w[fw(i, j, k + 1)], k + 1 < nz, cc + nx * ny, true);
+          }
+          R scale = std::fabs(rhs[cc]) + acc * inv;
+          if (scale > 0) worst = rmax(worst, std::fabs(res[cc]) / scale);
+        }
+      part[k] = worst;
+    }
+    R worst = 0;
+    for (R x : part) worst = rmax(worst, x);
+    return worst;
+  }
+
+  // correct (delta3d.rs:949-987) and correct_cut (:989-1038).
+  void correct_linear(R k1) {
+    size_t nx = d.nx, ny = d.ny, nz = d.nz;
+    R dx = d.dx;
+    u = us; v = vs; w = ws;
+    for (size_t k = 0; k < nz; ++k)
+      for (size_t j = 0; j < ny; ++j)
+        for (size_t i = 1; i < nx; ++i) {
+          size_t f = fu(i, j, k), l = c(i - 1, j, k), r = c(i, j, k);
+          if (!has_cut || (g.open_u[f] != 0 && g.frac[l] > 0 && g.frac[r] > 0)) u[f] -= k1 * (p[r] - p[l]) / dx;
+        }
+    for (size_t k = 0; k < nz; ++k)
+      for (size_t j = 1; j < ny; ++j)
+        for (size_t i = 0; i < nx; ++i) {
+          size_t f = fv(i, j, k), a = c(i, j - 1, k), b = c(i, j, k);
+          if (!has_cut || (g.open_v[f] != 0 && g.frac[a] > 0 && g.frac[b] > 0)) v[f] -= k1 * (p[b] - p[a]) / dx;
+        }
+    for (size_t k = 1; k <= nz; ++k)
+      for (size_t j = 0; j < ny; ++j)
+        for (size_t i = 0; i < nx; ++i) {
+          size_t f = fw(i, j, k), below = c(i, j, k - 1);
+          if (has_cut && (g.open_w[f] == 0 || g.frac[below] == 0)) continue;
+          if (k < nz) {
+            size_t above = c(i, j, k);
+            if (!has_cut || g.frac[above] > 0) w[f] -= k1 * (p[above] - p[below]) / dx;
+          } else {
+            w[f] -= k1 * (lid(i, j) - p[below]) / ((R)0.5 * dx);
+          }
+        }
+  }
+
+  // divergence_metric (delta3d.rs:1043-1052): max|div u| dx / max|u|, every row plain.
+  double divergence_metric_linear() {
+    divergence(u.data(), v.data(), w.data(), tmp.data());
+    R dmax = 0;
+    for (R x : tmp) dmax = rmax(dmax, std::fabs(x));
+    R umax = 0;
+    for (R x : u) umax = rmax(umax, std::fabs(x));
+    for (R x : v) umax = rmax(umax, std::fabs(x));
+    for (R x : w) umax = rmax(umax, std::fabs(x));
+    R ratio = umax > 0 ? d.dx / umax : (R)0;
+    return (double)(dmax * ratio);
+  }
+
+  // project (delta3d.rs:1060-1196): CG from p = 0, or Jacobi-PCG on a cut bottom with ny > 1
+  // (precondition_cut, S326); the acceptance, tightening and floor logic of project_mobile3.
+  int project_linear(R scale, R k1, uint32_t max_iters, double rep[8]) {
+    divergence(us.data(), vs.data(), ws.data(), rhs.data());
+    rhs_linear(scale);
+    R b2;
+    int e = norm2(rhs.data(), b2);
+    if (e) return e;
+    std::fill(p.begin(), p.end(), (R)0);
+    res = rhs;
+    R rr = b2;
+    bool primed = false;
+    const bool jacobi = has_cut && precondition_cut && d.ny > 1;
+    R rz = 0;
+    uint32_t it = 0;
+    R tolr = (R)tol;
+    bool floor_stop = false;
+    R physical_target = std::numeric_limits<R>::infinity();
+    bool has_checkpoint = false;
+    uint64_t checkpoint = 0;
+    uint32_t power = 1, since = 0;
+    R actual_rr;
+    bool settled = false;
+    double settled_d = 0;
+    for (;;) {
+      uint32_t before = it;
+      while (b2 > 0 && (rr > tolr * b2 || rr > physical_target) && it < max_iters) {
+        if (!primed) {
+          if (jacobi) { if ((e = prime_mobile3(0, rz))) return e; }
+          else dir = res;
+          primed = true;
+        }
+        apply_linear(dir.data(), tmp.data());
+        R dq = dot(dir.data(), tmp.data());
+        if (!(dq > 0)) break;
+        R alpha = jacobi ? rz / dq : rr / dq;
+        for (size_t q = 0; q < p.size(); ++q) {
+          p[q] += alpha * dir[q];
+          res[q] -= alpha * tmp[q];
+        }
+        R rn;
+        if ((e = norm2(res.data(), rn))) return e;
+        if (jacobi) {
+          R zn;
+          if ((e = dot_prec3(zn))) return e;
+          R beta = zn / rz;
+          R dummy;
+          if ((e = prime_mobile3(beta, dummy))) return e;
+          rz = zn;
+        } else {
+          R beta = rn / rr;
+          for (size_t q = 0; q < dir.size(); ++q) dir[q] = res[q] + beta * dir[q];
+        }
+        rr = rn;
+        ++it;
+      }
+      apply_linear(p.data(), tmp.data());
+      for (size_t q = 0; q < res.size(); ++q) res[q] = rhs[q] - tmp[q];
+      R actual;
+      if ((e = norm2(res.data(), actual))) return e;
+      bool exhausted = it >= max_iters || it == before;
+      bool has_measured = false;
+      double measured = 0;
+      if (actual <= tolr * b2) {
+        if (exhausted) { actual_rr = actual; break; }
+        correct_linear(k1);
+        double reached = divergence_metric_linear();
+        if (reached <= PROJECTION_DIVERGENCE_TOLERANCE) { actual_rr = actual; settled = true; settled_d = reached; break; }
+        has_measured = true; measured = reached;
+        R ratio = (R)(PROJECTION_DIVERGENCE_TOLERANCE / reached);
+        physical_target = actual * ratio * ratio;
+      } else if (exhausted) {
+        actual_rr = actual; break;
+      }
+      if ((float)backward_error_linear() <= ROUNDOFF_BACKWARD_ERROR_3D) {
+        floor_stop = true; actual_rr = actual;
+        if (has_measured) { settled = true; settled_d = measured; }
+        break;
+      }
+      uint64_t state = fingerprint(p);
+      if (has_checkpoint && checkpoint == state) {
+        floor_stop = true; actual_rr = actual;
+        if (has_measured) { settled = true; settled_d = measured; }
+        break;
+      }
+      since += 1;
+      if (since == power) {
+        has_checkpoint = true; checkpoint = state;
+        power = power > 0x7fffffffu ? 0xffffffffu : power * 2;
+        since = 0;
+      }
+      rr = actual;
+      if (jacobi) { if ((e = prime_mobile3(0, rz))) return e; }
+      else dir = res;
+    }
+    R residual = b2 > 0 ? std::sqrt(actual_rr / b2) : (R)0;
+    double divergence_out;
+    if (settled) divergence_out = settled_d;
+    else { correct_linear(k1); divergence_out = divergence_metric_linear(); }
+    bool accepted = (actual_rr <= tolr * b2 || floor_stop) && divergence_out <= PROJECTION_DIVERGENCE_TOLERANCE;
+    rep[0] = 0;
+    rep[1] = (double)it;
+    rep[2] = (b2 > 0 && !accepted) ? 1.0 : 0.0;
+    rep[3] = (double)residual;
+    rep[4] = divergence_out;
+    rep[5] = floor_stop ? 1.0 : 0.0;
+    rep[6] = (double)backward_error_linear();
+    rep[7] = divergence_out;
+    return OK;
+  }
+
+  // step_surface_linear (delta3d.rs:1209-1253) and linear (:1255-1357), without a sponge or a
+  // graded column: pressure first, then the heights carried by the column fluxes.
+  int step_surface_linear(uint64_t duration_us, uint32_t max_iters, double rep[8]) {
+    if (duration_us == 0 || duration_us > (1ull << 53)) return NOT_FINITE;
+    double dt = (double)duration_us * 1e-6;
+    R dx = d.dx;
+    if (g_eff <= 0 || dt * dt * (double)g_eff / (double)dx > 1.) return DOMAIN;
+    R scale = (R)(-(double)rho / dt);
+    R correction = (R)(dt / (double)rho);
+    R transport = (R)(dt / (double)dx);
+    if (!std::isfinite(scale) || !std::isfinite(correction) || correction == 0 || !std::isfinite(transport) ||
+        transport == 0)
+      return NOT_FINITE;
+    saved_u = u; saved_v = v; saved_w = w; saved_p = p; saved_eta = eta; saved_eta_roundoff = eta_roundoff;
+    int e = [&]() -> int {
+      size_t nx = d.nx, ny = d.ny, nz = d.nz;
+      if (has_cut) {
+        for (size_t q = 0; q < nx * ny; ++q)
+          if (g.open_w[nz * nx * ny + q] != 1) return DOMAIN;
+      }
+      us = u; vs = v; ws = w;
+      int err = project_linear(scale, correction, max_iters, rep);
+      if (err) return err;
+      if (rep[2] != 0) return CONVERGENCE;
+      for (size_t j = 0; j < ny; ++j)
+        for (size_t i = 0; i <= nx; ++i) {
+          R q = 0;
+          for (size_t k = 0; k < nz; ++k) {
+            size_t f = fu(i, j, k);
+            if (has_cut) q += g.open_u[f] * u[f] * dx; else q += u[f] * dx;
+          }
+          flux_x[j * (nx + 1) + i] = q;
+        }
+      for (size_t j = 0; j <= ny; ++j)
+        for (size_t i = 0; i < nx; ++i) {
+          R q = 0;
+          for (size_t k = 0; k < nz; ++k) {
+            size_t f = fv(i, j, k);
+            if (has_cut) q += g.open_v[f] * v[f] * dx; else q += v[f] * dx;
+          }
+          flux_y[j * nx + i] = q;
+        }
+      for (size_t j = 0; j < ny; ++j)
+        for (size_t i = 0; i < nx; ++i) {
+          R left = flux_x[j * (nx + 1) + i], right = flux_x[j * (nx + 1) + i + 1];
+          R front = flux_y[j * nx + i], back = flux_y[(j + 1) * nx + i];
+          size_t cc = col(i, j);
+          R increment = -transport * ((right - left) + (back - front)) - eta_roundoff[cc];
+          R height = eta[cc] + increment;
+          eta_roundoff[cc] = (height - eta[cc]) - increment;
+          eta[cc] = height;
+        }
+      const std::vector<R>* fields[] = {&u, &v, &w, &p, &eta, &eta_roundoff, &rhs, &res, &dir, &tmp};
+      for (auto f : fields)
+        for (R x : *f)
+          if (!std::isfinite(x)) return NOT_FINITE;
+      if (!std::isfinite(rep[3]) || !std::isfinite(rep[4])) return NOT_FINITE;
+      return OK;
+    }();
+    if (e) {
+      u = saved_u; v = saved_v; w = saved_w; p = saved_p; eta = saved_eta; eta_roundoff = saved_eta_roundoff;
+    }
+    return e;
+  }
 };
 
 // delta3d.rs:210-294
@@ -1568,6 +1900,26 @@ int od3_project_mobile(Volume3* v, float scale, float k1, uint32_t max_iters, do
   if (!v || !rep) return INVALID;
   v->us = v->u; v->vs = v->v; v->ws = v->w;
   return v->project_mobile3((R)scale, (R)k1, max_iters, rep);
+}
+
+// Projects the current velocity field on the linear (fixed-lid) path: us = u, then project
+// (tests_delta3d.rs:143-148).
+int od3_project_linear(Volume3* v, float scale, float k1, uint32_t max_iters, double rep[8]) {
+  if (!v || !rep) return INVALID;
+  v->us = v->u; v->vs = v->v; v->ws = v->w;
+  return v->project_linear((R)scale, (R)k1, max_iters, rep);
+}
+
+int od3_step_surface_linear(Volume3* v, uint64_t duration_us, uint32_t max_iters, double rep[8]) {
+  if (!v || !rep) return INVALID;
+  return v->step_surface_linear(duration_us, max_iters, rep);
+}
+
+// set_precondition_cut (delta3d.rs:526-528).
+int od3_set_precondition_cut(Volume3* v, int on) {
+  if (!v) return INVALID;
+  v->precondition_cut = on != 0;
+  return OK;
 }
 
 int od3_step_surface_mobile(Volume3* v, uint64_t duration_us, uint32_t max_iters, double rep[8]) {

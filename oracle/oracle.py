@@ -87,6 +87,11 @@ def lib(real: str = "f32") -> C.CDLL:
     L.od3_set_threads.argtypes = [C.c_int]
     L.od3_set_threads.restype = None
     L.od3_max_threads.restype = C.c_int
+    L.od3_set_smoother.argtypes = [C.c_int]
+    L.od3_set_smoother.restype = None
+    L.od3_project_linear.argtypes = [vp, f32, f32, u32, dp]
+    L.od3_step_surface_linear.argtypes = [vp, u64, u32, dp]
+    L.od3_set_precondition_cut.argtypes = [vp, C.c_int]
     _LIBS[real] = L
     return L
 
@@ -204,6 +209,21 @@ class OracleVolume:
         rep = (C.c_double * 8)()
         self._check(self.L.od3_step_surface_mobile(self.h, duration_us, max_iters, rep), "step_surface_mobile")
         return report_dict(rep)
+
+    def project_linear(self, scale, k1, max_iters=4000) -> dict:
+        """project (delta3d.rs:1060-1196) of the current velocity field, as tests_delta3d.rs:143-148."""
+        rep = (C.c_double * 8)()
+        self._check(self.L.od3_project_linear(self.h, np.float32(scale), np.float32(k1), max_iters, rep),
+                    "project_linear")
+        return report_dict(rep)
+
+    def step_surface_linear(self, duration_us, max_iters=4000) -> dict:
+        rep = (C.c_double * 8)()
+        self._check(self.L.od3_step_surface_linear(self.h, duration_us, max_iters, rep), "step_surface_linear")
+        return report_dict(rep)
+
+    def set_precondition_cut(self, on: bool):
+        self._check(self.L.od3_set_precondition_cut(self.h, 1 if on else 0), "set_precondition_cut")
 
     def last_refused_report(self):
         rep = (C.c_double * 8)()

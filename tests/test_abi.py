@@ -19,6 +19,7 @@ def test_header_declares_the_volume3_api():
     names = declared_symbols()
     for want in ["fd3_configure", "fd3_configure_with_bottom", "fd3_configure_with_solid", "fd3_enable_multigrid",
                  "fd3_set_free_surface", "fd3_set_velocity", "fd3_project_mobile", "fd3_step_surface_mobile",
+                 "fd3_project_linear", "fd3_step_surface_linear",
                  "fd3_get_pressure", "fd3_get_velocity", "fd3_apply_pressure_operator_for_trials",
                  "fd3_assemble_pressure_problem_for_trials", "fd3_destroy"]:
         assert want in names
