@@ -18,6 +18,7 @@ fits one GPU), one per rank, timed on the device, max over ranks.
 from __future__ import annotations
 
 import argparse
+import functools
 import json
 import os
 import statistics
@@ -188,9 +189,18 @@ def max_over_ranks(x: float, world: int) -> float:
     return float(t.item())
 
 
-def make_scene(size: int):
+@functools.lru_cache(maxsize=2)
+def make_scene(workload: str, size: int):
     from fluidisim_b200 import scenes
+    if workload == "wave":
+        return scenes.breaking_wave(size)
     return scenes.box_basin(size)
+
+
+WORKLOAD_NAMES = {
+    "basin": "box_basin {n}^3 (16 boxes, sinusoidal surface, curl background + N(0,0.5) noise)",
+    "wave": "breaking_wave {n}^3 (32 obstacles, tanh surface, 2 m/s crest + N(0,0.3) noise)",
+}
 
 
 def run_reference(args):
@@ -204,7 +214,7 @@ def run_reference(args):
     O.build()
     threads = O.max_threads()
     O.set_threads(threads)
-    s = make_scene(args.size)
+    s = make_scene(args.workload, args.size)
     scale, k1 = scenes.projection_scalars(s)
     v = O.OracleVolume(s["nx"], s["ny"], s["nz"], s["dx"], s["rho"], s["g"], bottom=s["bottom"], solid=s["solid"])
     v.enable_multigrid()
@@ -230,8 +240,9 @@ def run_reference(args):
     out = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "projections/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded box_basin scene)",
-        "config": {"workload": f"box_basin {args.size}^3 multigrid-PCG projection (reference recipe)",
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": f"synthetic (seeded {args.workload} scene)",
+        "config": {"workload": WORKLOAD_NAMES[args.workload].format(n=args.size)
+                   + ": multigrid-PCG projection (reference recipe)",
                    "cells": s["nx"] * s["ny"] * s["nz"], "solver": "mgpcg", "iterations": rep["iterations"],
                    "rel_residual": rep["residual"], "parallelism": "host threads"},
         "cpu_baseline": {"value": value, "unit": "projections/s", "cores": threads, "kind": "port",
@@ -242,14 +253,14 @@ def run_reference(args):
     print(json.dumps(out), flush=True)
 
 
-def cpu_baseline_sample(size: int, budget_s: float = 20.0):
+def cpu_baseline_sample(workload: str, size: int, budget_s: float = 20.0):
     """The oracle (OpenMP on every host core) timed on a bounded sample of the same workload."""
     from fluidisim_b200 import scenes
     from oracle import oracle as O
     O.build()
     threads = O.max_threads()
     O.set_threads(threads)
-    s = make_scene(size)
+    s = make_scene(workload, size)
     scale, k1 = scenes.projection_scalars(s)
     v = O.OracleVolume(s["nx"], s["ny"], s["nz"], s["dx"], s["rho"], s["g"], bottom=s["bottom"], solid=s["solid"])
     v.enable_multigrid()
@@ -263,7 +274,7 @@ def cpu_baseline_sample(size: int, budget_s: float = 20.0):
         times.append(time.perf_counter() - t0)
     ms = 1e3 * sum(times) / len(times)
     return {"value": 1e3 / ms, "unit": "projections/s", "cores": threads, "kind": "port",
-            "sample": f"{len(times)} full {size}^3 projections (same scene), oracle with OpenMP"}
+            "sample": f"{len(times)} full {size}^3 {workload} projections (same scene), oracle with OpenMP"}
 
 
 def run_b200(args):
@@ -276,7 +287,7 @@ def run_b200(args):
 
     rank, world, local = dist_setup(args.gpus)
     B.build()
-    s = make_scene(args.size)
+    s = make_scene(args.workload, args.size)
     scale, k1 = scenes.projection_scalars(s)
     stream = torch.cuda.Stream()
     vol = Volume3.configure_with_solid(s["nx"], s["ny"], s["nz"], s["dx"], s["rho"], s["g"], s["bottom"], s["solid"])
@@ -391,7 +402,7 @@ def run_b200(args):
     peak, peak_kind = peaks()
     achieved = alg_bytes / (avg_ms * 1e-3) / 1e9
     ncu_traffic = None
-    traffic_file = os.path.join(ROOT, "profiles", f"traffic_box_basin_{args.size}.txt")
+    traffic_file = os.path.join(ROOT, "profiles", f"traffic_{args.workload}_{args.size}.txt")
     if os.path.exists(traffic_file):
         with open(traffic_file) as f:
             for line in f:
@@ -400,12 +411,13 @@ def run_b200(args):
                     ncu_traffic = float(parts[1])
 
     if rank == 0:
-        cpu = cpu_baseline_sample(args.size) if (world == 1 and not args.no_cpu) else None
+        cpu = cpu_baseline_sample(args.workload, args.size) if (world == 1 and not args.no_cpu) else None
         out = {
             "impl": "b200", "metric": METRIC, "value": value, "unit": "projections/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded box_basin scene)",
-            "config": {"workload": f"box_basin {args.size}^3 multigrid-PCG projection (reference V-cycle recipe)",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": f"synthetic (seeded {args.workload} scene)",
+            "config": {"workload": WORKLOAD_NAMES[args.workload].format(n=args.size)
+                       + ": multigrid-PCG projection (reference V-cycle recipe)",
                        "cells": cells, "solver": "mgpcg", "reduction": "f64", "iterations": rep.iterations,
                        "rel_residual": rep.residual, "divergence_plain": rep.divergence_plain,
                        "l2": "flushed between steps (256 MiB write outside the timed events)",
@@ -435,12 +447,16 @@ def main():
     ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--size", type=int, default=128)
+    ap.add_argument("--workload", default="basin", choices=["basin", "wave"],
+                    help="basin: the 128^3 box basin the metric is quoted on; wave: the 256^3 breaking wave")
+    ap.add_argument("--size", type=int, default=None, help="grid side (default 128 for basin, 256 for wave)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--graphs", type=int, default=1,
                     help="1: the inner loop as a CUDA graph with a WHILE node; 0: host-driven (for ncu launch lists)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.size is None:
+        args.size = 256 if args.workload == "wave" else 128
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -315,6 +315,59 @@ def box_basin(n: int = 128, seed: int = 2, dx: float = 0.1, boxes: int = 16, noi
                 w=w.astype(np.float32), dt=1.0 / 60.0)
 
 
+def breaking_wave(n: int = 256, seed: int = 5, dx: float = 0.1, obstacles: int = 32, crest_speed: float = 2.0,
+                  noise_sigma: float = 0.3) -> dict:
+    """n^3 breaking-wave state: h = 0.4 n + 0.15 n tanh((x - x0)/8) (1 + 0.1 sin(y/5)) cells (x, y in
+    cells, x0 = n/2; one height per column, the reference's vertical axis being z), `obstacles`
+    random submerged solids (spheres and boxes alternately, clear of the walls and 4 cells below
+    the lowest surface), u = crest_speed m/s on the wet u faces of the crest (the columns with
+    h > 0.45 n) plus i.i.d. N(0, noise_sigma) m/s on every face."""
+    rng = SplitMix64(seed)
+    d = float(f32(dx))
+    i = np.arange(n) + 0.5
+    X, Y = np.meshgrid(i, i, indexing="xy")
+    x0 = 0.5 * n
+    h = 0.4 * n + 0.15 * n * np.tanh((X - x0) / 8.0) * (1.0 + 0.1 * np.sin(Y / 5.0))
+    hmin = float(h.min())
+    eta = (h * d).astype(np.float32).ravel()
+    top_limit = hmin - 4.0
+    sph_c, sph_r, box_c, box_h = [], [], [], []
+    for q in range(obstacles):
+        if q % 2 == 0:
+            r = rng.uniform(3.0, 8.0)
+            cx = rng.uniform(r + 1.0, n - r - 1.0)
+            cy = rng.uniform(r + 1.0, n - r - 1.0)
+            cz = rng.uniform(r + 1.0, max(r + 1.5, top_limit - r))
+            sph_c.append((cx * d, cy * d, cz * d))
+            sph_r.append(r * d)
+        else:
+            hx, hy, hz = rng.uniform(2.0, 8.0), rng.uniform(2.0, 8.0), rng.uniform(2.0, 6.0)
+            cx = rng.uniform(hx + 1.0, n - hx - 1.0)
+            cy = rng.uniform(hy + 1.0, n - hy - 1.0)
+            cz = rng.uniform(hz + 1.0, max(hz + 1.5, top_limit - hz))
+            box_c.append((cx * d, cy * d, cz * d))
+            box_h.append((hx * d, hy * d, hz * d))
+    sdf = np.minimum(spheres_sdf(n, n, n, dx, sph_c, sph_r), boxes_sdf(n, n, n, dx, box_c, box_h))
+    nu, nv, nw = face_counts(n, n, n)
+    # u faces (i, j, k), x = i: crest columns on either side, wet below the surface
+    crest = h > 0.45 * n
+    col_crest = np.zeros((n, n + 1), bool)
+    col_crest[:, :n] |= crest
+    col_crest[:, 1:] |= crest
+    zc = (np.arange(n) + 0.5)[:, None, None]
+    hh = np.zeros((n, n + 1))
+    hh[:, :n] = h
+    hh[:, n] = h[:, n - 1]
+    wet_u = zc < hh[None, :, :]
+    u = np.where(col_crest[None, :, :] & wet_u, crest_speed, 0.0).astype(np.float32).ravel()
+    u = u + rng.normal_array(nu, noise_sigma)
+    v = rng.normal_array(nv, noise_sigma)
+    w = rng.normal_array(nw, noise_sigma)
+    return dict(nx=n, ny=n, nz=n, dx=float(f32(dx)), rho=1025.0, g=9.81, bottom=np.zeros(n * n, np.float32),
+                solid=sdf.astype(np.float32), eta=eta, rest=float(f32(0.4 * n * d)), u=u.astype(np.float32),
+                v=v.astype(np.float32), w=w.astype(np.float32), dt=1.0 / 60.0)
+
+
 def projection_scalars(scene: dict):
     """(scale, k1) of a projection with the scene's dt: -rho/dt and dt/rho, rounded to f32 as
     step_surface_mobile does (delta3d_mobile.rs:838-840)."""
