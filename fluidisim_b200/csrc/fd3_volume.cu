@@ -98,6 +98,9 @@ struct fd3_volume {
   Scalars* hS = nullptr;  // pinned
   int* dflag = nullptr;
   int* hflag = nullptr;   // pinned
+  double* fsc = nullptr;  // dot products of the learned FCG and the training hooks
+  double* hfsc = nullptr; // pinned
+  float *fz = nullptr, *fin = nullptr;  // FCG preconditioned residual and network input (on first use)
   fd3_options opt{};
   bool has_refused = false;
   fd3_report refused{};
@@ -158,6 +161,7 @@ void release(fd3_volume* V) {
   for (void* q : V->allocations) cudaFree(q);
   if (V->hS) cudaFreeHost(V->hS);
   if (V->hflag) cudaFreeHost(V->hflag);
+  if (V->hfsc) cudaFreeHost(V->hfsc);
   if (V->own_stream) cudaStreamDestroy(V->own_stream);
 }
 
@@ -688,6 +692,8 @@ int alloc_state(fd3_volume* V) {
   TRY(dalloc(V, &q, 16)); V->dflag = (int*)q;
   CK(cudaMallocHost((void**)&V->hS, sizeof(Scalars)));
   CK(cudaMallocHost((void**)&V->hflag, sizeof(int)));
+  TRY(dalloc(V, &q, 32)); V->fsc = (double*)q;
+  CK(cudaMallocHost((void**)&V->hfsc, 8 * sizeof(double)));
   memset(V->hS, 0, sizeof(Scalars));
   // eta = z0 everywhere (delta3d.rs:255)
   std::vector<float> z0(V->ncol, V->z0);
@@ -1335,6 +1341,9 @@ int fd3_profile_entry(const fd3_volume* V, int idx, char* name, size_t len, uint
 }
 
 }  // extern "C"
+
+// =============================================================================== learned preconditioner
+#include "fd3_learned.cuh"
 
 // =============================================================================== no-alloc entry
 // fd3_assemble_pressure_problem_noalloc: the assembly of the pressure problem (rhs_mobile3 with

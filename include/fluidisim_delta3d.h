@@ -194,6 +194,49 @@ int fd3_profile_count(const fd3_volume* v);
 int fd3_profile_entry(const fd3_volume* v, int index, char* name, size_t name_len, uint64_t* launches,
                       double* total_ms);
 
+/* ------------------------------------------------------------------ learned preconditioner
+ * No reference counterpart: the learned part of the B200 build.  A 3-D U-Net (3 levels, 16/32/64
+ * channels, 3x3x3 convolutions, BF16 with FP32 accumulation) used as the preconditioner of a
+ * flexible CG, with the multigrid PCG of fd3_project_mobile as its fallback. */
+typedef struct fd3_unet fd3_unet;
+
+/* A network whose buffers hold max_batch samples of nz x ny x nx cells (each a multiple of 4). */
+int fd3_unet_create(int max_batch, int nz, int ny, int nx, fd3_unet** out);
+void fd3_unet_destroy(fd3_unet* net);
+int fd3_unet_set_stream(fd3_unet* net, void* stream);
+/* Parameters, f32, per layer (e0, e1, b, d1, d0, head): w[27][cout][cin] then b[cout]. */
+uint64_t fd3_unet_param_count(const fd3_unet* net);
+int fd3_unet_set_params(fd3_unet* net, const float* params, size_t len);
+int fd3_unet_get_params(const fd3_unet* net, float* params, size_t len);
+/* The accumulated parameter gradient (then cleared). */
+int fd3_unet_get_grads(fd3_unet* net, float* grads, size_t len);
+/* y = out_scale[b] * net(x), x[b*cells + c][3] = (residual * in_scale[b], solid, liquid); device
+ * pointers x and y, host arrays of B scales.  Stream-ordered. */
+int fd3_unet_forward(fd3_unet* net, int batch, int nz, int ny, int nx, const float* d_in, const float* in_scale,
+                     const float* out_scale, float* d_out);
+/* Accumulates the parameter gradient of the last forward for dL/dy = d_gout (device). */
+int fd3_unet_backward(fd3_unet* net, const float* d_gout);
+/* Adam step on the accumulated gradient (consumed). */
+int fd3_unet_adam(fd3_unet* net, float lr, float beta1, float beta2, float eps);
+int fd3_unet_sync(fd3_unet* net);
+uint64_t fd3_unet_kernel_launches(const fd3_unet* net);
+
+/* Device-side hooks of a training loop, on a volume: the rhs and row codes of project_mobile3 for
+ * the current velocity (us = u), their device pointers, A x, the network input of a residual
+ * (and its squared norm), and loss = w |A z - b|^2 with d_grad = 2 w A (A z - b). */
+int fd3_assemble_device(fd3_volume* v, float scale);
+int fd3_problem_device(fd3_volume* v, float** d_rhs, const unsigned short** d_codes);
+int fd3_apply_device(fd3_volume* v, const float* d_x, float* d_out);
+int fd3_learned_input(fd3_volume* v, const float* d_r, float* d_in3, double* rr);
+int fd3_residual_loss(fd3_volume* v, const float* d_z, const float* d_b, float weight, float* d_grad, double* loss);
+
+/* project_mobile3 with the learned FCG in front (from the current p): FCG(1) with the network as
+ * the preconditioner until the reference tolerance, max_fcg iterations or a stall, then the
+ * reference acceptance loop, whose multigrid PCG continues from FCG's p when needed.  report is
+ * that loop's (its iterations are the fallback's); fcg_iterations and fell_back describe FCG. */
+int fd3_project_learned(fd3_volume* v, fd3_unet* net, float scale, float k1, uint32_t max_iters, uint32_t max_fcg,
+                        fd3_report* report, uint32_t* fcg_iterations, int* fell_back);
+
 #ifdef __cplusplus
 }
 #endif
