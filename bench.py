@@ -277,6 +277,108 @@ def cpu_baseline_sample(workload: str, size: int, budget_s: float = 20.0):
             "sample": f"{len(times)} full {size}^3 {workload} projections (same scene), oracle with OpenMP"}
 
 
+def learned_fcg_measure(args, s, vol_plain_p, stream):
+    """The learned preconditioner, measured in the same run: training throughput at 64^3 (batch
+    32, sphere-lake scenes with seeded random velocities), the validation FCG iteration count on
+    held-out lakes, and learned-FCG projections/s on the bench scene (device-resident inputs, the
+    same L2 flush), with its fallback work and its pressure against plain MGPCG's."""
+    import numpy as np
+    import torch
+
+    from fluidisim_b200 import learned, scenes
+    from fluidisim_b200.delta3d import REDUCE_F64, Volume3
+
+    def lake(seed):
+        sc = scenes.sphere_lake(64, seed=seed)
+        v = Volume3.configure_with_solid(sc["nx"], sc["ny"], sc["nz"], sc["dx"], sc["rho"], sc["g"], sc["bottom"],
+                                         sc["solid"])
+        v.set_options(reduction=REDUCE_F64)
+        v.enable_multigrid()
+        v.set_free_surface(sc["eta"], sc["rest"])
+        return v, sc
+
+    train = [lake(1000 + q)[0] for q in range(8)]
+    sc0 = scenes.sphere_lake(64, seed=1000)
+    tscale, _ = scenes.projection_scalars(sc0)
+    net = learned.UNet(32, 64, 64, 64)
+    net.set_params(learned.init_params(0))
+    tr = learned.Trainer(net, train, tscale, batch=32, seed=1)
+    rng = np.random.default_rng(0)
+    steps = max(1, args.train_samples // 32)
+    tr.step(1e-3, rng)  # warm-up (kernel load)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    losses = [tr.step(1e-3 if q < 0.7 * steps else 3e-4, rng) for q in range(steps)]
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    params = net.params()
+    net.close()
+    # validation on held-out lakes: FCG + fallback iterations against plain MGPCG's
+    vnet = learned.UNet(1, 64, 64, 64)
+    vnet.set_params(params)
+    val = []
+    for seed in (2000, 2001):
+        v, sc = lake(seed)
+        v.set_velocity(sc["u"], sc["v"], sc["w"])
+        sc_s, sc_k = scenes.projection_scalars(sc)
+        r = learned.project_learned(v, vnet, sc_s, sc_k, 4000, 200)
+        ref, _ = lake(seed)
+        ref.set_velocity(sc["u"], sc["v"], sc["w"])
+        rr = ref.project_mobile3(sc_s, sc_k, 4000)
+        val.append({"fcg": r.fcg_iterations, "fallback_mg": r.report.iterations, "fell_back": r.fell_back,
+                    "plain_mgpcg": rr.iterations, "residual": r.report.residual})
+    vnet.close()
+    # the bench scene
+    n = s["nx"]
+    inet = learned.UNet(1, s["nz"], s["ny"], s["nx"])
+    inet.set_params(params)
+    scale, k1 = scenes.projection_scalars(s)
+    lv = Volume3.configure_with_solid(s["nx"], s["ny"], s["nz"], s["dx"], s["rho"], s["g"], s["bottom"], s["solid"])
+    lv.set_options(reduction=REDUCE_F64)
+    lv.set_stream(stream.cuda_stream)
+    lv.enable_multigrid()
+    lv.set_free_surface(s["eta"], s["rest"])
+    du = torch.from_numpy(s["u"]).cuda()
+    dv = torch.from_numpy(s["v"]).cuda()
+    dw = torch.from_numpy(s["w"]).cuda()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+
+    def step():
+        lv.set_velocity_device(du.data_ptr(), dv.data_ptr(), dw.data_ptr())
+        lv.reset_pressure()
+        return learned.project_learned(lv, inet, scale, k1, 4000, 100)
+
+    for _ in range(2):
+        step()
+    K = max(3, min(args.steps, 20))
+    ms, rep = [], None
+    for _ in range(K):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        rep = step()
+        b.record(stream)
+        torch.cuda.synchronize()
+        ms.append(a.elapsed_time(b))
+    p = lv.pressure()
+    dp = float(np.max(np.abs(p - vol_plain_p)) / max(np.max(np.abs(vol_plain_p)), 1e-30))
+    inet.close()
+    lv.close()
+    return {
+        "metric_value": K / (sum(ms) * 1e-3), "unit": "projections/s", "ms_per_projection": sum(ms) / K,
+        "fcg_iterations": rep.fcg_iterations, "fallback_mg_iterations": rep.report.iterations,
+        "fell_back": rep.fell_back, "rel_residual": rep.report.residual,
+        "divergence_plain": rep.report.divergence_plain, "pressure_linf_vs_plain_mgpcg": dp,
+        "network": "3-level U-Net 16/32/64, 3x3x3 convs, BF16 storage / FP32 accumulation (mma.sync m16n8k16)",
+        "training": {"samples": steps * 32, "batch": 32, "grid": "64^3 sphere lakes (8 geometries)",
+                     "samples_per_s": steps * 32 / train_s, "seconds": train_s,
+                     "loss_first": float(np.mean(losses[:3])), "loss_last": float(np.mean(losses[-3:]))},
+        "validation_64": val,
+    }
+
+
 def run_b200(args):
     import numpy as np
     import torch
@@ -410,6 +512,11 @@ def run_b200(args):
                 if len(parts) == 2 and not line.startswith("#") and parts[0] == name:
                     ncu_traffic = float(parts[1])
 
+    learned_line = None
+    if world == 1 and args.learned:
+        plain_p = vol.pressure()
+        learned_line = learned_fcg_measure(args, s, plain_p, stream)
+
     if rank == 0:
         cpu = cpu_baseline_sample(args.workload, args.size) if (world == 1 and not args.no_cpu) else None
         out = {
@@ -433,6 +540,7 @@ def run_b200(args):
             "e2e": {"value": e2e_value, "unit": "projections/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,
             "clocks": clocks.summary(),
+            "learned_fcg": learned_line,
         }
         print(json.dumps(out), flush=True)
     vol.close()
@@ -451,6 +559,9 @@ def main():
                     help="basin: the 128^3 box basin the metric is quoted on; wave: the 256^3 breaking wave")
     ap.add_argument("--size", type=int, default=None, help="grid side (default 128 for basin, 256 for wave)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    ap.add_argument("--learned", type=int, default=1,
+                    help="1: also train the learned preconditioner and time learned-FCG projections (N=1 only)")
+    ap.add_argument("--train-samples", type=int, default=4096, help="training samples of the learned preconditioner")
     ap.add_argument("--graphs", type=int, default=1,
                     help="1: the inner loop as a CUDA graph with a WHILE node; 0: host-driven (for ncu launch lists)")
     args = ap.parse_args()
