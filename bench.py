@@ -549,14 +549,155 @@ def run_b200(args):
         dist.destroy_process_group()
 
 
+def snake_owner(k: int, world: int) -> int:
+    """Rank of the k-th patch in decreasing cost: 0, 1, ..., w-1, w-1, ..., 0, 0, 1, ..."""
+    q, r = divmod(k, world)
+    return r if q % 2 == 0 else world - 1 - r
+
+
+def run_patches(args):
+    """Batched patches: every rank projects its share of the seeded patch set (dealt by decreasing
+    size) through fd3_project_batch, after the autotuner has picked the options per size class.
+    No data-path collective: only the timing max and a count reduction."""
+    import numpy as np
+    import torch
+
+    from fluidisim_b200 import batch, scenes
+    from fluidisim_b200 import build as B
+
+    rank, world, local = dist_setup(args.gpus)
+    B.build()
+    ps = batch.patch_scenes(args.patches, seed=3)
+    cells = [p["nx"] * p["ny"] * p["nz"] for p in ps]
+    order = sorted(range(len(ps)), key=lambda i: -cells[i])
+    mine = [ps[i] for k, i in enumerate(order) if snake_owner(k, world) == rank]
+    tuned = batch.autotune(batch.by_class(mine))
+    vols, inputs, sk = [], [], []
+    for p in mine:
+        t = tuned[batch.size_class(p["nx"] * p["ny"] * p["nz"])]
+        vols.append(batch.configure(p, t.kernels, t.levels))
+        inputs.append(tuple(torch.from_numpy(p[k]).cuda() for k in ("u", "v", "w")))
+        sk.append(scenes.projection_scalars(p))
+    torch.cuda.synchronize()
+    scales, k1s = [a for a, _ in sk], [b for _, b in sk]
+
+    def step():
+        for v, (du, dv, dw) in zip(vols, inputs):
+            v.set_velocity_device(du.data_ptr(), dv.data_ptr(), dw.data_ptr())
+            v.reset_pressure()
+        return batch.project_batch(vols, scales, k1s, threads=args.threads)
+
+    for _ in range(args.warmup):
+        reps, st = step()
+    torch.cuda.synchronize()
+    barrier(world)
+    ms = []
+    with ClockSampler(local) as clocks:
+        clocks.mark(True)
+        for _ in range(args.steps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            reps, st = step()
+            b.record()
+            torch.cuda.synchronize()
+            ms.append(a.elapsed_time(b))
+        clocks.mark(False)
+    assert all(x == 0 for x in st), st
+    ms_total = max_over_ranks(sum(ms), world)
+    my_ci = sum(p["nx"] * p["ny"] * p["nz"] * r.iterations for p, r in zip(mine, reps))
+    ci = my_ci
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([float(my_ci)], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t)
+        ci = float(t.item())
+    its = [r.iterations for r in reps]
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu:
+            cpu = cpu_patches_sample(ps)
+        out = {
+            "impl": "b200", "metric": f"patches/s ({args.patches} seeded delta patches, 16-96 cells per side)",
+            "value": args.steps * len(ps) / (ms_total * 1e-3), "unit": "patches/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_total / args.steps,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded patch set)",
+            "config": {"workload": f"{args.patches} patches: sides log-uniform in [16,96] rounded to 8, spheres "
+                                   f"5-15% of cells, fill U[0.3,0.8], faces U[-1,1]; one fd3_project_batch per step",
+                       "cells_total": sum(cells), "parallelism": f"patches sharded x{world}",
+                       "autotuned": {k: {"kernels": v.kernels, "mg_max_levels": v.levels, "ms": round(v.ms, 3)}
+                                     for k, v in tuned.items()},
+                       "iterations_rank0": {"min": min(its), "max": max(its), "mean": float(np.mean(its))},
+                       "l2": "inputs restored each step; the patch set exceeds L2"},
+            "cells_iterations_per_s": args.steps * ci / (ms_total * 1e-3),
+            "cpu_baseline": cpu,
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(out), flush=True)
+    for v in vols:
+        v.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def run_reference_patches(args):
+    """The reference arm of the patches workload: the oracle projects the patch set one patch at a
+    time on the host cores (the reference has no batched path); bounded to 90 s."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from fluidisim_b200 import batch
+    ps = batch.patch_scenes(args.patches, seed=3)
+    cpu = cpu_patches_sample(ps, budget_s=90.0)
+    out = {"impl": "reference", "metric": f"patches/s ({args.patches} seeded delta patches, 16-96 cells per side)",
+           "value": cpu["value"], "unit": "patches/s", "n_gpus": args.gpus, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": 1e3 * args.patches / cpu["value"], "higher_is_better": True,
+           "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded patch set)",
+           "config": {"workload": f"{args.patches} patches (see the b200 arm)", "parallelism": "host threads"},
+           "cpu_baseline": cpu,
+           "e2e": {"value": cpu["value"], "unit": "patches/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def cpu_patches_sample(ps, budget_s: float = 20.0):
+    """The oracle (OpenMP) on the patches in order until the budget is spent: patches/s and
+    cells x iterations / s of that sample."""
+    from fluidisim_b200 import scenes
+    from oracle import oracle as O
+    O.build()
+    threads = O.max_threads()
+    O.set_threads(threads)
+    t0 = time.perf_counter()
+    done, ci = 0, 0
+    for p in ps:
+        v = O.OracleVolume(p["nx"], p["ny"], p["nz"], p["dx"], p["rho"], p["g"], bottom=p["bottom"], solid=p["solid"])
+        v.enable_multigrid()
+        v.set_free_surface(p["eta"], p["rest"])
+        v.set_velocity(p["u"], p["v"], p["w"])
+        scale, k1 = scenes.projection_scalars(p)
+        r = v.project_mobile(scale, k1, 4000)
+        done += 1
+        ci += p["nx"] * p["ny"] * p["nz"] * r["iterations"]
+        if time.perf_counter() - t0 > budget_s:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": done / dt, "unit": "patches/s", "cores": threads, "kind": "port",
+            "cells_iterations_per_s": ci / dt,
+            "sample": f"the first {done} patches of the set, oracle with OpenMP (setup excluded)"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="basin", choices=["basin", "wave"],
-                    help="basin: the 128^3 box basin the metric is quoted on; wave: the 256^3 breaking wave")
+    ap.add_argument("--workload", default="basin", choices=["basin", "wave", "patches"],
+                    help="basin: the 128^3 box basin the metric is quoted on; wave: the 256^3 breaking wave; "
+                         "patches: the batched delta patches")
+    ap.add_argument("--patches", type=int, default=256, help="patch count of the patches workload")
+    ap.add_argument("--threads", type=int, default=0, help="host workers of fd3_project_batch (0 = up to 16)")
     ap.add_argument("--size", type=int, default=None, help="grid side (default 128 for basin, 256 for wave)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--learned", type=int, default=1,
@@ -568,7 +709,12 @@ def main():
     args.warmup = max(args.warmup, 3)
     if args.size is None:
         args.size = 256 if args.workload == "wave" else 128
-    if args.impl == "reference":
+    if args.workload == "patches":
+        if args.impl == "reference":
+            run_reference_patches(args)
+        else:
+            run_patches(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_b200(args)

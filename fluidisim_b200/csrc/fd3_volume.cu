@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstddef>
 #include <cstdio>
@@ -17,6 +18,7 @@
 #include <mutex>
 #include <new>
 #include <string>
+#include <thread>
 #include <utility>
 #include <vector>
 
@@ -1180,6 +1182,41 @@ int fd3_step_surface_linear(fd3_volume* V, uint64_t duration_us, uint32_t max_it
 int fd3_set_precondition_cut(fd3_volume* V, int on) {
   if (!V) return FD3_ERR_INVALID_ARGUMENT;
   V->precondition_cut = on != 0;
+  return FD3_OK;
+}
+
+// Many independent volumes (patches) projected concurrently: each keeps its own stream and its
+// device-side PCG loop; `threads` host workers (0 = up to 16) feed the GPU, largest patches first.
+int fd3_project_batch(fd3_volume* const* vols, size_t count, const float* scales, const float* k1s,
+                      uint32_t max_iters, int threads, fd3_report* reports, int* statuses) {
+  if ((!vols || !scales || !k1s || !reports || !statuses) && count) return FD3_ERR_INVALID_ARGUMENT;
+  std::vector<size_t> order(count);
+  for (size_t i = 0; i < count; ++i) {
+    if (!vols[i]) return FD3_ERR_INVALID_ARGUMENT;
+    order[i] = i;
+  }
+  std::sort(order.begin(), order.end(), [&](size_t a, size_t b) { return vols[a]->n > vols[b]->n; });
+  if (count > 1) {  // one volume twice would race on its buffers
+    std::vector<const fd3_volume*> seen(vols, vols + count);
+    std::sort(seen.begin(), seen.end());
+    if (std::adjacent_find(seen.begin(), seen.end()) != seen.end()) return FD3_ERR_INVALID_ARGUMENT;
+  }
+  size_t T = threads > 0 ? (size_t)threads : 16;
+  T = std::max<size_t>(1, std::min(T, count));
+  std::atomic<size_t> next{0};
+  auto worker = [&]() {
+    for (;;) {
+      const size_t q = next.fetch_add(1);
+      if (q >= count) break;
+      const size_t i = order[q];
+      cudaSetDevice(vols[i]->device);
+      statuses[i] = fd3_project_mobile(vols[i], scales[i], k1s[i], max_iters, &reports[i]);
+    }
+  };
+  std::vector<std::thread> pool;
+  for (size_t t = 1; t < T; ++t) pool.emplace_back(worker);
+  worker();
+  for (auto& th : pool) th.join();
   return FD3_OK;
 }
 

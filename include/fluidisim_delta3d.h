@@ -131,6 +131,13 @@ int fd3_reset_pressure(fd3_volume* v);
 int fd3_project_mobile(fd3_volume* v, float scale, float k1, uint32_t max_iters, fd3_report* report);
 /* Volume3::step_surface_mobile (delta3d_mobile.rs:819): advect, project, extrapolate, transport. */
 int fd3_step_surface_mobile(fd3_volume* v, uint64_t duration_us, uint32_t max_iters, fd3_report* report);
+/* No reference counterpart: many independent volumes (patches), each projected as
+ * fd3_project_mobile projects it, concurrently.  Every volume keeps its own stream and device-side
+ * loop; `threads` host workers (0 = up to 16) issue them, largest first.  statuses[i] and
+ * reports[i] are volume i's; the return value is FD3_OK unless the arguments are invalid (a null
+ * pointer, or one volume listed twice). */
+int fd3_project_batch(fd3_volume* const* volumes, size_t count, const float* scales, const float* k1s,
+                      uint32_t max_iters, int threads, fd3_report* reports, int* statuses);
 /* Volume3::last_refused_report (delta3d_mobile.rs:982); FD3_ERR_DOMAIN when none. */
 int fd3_last_refused_report(const fd3_volume* v, fd3_report* report);
 
