@@ -39,13 +39,19 @@ METRIC = "128³ projections/s at rel. residual 1e-6: learned-FCG vs plain MGPCG,
 # fluid fraction (4 B) and three face apertures (12 B).
 GEOM = 16
 BYTES_PER_CELL = {
-    # 2.5-D blocked fine kernels (f64 mode, the default)
+    # 2.5-D blocked fine kernels, one cell per thread (f64 mode with kernels = 2)
     "kz_dir_apply_dot": 2 + 4 + 4 + 4 + 4,     # code, z, d in, d out, q
     "kv_update_rn": 4 * 6,                     # p, r read+write; d, q
     "kz_fine_pre": 2 + 4 + 4 + 4,              # code, prec, r, z out
     "kz_fine_restrict": 2 + 4 + 4 + 0.5,       # code, r, z, coarse r (1/8 cell)
     "kz_fine_post1": 2 + 4 + 4 + 4 + 0.5 + 4,  # code, prec, r, z in, coarse x, z out
     "kz_fine_post2_rz": 2 + 4 + 4 + 4 + 4,     # code, prec, r, z in, z out
+    # the same passes with two cells per thread (f64 mode, the default when nx is even)
+    "kx_dir_apply_dot": 2 + 4 + 4 + 4 + 4,
+    "kx_fine_pre": 2 + 4 + 4 + 4,
+    "kx_fine_restrict": 2 + 4 + 4 + 0.5,
+    "kx_fine_post1": 2 + 4 + 4 + 4 + 0.5 + 4,
+    "kx_fine_post2_rz": 2 + 4 + 4 + 4 + 4,
     # one-cell-per-thread kernels (ordered mode, and f64 mode with kernels = 1)
     "k_dir_apply_dot": 2 + 4 + 4 + 4 + 4,
     "k_update_rn": 4 * 6,

@@ -18,7 +18,7 @@ from .delta3d import REDUCE_F64, Delta3dError, Report, Volume3, _Report, library
 
 SIZE_CLASSES = [("small", 0, 48 ** 3), ("medium", 48 ** 3, 80 ** 3), ("large", 80 ** 3, 1 << 62)]
 # (kernels, mg_max_levels): fine-level kernel family and V-cycle depth (0 = every level)
-CANDIDATES = [(0, 0), (1, 0), (0, 3), (1, 3), (0, 2)]
+CANDIDATES = [(0, 0), (1, 0), (2, 0), (0, 3), (1, 3)]
 
 
 def _bind(L):

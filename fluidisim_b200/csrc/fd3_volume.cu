@@ -24,7 +24,7 @@
 
 #include "../../include/fluidisim_delta3d.h"
 #include "fd3_cut.cuh"
-#include "fd3_zmarch.cuh"
+#include "fd3_zmarch2.cuh"
 #include "fd3_linear.cuh"
 
 using namespace fd3;
@@ -137,10 +137,12 @@ struct fd3_volume {
     return G;
   }
   bool ord() const { return opt.reduction == FD3_REDUCE_ORDERED_F32; }
-  bool blocked() const { return !ord() && opt.kernels == 0; }
+  bool blocked() const { return !ord() && opt.kernels != 1; }
+  bool paired() const { return blocked() && opt.kernels == 0 && nx % 2 == 0; }
   bool mg_on() const { return has_mg && !linear; }  // the linear path has no multigrid
   int loop_key() const {
-    return (ord() ? 1 : 0) | (mg_on() ? 2 : 0) | (blocked() ? 4 : 0) | (opt.no_overlap ? 8 : 0) | (linear ? 16 : 0);
+    return (ord() ? 1 : 0) | (mg_on() ? 2 : 0) | (blocked() ? 4 : 0) | (opt.no_overlap ? 8 : 0) | (linear ? 16 : 0) |
+           (paired() ? 32 : 0);
   }
   Red red() const { return Red{p64, p32, count}; }
 };
@@ -306,6 +308,26 @@ void coarse_cycle(fd3_volume* V, int gate) {
   }
 }
 
+// The fine passes of the V-cycle with the paired kernels of K2 layers per CTA.
+template <int K2>
+void paired_vcycle(fd3_volume* V, int gate, int op) {
+  Geo G = V->geo();
+  const Scalars* S = V->dS;
+  const bool levels = !V->levels.empty();
+  Lev L0 = levels ? V->levels[0] : Lev{};
+  const unsigned short* codes = V->codes;
+  const int zb = zblocks2(V->nx, V->ny, V->nz, K2);
+  LAUNCH_G(V, kx_fine_pre<K2>, zb, Z2T, G, codes, (const float*)V->prec, (const float*)V->res, V->z, S, gate);
+  if (levels) {
+    LAUNCH_G(V, kx_fine_restrict<K2>, zb, Z2T, G, codes, (const float*)V->res, (const float*)V->z, L0, S, gate);
+    coarse_cycle(V, gate);
+  }
+  LAUNCH_G(V, kx_fine_post1<K2>, zb, Z2T, G, codes, (const float*)V->prec, (const float*)V->res, (const float*)V->z, L0,
+           levels ? 1 : 0, V->z2, S, gate);
+  LAUNCH_G(V, kx_fine_post2_rz<K2>, zb, Z2T, G, codes, (const float*)V->prec, (const float*)V->res, (const float*)V->z2,
+           V->z, V->red(), V->dS, gate, op);
+}
+
 // v_cycle3 (delta3d_multigrid.rs:393-429) with res.z at its end (op FIN_RZ_PRIME or FIN_RZ_ITER);
 // z = M^-1 res is left in V->z.
 void vcycle(fd3_volume* V, int gate, int op) {
@@ -314,6 +336,11 @@ void vcycle(fd3_volume* V, int gate, int op) {
   const bool levels = !V->levels.empty();
   Lev L0 = levels ? V->levels[0] : Lev{};
   const unsigned short* codes = V->codes;
+  if (V->paired()) {  // 2.5-D blocked kernels, two cells per thread (f64 reductions)
+    if (pick_k2(V->nx, V->ny, V->nz) == 8) paired_vcycle<8>(V, gate, op);
+    else paired_vcycle<4>(V, gate, op);
+    return;
+  }
   if (V->blocked()) {  // 2.5-D blocked kernels (f64 reductions)
     const int zb = zblocks(V->nx, V->ny, V->nz);
     const bool full = zfull(V->nx, V->ny, V->nz);
@@ -369,7 +396,16 @@ void iteration(fd3_volume* V, int parity) {
   if (V->mg_on()) {
     float* din = parity ? V->dir2 : V->dir;
     float* dout = parity ? V->dir : V->dir2;
-    if (V->blocked()) {
+    if (V->paired()) {
+      if (pick_k2(V->nx, V->ny, V->nz) == 8)
+        LAUNCH_G(V, kx_dir_apply_dot<8>, zblocks2(V->nx, V->ny, V->nz, 8), Z2T, G, (const unsigned short*)V->codes,
+                 (const float*)V->z, (const float*)din, dout, V->tmp, V->red(), V->dS);
+      else
+        LAUNCH_G(V, kx_dir_apply_dot<4>, zblocks2(V->nx, V->ny, V->nz, 4), Z2T, G, (const unsigned short*)V->codes,
+                 (const float*)V->z, (const float*)din, dout, V->tmp, V->red(), V->dS);
+      LAUNCH_G(V, kv_update_rn, update_blocks(V->n), TPB, V->n, V->p, V->res, (const float*)dout,
+               (const float*)V->tmp, V->red(), V->dS);
+    } else if (V->blocked()) {
       if (zfull(V->nx, V->ny, V->nz))
         LAUNCH_G(V, kz_dir_apply_dot<true>, zblocks(V->nx, V->ny, V->nz), ZT, G, (const unsigned short*)V->codes,
                  (const float*)V->z, (const float*)din, dout, V->tmp, V->red(), V->dS);
@@ -687,7 +723,8 @@ int alloc_state(fd3_volume* V) {
   float* q;
   // one f64 partial per block of the largest reduction launch: linear (one cell per thread),
   // 2.5-D blocked, or the grid-stride update
-  V->p64_cap = std::max(std::max(blocks_for(V->n), zblocks(V->nx, V->ny, V->nz)), UPDATE_BLOCKS);
+  V->p64_cap = std::max(std::max(blocks_for(V->n), std::max(zblocks(V->nx, V->ny, V->nz), zblocks2(V->nx, V->ny, V->nz, 4))),
+                        UPDATE_BLOCKS);
   TRY(dalloc(V, &q, (size_t)V->p64_cap * 2 + 64)); V->p64 = (double*)q;
   TRY(dalloc(V, &V->p32, (size_t)(V->n + CHUNK - 1) / CHUNK + 64));
   TRY(dalloc(V, &q, sizeof(Scalars) / sizeof(float) + 16)); V->dS = (Scalars*)q;
@@ -1000,7 +1037,7 @@ void fd3_destroy(fd3_volume* v) {
 
 int fd3_set_options(fd3_volume* v, const fd3_options* o) {
   if (!v || !o) return FD3_ERR_INVALID_ARGUMENT;
-  if (o->reduction > 1 || o->kernels > 1 || o->no_overlap > 1) return FD3_ERR_DOMAIN;
+  if (o->reduction > 1 || o->kernels > 2 || o->no_overlap > 1) return FD3_ERR_DOMAIN;
   v->opt = *o;
   return FD3_OK;
 }

@@ -19,6 +19,11 @@ namespace fd3 {
 #ifndef FD3_ZMINB
 #define FD3_ZMINB 4
 #endif
+// Shared-memory planes of the march: with two, consecutive layers alternate and one barrier per
+// layer suffices (a plane is rewritten only after every thread has passed the next layer's barrier).
+#ifndef FD3_PLANES
+#define FD3_PLANES 2
+#endif
 constexpr int ZX = 32, ZY = 8, ZK = FD3_ZK, ZT = ZX * ZY;
 
 // apply_code with the six neighbour values given (only fluid-neighbour faces read them).
@@ -109,7 +114,7 @@ __device__ __forceinline__ void zmarch(const Geo& g, const unsigned short* __res
                                        A after = A()) {
   typedef typename L::Raw Raw;
   typedef typename L::Halo Halo;
-  __shared__ float s[ZY + 2][ZX + 2];
+  __shared__ float sbuf[FD3_PLANES][ZY + 2][ZX + 2];
   const int tx = threadIdx.x % ZX, ty = threadIdx.x / ZX;
   const ZTile t = ztile(g);
   const int nxny = g.nx * g.ny;
@@ -140,6 +145,7 @@ __device__ __forceinline__ void zmarch(const Geo& g, const unsigned short* __res
     unsigned code2 = fetch_code(k + 1);
     const float pc = t.inside ? ld.pv(rc) : 0.f;
     const float pn = (t.inside && k + 1 < g.nz) ? ld.pv(rn) : 0.f;
+    float (*s)[ZX + 2] = sbuf[(k - t.k0) % FD3_PLANES];
     s[ty + 1][tx + 1] = pc;
     if (hxi >= 0) s[ty + 1][hxs] = hx_on ? ld.hv(hx) : 0.f;
     if (hyj >= 0) s[hys][tx + 1] = hy_on ? ld.hv(hy) : 0.f;
@@ -151,7 +157,7 @@ __device__ __forceinline__ void zmarch(const Geo& g, const unsigned short* __res
                            pprev, pn);
       epi(c, rc, pc, ax);
     }
-    __syncthreads();
+    if (FD3_PLANES == 1) __syncthreads();  // with two planes, the next layer's barrier orders the reuse
     after(k);
     pprev = pc;
     rc = rn;
@@ -170,7 +176,7 @@ __device__ __forceinline__ void zmarch_full(const Geo& g, const unsigned short* 
                                             A after = A()) {
   typedef typename L::Raw Raw;
   typedef typename L::Halo Halo;
-  __shared__ float s[ZY + 2][ZX + 2];
+  __shared__ float sbuf[FD3_PLANES][ZY + 2][ZX + 2];
   const int tx = threadIdx.x % ZX, ty = threadIdx.x / ZX;
   const ZTile t = ztile(g);
   const int nxny = g.nx * g.ny;
@@ -207,6 +213,7 @@ __device__ __forceinline__ void zmarch_full(const Geo& g, const unsigned short* 
     }
     const float pc = ld.pv(rc);
     const float pn = (kk + 1 < ZK || !last_chunk) ? ld.pv(rn) : 0.f;
+    float (*s)[ZX + 2] = sbuf[kk % FD3_PLANES];
     s[ty + 1][tx + 1] = pc;
     if (hxi >= 0) s[ty + 1][hxs] = hx_on ? ld.hv(hx) : 0.f;
     if (hyj >= 0) s[hys][tx + 1] = hy_on ? ld.hv(hy) : 0.f;
@@ -216,7 +223,7 @@ __device__ __forceinline__ void zmarch_full(const Geo& g, const unsigned short* 
       ax = apply_code_nb(g, code, t.i, t.j, k, pc, s[ty + 1][tx], s[ty + 1][tx + 2], s[ty][tx + 1], s[ty + 2][tx + 1],
                          pprev, pn);
     epi(c, rc, pc, ax);
-    __syncthreads();
+    if (FD3_PLANES == 1) __syncthreads();
     after(k);
     pprev = pc;
     rc = rn;
@@ -408,6 +415,7 @@ __global__ void __launch_bounds__(ZT, FD3_ZMINB) kz_fine_restrict(Geo g, const u
       g, codes, ld,
       [&](int c, const LdLoadR::Raw& o, float, float ax) { tr[(c / nxny) & 1][ty][tx] = o.r - ax; },
       [&](int k) {
+        if (FD3_PLANES > 1 && (k & 1)) __syncthreads();  // the epilogue's tr writes before the reads below
         if ((k & 1) && t.inside && !(tx & 1) && !(ty & 1)) {
           float sum = 0.f;
           sum += tr[0][ty][tx];

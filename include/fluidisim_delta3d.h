@@ -76,8 +76,10 @@ typedef struct fd3_options {
   uint32_t mg_max_levels; /* coarse levels kept by fd3_enable_multigrid; 0 = every level the
                              reference's coarsening rule allows (delta3d_multigrid.rs:73-88) */
   uint32_t use_graphs;    /* 1 = run the inner PCG loop as a CUDA graph with a WHILE node */
-  uint32_t kernels;       /* fine-level kernels in f64 mode: 0 = 2.5-D blocked (default), 1 = one cell
-                             per thread (the family the ordered mode always uses) */
+  uint32_t kernels;       /* fine-level kernels in f64 mode: 0 = 2.5-D blocked with two cells per thread
+                             (default; one cell per thread when nx is odd), 1 = one cell per thread
+                             (the family the ordered mode always uses), 2 = 2.5-D blocked with one
+                             cell per thread */
   uint32_t no_overlap;    /* 1 = launch each kernel only after the previous one completes; 0 (default)
                              = programmatic dependent launch: the next kernel is scheduled early and
                              waits on the device (results are identical either way) */
