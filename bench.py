@@ -283,6 +283,87 @@ def cpu_baseline_sample(workload: str, size: int, budget_s: float = 20.0):
             "sample": f"{len(times)} full {size}^3 {workload} projections (same scene), oracle with OpenMP"}
 
 
+def fp64_pressure_check(workload: str, size: int, pressures: dict, max_cells: int = 128 ** 3):
+    """The checker of the mixed-precision leg (CPU, beside the CPU baseline): the oracle's f64
+    build solves the same projection to relative residual 1e-12, and each GPU pressure is reported
+    as its L-inf difference relative to that solution's L-inf.  Skipped above max_cells."""
+    import numpy as np
+
+    from fluidisim_b200 import scenes
+    from oracle import oracle as O
+    s = make_scene(workload, size)
+    if s["nx"] * s["ny"] * s["nz"] > max_cells:
+        return None
+    O.build()
+    O.set_threads(O.max_threads("f64"), "f64")
+    o = O.OracleVolume(s["nx"], s["ny"], s["nz"], s["dx"], s["rho"], s["g"], bottom=s["bottom"], solid=s["solid"],
+                       real="f64")
+    o.enable_multigrid()
+    o.set_free_surface(s["eta"], s["rest"])
+    o.set_velocity(s["u"], s["v"], s["w"])
+    o.set_tolerance(1e-24)
+    scale, k1 = scenes.projection_scalars(s)
+    t0 = time.perf_counter()
+    rep = o.project_mobile(scale, k1, 4000)
+    secs = time.perf_counter() - t0
+    p64 = o.pressure().astype(np.float64)
+    pmax = float(np.abs(p64).max())
+    out = {"fp64_rel_residual": rep["residual"], "fp64_iterations": rep["iterations"], "fp64_seconds": secs,
+           "fp64_pressure_max": pmax}
+    for k, p in pressures.items():
+        out[f"{k}_linf_rel"] = float(np.abs(p.astype(np.float64) - p64).max() / pmax)
+    return out
+
+
+def mixed_measure(args, s, stream, flush, p_f32, ms_f32):
+    """The FP16-storage V-cycle (fd3_options.storage = FP16) on the bench scene, timed as the main
+    leg (device-resident inputs, L2 flushed between steps, CUDA events on the solver's stream)."""
+    import numpy as np
+    import torch
+
+    from fluidisim_b200 import scenes
+    from fluidisim_b200.delta3d import STORAGE_F16, Volume3
+    scale, k1 = scenes.projection_scalars(s)
+    vol = Volume3.configure_with_solid(s["nx"], s["ny"], s["nz"], s["dx"], s["rho"], s["g"], s["bottom"], s["solid"])
+    vol.set_options(use_graphs=args.graphs, storage=STORAGE_F16)
+    vol.set_stream(stream.cuda_stream)
+    vol.enable_multigrid()
+    vol.set_free_surface(s["eta"], s["rest"])
+    du = torch.from_numpy(s["u"]).cuda()
+    dv = torch.from_numpy(s["v"]).cuda()
+    dw = torch.from_numpy(s["w"]).cuda()
+
+    def step():
+        vol.set_velocity_device(du.data_ptr(), dv.data_ptr(), dw.data_ptr())
+        vol.reset_pressure()
+        return vol.project_mobile3(scale, k1, 4000)
+
+    for _ in range(max(3, args.warmup)):
+        rep = step()
+    torch.cuda.synchronize()
+    steps = max(10, min(args.steps, 100))
+    evs = []
+    for _ in range(steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        rep = step()
+        b.record(stream)
+        evs.append((a, b))
+    torch.cuda.synchronize()
+    ms = sum(a.elapsed_time(b) for a, b in evs) / steps
+    p16 = vol.pressure()
+    vol.close()
+    pmax = float(np.abs(p_f32).max())
+    return {"storage": "fp16 V-cycle vectors (fine z, coarse x, r), f32 arithmetic; f32 CG vectors; f64 dots, "
+                       "alpha/beta and true residual; outer loop restarts from b - A p (defect correction)",
+            "value": 1e3 / ms, "unit": "projections/s", "ms_per_step": ms, "steps": steps,
+            "speedup_vs_f32_storage": ms_f32 / ms, "iterations": rep.iterations, "rel_residual": rep.residual,
+            "divergence_plain": rep.divergence_plain, "degraded": bool(rep.degraded),
+            "pressure_linf_rel_vs_f32_storage": float(np.abs(p16.astype(np.float64) - p_f32).max() / pmax)}, p16
+
+
 def learned_fcg_measure(args, s, vol_plain_p, stream):
     """The learned preconditioner, measured in the same run: training throughput at 64^3 (batch
     32, sphere-lake scenes with seeded random velocities), the validation FCG iteration count on
@@ -519,12 +600,18 @@ def run_b200(args):
                     ncu_traffic = float(parts[1])
 
     learned_line = None
+    mixed_line, p16 = None, None
+    plain_p = vol.pressure()
+    if world == 1 and args.mixed:
+        mixed_line, p16 = mixed_measure(args, s, stream, flush, plain_p.astype(np.float64), ms_per_step)
     if world == 1 and args.learned:
-        plain_p = vol.pressure()
         learned_line = learned_fcg_measure(args, s, plain_p, stream)
 
     if rank == 0:
         cpu = cpu_baseline_sample(args.workload, args.size) if (world == 1 and not args.no_cpu) else None
+        if mixed_line is not None and not args.no_cpu:
+            mixed_line["fp64_check"] = fp64_pressure_check(args.workload, args.size,
+                                                           {"f32_storage": plain_p, "fp16_storage": p16})
         out = {
             "impl": "b200", "metric": METRIC, "value": value, "unit": "projections/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
@@ -547,6 +634,7 @@ def run_b200(args):
             "gpu_launches": launches,
             "clocks": clocks.summary(),
             "learned_fcg": learned_line,
+            "mixed_precision": mixed_line,
         }
         print(json.dumps(out), flush=True)
     vol.close()
@@ -708,6 +796,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--learned", type=int, default=1,
                     help="1: also train the learned preconditioner and time learned-FCG projections (N=1 only)")
+    ap.add_argument("--mixed", type=int, default=1, help="1: also time the FP16-storage V-cycle on the same scene")
     ap.add_argument("--train-samples", type=int, default=4096, help="training samples of the learned preconditioner")
     ap.add_argument("--graphs", type=int, default=1,
                     help="1: the inner loop as a CUDA graph with a WHILE node; 0: host-driven (for ncu launch lists)")

@@ -117,6 +117,11 @@ struct Load {
   const float* __restrict__ x;
   __device__ __forceinline__ float operator()(int n) const { return x[n]; }
 };
+template <class T>
+struct LoadT {
+  const T* __restrict__ x;
+  __device__ __forceinline__ float operator()(int n) const { return Store<T>::ld(x, n); }
+};
 
 // ------------------------------------------------------------------------------------------------
 // Reductions finished in the kernel that produces them: each block leaves its partial(s), the last
@@ -137,6 +142,7 @@ __device__ __forceinline__ void apply_op(Scalars* S, double val, int op, int ord
     case FIN_ACTUAL:
       if (op == FIN_RR0) S->rr = val; else S->actual = val;
       if (!finite || zero_but_nonzero) S->status = 2;
+      if (S->vk > 0.f && val > 0.0) S->vinv = (float)((double)S->vk / sqrt(val));
       break;
     case FIN_DQ:
       S->dq = val;
@@ -146,6 +152,7 @@ __device__ __forceinline__ void apply_op(Scalars* S, double val, int op, int ord
     case FIN_RN:
       S->rn = val;
       if (!finite || zero_but_nonzero) { S->status = 2; S->active = 0; break; }
+      if (S->vk > 0.f && val > 0.0) S->vinv = (float)((double)S->vk / sqrt(val));
       if (!loop_continues(S, val, S->it + 1, ord)) { S->rr = val; S->it += 1; S->active = 0; }
       break;
     case FIN_RZ_ITER:
@@ -478,29 +485,33 @@ __device__ __forceinline__ float level_row_code(const Lev& L, unsigned code, int
   return acc * L.inv;
 }
 
-// x0 = 0 + w (r - 0)/diag (first sweep), recomputed per stencil point.
+// x0 = 0 + w (r - 0)/diag (first sweep), recomputed per stencil point.  T: the storage of the
+// level's vectors (f32, or FP16 in the mixed-precision mode).
+template <class T = float>
 __device__ __forceinline__ float level_x1(const Lev& L, int n) {
   float dg = L.diag[n];
-  return dg > 0.f ? 0.f + OMEGA * (L.r[n] - 0.f) / dg : 0.f;
+  return dg > 0.f ? 0.f + OMEGA * (Store<T>::ld(as<T>(L.r), n) - 0.f) / dg : 0.f;
 }
 
 // The two pre-sweeps of a coarse level from x = 0, written to L.x (smooth3 twice after fill(0)).
+template <class T>
 __global__ void __launch_bounds__(TPB) k_level_pre(Lev L, const Scalars* S, int gate) {
   KSTART();
   if (gate && !S->active) return;
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= L.n) return;
-  auto X1 = [&](int n) { return level_x1(L, n); };
+  auto X1 = [&](int n) { return level_x1<T>(L, n); };
   float dg = L.diag[c];
   float xc = X1(c);
   if (dg > 0.f) {
     int i = c % L.nx, t = c / L.nx, j = t % L.ny, k = t / L.ny;
-    xc += OMEGA * (L.r[c] - level_row_code(L, L.code[c], i, j, k, c, X1)) / dg;
+    xc += OMEGA * (Store<T>::ld(as<T>(L.r), c) - level_row_code(L, L.code[c], i, j, k, c, X1)) / dg;
   }
-  L.x[c] = xc;
+  Store<T>::st(as<T>(L.x), c, xc);
 }
 
 // t = r - L x on every cell of a coarse level (0 on inactive rows), the restriction's operand.
+template <class T>
 __global__ void __launch_bounds__(TPB) k_level_resid(Lev L, const Scalars* S, int gate) {
   KSTART();
   if (gate && !S->active) return;
@@ -510,12 +521,13 @@ __global__ void __launch_bounds__(TPB) k_level_resid(Lev L, const Scalars* S, in
   float lx = 0.f;
   if (code & RC_WET) {
     int i = c % L.nx, t = c / L.nx, j = t % L.ny, k = t / L.ny;
-    lx = level_row_code(L, code, i, j, k, c, Load{L.x});
+    lx = level_row_code(L, code, i, j, k, c, LoadT<T>{as<T>(L.x)});
   }
-  L.t[c] = L.r[c] - lx;
+  Store<T>::st(as<T>(L.t), c, Store<T>::ld(as<T>(L.r), c) - lx);
 }
 
 // C.r = mean of the 8 children of F.t, in the reference's CHILDREN order (restrict3).
+template <class T>
 __global__ void __launch_bounds__(TPB) k_level_sum8(Lev F, Lev C, const Scalars* S, int gate) {
   KSTART();
   if (gate && !S->active) return;
@@ -526,12 +538,13 @@ __global__ void __launch_bounds__(TPB) k_level_sum8(Lev F, Lev C, const Scalars*
 #pragma unroll
   for (int e = 0; e < 8; ++e) {
     int i = 2 * ci + (e & 1), j = 2 * cj + ((e >> 1) & 1), k = 2 * ck + (e >> 2);
-    s += F.t[(k * F.ny + j) * F.nx + i];
+    s += Store<T>::ld(as<T>(F.t), (k * F.ny + j) * F.nx + i);
   }
-  C.r[q] = 0.125f * s;
+  Store<T>::st(as<T>(C.r), q, 0.125f * s);
 }
 
 // Prolongation from C (x += parent) fused with the first post-sweep, L.x -> L.x2.
+template <class T>
 __global__ void __launch_bounds__(TPB) k_level_post1(Lev L, Lev C, const Scalars* S, int gate) {
   KSTART();
   if (gate && !S->active) return;
@@ -539,47 +552,52 @@ __global__ void __launch_bounds__(TPB) k_level_post1(Lev L, Lev C, const Scalars
   if (c >= L.n) return;
   auto XP = [&](int n) {
     int i = n % L.nx, t = n / L.nx, j = t % L.ny, k = t / L.ny;
-    return L.x[n] + C.x[((k >> 1) * C.ny + (j >> 1)) * C.nx + (i >> 1)];
+    return Store<T>::ld(as<T>(L.x), n) + Store<T>::ld(as<T>(C.x), ((k >> 1) * C.ny + (j >> 1)) * C.nx + (i >> 1));
   };
   float dg = L.diag[c];
   float xc = XP(c);
   if (dg > 0.f) {
     int i = c % L.nx, t = c / L.nx, j = t % L.ny, k = t / L.ny;
-    xc += OMEGA * (L.r[c] - level_row_code(L, L.code[c], i, j, k, c, XP)) / dg;
+    xc += OMEGA * (Store<T>::ld(as<T>(L.r), c) - level_row_code(L, L.code[c], i, j, k, c, XP)) / dg;
   }
-  L.x2[c] = xc;
+  Store<T>::st(as<T>(L.x2), c, xc);
 }
 
 // The second post-sweep, L.x2 -> L.x.
+template <class T>
 __global__ void __launch_bounds__(TPB) k_level_post2(Lev L, const Scalars* S, int gate) {
   KSTART();
   if (gate && !S->active) return;
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= L.n) return;
   float dg = L.diag[c];
-  float xc = L.x2[c];
+  float xc = Store<T>::ld(as<T>(L.x2), c);
   if (dg > 0.f) {
     int i = c % L.nx, t = c / L.nx, j = t % L.ny, k = t / L.ny;
-    xc += OMEGA * (L.r[c] - level_row_code(L, L.code[c], i, j, k, c, Load{L.x2})) / dg;
+    xc += OMEGA * (Store<T>::ld(as<T>(L.r), c) - level_row_code(L, L.code[c], i, j, k, c, LoadT<T>{as<T>(L.x2)})) / dg;
   }
-  L.x[c] = xc;
+  Store<T>::st(as<T>(L.x), c, xc);
 }
 
 // One damped Jacobi sweep from codes (a large coarsest level's 8 sweeps); zero_in: from x = 0.
-__global__ void __launch_bounds__(TPB) k_level_sweep_c(Lev L, const float* __restrict__ xin, float* __restrict__ xout,
+template <class T>
+__global__ void __launch_bounds__(TPB) k_level_sweep_c(Lev L, const float* __restrict__ xin_, float* __restrict__ xout_,
                                                        int zero_in, const Scalars* S, int gate) {
   KSTART();
   if (gate && !S->active) return;
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= L.n) return;
+  const T* xin = reinterpret_cast<const T*>(xin_);
+  T* xout = reinterpret_cast<T*>(xout_);
   float dg = L.diag[c];
-  if (zero_in) { xout[c] = dg > 0.f ? 0.f + OMEGA * (L.r[c] - 0.f) / dg : 0.f; return; }
-  float xc = xin[c];
+  const float rc = Store<T>::ld(as<T>(L.r), c);
+  if (zero_in) { Store<T>::st(xout, c, dg > 0.f ? 0.f + OMEGA * (rc - 0.f) / dg : 0.f); return; }
+  float xc = Store<T>::ld(xin, c);
   if (dg > 0.f) {
     int i = c % L.nx, t = c / L.nx, j = t % L.ny, k = t / L.ny;
-    xc += OMEGA * (L.r[c] - level_row_code(L, L.code[c], i, j, k, c, Load{xin})) / dg;
+    xc += OMEGA * (rc - level_row_code(L, L.code[c], i, j, k, c, LoadT<T>{xin})) / dg;
   }
-  xout[c] = xc;
+  Store<T>::st(xout, c, xc);
 }
 
 // All levels from `first` to `last` in one CTA (coarse_cycle3 restricted to them): each phase is a
@@ -754,6 +772,7 @@ __device__ __forceinline__ float tail_rowsum(const TailRow& w, int c, int nx, in
   return acc * inv;
 }
 
+template <class ST>
 __global__ void __launch_bounds__(TAIL_REG_THREADS) k_coarse_tail_reg(const Lev* __restrict__ T, int first, int last,
                                                                      const Scalars* S, int gate) {
   KSTART();
@@ -774,7 +793,7 @@ __global__ void __launch_bounds__(TAIL_REG_THREADS) k_coarse_tail_reg(const Lev*
   for (int l = 0; l < TAIL_REG_LEVELS; ++l) {
     if (l < nl) w[l] = tail_row(Ls[l], c);
   }
-  if (c < Ls[0].n) R[0][c] = Ls[0].r[c];
+  if (c < Ls[0].n) R[0][c] = Store<ST>::ld(as<ST>(Ls[0].r), c);
   __syncthreads();
   // descent
 #pragma unroll
@@ -853,7 +872,7 @@ __global__ void __launch_bounds__(TAIL_REG_THREADS) k_coarse_tail_reg(const Lev*
       __syncthreads();
     }
   }
-  if (c < Ls[0].n) Ls[0].x[c] = XF[0][c];
+  if (c < Ls[0].n) Store<ST>::st(as<ST>(Ls[0].x), c, XF[0][c]);
 }
 
 // ------------------------------------------------------------------------------------------------

@@ -12,6 +12,7 @@
 // geometry (nothing for a flat bottom) instead of stored coefficients.
 #pragma once
 
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -77,7 +78,48 @@ struct Scalars {
   unsigned long long hash; // fingerprint of p
   int dir_mode;            // next direction: 0 d = z (after a prime), 1 d = z + beta d
   unsigned body_runs;      // executions of the device loop body since the loop started
+  // FP16-storage V-cycle: it runs on r * vinv, vinv = vk / |r| = 6 sqrt(n) / (dx^2 |r|), i.e. on
+  // r / sigma with sigma = rms(r) dx^2 / 6, so its vectors stay near 1 whatever the pressure scale.
+  // vk = 0 (f32 storage) leaves vinv unused.
+  float vk, vinv;
 };
+
+// Storage of the V-cycle vectors (the fine z, z2 and every coarse level's x, x2, r, t): f32, or
+// FP16 with f32 arithmetic.  Stores round to nearest and clamp to the finite FP16 range (a NaN
+// stays a NaN, so the non-finite checks still see it).
+template <class T>
+struct Store;
+template <>
+struct Store<float> {
+  static constexpr bool half = false;
+  __device__ __forceinline__ static float ld(const float* p, int c) { return p[c]; }
+  __device__ __forceinline__ static float2 ld2(const float* p, int c) { return *reinterpret_cast<const float2*>(p + c); }
+  __device__ __forceinline__ static void st(float* p, int c, float v) { p[c] = v; }
+  __device__ __forceinline__ static void st2(float* p, int c, float a, float b) {
+    *reinterpret_cast<float2*>(p + c) = make_float2(a, b);
+  }
+  __device__ __forceinline__ static float rt(float v) { return v; }  // the value a load returns after a store
+};
+__device__ __forceinline__ float clamp_h(float v) { return v > 65504.f ? 65504.f : (v < -65504.f ? -65504.f : v); }
+template <>
+struct Store<__half> {
+  static constexpr bool half = true;
+  __device__ __forceinline__ static float ld(const __half* p, int c) { return __half2float(p[c]); }
+  __device__ __forceinline__ static float2 ld2(const __half* p, int c) {
+    return __half22float2(*reinterpret_cast<const __half2*>(p + c));
+  }
+  __device__ __forceinline__ static void st(__half* p, int c, float v) { p[c] = __float2half_rn(clamp_h(v)); }
+  __device__ __forceinline__ static void st2(__half* p, int c, float a, float b) {
+    *reinterpret_cast<__half2*>(p + c) = __floats2half2_rn(clamp_h(a), clamp_h(b));
+  }
+  __device__ __forceinline__ static float rt(float v) { return __half2float(__float2half_rn(clamp_h(v))); }
+};
+// A level's vector buffers are allocated as f32 arrays; the FP16 mode uses their first half.
+template <class T>
+__device__ __forceinline__ T* as(float* p) { return reinterpret_cast<T*>(p); }
+// The scale applied to r on its way into the V-cycle (1 in f32 storage).
+template <class T>
+__device__ __forceinline__ float vscale(const Scalars* S) { return Store<T>::half ? S->vinv : 1.f; }
 
 // Reduction scratch: per-block f64 partials, or per-64-chunk f32 partials.
 struct Red {

@@ -140,9 +140,11 @@ struct fd3_volume {
   bool blocked() const { return !ord() && opt.kernels != 1; }
   bool paired() const { return blocked() && opt.kernels == 0 && nx % 2 == 0; }
   bool mg_on() const { return has_mg && !linear; }  // the linear path has no multigrid
+  // FP16 storage of the V-cycle vectors (fd3_set_options accepts it only with the paired kernels)
+  bool half() const { return opt.storage == FD3_STORAGE_F16 && paired() && mg_on(); }
   int loop_key() const {
     return (ord() ? 1 : 0) | (mg_on() ? 2 : 0) | (blocked() ? 4 : 0) | (opt.no_overlap ? 8 : 0) | (linear ? 16 : 0) |
-           (paired() ? 32 : 0);
+           (paired() ? 32 : 0) | (half() ? 64 : 0);
   }
   Red red() const { return Red{p64, p32, count}; }
 };
@@ -275,27 +277,31 @@ void prepare_multigrid(fd3_volume* V) {
 }
 
 // coarse_cycle3 (delta3d_multigrid.rs:303-332); levels[0].r already restricted.  Levels from
-// V->tail_first on are solved by one CTA; the larger ones by grid-wide fused kernels.
-void coarse_cycle(fd3_volume* V, int gate) {
+// V->tail_first on are solved by one CTA; the larger ones by grid-wide fused kernels.  T is the
+// storage of the level vectors; with FP16 storage the tail is the one-cell-per-thread CTA, or, if
+// the tail does not fit it, every level is launched.
+template <class T>
+void coarse_cycle_t(fd3_volume* V, int gate) {
   std::vector<Lev>& Ls = V->levels;
   const int last = (int)Ls.size() - 1;
-  const int first_tail = V->tail_first;
+  const bool half = Store<T>::half;
+  const int first_tail = (half && !V->tail_reg) ? (int)Ls.size() : V->tail_first;
   const Scalars* S = V->dS;
   for (int l = 0; l < first_tail && l <= last; ++l) {
     Lev& L = Ls[l];
     if (l == last) {  // a large coarsest level: its 8 sweeps one by one
       for (int s = 0; s < 8; ++s)
-        LAUNCH(V, k_level_sweep_c, L.n, L, (const float*)((s % 2 == 0) ? L.x : L.x2), (s % 2 == 0) ? L.x2 : L.x,
+        LAUNCH(V, k_level_sweep_c<T>, L.n, L, (const float*)((s % 2 == 0) ? L.x : L.x2), (s % 2 == 0) ? L.x2 : L.x,
                s == 0 ? 1 : 0, S, gate);
     } else {
-      LAUNCH(V, k_level_pre, L.n, L, S, gate);
-      LAUNCH(V, k_level_resid, L.n, L, S, gate);
-      LAUNCH(V, k_level_sum8, Ls[l + 1].n, L, Ls[l + 1], S, gate);
+      LAUNCH(V, k_level_pre<T>, L.n, L, S, gate);
+      LAUNCH(V, k_level_resid<T>, L.n, L, S, gate);
+      LAUNCH(V, k_level_sum8<T>, Ls[l + 1].n, L, Ls[l + 1], S, gate);
     }
   }
   if (first_tail <= last) {
     if (V->tail_reg)
-      LAUNCH_G(V, k_coarse_tail_reg, 1, TAIL_REG_THREADS, (const Lev*)V->dlev, first_tail, last, S, gate);
+      LAUNCH_G(V, k_coarse_tail_reg<T>, 1, TAIL_REG_THREADS, (const Lev*)V->dlev, first_tail, last, S, gate);
     else if (V->tail_smem_bytes > 0)
       launch_grid_smem(V, "k_coarse_tail_smem", 1, TAIL_THREADS, V->tail_smem_bytes, k_coarse_tail_smem,
                        (const Lev*)V->dlev, first_tail, last, S, gate);
@@ -303,13 +309,18 @@ void coarse_cycle(fd3_volume* V, int gate) {
       LAUNCH_G(V, k_coarse_tail, 1, TAIL_THREADS, (const Lev*)V->dlev, first_tail, last, S, gate);
   }
   for (int l = std::min(first_tail, last) - 1; l >= 0; --l) {
-    LAUNCH(V, k_level_post1, Ls[l].n, Ls[l], Ls[l + 1], S, gate);
-    LAUNCH(V, k_level_post2, Ls[l].n, Ls[l], S, gate);
+    LAUNCH(V, k_level_post1<T>, Ls[l].n, Ls[l], Ls[l + 1], S, gate);
+    LAUNCH(V, k_level_post2<T>, Ls[l].n, Ls[l], S, gate);
   }
+}
+void coarse_cycle(fd3_volume* V, int gate) {
+  if (V->half()) coarse_cycle_t<__half>(V, gate);
+  else coarse_cycle_t<float>(V, gate);
 }
 
 // The fine passes of the V-cycle with the paired kernels of K2 layers per CTA.
-template <int K2>
+// T: the storage of z, z2 and the coarse vectors (f32, or FP16 in the mixed-precision mode).
+template <int K2, class T>
 void paired_vcycle(fd3_volume* V, int gate, int op) {
   Geo G = V->geo();
   const Scalars* S = V->dS;
@@ -317,15 +328,24 @@ void paired_vcycle(fd3_volume* V, int gate, int op) {
   Lev L0 = levels ? V->levels[0] : Lev{};
   const unsigned short* codes = V->codes;
   const int zb = zblocks2(V->nx, V->ny, V->nz, K2);
-  LAUNCH_G(V, kx_fine_pre<K2>, zb, Z2T, G, codes, (const float*)V->prec, (const float*)V->res, V->z, S, gate);
+  T* z = reinterpret_cast<T*>(V->z);
+  T* z2 = reinterpret_cast<T*>(V->z2);
+  launch_grid(V, "kx_fine_pre<K2>", zb, Z2T, kx_fine_pre<K2, T>, G, codes, (const float*)V->prec,
+              (const float*)V->res, z, S, gate);
   if (levels) {
-    LAUNCH_G(V, kx_fine_restrict<K2>, zb, Z2T, G, codes, (const float*)V->res, (const float*)V->z, L0, S, gate);
+    launch_grid(V, "kx_fine_restrict<K2>", zb, Z2T, kx_fine_restrict<K2, T>, G, codes, (const float*)V->res,
+                (const T*)z, L0, S, gate);
     coarse_cycle(V, gate);
   }
-  LAUNCH_G(V, kx_fine_post1<K2>, zb, Z2T, G, codes, (const float*)V->prec, (const float*)V->res, (const float*)V->z, L0,
-           levels ? 1 : 0, V->z2, S, gate);
-  LAUNCH_G(V, kx_fine_post2_rz<K2>, zb, Z2T, G, codes, (const float*)V->prec, (const float*)V->res, (const float*)V->z2,
-           V->z, V->red(), V->dS, gate, op);
+  launch_grid(V, "kx_fine_post1<K2>", zb, Z2T, kx_fine_post1<K2, T>, G, codes, (const float*)V->prec,
+              (const float*)V->res, (const T*)z, L0, levels ? 1 : 0, z2, S, gate);
+  launch_grid(V, "kx_fine_post2_rz<K2>", zb, Z2T, kx_fine_post2_rz<K2, T>, G, codes, (const float*)V->prec,
+              (const float*)V->res, (const T*)z2, z, V->red(), V->dS, gate, op);
+}
+template <int K2>
+void paired_vcycle(fd3_volume* V, int gate, int op) {
+  if (V->half()) paired_vcycle<K2, __half>(V, gate, op);
+  else paired_vcycle<K2, float>(V, gate, op);
 }
 
 // v_cycle3 (delta3d_multigrid.rs:393-429) with res.z at its end (op FIN_RZ_PRIME or FIN_RZ_ITER);
@@ -397,12 +417,26 @@ void iteration(fd3_volume* V, int parity) {
     float* din = parity ? V->dir2 : V->dir;
     float* dout = parity ? V->dir : V->dir2;
     if (V->paired()) {
-      if (pick_k2(V->nx, V->ny, V->nz) == 8)
-        LAUNCH_G(V, kx_dir_apply_dot<8>, zblocks2(V->nx, V->ny, V->nz, 8), Z2T, G, (const unsigned short*)V->codes,
-                 (const float*)V->z, (const float*)din, dout, V->tmp, V->red(), V->dS);
-      else
-        LAUNCH_G(V, kx_dir_apply_dot<4>, zblocks2(V->nx, V->ny, V->nz, 4), Z2T, G, (const unsigned short*)V->codes,
-                 (const float*)V->z, (const float*)din, dout, V->tmp, V->red(), V->dS);
+      const int k2 = pick_k2(V->nx, V->ny, V->nz);
+      const int zb = zblocks2(V->nx, V->ny, V->nz, k2);
+      const unsigned short* codes = V->codes;
+      const float* z = V->z;
+      if (V->half()) {
+        const __half* zh = reinterpret_cast<const __half*>(z);
+        if (k2 == 8)
+          launch_grid(V, "kx_dir_apply_dot<8>", zb, Z2T, kx_dir_apply_dot<8, __half>, G, codes, zh, (const float*)din,
+                      dout, V->tmp, V->red(), V->dS);
+        else
+          launch_grid(V, "kx_dir_apply_dot<4>", zb, Z2T, kx_dir_apply_dot<4, __half>, G, codes, zh, (const float*)din,
+                      dout, V->tmp, V->red(), V->dS);
+      } else {
+        if (k2 == 8)
+          launch_grid(V, "kx_dir_apply_dot<8>", zb, Z2T, kx_dir_apply_dot<8, float>, G, codes, z, (const float*)din,
+                      dout, V->tmp, V->red(), V->dS);
+        else
+          launch_grid(V, "kx_dir_apply_dot<4>", zb, Z2T, kx_dir_apply_dot<4, float>, G, codes, z, (const float*)din,
+                      dout, V->tmp, V->red(), V->dS);
+      }
       LAUNCH_G(V, kv_update_rn, update_blocks(V->n), TPB, V->n, V->p, V->res, (const float*)dout,
                (const float*)V->tmp, V->red(), V->dS);
     } else if (V->blocked()) {
@@ -545,10 +579,22 @@ int outer_checks(fd3_volume* V, float k1, Checks* out) {
   return FD3_OK;
 }
 
-__global__ void k_reset_scalars(Scalars* S) {
+__global__ void k_widen(int n, const __half* __restrict__ a, float* __restrict__ b) {
+  KSTART();
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < n) b[c] = __half2float(a[c]);
+}
+
+// vk: 6 sqrt(n) / dx^2 in the FP16-storage mode (Scalars::vinv), else 0.
+__global__ void k_reset_scalars(Scalars* S, float vk) {
   Scalars z;
   memset(&z, 0, sizeof z);
+  z.vk = vk;
+  z.vinv = 1.f;
   *S = z;
+}
+float vscale_k(const fd3_volume* V) {
+  return V->half() ? (float)(6.0 * std::sqrt((double)V->n) / ((double)V->dx * (double)V->dx)) : 0.f;
 }
 
 // project_mobile3 (delta3d_mobile.rs:465-609), or, with V->linear, project (delta3d.rs:1060-1196):
@@ -556,7 +602,7 @@ __global__ void k_reset_scalars(Scalars* S) {
 int project_mobile3(fd3_volume* V, float scale, float k1, uint32_t max_iters, fd3_report* rep) {
   const bool ord = V->ord();
   Geo G = V->geo();
-  LAUNCH_G(V, k_reset_scalars, 1, 1, V->dS);
+  LAUNCH_G(V, k_reset_scalars, 1, 1, V->dS, vscale_k(V));
   LAUNCH(V, k_divergence, V->n, G, (const float*)V->us, (const float*)V->vs, (const float*)V->ws, V->rhs);
   if (V->linear) {
     const int jacobi = V->cut && V->precondition_cut && V->ny > 1;  // delta3d.rs:1091
@@ -1037,7 +1083,10 @@ void fd3_destroy(fd3_volume* v) {
 
 int fd3_set_options(fd3_volume* v, const fd3_options* o) {
   if (!v || !o) return FD3_ERR_INVALID_ARGUMENT;
-  if (o->reduction > 1 || o->kernels > 2 || o->no_overlap > 1) return FD3_ERR_DOMAIN;
+  if (o->reduction > 1 || o->kernels > 2 || o->no_overlap > 1 || o->storage > 1) return FD3_ERR_DOMAIN;
+  // FP16 storage runs on the paired fine kernels: f64 reductions, kernels = 0 and an even nx
+  if (o->storage == FD3_STORAGE_F16 && (o->reduction != FD3_REDUCE_F64 || o->kernels != 0 || v->nx % 2 != 0))
+    return FD3_ERR_DOMAIN;
   v->opt = *o;
   return FD3_OK;
 }
@@ -1373,8 +1422,14 @@ int fd3_vcycle_for_tests(fd3_volume* V, const float* x, float* z, size_t len) {
   LAUNCH(V, k_row_codes, V->n, V->geo(), V->codes);
   prepare_multigrid(V);
   CK(cudaMemcpyAsync(V->res, x, len * 4, cudaMemcpyHostToDevice, V->stream));
+  if (V->half()) LAUNCH_G(V, k_reset_scalars, 1, 1, V->dS, 0.f);  // FP16 storage, r unscaled (vinv = 1)
   vcycle(V, 0, FIN_RZ_PRIME);
-  CK(cudaMemcpyAsync(z, V->z, len * 4, cudaMemcpyDeviceToHost, V->stream));
+  const float* zf = V->z;
+  if (V->half()) {
+    LAUNCH(V, k_widen, V->n, V->n, (const __half*)V->z, V->tmp);
+    zf = V->tmp;
+  }
+  CK(cudaMemcpyAsync(z, zf, len * 4, cudaMemcpyDeviceToHost, V->stream));
   return sync(V);
 }
 

@@ -133,9 +133,11 @@ __device__ __forceinline__ void zmarch2(const Geo& g, const unsigned short* __re
   }
 }
 
-// Loaders.
+// Loaders.  T is the storage of the V-cycle vectors (z, z2, the coarse x): f32, or FP16 in the
+// mixed-precision mode, where the V-cycle also sees r scaled by rs (Scalars::vinv).
+template <class T>
 struct L2Dir {  // d = z (+ beta d)
-  const float* __restrict__ z;
+  const T* __restrict__ z;
   const float* __restrict__ din;
   int mode;
   float beta;
@@ -143,49 +145,59 @@ struct L2Dir {  // d = z (+ beta d)
   typedef Raw2 Halo2;
   struct Halo { float z = 0.f, d = 0.f; };
   __device__ __forceinline__ Raw2 full2(int, int, int, int c) const {
-    Raw2 o; o.z = ld2(z, c); if (mode) o.d = ld2(din, c); return o;
+    Raw2 o; o.z = Store<T>::ld2(z, c); if (mode) o.d = ld2(din, c); return o;
   }
   __device__ __forceinline__ Halo2 halo2(int i, int j, int k, int c) const { return full2(i, j, k, c); }
-  __device__ __forceinline__ Halo halo(int, int, int, int c) const { Halo h; h.z = z[c]; if (mode) h.d = din[c]; return h; }
+  __device__ __forceinline__ Halo halo(int, int, int, int c) const {
+    Halo h; h.z = Store<T>::ld(z, c); if (mode) h.d = din[c]; return h;
+  }
   __device__ __forceinline__ float v(float zz, float dd) const { return mode ? zz + beta * dd : zz; }
   __device__ __forceinline__ float2 pv2(const Raw2& o) const { return make_float2(v(o.z.x, o.d.x), v(o.z.y, o.d.y)); }
   __device__ __forceinline__ float2 hv2(const Halo2& o) const { return pv2(o); }
   __device__ __forceinline__ float hv(const Halo& h) const { return v(h.z, h.d); }
 };
+// r as the V-cycle sees it: r * rs in the FP16 mode, r itself (no multiply) in f32.
+template <class T>
+__device__ __forceinline__ float rsc(float r, float rs) { return Store<T>::half ? r * rs : r; }
+template <class T>
 struct L2Z1 {  // first pre-sweep from zero: w prec r where prec > 0
   const float* __restrict__ prec;
   const float* __restrict__ r;
+  float rs;
   struct Raw2 { float2 m = make_float2(0.f, 0.f), r = make_float2(0.f, 0.f); };
   typedef Raw2 Halo2;
   struct Halo { float m = 0.f, r = 0.f; };
   __device__ __forceinline__ Raw2 full2(int, int, int, int c) const { Raw2 o; o.m = ld2(prec, c); o.r = ld2(r, c); return o; }
   __device__ __forceinline__ Halo2 halo2(int i, int j, int k, int c) const { return full2(i, j, k, c); }
   __device__ __forceinline__ Halo halo(int, int, int, int c) const { Halo h; h.m = prec[c]; h.r = r[c]; return h; }
-  __device__ __forceinline__ static float v(float m, float rr) { return m > 0.f ? 0.f + OMEGA * m * (rr - 0.f) : 0.f; }
+  __device__ __forceinline__ float v(float m, float rr) const {
+    return m > 0.f ? 0.f + OMEGA * m * (rsc<T>(rr, rs) - 0.f) : 0.f;
+  }
   __device__ __forceinline__ float2 pv2(const Raw2& o) const { return make_float2(v(o.m.x, o.r.x), v(o.m.y, o.r.y)); }
   __device__ __forceinline__ float2 hv2(const Halo2& o) const { return pv2(o); }
   __device__ __forceinline__ float hv(const Halo& h) const { return v(h.m, h.r); }
 };
+template <class T>
 struct L2Prolong {  // z + parent x, zeroed where prec == 0 (or z alone without prolongation)
-  const float* __restrict__ zin;
+  const T* __restrict__ zin;
   const float* __restrict__ prec;
   const float* __restrict__ r;
-  const float* __restrict__ xc;
+  const T* __restrict__ xc;
   int lnx, lny, prolong;
   struct Raw2 { float2 z = make_float2(0.f, 0.f), m = make_float2(0.f, 0.f), r = make_float2(0.f, 0.f); float x = 0.f; };
   struct Halo2 { float2 z = make_float2(0.f, 0.f), m = make_float2(0.f, 0.f); float x = 0.f; };
   struct Halo { float z = 0.f, m = 0.f, x = 0.f; };
   __device__ __forceinline__ float parent(int i, int j, int k) const {  // the pair (even i0, i0 + 1) shares it
-    return prolong ? xc[((k >> 1) * lny + (j >> 1)) * lnx + (i >> 1)] : 0.f;
+    return prolong ? Store<T>::ld(xc, ((k >> 1) * lny + (j >> 1)) * lnx + (i >> 1)) : 0.f;
   }
   __device__ __forceinline__ Raw2 full2(int i, int j, int k, int c) const {
-    Raw2 o; o.z = ld2(zin, c); o.m = ld2(prec, c); o.r = ld2(r, c); o.x = parent(i, j, k); return o;
+    Raw2 o; o.z = Store<T>::ld2(zin, c); o.m = ld2(prec, c); o.r = ld2(r, c); o.x = parent(i, j, k); return o;
   }
   __device__ __forceinline__ Halo2 halo2(int i, int j, int k, int c) const {
-    Halo2 h; h.z = ld2(zin, c); if (prolong) h.m = ld2(prec, c); h.x = parent(i, j, k); return h;
+    Halo2 h; h.z = Store<T>::ld2(zin, c); if (prolong) h.m = ld2(prec, c); h.x = parent(i, j, k); return h;
   }
   __device__ __forceinline__ Halo halo(int i, int j, int k, int c) const {
-    Halo h; h.z = zin[c]; h.m = prolong ? prec[c] : 0.f; h.x = parent(i, j, k); return h;
+    Halo h; h.z = Store<T>::ld(zin, c); h.m = prolong ? prec[c] : 0.f; h.x = parent(i, j, k); return h;
   }
   __device__ __forceinline__ float val(float z, float m, float x) const {
     if (!prolong) return z;
@@ -196,47 +208,49 @@ struct L2Prolong {  // z + parent x, zeroed where prec == 0 (or z alone without 
   __device__ __forceinline__ float2 hv2(const Halo2& h) const { return make_float2(val(h.z.x, h.m.x, h.x), val(h.z.y, h.m.y, h.x)); }
   __device__ __forceinline__ float hv(const Halo& h) const { return val(h.z, h.m, h.x); }
 };
+template <class T>
 struct L2Sweep {  // z, with prec and r carried for the epilogue
-  const float* __restrict__ zin;
+  const T* __restrict__ zin;
   const float* __restrict__ prec;
   const float* __restrict__ r;
   struct Raw2 { float2 z = make_float2(0.f, 0.f), m = make_float2(0.f, 0.f), r = make_float2(0.f, 0.f); };
   struct Halo2 { float2 z = make_float2(0.f, 0.f); };
   struct Halo { float z = 0.f; };
   __device__ __forceinline__ Raw2 full2(int, int, int, int c) const {
-    Raw2 o; o.z = ld2(zin, c); o.m = ld2(prec, c); o.r = ld2(r, c); return o;
+    Raw2 o; o.z = Store<T>::ld2(zin, c); o.m = ld2(prec, c); o.r = ld2(r, c); return o;
   }
-  __device__ __forceinline__ Halo2 halo2(int, int, int, int c) const { Halo2 h; h.z = ld2(zin, c); return h; }
-  __device__ __forceinline__ Halo halo(int, int, int, int c) const { Halo h; h.z = zin[c]; return h; }
+  __device__ __forceinline__ Halo2 halo2(int, int, int, int c) const { Halo2 h; h.z = Store<T>::ld2(zin, c); return h; }
+  __device__ __forceinline__ Halo halo(int, int, int, int c) const { Halo h; h.z = Store<T>::ld(zin, c); return h; }
   __device__ __forceinline__ float2 pv2(const Raw2& o) const { return o.z; }
   __device__ __forceinline__ float2 hv2(const Halo2& h) const { return h.z; }
   __device__ __forceinline__ float hv(const Halo& h) const { return h.z; }
 };
+template <class T>
 struct L2LoadR {  // operand x, with r carried for the epilogue
-  const float* __restrict__ x;
+  const T* __restrict__ x;
   const float* __restrict__ r;
   struct Raw2 { float2 v = make_float2(0.f, 0.f), r = make_float2(0.f, 0.f); };
   struct Halo2 { float2 v = make_float2(0.f, 0.f); };
   struct Halo { float v = 0.f; };
-  __device__ __forceinline__ Raw2 full2(int, int, int, int c) const { Raw2 o; o.v = ld2(x, c); o.r = ld2(r, c); return o; }
-  __device__ __forceinline__ Halo2 halo2(int, int, int, int c) const { Halo2 h; h.v = ld2(x, c); return h; }
-  __device__ __forceinline__ Halo halo(int, int, int, int c) const { Halo h; h.v = x[c]; return h; }
+  __device__ __forceinline__ Raw2 full2(int, int, int, int c) const { Raw2 o; o.v = Store<T>::ld2(x, c); o.r = ld2(r, c); return o; }
+  __device__ __forceinline__ Halo2 halo2(int, int, int, int c) const { Halo2 h; h.v = Store<T>::ld2(x, c); return h; }
+  __device__ __forceinline__ Halo halo(int, int, int, int c) const { Halo h; h.v = Store<T>::ld(x, c); return h; }
   __device__ __forceinline__ float2 pv2(const Raw2& o) const { return o.v; }
   __device__ __forceinline__ float2 hv2(const Halo2& h) const { return h.v; }
   __device__ __forceinline__ float hv(const Halo& h) const { return h.v; }
 };
 
 // d = z (+ beta d); q = A d; d.q; alpha (FIN_DQ).
-template <int K2>
+template <int K2, class T>
 __global__ void __launch_bounds__(Z2T, FD3_ZMINB2) kx_dir_apply_dot(Geo g, const unsigned short* __restrict__ codes,
-                                                                  const float* __restrict__ z,
+                                                                  const T* __restrict__ z,
                                                                   const float* __restrict__ din, float* __restrict__ dout,
                                                                   float* __restrict__ q, Red red, Scalars* S) {
   KSTART();
   if (!S->active) return;
-  L2Dir ld{z, din, S->dir_mode, S->beta};
+  L2Dir<T> ld{z, din, S->dir_mode, S->beta};
   double acc = 0.0;
-  zmarch2<K2>(g, codes, ld, [&](int c, const L2Dir::Raw2&, float2 pc, float a0, float a1) {
+  zmarch2<K2>(g, codes, ld, [&](int c, const typename L2Dir<T>::Raw2&, float2 pc, float a0, float a1) {
     st2(dout, c, pc.x, pc.y);
     st2(q, c, a0, a1);
     acc += (double)pc.x * (double)a0;
@@ -246,56 +260,60 @@ __global__ void __launch_bounds__(Z2T, FD3_ZMINB2) kx_dir_apply_dot(Geo g, const
 }
 
 // The two pre-sweeps from z = 0.
-template <int K2>
+template <int K2, class T>
 __global__ void __launch_bounds__(Z2T, FD3_ZMINB2) kx_fine_pre(Geo g, const unsigned short* __restrict__ codes,
                                                              const float* __restrict__ prec, const float* __restrict__ r,
-                                                             float* __restrict__ z2, const Scalars* S, int gate) {
+                                                             T* __restrict__ z2, const Scalars* S, int gate) {
   KSTART();
   if (gate && !S->active) return;
-  L2Z1 ld{prec, r};
-  zmarch2<K2>(g, codes, ld, [&](int c, const L2Z1::Raw2& o, float2 pc, float a0, float a1) {
+  const float rs = vscale<T>(S);
+  L2Z1<T> ld{prec, r, rs};
+  zmarch2<K2>(g, codes, ld, [&](int c, const typename L2Z1<T>::Raw2& o, float2 pc, float a0, float a1) {
     float z0 = pc.x, z1 = pc.y;
-    if (o.m.x > 0.f) z0 += OMEGA * o.m.x * (o.r.x - a0);
-    if (o.m.y > 0.f) z1 += OMEGA * o.m.y * (o.r.y - a1);
-    st2(z2, c, z0, z1);
+    if (o.m.x > 0.f) z0 += OMEGA * o.m.x * (rsc<T>(o.r.x, rs) - a0);
+    if (o.m.y > 0.f) z1 += OMEGA * o.m.y * (rsc<T>(o.r.y, rs) - a1);
+    Store<T>::st2(z2, c, z0, z1);
   });
 }
 
 // Prolongation + zeroing + first post-sweep (or the plain third sweep without coarse levels).
-template <int K2>
+template <int K2, class T>
 __global__ void __launch_bounds__(Z2T, FD3_ZMINB2) kx_fine_post1(Geo g, const unsigned short* __restrict__ codes,
                                                                const float* __restrict__ prec, const float* __restrict__ r,
-                                                               const float* __restrict__ zin, Lev L, int prolong,
-                                                               float* __restrict__ zout, const Scalars* S, int gate) {
+                                                               const T* __restrict__ zin, Lev L, int prolong,
+                                                               T* __restrict__ zout, const Scalars* S, int gate) {
   KSTART();
   if (gate && !S->active) return;
-  L2Prolong ld{zin, prec, r, L.x, L.nx, L.ny, prolong};
-  zmarch2<K2>(g, codes, ld, [&](int c, const L2Prolong::Raw2& o, float2 pc, float a0, float a1) {
+  const float rs = vscale<T>(S);
+  L2Prolong<T> ld{zin, prec, r, as<T>(L.x), L.nx, L.ny, prolong};
+  zmarch2<K2>(g, codes, ld, [&](int c, const typename L2Prolong<T>::Raw2& o, float2 pc, float a0, float a1) {
     float z0 = pc.x, z1 = pc.y;
-    if (o.m.x > 0.f) z0 += OMEGA * o.m.x * (o.r.x - a0);
-    if (o.m.y > 0.f) z1 += OMEGA * o.m.y * (o.r.y - a1);
-    st2(zout, c, z0, z1);
+    if (o.m.x > 0.f) z0 += OMEGA * o.m.x * (rsc<T>(o.r.x, rs) - a0);
+    if (o.m.y > 0.f) z1 += OMEGA * o.m.y * (rsc<T>(o.r.y, rs) - a1);
+    Store<T>::st2(zout, c, z0, z1);
   });
 }
 
-// Second post-sweep with r.z (FIN_RZ_PRIME or FIN_RZ_ITER).
-template <int K2>
+// Second post-sweep with r.z (FIN_RZ_PRIME or FIN_RZ_ITER).  The dot takes the z that is stored
+// (the value the direction update reads back) and the unscaled r.
+template <int K2, class T>
 __global__ void __launch_bounds__(Z2T, FD3_ZMINB2) kx_fine_post2_rz(Geo g, const unsigned short* __restrict__ codes,
                                                                   const float* __restrict__ prec,
                                                                   const float* __restrict__ r,
-                                                                  const float* __restrict__ zin, float* __restrict__ zout,
+                                                                  const T* __restrict__ zin, T* __restrict__ zout,
                                                                   Red red, Scalars* S, int gate, int op) {
   KSTART();
   if (gate && !S->active) return;
-  L2Sweep ld{zin, prec, r};
+  const float rs = vscale<T>(S);
+  L2Sweep<T> ld{zin, prec, r};
   double acc = 0.0;
-  zmarch2<K2>(g, codes, ld, [&](int c, const L2Sweep::Raw2& o, float2 pc, float a0, float a1) {
+  zmarch2<K2>(g, codes, ld, [&](int c, const typename L2Sweep<T>::Raw2& o, float2 pc, float a0, float a1) {
     float z0 = pc.x, z1 = pc.y;
-    if (o.m.x > 0.f) z0 += OMEGA * o.m.x * (o.r.x - a0);
-    if (o.m.y > 0.f) z1 += OMEGA * o.m.y * (o.r.y - a1);
-    st2(zout, c, z0, z1);
-    acc += (double)o.r.x * (double)z0;
-    acc += (double)o.r.y * (double)z1;
+    if (o.m.x > 0.f) z0 += OMEGA * o.m.x * (rsc<T>(o.r.x, rs) - a0);
+    if (o.m.y > 0.f) z1 += OMEGA * o.m.y * (rsc<T>(o.r.y, rs) - a1);
+    Store<T>::st2(zout, c, z0, z1);
+    acc += (double)o.r.x * (double)Store<T>::rt(z0);
+    acc += (double)o.r.y * (double)Store<T>::rt(z1);
   });
   zreduce_finish(acc, red, S, op);
 }
@@ -303,10 +321,10 @@ __global__ void __launch_bounds__(Z2T, FD3_ZMINB2) kx_fine_post2_rz(Geo g, const
 // Residual r - A z at every fine cell and its 8-child mean (restrict3, delta3d_multigrid.rs:258-272):
 // each thread's pair is one coarse cell's x children; the even rows sum the eight children, in the
 // reference's CHILDREN order, from the two layers kept in shared memory.
-template <int K2>
+template <int K2, class T>
 __global__ void __launch_bounds__(Z2T, FD3_ZMINB2) kx_fine_restrict(Geo g, const unsigned short* __restrict__ codes,
                                                                   const float* __restrict__ r,
-                                                                  const float* __restrict__ z, Lev L, const Scalars* S,
+                                                                  const T* __restrict__ z, Lev L, const Scalars* S,
                                                                   int gate) {
   KSTART();
   if (gate && !S->active) return;
@@ -314,11 +332,13 @@ __global__ void __launch_bounds__(Z2T, FD3_ZMINB2) kx_fine_restrict(Geo g, const
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
   const ZTile2 t = ztile2<K2>(g);
   const int nxny = g.nx * g.ny;
-  L2LoadR ld{z, r};
+  const float rs = vscale<T>(S);
+  L2LoadR<T> ld{z, r};
   zmarch2<K2>(
       g, codes, ld,
-      [&](int c, const L2LoadR::Raw2& o, float2, float a0, float a1) {
-        *reinterpret_cast<float2*>(&tr[(c / nxny) & 1][ty][2 * tx]) = make_float2(o.r.x - a0, o.r.y - a1);
+      [&](int c, const typename L2LoadR<T>::Raw2& o, float2, float a0, float a1) {
+        *reinterpret_cast<float2*>(&tr[(c / nxny) & 1][ty][2 * tx]) =
+            make_float2(rsc<T>(o.r.x, rs) - a0, rsc<T>(o.r.y, rs) - a1);
       },
       [&](int k) {
         if (k & 1) {
@@ -333,7 +353,7 @@ __global__ void __launch_bounds__(Z2T, FD3_ZMINB2) kx_fine_restrict(Geo g, const
             sum += tr[1][ty][2 * tx + 1];
             sum += tr[1][ty + 1][2 * tx];
             sum += tr[1][ty + 1][2 * tx + 1];
-            L.r[((k >> 1) * L.ny + (t.j >> 1)) * L.nx + (t.i0 >> 1)] = 0.125f * sum;
+            Store<T>::st(as<T>(L.r), ((k >> 1) * L.ny + (t.j >> 1)) * L.nx + (t.i0 >> 1), 0.125f * sum);
           }
         }
       });

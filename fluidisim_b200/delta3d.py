@@ -25,6 +25,9 @@ STATUS = {0: "Ok", 1: "Domain", 2: "NotFinite", 3: "Shape", 4: "Budget", 5: "Clo
 
 REDUCE_F64 = 0
 REDUCE_ORDERED_F32 = 1
+# storage of the V-cycle vectors (fd3_storage)
+STORAGE_F32 = 0
+STORAGE_F16 = 1
 
 
 class Delta3dError(Exception):
@@ -48,7 +51,8 @@ class _Report(C.Structure):
 
 class _Options(C.Structure):
     _fields_ = [("reduction", C.c_uint32), ("mg_max_levels", C.c_uint32), ("use_graphs", C.c_uint32),
-                ("kernels", C.c_uint32), ("no_overlap", C.c_uint32), ("reserved", C.c_uint32 * 3)]
+                ("kernels", C.c_uint32), ("no_overlap", C.c_uint32), ("storage", C.c_uint32),
+                ("reserved", C.c_uint32 * 2)]
 
 
 @dataclass
@@ -194,7 +198,8 @@ class Volume3:
             raise Delta3dError(e, where, self._L.fd3_last_cuda_error().decode() if e >= 100 else "")
 
     # ---- options
-    def set_options(self, reduction=None, mg_max_levels=None, use_graphs=None, kernels=None, no_overlap=None):
+    def set_options(self, reduction=None, mg_max_levels=None, use_graphs=None, kernels=None, no_overlap=None,
+                    storage=None):
         o = _Options()
         self._check(self._L.fd3_get_options(self._h, C.byref(o)), "get_options")
         if reduction is not None:
@@ -207,6 +212,8 @@ class Volume3:
             o.kernels = int(kernels)
         if no_overlap is not None:
             o.no_overlap = int(no_overlap)
+        if storage is not None:
+            o.storage = int(storage)
         self._check(self._L.fd3_set_options(self._h, C.byref(o)), "set_options")
 
     def set_stream(self, stream_ptr: int):

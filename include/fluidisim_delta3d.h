@@ -71,6 +71,17 @@ typedef struct fd3_report {
  *                          bit for bit; the in-order merge is serial, so it is a parity mode. */
 typedef enum fd3_reduction { FD3_REDUCE_F64 = 0, FD3_REDUCE_ORDERED_F32 = 1 } fd3_reduction;
 
+/* Storage of the multigrid V-cycle's vectors (no reference counterpart; the reference stores f32).
+ *  FD3_STORAGE_F32  the reference's f32 (default).
+ *  FD3_STORAGE_F16  FP16 storage with f32 arithmetic for the fine z and every coarse level's x, r
+ *                   and residual; CG vectors stay f32, dots and the true residual f64.  The V-cycle
+ *                   runs on r / sigma, sigma = rms(r) dx^2 / 6, which keeps its values well inside
+ *                   the FP16 range whatever the pressure scale; PCG is unchanged by that positive
+ *                   scale.  The reference's outer loop (true residual, restart from b - A p,
+ *                   delta3d_mobile.rs:547-588) is the defect correction that restores the 1e-6
+ *                   tolerance.  Needs FD3_REDUCE_F64, kernels = 0 and an even nx. */
+typedef enum fd3_storage { FD3_STORAGE_F32 = 0, FD3_STORAGE_F16 = 1 } fd3_storage;
+
 typedef struct fd3_options {
   uint32_t reduction;     /* fd3_reduction */
   uint32_t mg_max_levels; /* coarse levels kept by fd3_enable_multigrid; 0 = every level the
@@ -83,7 +94,8 @@ typedef struct fd3_options {
   uint32_t no_overlap;    /* 1 = launch each kernel only after the previous one completes; 0 (default)
                              = programmatic dependent launch: the next kernel is scheduled early and
                              waits on the device (results are identical either way) */
-  uint32_t reserved[3];
+  uint32_t storage;       /* fd3_storage of the V-cycle vectors */
+  uint32_t reserved[2];
 } fd3_options;
 
 typedef struct fd3_volume fd3_volume;

@@ -71,6 +71,28 @@ int g_threads = 1;
 // the coarsest level's sweeps forward then backward, so the preconditioner stays symmetric.
 int g_smoother = 0;
 
+// Storage of the V-cycle vectors.  0 = the reference's f32.  1 = the B200 library's mixed-precision
+// mode (no reference counterpart): the V-cycle runs on r / sigma, sigma = rms(r over all cells) *
+// dx^2 / 6 (a positive scalar per V-cycle, which leaves PCG's iterates unchanged in exact
+// arithmetic), with f32 arithmetic and FP16 storage.  The rounding is emulated here by a round trip
+// through _Float16 (round to nearest even, clamped to +-65504) at the points where the device
+// stores a V-cycle vector: the fine z after the two pre-sweeps and after each post-sweep, every
+// restricted residual, and on levels of more than TAIL_CELLS cells the x after the pre-sweeps and
+// after each post-sweep, and the residual before restriction.  Smaller levels run in f32 in one
+// CTA on the device; only the x of the first of them is stored.
+int g_storage = 0;
+const size_t TAIL_CELLS = 512;
+double g_zmax = 0;  // largest |z| a V-cycle returned since the last reset (FP16-mode statistics)
+
+inline R h16(R v) {
+  float f = (float)v;
+  f = f > 65504.f ? 65504.f : (f < -65504.f ? -65504.f : f);
+  return (R)(float)(_Float16)f;
+}
+inline void round16(std::vector<R>& a) {
+  if (g_storage) for (auto& x : a) x = h16(x);
+}
+
 // ---------------------------------------------------------------------------------------------
 // Ordered reduction: host.rs:60-72 contract, host_impl.rs:75-92 sequential reference.  Chunks of
 // `grain` are reduced in index order inside the chunk; the chunk results are merged in increasing
@@ -669,23 +691,36 @@ void smooth_level(Level3& L, int count, bool forward) {
 // delta3d_multigrid.rs:303-332
 void coarse_cycle3(std::vector<Level3>& levels) {
   size_t last = levels.size() - 1;
+  auto big = [&](size_t l) { return levels[l].cells() > TAIL_CELLS; };
   for (size_t l = 0; l <= last; ++l) {
     int sweeps = l == last ? COARSE_SWEEPS_3D : PRE_SWEEPS_3D;
     Level3& L = levels[l];
     std::fill(L.x.begin(), L.x.end(), (R)0);
-    if (g_smoother == 0 || l < last) smooth_level(L, sweeps, true);
-    else { smooth_level(L, sweeps / 2, true); smooth_level(L, sweeps / 2, false); }
+    if (g_storage && big(l) && l == last) {
+      for (int s = 0; s < sweeps; ++s) { smooth_level(L, 1, true); round16(L.x); }
+    } else if (g_smoother == 0 || l < last) {
+      smooth_level(L, sweeps, true);
+      if (big(l)) round16(L.x);
+    } else { smooth_level(L, sweeps / 2, true); smooth_level(L, sweeps / 2, false); }
     if (l < last) {
       row_sums(L, L.x.data(), L.t.data());
       for (size_t c = 0; c < L.cells(); ++c) L.t[c] = L.r[c] - L.t[c];
+      if (big(l)) round16(L.t);
       restrict3(L.nx, L.ny, L.t.data(), levels[l + 1]);
+      if (big(l)) round16(levels[l + 1].r);
     }
   }
   for (size_t l = last; l-- > 0;) {
     Level3& L = levels[l];
     prolong_add3(L.nx, L.ny, L.x.data(), levels[l + 1]);
-    smooth_level(L, POST_SWEEPS_3D, false);
+    if (g_storage && big(l)) {
+      for (int s = 0; s < POST_SWEEPS_3D; ++s) { smooth_level(L, 1, false); round16(L.x); }
+    } else {
+      smooth_level(L, POST_SWEEPS_3D, false);
+    }
+    if (!big(l) && (l == 0 || big(l - 1))) round16(L.x);  // the tail's top level, read by the level above
   }
+  if (!big(0) && last == 0) round16(levels[0].x);
 }
 
 // ------------------------------------------------------------------- delta3d.rs Volume3
@@ -1036,15 +1071,26 @@ struct Volume3 {
     }
   }
   // delta3d_multigrid.rs:393-429
+  std::vector<R> res_scaled;  // r / sigma in the FP16-storage mode
   void v_cycle3() {
     size_t nx = d.nx, ny = d.ny, cells = p.size();
     std::fill(mg.z.begin(), mg.z.end(), (R)0);
+    const R* rv = res.data();
+    if (g_storage) {
+      double ss = 0;  // r is 0 on dry rows: the rms over all cells, as the device computes it
+      for (size_t q = 0; q < cells; ++q) ss += (double)res[q] * (double)res[q];
+      double sigma = std::sqrt(ss / (double)cells) * (double)d.dx * (double)d.dx / 6.0;
+      R inv = (sigma > 0 && std::isfinite(sigma)) ? (R)(float)(1.0 / sigma) : (R)1;
+      res_scaled.resize(cells);
+      for (size_t q = 0; q < cells; ++q) res_scaled[q] = res[q] * inv;
+      rv = res_scaled.data();
+    }
     // one fine sweep: Jacobi (the reference) or a red-black half sweep pair in the given order
     auto fine_sweep = [&](bool forward) {
       if (g_smoother == 0) {
         apply_mobile3(mg.z.data(), mg.t.data());
         for (size_t q = 0; q < cells; ++q)
-          if (prec[q] > 0) mg.z[q] += SMOOTH_DAMPING_3D * prec[q] * (res[q] - mg.t[q]);
+          if (prec[q] > 0) mg.z[q] += SMOOTH_DAMPING_3D * prec[q] * (rv[q] - mg.t[q]);
         return;
       }
       for (int h = 0; h < 2; ++h) {
@@ -1053,21 +1099,25 @@ struct Volume3 {
         for (size_t q = 0; q < cells; ++q) {
           size_t i = q % nx, j = (q / nx) % ny, k = q / (nx * ny);
           if ((int)((i + j + k) & 1) != color) continue;
-          if (prec[q] > 0) mg.z[q] += prec[q] * (res[q] - mg.t[q]);
+          if (prec[q] > 0) mg.z[q] += prec[q] * (rv[q] - mg.t[q]);
         }
       }
     };
     for (int s = 0; s < PRE_SWEEPS_3D; ++s) fine_sweep(true);
+    round16(mg.z);
     if (!mg.levels.empty()) {
       apply_mobile3(mg.z.data(), mg.t.data());
-      for (size_t q = 0; q < cells; ++q) mg.t[q] = res[q] - mg.t[q];
+      for (size_t q = 0; q < cells; ++q) mg.t[q] = rv[q] - mg.t[q];
       restrict3(nx, ny, mg.t.data(), mg.levels[0]);
+      round16(mg.levels[0].r);
       coarse_cycle3(mg.levels);
       prolong_add3(nx, ny, mg.z.data(), mg.levels[0]);
       for (size_t q = 0; q < cells; ++q)
         if (prec[q] == 0) mg.z[q] = 0;
     }
-    for (int s = 0; s < POST_SWEEPS_3D; ++s) fine_sweep(false);
+    for (int s = 0; s < POST_SWEEPS_3D; ++s) { fine_sweep(false); round16(mg.z); }
+    if (g_storage)
+      for (size_t q = 0; q < cells; ++q) g_zmax = std::max(g_zmax, (double)std::fabs(mg.z[q]));
   }
   // delta3d_multigrid.rs:433-465
   int prime_multigrid3(R beta, R& out) {
@@ -1773,6 +1823,8 @@ struct od3_domain { uint64_t nx, ny, nz; float dx; };
 int od3_real_bytes(void) { return (int)sizeof(R); }
 void od3_set_threads(int n) { g_threads = n > 0 ? n : 1; }
 void od3_set_smoother(int s) { g_smoother = s == 1 ? 1 : 0; }
+void od3_set_storage(int s) { g_storage = s == 1 ? 1 : 0; }
+double od3_take_zmax(void) { double z = g_zmax; g_zmax = 0; return z; }
 int od3_max_threads(void) {
 #ifdef _OPENMP
   return omp_get_max_threads();

@@ -89,6 +89,10 @@ def lib(real: str = "f32") -> C.CDLL:
     L.od3_max_threads.restype = C.c_int
     L.od3_set_smoother.argtypes = [C.c_int]
     L.od3_set_smoother.restype = None
+    L.od3_set_storage.argtypes = [C.c_int]
+    L.od3_set_storage.restype = None
+    L.od3_take_zmax.argtypes = []
+    L.od3_take_zmax.restype = C.c_double
     L.od3_project_linear.argtypes = [vp, f32, f32, u32, dp]
     L.od3_step_surface_linear.argtypes = [vp, u64, u32, dp]
     L.od3_set_precondition_cut.argtypes = [vp, C.c_int]
@@ -119,6 +123,16 @@ def report_dict(rep) -> dict:
 
 def set_threads(n: int, real: str = "f32") -> None:
     lib(real).od3_set_threads(int(n))
+
+
+def set_storage(storage: int, real: str = "f32") -> None:
+    """0: f32 V-cycle storage (the reference); 1: emulate the library's FP16 storage mode."""
+    lib(real).od3_set_storage(int(storage))
+
+
+def take_zmax(real: str = "f32") -> float:
+    """Largest |z| a V-cycle returned in the FP16 mode since the last call."""
+    return float(lib(real).od3_take_zmax())
 
 
 def max_threads(real: str = "f32") -> int:
