@@ -458,7 +458,7 @@ def learned_fcg_measure(args, s, vol_plain_p, stream):
         "fcg_iterations": rep.fcg_iterations, "fallback_mg_iterations": rep.report.iterations,
         "fell_back": rep.fell_back, "rel_residual": rep.report.residual,
         "divergence_plain": rep.report.divergence_plain, "pressure_linf_vs_plain_mgpcg": dp,
-        "network": "3-level U-Net 16/32/64, 3x3x3 convs, BF16 storage / FP32 accumulation (mma.sync m16n8k16)",
+        "network": "3-level U-Net 16/32/64, 3x3x3 convs, BF16 storage / FP32 accumulation; convolutions on tcgen05.mma (TMEM accumulators), weight gradients on mma.sync m16n8k16",
         "training": {"samples": steps * 32, "batch": 32, "grid": "64^3 sphere lakes (8 geometries)",
                      "samples_per_s": steps * 32 / train_s, "seconds": train_s,
                      "loss_first": float(np.mean(losses[:3])), "loss_last": float(np.mean(losses[-3:]))},

@@ -6,6 +6,7 @@
 // Included by fd3_volume.cu after the volume driver: it uses the driver's launch helpers.
 #pragma once
 
+#include "fd3_conv_tc.cuh"
 #include "fd3_unet.cuh"
 
 using namespace fd3u;
@@ -38,6 +39,8 @@ struct fd3_unet {
   Dims last{0, 0, 0, 0};
   std::vector<void*> allocations;
   unsigned long long launches = 0;
+  int conv_tc = 1;        // 1: convolutions on tcgen05 (k_conv_tc), 0: on mma.sync (k_conv)
+  int* dflag = nullptr;   // set by k_conv_tc when a bounded wait ran out
 };
 
 namespace {
@@ -75,9 +78,48 @@ int ulaunch(fd3_unet* N, dim3 grid, int block, K kernel, A... args) {
   return FD3_OK;
 }
 
-// k_conv for the (CIN, COUT) pairs the network uses.
+// k_conv_tc with its dynamic shared memory (the opt-in limit is raised once per instantiation).
+template <int CI, int CO, int E>
+int conv_tc_launch(fd3_unet* N, Dims d, const __nv_bfloat16* in, const __nv_bfloat16* w, const float* bias,
+                   __nv_bfloat16* out, float* out32) {
+  static unsigned attr_set = 0;  // devices on which the limit was raised
+  const int BY = tc_rows(d.X, d.Y), NTM = tc_tiles(d.X, BY);
+  if (NTM > TC_MAX_TILES) return FD3_ERR_SHAPE;
+  const size_t smem = tc_smem_bytes(d.X, BY, CO);
+  if (smem > 227 * 1024) return FD3_ERR_SHAPE;
+  if (N->device < 32 && !(attr_set & (1u << N->device))) {
+    CK(cudaFuncSetAttribute(k_conv_tc<CI, CO, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+    attr_set |= 1u << N->device;
+  }
+  const long long grid = (long long)d.B * d.Z * ((d.Y + BY - 1) / BY);
+  k_conv_tc<CI, CO, E><<<dim3((unsigned)grid), TC_THREADS, smem, N->stream>>>(d, BY, NTM, in, w, bias, out, out32,
+                                                                             N->dflag);
+  N->launches++;
+  CK(cudaGetLastError());
+  return FD3_OK;
+}
+
+// The convolution for the (CIN, COUT, epilogue) triples the network uses: k_conv_tc (tcgen05), or
+// k_conv (mma.sync) when N->conv_tc is 0.
 int conv_fwd(fd3_unet* N, Dims d, int cin, int cout, int epi, const __nv_bfloat16* in, const __nv_bfloat16* w,
              const float* bias, __nv_bfloat16* out, float* out32) {
+  if (N->conv_tc) {
+#define FD3_CONV_TC(CI, CO, E) \
+  if (cin == CI && cout == CO && epi == E) return conv_tc_launch<CI, CO, E>(N, d, in, w, bias, out, out32);
+    FD3_CONV_TC(16, 16, EPI_BIAS_RELU)
+    FD3_CONV_TC(16, 32, EPI_BIAS_RELU)
+    FD3_CONV_TC(32, 64, EPI_BIAS_RELU)
+    FD3_CONV_TC(96, 32, EPI_BIAS_RELU)
+    FD3_CONV_TC(48, 16, EPI_BIAS_RELU)
+    FD3_CONV_TC(16, 16, EPI_BIAS_F32_CH0)
+    FD3_CONV_TC(16, 16, EPI_PLAIN)
+    FD3_CONV_TC(16, 48, EPI_PLAIN)
+    FD3_CONV_TC(32, 96, EPI_PLAIN)
+    FD3_CONV_TC(64, 32, EPI_PLAIN)
+    FD3_CONV_TC(32, 16, EPI_PLAIN)
+#undef FD3_CONV_TC
+    return FD3_ERR_INVALID_ARGUMENT;
+  }
   const int grid = (int)((d.cells() + CONV_CELLS - 1) / CONV_CELLS);
 #define FD3_CONV(CI, CO, E)                                                              \
   if (cin == CI && cout == CO && epi == E)                                               \
@@ -125,8 +167,21 @@ int unet_pack(fd3_unet* N) {
   return FD3_OK;
 }
 
+// The error word of the tensor-core convolution (a bounded wait that ran out); read after a
+// synchronisation of the network's stream, then cleared.
+int unet_check_flag(fd3_unet* N) {
+  int h = 0;
+  CK(cudaMemcpy(&h, N->dflag, sizeof h, cudaMemcpyDeviceToHost));
+  if (h) {
+    CK(cudaMemset(N->dflag, 0, sizeof h));
+    g_last_cuda_error = "k_conv_tc: a wait for the tensor-core MMAs ran out";
+    return FD3_ERR_CUDA;
+  }
+  return FD3_OK;
+}
+
 int unet_check_dims(const fd3_unet* N, int B, int Z, int Y, int X) {
-  if (B <= 0 || Z <= 0 || Y <= 0 || X <= 0 || Z % 4 || Y % 4 || X % 4) return FD3_ERR_SHAPE;
+  if (B <= 0 || Z <= 0 || Y <= 0 || X <= 0 || Z % 4 || Y % 4 || X % 4 || X > 512) return FD3_ERR_SHAPE;
   if ((long long)B * Z * Y * X > N->cap || B > N->scale_cap) return FD3_ERR_SCRATCH_LIMIT;
   return FD3_OK;
 }
@@ -172,14 +227,14 @@ int unet_forward(fd3_unet* N, int B, int Z, int Y, int X, const float* in3, floa
   UnetLayer* L = N->layer;
   TRY(ulaunch(N, dim3(grid_for(n0)), 256, k_input_scaled, n0, per, in3, (const float*)N->in_scale, N->x0));
   TRY(conv_fwd(N, d0, 16, 16, EPI_BIAS_RELU, N->x0, L[L_E0].w, L[L_E0].bias, N->e0, nullptr));
-  TRY(ulaunch(N, dim3(grid_for(n1 * 16)), 256, k_pool, d1, 16, (const __nv_bfloat16*)N->e0, N->p0));
+  TRY(ulaunch(N, dim3(grid_for(n1 * 2)), 256, k_pool, d1, 16, (const __nv_bfloat16*)N->e0, N->p0));
   TRY(conv_fwd(N, d1, 16, 32, EPI_BIAS_RELU, N->p0, L[L_E1].w, L[L_E1].bias, N->e1, nullptr));
-  TRY(ulaunch(N, dim3(grid_for(n2 * 32)), 256, k_pool, d2, 32, (const __nv_bfloat16*)N->e1, N->p1));
+  TRY(ulaunch(N, dim3(grid_for(n2 * 4)), 256, k_pool, d2, 32, (const __nv_bfloat16*)N->e1, N->p1));
   TRY(conv_fwd(N, d2, 32, 64, EPI_BIAS_RELU, N->p1, L[L_B].w, L[L_B].bias, N->bq, nullptr));
-  TRY(ulaunch(N, dim3(grid_for(n1 * 96)), 256, k_up_cat, d1, 64, 32, (const __nv_bfloat16*)N->bq,
+  TRY(ulaunch(N, dim3(grid_for(n1 * 12)), 256, k_up_cat, d1, 64, 32, (const __nv_bfloat16*)N->bq,
               (const __nv_bfloat16*)N->e1, N->c1));
   TRY(conv_fwd(N, d1, 96, 32, EPI_BIAS_RELU, N->c1, L[L_D1].w, L[L_D1].bias, N->d1, nullptr));
-  TRY(ulaunch(N, dim3(grid_for(n0 * 48)), 256, k_up_cat, d0, 32, 16, (const __nv_bfloat16*)N->d1,
+  TRY(ulaunch(N, dim3(grid_for(n0 * 6)), 256, k_up_cat, d0, 32, 16, (const __nv_bfloat16*)N->d1,
               (const __nv_bfloat16*)N->e0, N->c0));
   TRY(conv_fwd(N, d0, 48, 16, EPI_BIAS_RELU, N->c0, L[L_D0].w, L[L_D0].bias, N->d0, nullptr));
   TRY(conv_fwd(N, d0, 16, 16, EPI_BIAS_F32_CH0, N->d0, L[L_HEAD].w, L[L_HEAD].bias, nullptr, out));
@@ -384,6 +439,7 @@ int fd3_unet_create(int max_batch, int nz, int ny, int nx, fd3_unet** out) {
   UA(N->bq, n2 * 64); UA(N->c1, n1 * 96); UA(N->d1, n1 * 32); UA(N->c0, n0 * 48); UA(N->d0, n0 * 16);
   UA(N->gy, n0 * 16); UA(N->gd0, n0 * 16); UA(N->gc0, n0 * 48); UA(N->gd1, n1 * 32); UA(N->gc1, n1 * 96);
   UA(N->gbq, n2 * 64); UA(N->gp1, n2 * 32); UA(N->ge1, n1 * 32); UA(N->gp0, n1 * 16); UA(N->ge0, n0 * 16);
+  UA(N->dflag, 1);
 #undef UA
   if (cudaStreamSynchronize(N->stream) != cudaSuccess) return fail(cuda_fail(cudaGetLastError(), "create", __LINE__));
   *out = N;
@@ -468,6 +524,12 @@ int fd3_unet_adam(fd3_unet* N, float lr, float beta1, float beta2, float eps) {
 int fd3_unet_sync(fd3_unet* N) {
   if (!N) return FD3_ERR_INVALID_ARGUMENT;
   CK(cudaStreamSynchronize(N->stream));
+  return unet_check_flag(N);
+}
+
+int fd3_unet_set_conv_kernels(fd3_unet* N, int tc) {
+  if (!N || (tc != 0 && tc != 1)) return FD3_ERR_INVALID_ARGUMENT;
+  N->conv_tc = tc;
   return FD3_OK;
 }
 

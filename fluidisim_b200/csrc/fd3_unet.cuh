@@ -243,41 +243,62 @@ __global__ void k_bias_grad(long long cells, int C, const __nv_bfloat16* __restr
 }
 
 // Mean of the 8 children: fine [B][2Z][2Y][2X][C] -> coarse [B][Z][Y][X][C] (d = coarse dims).
+// One thread per (coarse cell, 8-channel group): 16-byte loads and stores, the children summed in
+// f32 in the order e = 0..7.
 __global__ void k_pool(Dims d, int C, const __nv_bfloat16* __restrict__ fine, __nv_bfloat16* __restrict__ coarse) {
-  const long long n = d.cells() * C;
+  const int G = C / 8;
+  const long long n = d.cells() * G;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
-    const int ch = (int)(q % C);
-    long long c = q / C;
+    const int g = (int)(q % G);
+    long long c = q / G;
+    const long long cell = c;
     const int x = (int)(c % d.X); c /= d.X;
     const int y = (int)(c % d.Y); c /= d.Y;
     const int z = (int)(c % d.Z);
     const long long b = c / d.Z;
     const int FX = 2 * d.X, FY = 2 * d.Y, FZ = 2 * d.Z;
-    float s = 0.f;
+    float s[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
 #pragma unroll
     for (int e = 0; e < 8; ++e) {
       const long long f = ((b * FZ + 2 * z + (e >> 2)) * FY + 2 * y + ((e >> 1) & 1)) * FX + 2 * x + (e & 1);
-      s += __bfloat162float(fine[f * C + ch]);
+      const uint4 v = *reinterpret_cast<const uint4*>(fine + f * C + g * 8);
+      const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&v);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const float2 t = __bfloat1622float2(h[k]);
+        s[2 * k] += t.x;
+        s[2 * k + 1] += t.y;
+      }
     }
-    coarse[q] = __float2bfloat16(0.125f * s);
+    __align__(16) __nv_bfloat162 o[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) o[k] = __floats2bfloat162_rn(0.125f * s[2 * k], 0.125f * s[2 * k + 1]);
+    *reinterpret_cast<uint4*>(coarse + cell * C + g * 8) = *reinterpret_cast<const uint4*>(o);
   }
 }
 
 // cat(up(coarse), skip): out[fine cell][0..C1) = coarse[parent][..], out[..][C1..C1+C2) = skip.
+// One thread per (fine cell, 8-channel group of the C1 + C2 outputs): 16-byte copies.
 __global__ void k_up_cat(Dims fd, int C1, int C2, const __nv_bfloat16* __restrict__ coarse,
                          const __nv_bfloat16* __restrict__ skip, __nv_bfloat16* __restrict__ out) {
-  const int C = C1 + C2;
-  const long long n = fd.cells() * C;
+  const int C = C1 + C2, G = C / 8, G1 = C1 / 8;
+  const long long n = fd.cells() * G;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
-    const int ch = (int)(q % C);
-    long long c = q / C;
-    if (ch >= C1) { out[q] = skip[c * C2 + ch - C1]; continue; }
-    const int x = (int)(c % fd.X); c /= fd.X;
-    const int y = (int)(c % fd.Y); c /= fd.Y;
-    const int z = (int)(c % fd.Z);
-    const long long b = c / fd.Z;
-    const long long p = ((b * (fd.Z / 2) + z / 2) * (fd.Y / 2) + y / 2) * (fd.X / 2) + x / 2;
-    out[q] = coarse[p * C1 + ch];
+    const int g = (int)(q % G);
+    long long c = q / G;
+    const long long cell = c;
+    uint4 v;
+    if (g >= G1) {
+      v = *reinterpret_cast<const uint4*>(skip + cell * C2 + (g - G1) * 8);
+    } else {
+      const int x = (int)(c % fd.X); c /= fd.X;
+      const int y = (int)(c % fd.Y); c /= fd.Y;
+      const int z = (int)(c % fd.Z);
+      const long long b = c / fd.Z;
+      const long long p = ((b * (fd.Z / 2) + z / 2) * (fd.Y / 2) + y / 2) * (fd.X / 2) + x / 2;
+      v = *reinterpret_cast<const uint4*>(coarse + p * C1 + g * 8);
+    }
+    *reinterpret_cast<uint4*>(out + cell * C + g * 8) = v;
   }
 }
 

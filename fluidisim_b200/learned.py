@@ -57,6 +57,7 @@ def _bind(L: C.CDLL) -> C.CDLL:
     L.fd3_unet_backward.argtypes = [vp, vp]
     L.fd3_unet_adam.argtypes = [vp, f32, f32, f32, f32]
     L.fd3_unet_sync.argtypes = [vp]
+    L.fd3_unet_set_conv_kernels.argtypes = [vp, i32]
     L.fd3_unet_kernel_launches.argtypes = [vp]
     L.fd3_unet_kernel_launches.restype = C.c_uint64
     L.fd3_assemble_device.argtypes = [vp, f32]
@@ -136,6 +137,10 @@ class UNet:
 
     def sync(self):
         self._check(self._L.fd3_unet_sync(self._h), "sync")
+
+    def set_conv_kernels(self, tcgen05: bool):
+        """True: convolutions on tcgen05.mma (default); False: on mma.sync (for cross-checks)."""
+        self._check(self._L.fd3_unet_set_conv_kernels(self._h, 1 if tcgen05 else 0), "set_conv_kernels")
 
     def kernel_launches(self) -> int:
         return int(self._L.fd3_unet_kernel_launches(self._h))

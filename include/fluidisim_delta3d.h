@@ -221,7 +221,8 @@ int fd3_profile_entry(const fd3_volume* v, int index, char* name, size_t name_le
  * flexible CG, with the multigrid PCG of fd3_project_mobile as its fallback. */
 typedef struct fd3_unet fd3_unet;
 
-/* A network whose buffers hold max_batch samples of nz x ny x nx cells (each a multiple of 4). */
+/* A network whose buffers hold max_batch samples of nz x ny x nx cells (each a multiple of 4; a
+ * forward pass takes nx <= 512). */
 int fd3_unet_create(int max_batch, int nz, int ny, int nx, fd3_unet** out);
 void fd3_unet_destroy(fd3_unet* net);
 int fd3_unet_set_stream(fd3_unet* net, void* stream);
@@ -240,6 +241,9 @@ int fd3_unet_backward(fd3_unet* net, const float* d_gout);
 /* Adam step on the accumulated gradient (consumed). */
 int fd3_unet_adam(fd3_unet* net, float lr, float beta1, float beta2, float eps);
 int fd3_unet_sync(fd3_unet* net);
+/* Convolution kernels of the network: 1 = tcgen05.mma with tensor-memory accumulators (default),
+ * 0 = mma.sync m16n8k16 (the earlier tensor-core path, kept to cross-check the first). */
+int fd3_unet_set_conv_kernels(fd3_unet* net, int tcgen05);
 uint64_t fd3_unet_kernel_launches(const fd3_unet* net);
 
 /* Device-side hooks of a training loop, on a volume: the rhs and row codes of project_mobile3 for

@@ -48,13 +48,15 @@ def test_param_layout_matches_the_oracle():
     assert learned.param_count() == sum(v.size for v in U.init_params(0).values())
 
 
+@pytest.mark.parametrize("conv", ["tcgen05", "mma.sync"])
 @pytest.mark.parametrize("shape,batch", [((8, 8, 8), 2), ((4, 12, 8), 3)])
-def test_forward_and_backward_match_the_fp64_oracle(shape, batch):
+def test_forward_and_backward_match_the_fp64_oracle(shape, batch, conv):
     Z, Y, X = shape
     rng = np.random.default_rng(7)
     flat = learned.init_params(3)
     flat = flat + (0.02 * rng.standard_normal(flat.size)).astype(np.float32)  # non-zero biases
     net = learned.UNet(batch, Z, Y, X)
+    net.set_conv_kernels(conv == "tcgen05")
     net.set_params(flat)
     assert np.array_equal(net.params(), flat)
     cells = Z * Y * X
@@ -114,3 +116,35 @@ def test_adam_step_moves_the_parameters_against_the_gradient():
     moved = net.params() - flat
     head_b = learned.param_count() - 1
     assert moved[head_b] == pytest.approx(-1e-3, rel=1e-3)  # d(sum y)/d(head bias) > 0: the bias goes down
+
+
+@pytest.mark.parametrize("shape,batch", [((4, 8, 128), 1), ((8, 16, 64), 2), ((8, 8, 256), 1)])
+def test_tcgen05_convolutions_match_mma_sync(shape, batch):
+    """The tcgen05 convolutions (several M tiles per CTA, rows of up to 256 cells) against the
+    mma.sync ones on the same network and input: forward output and every parameter gradient.
+    Both store BF16 and accumulate in FP32; only the order of the accumulation differs."""
+    Z, Y, X = shape
+    rng = np.random.default_rng(11)
+    flat = learned.init_params(5) + (0.02 * rng.standard_normal(learned.param_count())).astype(np.float32)
+    cells = Z * Y * X
+    x = rng.standard_normal((batch, cells, 3)).astype(np.float32)
+    x[..., 1:] = (x[..., 1:] > 0).astype(np.float32)
+    gy = rng.standard_normal(batch * cells).astype(np.float32)
+    out = {}
+    for tc in (True, False):
+        net = learned.UNet(batch, Z, Y, X)
+        net.set_conv_kernels(tc)
+        net.set_params(flat)
+        dx = torch.from_numpy(x.ravel()).cuda()
+        dy = torch.empty(batch * cells, dtype=torch.float32, device="cuda")
+        dg = torch.from_numpy(gy).cuda()
+        net.forward(batch, Z, Y, X, dx.data_ptr(), 1.0, 1.0, dy.data_ptr())
+        net.backward(dg.data_ptr())
+        net.sync()
+        out[tc] = (dy.cpu().numpy(), net.grads())
+    assert rel(out[True][0], out[False][0]) < 5e-3
+    off = 0
+    for name, cin, cout, _ in learned.LAYERS:
+        n = 27 * cout * cin
+        assert rel(out[True][1][off:off + n], out[False][1][off:off + n]) < 2e-2, name
+        off += n + cout
