@@ -43,6 +43,7 @@ struct Geo {
   int nx, ny, nz, n;
   int cut;                // 0: flat bottom (every aperture 1, nothing solid)
   int linear;             // 1: the linear path's rows (the only ghost is the lid, coefficient 2)
+  int homog;              // 1: homogeneous ghosts, value 0 (refine_mobile3, delta3d_coupling.rs:238)
   float dx, inv, rho_g, rest;
   const float* eta;       // column heights
   const float* rof;       // column roundoff (compensated sum)
@@ -153,7 +154,7 @@ __device__ __forceinline__ void ghost_up3(const Geo& g, int i, int j, int k, flo
   int col = j * g.nx + i;
   float h = __ldg(g.eta + col);
   float theta = fmaxf((h - ((float)k + 0.5f) * g.dx) / g.dx, SURFACE_THETA_MIN);
-  value = g.rho_g * ((h - g.rest) - __ldg(g.rof + col));
+  value = g.homog ? 0.f : g.rho_g * ((h - g.rest) - __ldg(g.rof + col));
   it = 1.f / theta;
 }
 
@@ -162,7 +163,7 @@ __device__ __forceinline__ void ghost_side3(const Geo& g, int i, int j, int k, i
   float zc = ((float)k + 0.5f) * g.dx;
   float h = __ldg(g.eta + j * g.nx + i);
   float theta = fmaxf((h - zc) / (h - __ldg(g.eta + y * g.nx + x)), SURFACE_THETA_MIN);
-  value = g.rho_g * (zc - g.rest);
+  value = g.homog ? 0.f : g.rho_g * (zc - g.rest);
   it = 1.f / theta;
 }
 

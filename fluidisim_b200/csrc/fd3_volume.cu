@@ -84,6 +84,9 @@ struct fd3_volume {
   // multigrid
   bool has_mg = false;
   bool linear = false;            // the current projection is the linear path's
+  // homogeneous ghosts (refine_mobile3).  Only the assembly and the correction read ghost values;
+  // the inner loop's kernels read ghost coefficients only, so the loop graph does not depend on it.
+  bool homog = false;
   bool precondition_cut = true;   // Jacobi on the linear cut path (set_precondition_cut, delta3d.rs:526)
   float *z = nullptr, *z2 = nullptr;
   std::vector<Lev> levels;
@@ -128,6 +131,7 @@ struct fd3_volume {
     G.nx = nx; G.ny = ny; G.nz = nz; G.n = n;
     G.cut = cut ? 1 : 0;
     G.linear = linear ? 1 : 0;
+    G.homog = homog ? 1 : 0;
     G.dx = dx;
     G.inv = 1.f / (dx * dx);
     G.rho_g = rho * g;
@@ -1235,6 +1239,39 @@ int fd3_project_mobile(fd3_volume* V, float scale, float k1, uint32_t max_iters,
     cudaStreamSynchronize(V->stream);
   }
   return e;
+}
+
+__global__ void k_add_into(int n, float* __restrict__ p, const float* __restrict__ base) {
+  KSTART();
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < n) p[c] += base[c];
+}
+
+// refine_mobile3 (delta3d_coupling.rs:226-248): the pressure before the call is the base; the
+// current field is projected again from p = 0 with homogeneous ghosts and the increment is added
+// to the base.  A refusal leaves u, v, w, p untouched.
+int fd3_refine_mobile(fd3_volume* V, float scale, float k1, uint32_t max_iters, fd3_report* rep) {
+  if (!V || !rep) return FD3_ERR_INVALID_ARGUMENT;
+  CK(cudaMemcpyAsync(V->us, V->u, (size_t)V->nu * 4, cudaMemcpyDeviceToDevice, V->stream));
+  CK(cudaMemcpyAsync(V->vs, V->v, (size_t)V->nv * 4, cudaMemcpyDeviceToDevice, V->stream));
+  CK(cudaMemcpyAsync(V->ws, V->w, (size_t)V->nw * 4, cudaMemcpyDeviceToDevice, V->stream));
+  CK(cudaMemcpyAsync(V->sv_p, V->p, (size_t)V->n * 4, cudaMemcpyDeviceToDevice, V->stream));
+  CK(cudaMemsetAsync(V->p, 0, (size_t)V->n * 4, V->stream));
+  V->homog = true;
+  int e = project_mobile3(V, scale, k1, max_iters, rep);
+  V->homog = false;
+  if (e) {
+    cudaMemcpyAsync(V->u, V->us, (size_t)V->nu * 4, cudaMemcpyDeviceToDevice, V->stream);
+    cudaMemcpyAsync(V->v, V->vs, (size_t)V->nv * 4, cudaMemcpyDeviceToDevice, V->stream);
+    cudaMemcpyAsync(V->w, V->ws, (size_t)V->nw * 4, cudaMemcpyDeviceToDevice, V->stream);
+    cudaMemcpyAsync(V->p, V->sv_p, (size_t)V->n * 4, cudaMemcpyDeviceToDevice, V->stream);
+    cudaStreamSynchronize(V->stream);
+    return e;
+  }
+  LAUNCH(V, k_add_into, V->n, V->n, V->p, (const float*)V->sv_p);
+  TRY(sync(V));
+  rep->refinements = 1;
+  return FD3_OK;
 }
 
 int fd3_step_surface_mobile(fd3_volume* V, uint64_t duration_us, uint32_t max_iters, fd3_report* rep) {

@@ -107,6 +107,7 @@ def library() -> C.CDLL:
     L.fd3_set_velocity_device.argtypes = [vp, vp, vp, vp]
     L.fd3_reset_pressure.argtypes = [vp]
     L.fd3_project_mobile.argtypes = [vp, f32, f32, u32, C.POINTER(_Report)]
+    L.fd3_refine_mobile.argtypes = [vp, f32, f32, u32, C.POINTER(_Report)]
     L.fd3_step_surface_mobile.argtypes = [vp, u64, u32, C.POINTER(_Report)]
     L.fd3_last_refused_report.argtypes = [vp, C.POINTER(_Report)]
     L.fd3_project_linear.argtypes = [vp, f32, f32, u32, C.POINTER(_Report)]
@@ -254,6 +255,14 @@ class Volume3:
         r = _Report()
         self._check(self._L.fd3_project_mobile(self._h, np.float32(scale), np.float32(k1), int(max_iters),
                                                C.byref(r)), "project_mobile3")
+        return Report._from(r)
+
+    def refine_mobile3(self, scale, k1, max_iters=4000) -> Report:
+        """refine_mobile3 (delta3d_coupling.rs:226-248): project the current field again from p = 0 with
+        homogeneous ghosts and add the increment to the current pressure."""
+        r = _Report()
+        self._check(self._L.fd3_refine_mobile(self._h, np.float32(scale), np.float32(k1), int(max_iters),
+                                              C.byref(r)), "refine_mobile3")
         return Report._from(r)
 
     def step_surface_mobile(self, duration_us, max_iters=4000) -> Report:

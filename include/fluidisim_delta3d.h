@@ -143,6 +143,12 @@ int fd3_reset_pressure(fd3_volume* v);
 /* project_mobile3 (delta3d_mobile.rs:465) of the current velocity field: us = u, then the
  * projection with `scale` (-rho/dt) and `k1` (dt/rho), as tests_delta3d.rs:389-400 does. */
 int fd3_project_mobile(fd3_volume* v, float scale, float k1, uint32_t max_iters, fd3_report* report);
+/* refine_mobile3 (delta3d_coupling.rs:226-248), the reference's defect correction of a projection
+ * that stopped at its floor: the current pressure is kept as the base, the current (corrected)
+ * velocity field is projected again from p = 0 with homogeneous ghosts (ghost values 0,
+ * delta3d_mobile.rs:130, 140), and the pressure increment is added to the base.  report is that
+ * second projection's, with refinements = 1.  A refusal leaves u, v, w and p untouched. */
+int fd3_refine_mobile(fd3_volume* v, float scale, float k1, uint32_t max_iters, fd3_report* report);
 /* Volume3::step_surface_mobile (delta3d_mobile.rs:819): advect, project, extrapolate, transport. */
 int fd3_step_surface_mobile(fd3_volume* v, uint64_t duration_us, uint32_t max_iters, fd3_report* report);
 /* No reference counterpart: many independent volumes (patches), each projected as

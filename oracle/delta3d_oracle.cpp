@@ -729,6 +729,7 @@ struct Row { bool has; size_t n; R a, it, value; };
 struct Volume3 {
   Domain3 d;
   R rho, g_eff, rest;
+  bool homogeneous_ghost = false;  // delta3d.rs:110: ghost values 0 (the refinement's increment problem)
   std::vector<R> prec, eta, eta_roundoff, u, v, w, us, vs, ws, p, rhs, res, dir, tmp;
   std::vector<R> saved_u, saved_v, saved_w, saved_p, saved_eta, saved_eta_roundoff, flux_x, flux_y;
   bool has_cut = false;
@@ -763,7 +764,7 @@ struct Volume3 {
   void ghost_up3(size_t i, size_t j, size_t k, R& it, R& value) const {
     size_t cc = col(i, j);
     R theta = rmax((height3(i, j) - ((R)k + (R)0.5) * d.dx) / d.dx, SURFACE_THETA_MIN);
-    value = rho * g_eff * ((eta[cc] - rest) - eta_roundoff[cc]);
+    value = homogeneous_ghost ? (R)0 : rho * g_eff * ((eta[cc] - rest) - eta_roundoff[cc]);
     it = (R)1 / theta;
   }
   // delta3d_mobile.rs:136-147
@@ -771,7 +772,7 @@ struct Volume3 {
     R zc = ((R)k + (R)0.5) * d.dx;
     R h = height3(i, j);
     R theta = rmax((h - zc) / (h - height3(x, y)), SURFACE_THETA_MIN);
-    value = rho * g_eff * (zc - rest);
+    value = homogeneous_ghost ? (R)0 : rho * g_eff * (zc - rest);
     it = (R)1 / theta;
   }
   // delta3d_mobile.rs:152-188
@@ -1952,6 +1953,23 @@ int od3_project_mobile(Volume3* v, float scale, float k1, uint32_t max_iters, do
   if (!v || !rep) return INVALID;
   v->us = v->u; v->vs = v->v; v->ws = v->w;
   return v->project_mobile3((R)scale, (R)k1, max_iters, rep);
+}
+
+// refine_mobile3 (delta3d_coupling.rs:226-248): one defect-correction pass of the mobile projection.
+// The corrected field is projected again from p = 0 with homogeneous ghosts, and the pressure
+// increment is added to the pressure it starts from.
+int od3_refine_mobile(Volume3* v, float scale, float k1, uint32_t max_iters, double rep[8]) {
+  if (!v || !rep) return INVALID;
+  std::vector<R> base = v->p;
+  v->us = v->u; v->vs = v->v; v->ws = v->w;
+  std::fill(v->p.begin(), v->p.end(), (R)0);
+  v->homogeneous_ghost = true;
+  int e = v->project_mobile3((R)scale, (R)k1, max_iters, rep);
+  v->homogeneous_ghost = false;
+  if (e) return e;
+  for (size_t q = 0; q < v->p.size(); ++q) v->p[q] += base[q];
+  rep[0] = 1;  // refinements
+  return OK;
 }
 
 // Projects the current velocity field on the linear (fixed-lid) path: us = u, then project

@@ -94,6 +94,7 @@ def lib(real: str = "f32") -> C.CDLL:
     L.od3_take_zmax.argtypes = []
     L.od3_take_zmax.restype = C.c_double
     L.od3_project_linear.argtypes = [vp, f32, f32, u32, dp]
+    L.od3_refine_mobile.argtypes = [vp, f32, f32, u32, dp]
     L.od3_step_surface_linear.argtypes = [vp, u64, u32, dp]
     L.od3_set_precondition_cut.argtypes = [vp, C.c_int]
     _LIBS[real] = L
@@ -217,6 +218,13 @@ class OracleVolume:
         rep = (C.c_double * 8)()
         self._check(self.L.od3_project_mobile(self.h, np.float32(scale), np.float32(k1), max_iters, rep),
                     "project_mobile")
+        return report_dict(rep)
+
+    def refine_mobile(self, scale, k1, max_iters=4000) -> dict:
+        """refine_mobile3 (delta3d_coupling.rs:226-248) of the current state."""
+        rep = (C.c_double * 8)()
+        self._check(self.L.od3_refine_mobile(self.h, np.float32(scale), np.float32(k1), max_iters, rep),
+                    "refine_mobile")
         return report_dict(rep)
 
     def step_surface_mobile(self, duration_us, max_iters=4000) -> dict:

@@ -198,3 +198,31 @@ def test_refusals_leave_the_published_fields_untouched():
     with pytest.raises(Delta3dError) as e:
         Volume3.configure(0, 4, 4, 0.25)
     assert e.value.kind == "Domain"
+
+
+# ------------------------------------------------------------------------------------ refinement
+@pytest.mark.parametrize("reduction", [REDUCE_ORDERED_F32, REDUCE_F64])
+@pytest.mark.parametrize("cap", [3, 4000])
+def test_refinement_matches_the_oracle(reduction, cap):
+    """refine_mobile3 (delta3d_coupling.rs:226-248) after a capped or a converged projection."""
+    o, d, s = lake_pair(32, mg=True, reduction=reduction)
+    scale, k1 = scenes.projection_scalars(s)
+    ro = o.project_mobile(scale, k1, cap)
+    rd = d.project_mobile3(scale, k1, cap)
+    assert rd.degraded == ro["degraded"]
+    ro = o.refine_mobile(scale, k1, 4000)
+    rd = d.refine_mobile3(scale, k1, 4000)
+    assert rd.refinements == 1 and ro["refinements"] == 1
+    _compare_projection(o, d, ro, rd, reduction == REDUCE_ORDERED_F32)
+
+
+def test_refinement_refusal_leaves_the_fields_untouched():
+    o, d, s = lake_pair(32, mg=True)
+    scale, k1 = scenes.projection_scalars(s)
+    d.project_mobile3(scale, k1, 3)
+    before = [d.pressure().copy(), *[x.copy() for x in d.velocity()]]
+    with pytest.raises(Delta3dError) as e:
+        d.refine_mobile3(float("nan"), k1, 4000)
+    assert e.value.kind == "NotFinite"
+    for a, b in zip(before, [d.pressure(), *d.velocity()]):
+        assert_bits(a, b, "published field")
