@@ -81,6 +81,11 @@ struct fd3_volume {
   unsigned short* codes = nullptr;  // row codes of the current projection
   float *sv_u = nullptr, *sv_v = nullptr, *sv_w = nullptr, *sv_p = nullptr, *sv_eta = nullptr, *sv_rof = nullptr;
   float *flux_x = nullptr, *flux_y = nullptr;
+  // a volume configured with a solid: its node SDF buffer and the bottom-only base geometry the
+  // cut is redone from when the solid moves (Base3, delta3d_cut.rs:53-80): fractions, apertures,
+  // floors, the solid volume per column and the water it deposited
+  float *sdf = nullptr, *bfrac = nullptr, *bou = nullptr, *bov = nullptr, *bow = nullptr, *bfloor = nullptr;
+  float *bcol = nullptr, *bdep = nullptr;
   // multigrid
   bool has_mg = false;
   bool linear = false;            // the current projection is the linear path's
@@ -747,6 +752,89 @@ __global__ void k_close_walls(Geo g, float* __restrict__ u, float* __restrict__ 
   }
 }
 
+// Geometry copies: fractions, the three aperture families and the floors.
+int copy_cut(fd3_volume* V, float* frac, float* ou, float* ov, float* ow, float* floor, const float* sfrac,
+             const float* sou, const float* sov, const float* sow, const float* sfloor) {
+  CK(cudaMemcpyAsync(frac, sfrac, (size_t)V->n * 4, cudaMemcpyDeviceToDevice, V->stream));
+  CK(cudaMemcpyAsync(ou, sou, (size_t)V->nu * 4, cudaMemcpyDeviceToDevice, V->stream));
+  CK(cudaMemcpyAsync(ov, sov, (size_t)V->nv * 4, cudaMemcpyDeviceToDevice, V->stream));
+  CK(cudaMemcpyAsync(ow, sow, (size_t)V->nw * 4, cudaMemcpyDeviceToDevice, V->stream));
+  CK(cudaMemcpyAsync(floor, sfloor, (size_t)V->ncol * 4, cudaMemcpyDeviceToDevice, V->stream));
+  return FD3_OK;
+}
+
+// solid_columns (delta3d.rs:85-98): the solid volume of each column, (sum over k of base - frac in
+// f64, in k order) * dx^3, rounded to f32.
+__global__ void k_solid_columns(int nx, int ny, int nz, float dx, const float* __restrict__ base,
+                                const float* __restrict__ frac, float* __restrict__ out) {
+  KSTART();
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nx * ny) return;
+  double s = 0.;
+  for (int k = 0; k < nz; ++k) s += (double)(base[(long long)k * nx * ny + c] - frac[(long long)k * nx * ny + c]);
+  const double d = (double)dx;
+  out[c] = (float)(s * (d * d * d));
+}
+
+// The rigid motion of a solid: translation v, rotation w (rad/s) about c.
+struct Rigid {
+  float v[3], w[3], c[3];
+};
+// wall_velocity (delta3d.rs:75-82): component `axis` of v + w x (x - c).
+__device__ __forceinline__ float wall_velocity(const Rigid& R, int axis, float x0, float x1, float x2) {
+  const float r0 = x0 - R.c[0], r1 = x1 - R.c[1], r2 = x2 - R.c[2];
+  if (axis == 0) return R.v[0] + (R.w[1] * r2 - R.w[2] * r1);
+  if (axis == 1) return R.v[1] + (R.w[2] * r0 - R.w[0] * r2);
+  return R.v[2] + (R.w[0] * r1 - R.w[1] * r0);
+}
+
+// delta3d.rs:412-441: a face the new cut closes loses its velocity; a face it opens starts at the
+// wall's velocity at the face centre.
+__global__ void k_wall_faces(int nx, int ny, int nz, float dx, const float* __restrict__ ou, const float* __restrict__ ov,
+                             const float* __restrict__ ow, const float* __restrict__ old_u,
+                             const float* __restrict__ old_v, const float* __restrict__ old_w, float* __restrict__ u,
+                             float* __restrict__ v, float* __restrict__ w, Rigid R) {
+  KSTART();
+  const long long nu = (long long)(nx + 1) * ny * nz, nv = (long long)nx * (ny + 1) * nz,
+                  nw = (long long)nx * ny * (nz + 1);
+  long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (q < nu) {
+    const int i = (int)(q % (nx + 1)), t = (int)(q / (nx + 1)), j = t % ny, k = t / ny;
+    if (ou[q] == 0.f) u[q] = 0.f;
+    else if (old_u[q] == 0.f) u[q] = wall_velocity(R, 0, (float)i * dx, ((float)j + 0.5f) * dx, ((float)k + 0.5f) * dx);
+    return;
+  }
+  q -= nu;
+  if (q < nv) {
+    const int i = (int)(q % nx), t = (int)(q / nx), j = t % (ny + 1), k = t / (ny + 1);
+    if (ov[q] == 0.f) v[q] = 0.f;
+    else if (old_v[q] == 0.f) v[q] = wall_velocity(R, 1, ((float)i + 0.5f) * dx, (float)j * dx, ((float)k + 0.5f) * dx);
+    return;
+  }
+  q -= nv;
+  if (q < nw) {
+    const int i = (int)(q % nx), t = (int)(q / nx), j = t % ny, k = t / ny;
+    if (ow[q] == 0.f) w[q] = 0.f;
+    else if (old_w[q] == 0.f) w[q] = wall_velocity(R, 2, ((float)i + 0.5f) * dx, ((float)j + 0.5f) * dx, (float)k * dx);
+  }
+}
+
+// delta3d.rs:443-453: the solid volume a column gains raises its surface, a compensated f32 sum
+// on (eta, roundoff); the deposit and the base column volume follow.
+__global__ void k_displace_columns(int ncol, float area, const float* __restrict__ cols, float* __restrict__ bcol,
+                                   float* __restrict__ bdep, float* __restrict__ eta, float* __restrict__ rof) {
+  KSTART();
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncol) return;
+  const float nc = cols[c], oc = bcol[c];
+  bdep[c] += (nc - oc) / area;
+  const float increment = (nc - oc) / area - rof[c];
+  const float height = eta[c] + increment;
+  rof[c] = (height - eta[c]) - increment;
+  eta[c] = height;
+  bcol[c] = nc;
+}
+
 int check_finite_device(fd3_volume* V, const float* x, long long n, bool* ok) {
   CK(cudaMemsetAsync(V->dflag, 0, sizeof(int), V->stream));
   LAUNCH_G(V, k_check_finite, 592, TPB, n, x, V->dflag);
@@ -1070,12 +1158,74 @@ int fd3_configure_with_solid(const fd3_domain* domain, float rho, float g_eff, c
   cudaMemcpyAsync(V->hflag, V->dflag, sizeof(int), cudaMemcpyDeviceToHost, V->stream);
   if ((e = sync(V))) return fail(e);
   if (*V->hflag) return fail(FD3_ERR_DOMAIN);
+  // the bottom-only cut, kept as the base (delta3d.rs:359-363)
+  V->sdf = dsdf;
+  if ((e = dalloc(V, &V->bfrac, V->n)) || (e = dalloc(V, &V->bou, V->nu)) || (e = dalloc(V, &V->bov, V->nv)) ||
+      (e = dalloc(V, &V->bow, V->nw)) || (e = dalloc(V, &V->bfloor, V->ncol)) || (e = dalloc(V, &V->bcol, V->ncol)) ||
+      (e = dalloc(V, &V->bdep, V->ncol)))
+    return fail(e);
+  if ((e = copy_cut(V, V->bfrac, V->bou, V->bov, V->bow, V->bfloor, V->frac, V->ou, V->ov, V->ow, V->floor_)))
+    return fail(e);
   LAUNCH(V, k_add_solid, all, S, V->frac, V->ou, V->ov, V->ow, V->floor_);
   CutGeo C{V->nx, V->ny, V->nz, V->dx, nullptr, V->frac, V->ou, V->ov, V->ow, V->floor_};
   LAUNCH(V, k_seal_isolated, V->n, C);
+  LAUNCH(V, k_solid_columns, V->ncol, V->nx, V->ny, V->nz, V->dx, (const float*)V->bfrac, (const float*)V->frac,
+         V->bcol);
   if ((e = sync(V))) return fail(e);
   *out = V;
   return FD3_OK;
+}
+
+// set_solid_rigid (delta3d.rs:382-509).  Volumes of this API carry a solid that may not reach the
+// lid layer (configure_with_solid: piercing = false, check_solid), so no lid face is ever cut and
+// the partial-lid transfer of delta3d.rs:460-503 moves nothing; it is not carried out.  The cut
+// is redone from the base on the device: k_check_solid against the base, the base copied back,
+// k_add_solid and k_seal_isolated; then the faces' velocities, the solid volume per column and
+// the compensated rise of the surface.  The previous apertures go to the saved-velocity buffers,
+// free between steps as in the reference, and the new column volumes to rhs.
+int fd3_set_solid_rigid(fd3_volume* V, const float* solid, size_t len, const float* velocity, const float* angular,
+                        const float* center) {
+  if (!V || !solid || !velocity || !angular || !center) return FD3_ERR_INVALID_ARGUMENT;
+  if (len != (size_t)(V->nx + 1) * (V->ny + 1) * (V->nz + 1)) return FD3_ERR_SHAPE;
+  for (int a = 0; a < 3; ++a)
+    if (!std::isfinite(velocity[a]) || !std::isfinite(angular[a]) || !std::isfinite(center[a]))
+      return FD3_ERR_NOT_FINITE;
+  if (!V->sdf) return FD3_ERR_DOMAIN;
+  CK(cudaMemcpyAsync(V->sdf, solid, len * sizeof(float), cudaMemcpyHostToDevice, V->stream));
+  bool ok = false;
+  TRY(check_finite_device(V, V->sdf, (long long)len, &ok));
+  if (!ok) return FD3_ERR_NOT_FINITE;
+  SolidGeo S{V->nx, V->ny, V->nz, V->dx, V->sdf, 0};
+  const long long all = (long long)V->n + V->nu + V->nv + V->nw;
+  CK(cudaMemsetAsync(V->dflag, 0, sizeof(int), V->stream));
+  LAUNCH(V, k_check_solid, all, S, (const float*)V->bfrac, (const float*)V->bou, (const float*)V->bov,
+         (const float*)V->bow, V->dflag);
+  CK(cudaMemcpyAsync(V->hflag, V->dflag, sizeof(int), cudaMemcpyDeviceToHost, V->stream));
+  TRY(sync(V));
+  if (*V->hflag) return FD3_ERR_DOMAIN;
+  CK(cudaMemcpyAsync(V->sv_u, V->ou, (size_t)V->nu * 4, cudaMemcpyDeviceToDevice, V->stream));
+  CK(cudaMemcpyAsync(V->sv_v, V->ov, (size_t)V->nv * 4, cudaMemcpyDeviceToDevice, V->stream));
+  CK(cudaMemcpyAsync(V->sv_w, V->ow, (size_t)V->nw * 4, cudaMemcpyDeviceToDevice, V->stream));
+  TRY(copy_cut(V, V->frac, V->ou, V->ov, V->ow, V->floor_, V->bfrac, V->bou, V->bov, V->bow, V->bfloor));
+  LAUNCH(V, k_add_solid, all, S, V->frac, V->ou, V->ov, V->ow, V->floor_);
+  CutGeo C{V->nx, V->ny, V->nz, V->dx, nullptr, V->frac, V->ou, V->ov, V->ow, V->floor_};
+  LAUNCH(V, k_seal_isolated, V->n, C);
+  Rigid R;
+  for (int a = 0; a < 3; ++a) { R.v[a] = velocity[a]; R.w[a] = angular[a]; R.c[a] = center[a]; }
+  LAUNCH(V, k_wall_faces, (long long)V->nu + V->nv + V->nw, V->nx, V->ny, V->nz, V->dx, (const float*)V->ou,
+         (const float*)V->ov, (const float*)V->ow, (const float*)V->sv_u, (const float*)V->sv_v,
+         (const float*)V->sv_w, V->u, V->v, V->w, R);
+  LAUNCH(V, k_solid_columns, V->ncol, V->nx, V->ny, V->nz, V->dx, (const float*)V->bfrac, (const float*)V->frac,
+         V->rhs);
+  LAUNCH(V, k_displace_columns, V->ncol, V->ncol, V->dx * V->dx, (const float*)V->rhs, V->bcol, V->bdep, V->eta,
+         V->rof);
+  return sync(V);
+}
+
+// Volume3::set_solid (delta3d.rs:376-378): set_solid_rigid without rotation.
+int fd3_set_solid(fd3_volume* V, const float* solid, size_t len, const float* velocity) {
+  const float zero[3] = {0.f, 0.f, 0.f};
+  return fd3_set_solid_rigid(V, solid, len, velocity, zero, zero);
 }
 
 void fd3_destroy(fd3_volume* v) {

@@ -108,6 +108,8 @@ def library() -> C.CDLL:
     L.fd3_reset_pressure.argtypes = [vp]
     L.fd3_project_mobile.argtypes = [vp, f32, f32, u32, C.POINTER(_Report)]
     L.fd3_refine_mobile.argtypes = [vp, f32, f32, u32, C.POINTER(_Report)]
+    L.fd3_set_solid_rigid.argtypes = [vp, fp, C.c_size_t, fp, fp, fp]
+    L.fd3_set_solid.argtypes = [vp, fp, C.c_size_t, fp]
     L.fd3_step_surface_mobile.argtypes = [vp, u64, u32, C.POINTER(_Report)]
     L.fd3_last_refused_report.argtypes = [vp, C.POINTER(_Report)]
     L.fd3_project_linear.argtypes = [vp, f32, f32, u32, C.POINTER(_Report)]
@@ -229,6 +231,20 @@ class Volume3:
         return None if n < 0 else n
 
     # ---- inputs
+    def set_solid_rigid(self, solid, velocity=(0.0, 0.0, 0.0), angular=(0.0, 0.0, 0.0), center=(0.0, 0.0, 0.0)):
+        """Volume3::set_solid_rigid (delta3d.rs:382-509): the solid's new signed distance at the nodes and
+        its rigid motion (translation, rotation in rad/s about `center`)."""
+        a = _f32(solid)
+        vel, ang, cen = _f32(velocity), _f32(angular), _f32(center)
+        self._check(self._L.fd3_set_solid_rigid(self._h, _fp(a), a.size, _fp(vel), _fp(ang), _fp(cen)),
+                    "set_solid_rigid")
+
+    def set_solid(self, solid, velocity=(0.0, 0.0, 0.0)):
+        """Volume3::set_solid (delta3d.rs:376-378)."""
+        a = _f32(solid)
+        vel = _f32(velocity)
+        self._check(self._L.fd3_set_solid(self._h, _fp(a), a.size, _fp(vel)), "set_solid")
+
     def set_free_surface(self, eta, rest):
         a = _f32(eta)
         self._check(self._L.fd3_set_free_surface(self._h, _fp(a), a.size, np.float32(rest)), "set_free_surface")

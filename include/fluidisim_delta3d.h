@@ -128,6 +128,18 @@ int fd3_enable_multigrid(fd3_volume* v);
 /* Volume3::multigrid_levels (delta3d_multigrid.rs:353); -1 when not enabled. */
 int fd3_multigrid_levels(const fd3_volume* v);
 
+/* Volume3::set_solid_rigid (delta3d.rs:382-509): the solid of a volume configured with one moves
+ * as a rigid body (translation `velocity`, rotation `angular` in rad/s about `center`).  `solid` is
+ * its new signed distance at the nodes.  The cut is redone on the device from the bottom-only
+ * geometry; a face that opens takes the wall's normal velocity at its centre, a face that closes
+ * loses its own; the solid volume a column gains raises its surface (compensated).  Refusal is
+ * atomic: FD3_ERR_SHAPE, FD3_ERR_NOT_FINITE, FD3_ERR_DOMAIN (no solid, or the solid shares a cell
+ * or a face with the bottom cut or reaches the lid layer, delta3d_cut.rs:485). */
+int fd3_set_solid_rigid(fd3_volume* v, const float* solid, size_t solid_len, const float velocity[3],
+                        const float angular[3], const float center[3]);
+/* Volume3::set_solid (delta3d.rs:376-378): set_solid_rigid without rotation. */
+int fd3_set_solid(fd3_volume* v, const float* solid, size_t solid_len, const float velocity[3]);
+
 /* Volume3::set_free_surface (delta3d_mobile.rs:9): eta per column and the rest level; p = 0. */
 int fd3_set_free_surface(fd3_volume* v, const float* eta, size_t len, float rest);
 /* Volume3::set_surface (delta3d.rs:614). */

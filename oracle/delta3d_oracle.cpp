@@ -1888,6 +1888,74 @@ int od3_configure_with_solid(const od3_domain* dom, float rho, float g, const fl
   return OK;
 }
 
+// delta3d.rs:75-82: the axis component of the rigid wall velocity V + W x (x - c) at x.
+static R wall_velocity(const float vel[3], const float ang[3], const float cen[3], int axis, R x0, R x1, R x2) {
+  R r0 = x0 - (R)cen[0], r1 = x1 - (R)cen[1], r2 = x2 - (R)cen[2];
+  if (axis == 0) return (R)vel[0] + ((R)ang[1] * r2 - (R)ang[2] * r1);
+  if (axis == 1) return (R)vel[1] + ((R)ang[2] * r0 - (R)ang[0] * r2);
+  return (R)vel[2] + ((R)ang[0] * r1 - (R)ang[1] * r0);
+}
+
+// set_solid_rigid (delta3d.rs:382-509): the solid moved as a rigid body.  The cut is redone from
+// the bottom-only base; a face that opens takes the wall's normal velocity at its centre, a face
+// that closes loses its own; the solid volume a column gains raises its surface (compensated f32
+// sum).  Volumes of this API carry a solid that may not reach the lid layer (configure_with_solid,
+// piercing = false), so no lid face is ever cut and the partial-lid transfer of delta3d.rs:460-503
+// moves nothing: it is not restated.  Refusal is atomic: Shape, NotFinite, Domain (no solid, or
+// check_solid fails).
+int od3_set_solid_rigid(Volume3* v, const float* solid, uint64_t len, const float* vel, const float* ang,
+                        const float* cen) {
+  if (!v || !vel || !ang || !cen || (!solid && len)) return INVALID;
+  const Domain3 d = v->d;
+  const size_t nx = d.nx, ny = d.ny, nz = d.nz;
+  if (len != (nx + 1) * (ny + 1) * (nz + 1)) return SHAPE;
+  for (size_t q = 0; q < len; ++q) if (!std::isfinite(solid[q])) return NOT_FINITE;
+  for (int a = 0; a < 3; ++a) if (!std::isfinite(vel[a]) || !std::isfinite(ang[a]) || !std::isfinite(cen[a])) return NOT_FINITE;
+  if (!v->has_cut || !v->g.has_base) return DOMAIN;
+  Cut3& g = v->g;
+  Base3& base = g.base;
+  int e = check_solid(base.frac, base.open_u, base.open_v, base.open_w, d, solid, g.piercing);
+  if (e) return e;
+  v->saved_u = g.open_u; v->saved_v = g.open_v; v->saved_w = g.open_w;
+  g.frac = base.frac; g.open_u = base.open_u; g.open_v = base.open_v; g.open_w = base.open_w; g.floor = base.floor;
+  add_solid(g, d, solid);
+  const R dx = d.dx;
+  for (size_t k = 0; k < nz; ++k) {
+    for (size_t j = 0; j < ny; ++j)
+      for (size_t i = 0; i <= nx; ++i) {
+        size_t f = (k * ny + j) * (nx + 1) + i;
+        if (g.open_u[f] == 0) v->u[f] = 0;
+        else if (v->saved_u[f] == 0) v->u[f] = wall_velocity(vel, ang, cen, 0, (R)i * dx, ((R)j + (R)0.5) * dx, ((R)k + (R)0.5) * dx);
+      }
+    for (size_t j = 0; j <= ny; ++j)
+      for (size_t i = 0; i < nx; ++i) {
+        size_t f = (k * (ny + 1) + j) * nx + i;
+        if (g.open_v[f] == 0) v->v[f] = 0;
+        else if (v->saved_v[f] == 0) v->v[f] = wall_velocity(vel, ang, cen, 1, ((R)i + (R)0.5) * dx, (R)j * dx, ((R)k + (R)0.5) * dx);
+      }
+  }
+  for (size_t k = 0; k <= nz; ++k)
+    for (size_t j = 0; j < ny; ++j)
+      for (size_t i = 0; i < nx; ++i) {
+        size_t f = (k * ny + j) * nx + i;
+        if (g.open_w[f] == 0) v->w[f] = 0;
+        else if (v->saved_w[f] == 0) v->w[f] = wall_velocity(vel, ang, cen, 2, ((R)i + (R)0.5) * dx, ((R)j + (R)0.5) * dx, (R)k * dx);
+      }
+  std::vector<R> cols(nx * ny);
+  solid_columns(d, base.frac, g.frac, cols);
+  const R area = dx * dx;
+  for (size_t c = 0; c < nx * ny; ++c) {
+    base.deposit[c] += (cols[c] - base.solid_col[c]) / area;
+    R increment = (cols[c] - base.solid_col[c]) / area - v->eta_roundoff[c];
+    R height = v->eta[c] + increment;
+    v->eta_roundoff[c] = (height - v->eta[c]) - increment;
+    v->eta[c] = height;
+    base.solid_col[c] = cols[c];
+  }
+  v->prec_cut();
+  return OK;
+}
+
 void od3_destroy(Volume3* v) { delete v; }
 
 // delta3d_multigrid.rs:339-349 (max_levels 0 = the reference hierarchy)

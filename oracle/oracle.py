@@ -95,6 +95,7 @@ def lib(real: str = "f32") -> C.CDLL:
     L.od3_take_zmax.restype = C.c_double
     L.od3_project_linear.argtypes = [vp, f32, f32, u32, dp]
     L.od3_refine_mobile.argtypes = [vp, f32, f32, u32, dp]
+    L.od3_set_solid_rigid.argtypes = [vp, fp, u64, fp, fp, fp]
     L.od3_step_surface_linear.argtypes = [vp, u64, u32, dp]
     L.od3_set_precondition_cut.argtypes = [vp, C.c_int]
     _LIBS[real] = L
@@ -219,6 +220,13 @@ class OracleVolume:
         self._check(self.L.od3_project_mobile(self.h, np.float32(scale), np.float32(k1), max_iters, rep),
                     "project_mobile")
         return report_dict(rep)
+
+    def set_solid_rigid(self, solid, velocity=(0.0, 0.0, 0.0), angular=(0.0, 0.0, 0.0), center=(0.0, 0.0, 0.0)):
+        """set_solid_rigid (delta3d.rs:382-509): the solid's new signed distance at the nodes."""
+        a = _f32(solid)
+        vel, ang, cen = _f32(velocity), _f32(angular), _f32(center)
+        self._check(self.L.od3_set_solid_rigid(self.h, _fptr(a), a.size, _fptr(vel), _fptr(ang), _fptr(cen)),
+                    "set_solid_rigid")
 
     def refine_mobile(self, scale, k1, max_iters=4000) -> dict:
         """refine_mobile3 (delta3d_coupling.rs:226-248) of the current state."""

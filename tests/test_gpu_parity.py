@@ -226,3 +226,64 @@ def test_refinement_refusal_leaves_the_fields_untouched():
     assert e.value.kind == "NotFinite"
     for a, b in zip(before, [d.pressure(), *d.velocity()]):
         assert_bits(a, b, "published field")
+
+
+# ------------------------------------------------------------------------------------ moving solids
+def _moving_pair(reduction):
+    n, dx = 32, 0.1
+    centres = [(1.24, 1.42, 0.86), (2.10, 1.96, 1.10)]
+    radii = [0.54, 0.44]
+    sdf = scenes.spheres_sdf(n, n, n, dx, centres, radii)
+    bottom = np.zeros(n * n, np.float32)
+    o, d = pair(n, n, n, dx, bottom=bottom, solid=sdf, mg=True, reduction=reduction)
+    rng = np.random.default_rng(9)
+    u, v, w = (rng.uniform(-1, 1, k).astype(np.float32) for k in scenes.face_counts(n, n, n))
+    for x in (o, d):
+        x.set_free_surface(np.full(n * n, 2.1, np.float32), 2.1)
+        x.set_velocity(u, v, w)
+    moved = scenes.spheres_sdf(n, n, n, dx, [(x + 0.13, y - 0.06, z + 0.08) for x, y, z in centres], radii)
+    return o, d, moved, n
+
+
+@pytest.mark.parametrize("reduction", [REDUCE_ORDERED_F32, REDUCE_F64])
+def test_moving_solid_matches_the_oracle(reduction):
+    """set_solid_rigid (delta3d.rs:382-509): the re-cut geometry, the face velocities and the raised
+    surface are bit-identical to the oracle's; so is the next projection in ordered mode."""
+    o, d, moved, n = _moving_pair(reduction)
+    motion = ((0.5, -0.2, 0.1), (0.0, 0.3, -0.2), (1.6, 1.6, 1.0))
+    o.set_solid_rigid(moved, *motion)
+    d.set_solid_rigid(moved, *motion)
+    for a, b, name in zip(o.geometry(), d.geometry(), ["frac", "open_u", "open_v", "open_w", "floor"]):
+        assert_bits(a, b, name)
+    for a, b, name in zip(o.velocity(), d.velocity(), "uvw"):
+        assert_bits(a, b, name)
+    for a, b in zip(o.surface(), d.surface_and_roundoff()):
+        assert_bits(a, b, "eta/roundoff")
+    ro = o.project_mobile(-1025.0 * 60.0, 1.0 / (60.0 * 1025.0), 4000)
+    rd = d.project_mobile3(-1025.0 * 60.0, 1.0 / (60.0 * 1025.0), 4000)
+    _compare_projection(o, d, ro, rd, reduction == REDUCE_ORDERED_F32)
+
+
+@pytest.mark.parametrize("case", ["shape", "nan", "lid", "no_solid"])
+def test_moving_solid_refusals_change_nothing(case):
+    o, d, moved, n = _moving_pair(REDUCE_ORDERED_F32)
+    before = [x.copy() for x in (*d.geometry(), *d.velocity(), *d.surface_and_roundoff())]
+    kind = {"shape": "Shape", "nan": "NotFinite", "lid": "Domain", "no_solid": "Domain"}[case]
+    if case == "no_solid":
+        plain = Volume3.configure(n, n, n, 0.1)
+        with pytest.raises(Delta3dError) as e:
+            plain.set_solid_rigid(moved)
+        assert e.value.kind == kind
+        plain.close()
+        return
+    bad = moved[:-1] if case == "shape" else moved.copy()
+    if case == "nan":
+        bad[100] = np.nan
+    if case == "lid":
+        bad = scenes.spheres_sdf(n, n, n, 0.1, [(1.6, 1.6, 3.15)], [0.2])
+    with pytest.raises(Delta3dError) as e:
+        d.set_solid_rigid(bad)
+    assert e.value.kind == kind
+    after = [*d.geometry(), *d.velocity(), *d.surface_and_roundoff()]
+    for a, b in zip(before, after):
+        assert_bits(a, b, "field after a refusal")
