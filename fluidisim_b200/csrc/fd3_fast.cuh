@@ -62,6 +62,14 @@ __device__ __forceinline__ float ghost_it_up(const Geo& g, int i, int j, int k) 
 // recomputed on the fly by a fused kernel).
 // The code of a wet cell whose six faces are open (aperture 1) onto fluid neighbours: the bulk.
 constexpr unsigned RC_INTERIOR = RC_WET | RC_UNIT | (1u << 1) | (1u << 3) | (1u << 5) | (1u << 7) | (1u << 9) | (1u << 11);
+// The high bit of every face state: set on a ghost (or, on a coarse level, Dirichlet) face.
+constexpr unsigned RC_GHOSTS = (2u << 1) | (2u << 3) | (2u << 5) | (2u << 7) | (2u << 9) | (2u << 11);
+// A row whose live faces all have aperture 1 and all lead to a fluid neighbour: the bulk, and also
+// the cells along walls, closed faces and solids.  Its sum is the six differences masked by the
+// face states: a = 1 makes a (pc - x) exactly pc - x, and a missing face adds +0, which changes no
+// partial sum (the sum starts at +0 and a sum of such terms is never -0).  So the masked sum has
+// the bits of the reference's sum over the live faces in the same order.
+__device__ __forceinline__ bool rc_plain(unsigned code) { return (code & (RC_UNIT | RC_GHOSTS)) == RC_UNIT; }
 
 template <class P>
 __device__ __forceinline__ float apply_code(const Geo& g, unsigned code, int i, int j, int k, int c, P p) {
@@ -69,13 +77,13 @@ __device__ __forceinline__ float apply_code(const Geo& g, unsigned code, int i, 
   const bool unit = code & RC_UNIT;
   const int nxny = g.nx * g.ny;
   float acc = 0.f;
-  if (code == RC_INTERIOR) {  // a = 1 on every face: the same sum without the decoding
-    acc += pc - p(c - 1);
-    acc += pc - p(c + 1);
-    acc += pc - p(c - g.nx);
-    acc += pc - p(c + g.nx);
-    acc += pc - p(c - nxny);
-    acc += pc - p(c + nxny);
+  if (rc_plain(code)) {  // a = 1 on every live face, no ghost: the masked sum, without the decoding
+    acc += (code & (1u << 1)) ? pc - p(c - 1) : 0.f;
+    acc += (code & (1u << 3)) ? pc - p(c + 1) : 0.f;
+    acc += (code & (1u << 5)) ? pc - p(c - g.nx) : 0.f;
+    acc += (code & (1u << 7)) ? pc - p(c + g.nx) : 0.f;
+    acc += (code & (1u << 9)) ? pc - p(c - nxny) : 0.f;
+    acc += (code & (1u << 11)) ? pc - p(c + nxny) : 0.f;
     return acc * g.inv;
   }
   unsigned st = face_state(code, 0);
@@ -459,13 +467,13 @@ __device__ __forceinline__ float level_row_code(const Lev& L, unsigned code, int
   const float pc = p(c);
   const int nxny = L.nx * L.ny;
   float acc = 0.f;
-  if (code == RC_INTERIOR) {
-    acc += pc - p(c - 1);
-    acc += pc - p(c + 1);
-    acc += pc - p(c - L.nx);
-    acc += pc - p(c + L.nx);
-    acc += pc - p(c - nxny);
-    acc += pc - p(c + nxny);
+  if (rc_plain(code)) {  // unit apertures, no Dirichlet face: the masked sum (see rc_plain)
+    acc += (code & (1u << 1)) ? pc - p(c - 1) : 0.f;
+    acc += (code & (1u << 3)) ? pc - p(c + 1) : 0.f;
+    acc += (code & (1u << 5)) ? pc - p(c - L.nx) : 0.f;
+    acc += (code & (1u << 7)) ? pc - p(c + L.nx) : 0.f;
+    acc += (code & (1u << 9)) ? pc - p(c - nxny) : 0.f;
+    acc += (code & (1u << 11)) ? pc - p(c + nxny) : 0.f;
     return acc * L.inv;
   }
   const bool unit = code & RC_UNIT;

@@ -30,13 +30,13 @@ constexpr int ZX = 32, ZY = 8, ZK = FD3_ZK, ZT = ZX * ZY;
 __device__ __forceinline__ float apply_code_nb(const Geo& g, unsigned code, int i, int j, int k, float pc,
                                                float xm, float xp, float ym, float yp, float zm, float zp) {
   float acc = 0.f;
-  if (code == RC_INTERIOR) {  // a = 1 on every face: the same sum without the decoding
-    acc += pc - xm;
-    acc += pc - xp;
-    acc += pc - ym;
-    acc += pc - yp;
-    acc += pc - zm;
-    acc += pc - zp;
+  if (rc_plain(code)) {  // a = 1 on every live face, no ghost: the masked sum (see rc_plain)
+    acc += (code & (1u << 1)) ? pc - xm : 0.f;
+    acc += (code & (1u << 3)) ? pc - xp : 0.f;
+    acc += (code & (1u << 5)) ? pc - ym : 0.f;
+    acc += (code & (1u << 7)) ? pc - yp : 0.f;
+    acc += (code & (1u << 9)) ? pc - zm : 0.f;
+    acc += (code & (1u << 11)) ? pc - zp : 0.f;
     return acc * g.inv;
   }
   const bool unit = code & RC_UNIT;
