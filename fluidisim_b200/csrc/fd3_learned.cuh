@@ -6,6 +6,7 @@
 // Included by fd3_volume.cu after the volume driver: it uses the driver's launch helpers.
 #pragma once
 
+#include "fd3_conv_dw.cuh"
 #include "fd3_conv_tc.cuh"
 #include "fd3_unet.cuh"
 
@@ -139,7 +140,34 @@ int conv_fwd(fd3_unet* N, Dims d, int cin, int cout, int epi, const __nv_bfloat1
   return FD3_ERR_INVALID_ARGUMENT;
 }
 
+// k_conv_dw2 (all taps per CTA, persistent grid) with its dynamic shared memory.
+template <int CI, int CO>
+int conv_dw2_launch(fd3_unet* N, Dims d, const __nv_bfloat16* in, const __nv_bfloat16* gout, float* gw) {
+  static unsigned attr_set = 0;  // devices on which the limit was raised
+  const int BY = dw2_rows(d.X, d.Y);
+  const size_t smem = dw2_smem_bytes(d.X, BY, CO);
+  if (N->device < 32 && !(attr_set & (1u << N->device))) {
+    CK(cudaFuncSetAttribute(k_conv_dw2<CI, CO>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+    attr_set |= 1u << N->device;
+  }
+  int sms = 148;
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, N->device));
+  const long long nblk = (long long)d.B * d.Z * ((d.Y + BY - 1) / BY);
+  const int grid = (int)std::min<long long>(nblk, sms);
+  k_conv_dw2<CI, CO><<<grid, DW2_THREADS, smem, N->stream>>>(d, BY, in, gout, gw);
+  N->launches++;
+  CK(cudaGetLastError());
+  return FD3_OK;
+}
+
 int conv_dw(fd3_unet* N, Dims d, int cin, int cout, const __nv_bfloat16* in, const __nv_bfloat16* gout, float* gw) {
+  // the all-taps kernel where its staging fits shared memory (output channels 16 or 32)
+  if (d.X <= 256 && (cout == 16 || cout == 32) && dw2_smem_bytes(d.X, dw2_rows(d.X, d.Y), cout) <= 227 * 1024) {
+    if (cin == 16 && cout == 16) return conv_dw2_launch<16, 16>(N, d, in, gout, gw);
+    if (cin == 48 && cout == 16) return conv_dw2_launch<48, 16>(N, d, in, gout, gw);
+    if (cin == 96 && cout == 32) return conv_dw2_launch<96, 32>(N, d, in, gout, gw);
+    if (cin == 16 && cout == 32) return conv_dw2_launch<16, 32>(N, d, in, gout, gw);
+  }
   const long long cells = d.cells();
   long long slices = std::max<long long>(1, std::min<long long>(44, (cells + DW_ROWS - 1) / DW_ROWS));
   long long chunk = (cells + slices - 1) / slices;
@@ -250,7 +278,7 @@ int unet_backward(fd3_unet* N, const float* gout) {
   const long long per = (long long)d0.Z * d0.Y * d0.X;
   UnetLayer* L = N->layer;
   auto bias_grad = [&](long long cells, int C, const __nv_bfloat16* g, float* gb) {
-    return ulaunch(N, dim3(std::min<long long>(256, (cells + 255) / 256), C), 256, k_bias_grad, cells, C, g, gb);
+    return ulaunch(N, dim3(std::min<long long>(256, (cells + 255) / 256), C / 8), 256, k_bias_grad, cells, C, g, gb);
   };
   // head
   TRY(ulaunch(N, dim3(grid_for(n0)), 256, k_out_grad_scaled, n0, per, gout, (const float*)N->out_scale, N->gy));
@@ -262,25 +290,25 @@ int unet_backward(fd3_unet* N, const float* gout) {
   TRY(conv_dw(N, d0, 48, 16, N->c0, N->gd0, L[L_D0].gw));
   TRY(bias_grad(n0, 16, N->gd0, L[L_D0].gb));
   TRY(conv_fwd(N, d0, 16, 48, EPI_PLAIN, N->gd0, L[L_D0].wt, nullptr, N->gc0, nullptr));
-  TRY(ulaunch(N, dim3(grid_for(n1 * 32)), 256, k_up_bwd, d1, 48, 32, (const __nv_bfloat16*)N->gc0,
+  TRY(ulaunch(N, dim3(grid_for(n1 * 4)), 256, k_up_bwd, d1, 48, 32, (const __nv_bfloat16*)N->gc0,
               (const __nv_bfloat16*)N->d1, N->gd1));
   // d1: input c1 = cat(up(b), e1)
   TRY(conv_dw(N, d1, 96, 32, N->c1, N->gd1, L[L_D1].gw));
   TRY(bias_grad(n1, 32, N->gd1, L[L_D1].gb));
   TRY(conv_fwd(N, d1, 32, 96, EPI_PLAIN, N->gd1, L[L_D1].wt, nullptr, N->gc1, nullptr));
-  TRY(ulaunch(N, dim3(grid_for(n2 * 64)), 256, k_up_bwd, d2, 96, 64, (const __nv_bfloat16*)N->gc1,
+  TRY(ulaunch(N, dim3(grid_for(n2 * 8)), 256, k_up_bwd, d2, 96, 64, (const __nv_bfloat16*)N->gc1,
               (const __nv_bfloat16*)N->bq, N->gbq));
   // b: input p1 = pool(e1)
   TRY(conv_dw(N, d2, 32, 64, N->p1, N->gbq, L[L_B].gw));
   TRY(bias_grad(n2, 64, N->gbq, L[L_B].gb));
   TRY(conv_fwd(N, d2, 64, 32, EPI_PLAIN, N->gbq, L[L_B].wt, nullptr, N->gp1, nullptr));
-  TRY(ulaunch(N, dim3(grid_for(n1 * 32)), 256, k_enc_grad, d1, 32, (const __nv_bfloat16*)N->gc1, 96, 64,
+  TRY(ulaunch(N, dim3(grid_for(n1 * 4)), 256, k_enc_grad, d1, 32, (const __nv_bfloat16*)N->gc1, 96, 64,
               (const __nv_bfloat16*)N->gp1, (const __nv_bfloat16*)N->e1, N->ge1));
   // e1: input p0 = pool(e0)
   TRY(conv_dw(N, d1, 16, 32, N->p0, N->ge1, L[L_E1].gw));
   TRY(bias_grad(n1, 32, N->ge1, L[L_E1].gb));
   TRY(conv_fwd(N, d1, 32, 16, EPI_PLAIN, N->ge1, L[L_E1].wt, nullptr, N->gp0, nullptr));
-  TRY(ulaunch(N, dim3(grid_for(n0 * 16)), 256, k_enc_grad, d0, 16, (const __nv_bfloat16*)N->gc0, 48, 32,
+  TRY(ulaunch(N, dim3(grid_for(n0 * 2)), 256, k_enc_grad, d0, 16, (const __nv_bfloat16*)N->gc0, 48, 32,
               (const __nv_bfloat16*)N->gp0, (const __nv_bfloat16*)N->e0, N->ge0));
   // e0: input x0
   TRY(conv_dw(N, d0, 16, 16, N->x0, N->ge0, L[L_E0].gw));

@@ -18,7 +18,7 @@ namespace fd3u {
 constexpr int CONV_THREADS = 256;          // 8 warps, 32 cells each
 constexpr int CONV_CELLS = CONV_THREADS;   // cells per CTA
 constexpr int DW_THREADS = 256;
-constexpr int DW_ROWS = 64;                // cells staged per step of the weight-gradient GEMM
+constexpr int DW_ROWS = 128;               // cells staged per step of the weight-gradient GEMM
 
 struct Dims {
   int B, Z, Y, X;  // samples and grid of this level
@@ -161,6 +161,7 @@ __global__ void __launch_bounds__(DW_THREADS) k_conv_dw(Dims d, const __nv_bfloa
   constexpr int TPW = (TILES + 7) / 8;  // tiles per warp
   __shared__ __align__(16) __nv_bfloat16 sG[DW_ROWS * GS];
   __shared__ __align__(16) __nv_bfloat16 sI[DW_ROWS * IS];
+  __shared__ long long snb[DW_ROWS];  // the tap's neighbour of each staged row (-1: outside)
   const int tap = blockIdx.x;
   const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -173,6 +174,10 @@ __global__ void __launch_bounds__(DW_THREADS) k_conv_dw(Dims d, const __nv_bfloa
     for (int e = 0; e < 4; ++e) acc[q][e] = 0.f;
 
   for (long long s = c0; s < c1; s += DW_ROWS) {
+    // the neighbour of each row once (one cell position per row, not per 16-byte piece)
+    for (int r = threadIdx.x; r < DW_ROWS; r += DW_THREADS)
+      snb[r] = s + r < c1 ? neighbour(d, cell_pos(d, s + r), dz, dy, dx) : -1;
+    __syncthreads();
     // stage: 16-byte pieces (8 channels) of DW_ROWS rows
     for (int p = threadIdx.x; p < DW_ROWS * (COUT / 8); p += DW_THREADS) {
       const int r = p / (COUT / 8), k = p % (COUT / 8);
@@ -185,10 +190,8 @@ __global__ void __launch_bounds__(DW_THREADS) k_conv_dw(Dims d, const __nv_bfloa
       const int r = p / (CIN / 8), k = p % (CIN / 8);
       const long long q = s + r;
       uint4 v = make_uint4(0, 0, 0, 0);
-      if (q < c1) {
-        const long long nb = neighbour(d, cell_pos(d, q), dz, dy, dx);
-        if (nb >= 0) v = *reinterpret_cast<const uint4*>(in + nb * CIN + k * 8);
-      }
+      const long long nb = snb[r];
+      if (q < c1 && nb >= 0) v = *reinterpret_cast<const uint4*>(in + nb * CIN + k * 8);
       *reinterpret_cast<uint4*>(sI + r * IS + k * 8) = v;
     }
     __syncthreads();
@@ -231,15 +234,30 @@ __global__ void __launch_bounds__(DW_THREADS) k_conv_dw(Dims d, const __nv_bfloa
   }
 }
 
-// Bias gradient: gb[co] += sum over cells of gOut[cell][co] (grid-stride, one atomic per warp).
+// Bias gradient: gb[co] += sum over cells of gOut[cell][co].  blockIdx.y picks an 8-channel group;
+// each thread sums the 16-byte group of its cells (grid-stride), then one atomic per warp and channel.
 __global__ void k_bias_grad(long long cells, int C, const __nv_bfloat16* __restrict__ g, float* __restrict__ gb) {
-  const int co = blockIdx.y;
-  float s = 0.f;
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < cells; q += (long long)gridDim.x * blockDim.x)
-    s += __bfloat162float(g[q * C + co]);
+  const int grp = blockIdx.y;
+  float s[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < cells; q += (long long)gridDim.x * blockDim.x) {
+    const uint4 v = *reinterpret_cast<const uint4*>(g + q * C + grp * 8);
+    const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&v);
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-  if ((threadIdx.x & 31) == 0) atomicAdd(gb + co, s);
+    for (int k = 0; k < 4; ++k) {
+      const float2 t = __bfloat1622float2(h[k]);
+      s[2 * k] += t.x;
+      s[2 * k + 1] += t.y;
+    }
+  }
+#pragma unroll
+  for (int e = 0; e < 8; ++e) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s[e] += __shfl_down_sync(0xffffffffu, s[e], o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+    for (int e = 0; e < 8; ++e) atomicAdd(gb + grp * 8 + e, s[e]);
+  }
 }
 
 // Mean of the 8 children: fine [B][2Z][2Y][2X][C] -> coarse [B][Z][Y][X][C] (d = coarse dims).
@@ -303,46 +321,73 @@ __global__ void k_up_cat(Dims fd, int C1, int C2, const __nv_bfloat16* __restric
 }
 
 // Gradient through cat(up(.), skip) into the coarse part: gc[parent][ch] = sum over the 8
-// children of g[child][ch] (ch < C1 of the C-wide gradient), times the ReLU mask of act.
+// children of g[child][ch] (ch < C1 of the C-wide gradient), times the ReLU mask of act.  One thread
+// per (coarse cell, 8-channel group); the children are summed in f32 in the order e = 0..7.
 __global__ void k_up_bwd(Dims cd, int C, int C1, const __nv_bfloat16* __restrict__ g,
                          const __nv_bfloat16* __restrict__ act, __nv_bfloat16* __restrict__ gc) {
-  const long long n = cd.cells() * C1;
+  const int G1 = C1 / 8;
+  const long long n = cd.cells() * G1;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
-    const int ch = (int)(q % C1);
-    long long c = q / C1;
+    const int grp = (int)(q % G1);
+    long long c = q / G1;
+    const long long cell = c;
     const int x = (int)(c % cd.X); c /= cd.X;
     const int y = (int)(c % cd.Y); c /= cd.Y;
     const int z = (int)(c % cd.Z);
     const long long b = c / cd.Z;
     const int FX = 2 * cd.X, FY = 2 * cd.Y, FZ = 2 * cd.Z;
-    float s = 0.f;
+    float s[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
 #pragma unroll
     for (int e = 0; e < 8; ++e) {
       const long long f = ((b * FZ + 2 * z + (e >> 2)) * FY + 2 * y + ((e >> 1) & 1)) * FX + 2 * x + (e & 1);
-      s += __bfloat162float(g[f * C + ch]);
+      const uint4 v = *reinterpret_cast<const uint4*>(g + f * C + grp * 8);
+      const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&v);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const float2 t = __bfloat1622float2(h[k]);
+        s[2 * k] += t.x;
+        s[2 * k + 1] += t.y;
+      }
     }
-    gc[q] = __float2bfloat16(__bfloat162float(act[q]) > 0.f ? s : 0.f);
+    const uint4 av = *reinterpret_cast<const uint4*>(act + cell * C1 + grp * 8);
+    const __nv_bfloat16* a = reinterpret_cast<const __nv_bfloat16*>(&av);
+    __align__(16) __nv_bfloat16 o[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) o[e] = __float2bfloat16(__bfloat162float(a[e]) > 0.f ? s[e] : 0.f);
+    *reinterpret_cast<uint4*>(gc + cell * C1 + grp * 8) = *reinterpret_cast<const uint4*>(o);
   }
 }
 
 // Gradient of an encoder activation: (skip part of the concat gradient + pool backward of the next
 // level's input gradient) times its ReLU mask.  g: [fine][C] slice at channel offset off of a
-// Cg-wide tensor; gp: [coarse][C]; act, out: [fine][C].
+// Cg-wide tensor; gp: [coarse][C]; act, out: [fine][C].  One thread per (fine cell, 8-channel group).
 __global__ void k_enc_grad(Dims fd, int C, const __nv_bfloat16* __restrict__ g, int Cg, int off,
                            const __nv_bfloat16* __restrict__ gp, const __nv_bfloat16* __restrict__ act,
                            __nv_bfloat16* __restrict__ out) {
-  const long long n = fd.cells() * C;
+  const int G = C / 8;
+  const long long n = fd.cells() * G;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
-    const int ch = (int)(q % C);
-    long long c = q / C;
+    const int grp = (int)(q % G);
+    long long c = q / G;
     const long long cell = c;
     const int x = (int)(c % fd.X); c /= fd.X;
     const int y = (int)(c % fd.Y); c /= fd.Y;
     const int z = (int)(c % fd.Z);
     const long long b = c / fd.Z;
     const long long p = ((b * (fd.Z / 2) + z / 2) * (fd.Y / 2) + y / 2) * (fd.X / 2) + x / 2;
-    const float v = __bfloat162float(g[cell * Cg + off + ch]) + 0.125f * __bfloat162float(gp[p * C + ch]);
-    out[q] = __float2bfloat16(__bfloat162float(act[q]) > 0.f ? v : 0.f);
+    const uint4 gv = *reinterpret_cast<const uint4*>(g + cell * Cg + off + grp * 8);
+    const uint4 pv = *reinterpret_cast<const uint4*>(gp + p * C + grp * 8);
+    const uint4 av = *reinterpret_cast<const uint4*>(act + cell * C + grp * 8);
+    const __nv_bfloat16* ge = reinterpret_cast<const __nv_bfloat16*>(&gv);
+    const __nv_bfloat16* pe = reinterpret_cast<const __nv_bfloat16*>(&pv);
+    const __nv_bfloat16* ae = reinterpret_cast<const __nv_bfloat16*>(&av);
+    __align__(16) __nv_bfloat16 o[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      const float v = __bfloat162float(ge[e]) + 0.125f * __bfloat162float(pe[e]);
+      o[e] = __float2bfloat16(__bfloat162float(ae[e]) > 0.f ? v : 0.f);
+    }
+    *reinterpret_cast<uint4*>(out + cell * C + grp * 8) = *reinterpret_cast<const uint4*>(o);
   }
 }
 
