@@ -24,6 +24,20 @@ constexpr unsigned RC_UNIT = 1u << 13;
 
 __device__ __forceinline__ unsigned face_state(unsigned code, int f) { return (code >> (1 + 2 * f)) & 3u; }
 
+// The code of a wet cell's row.
+__device__ __forceinline__ unsigned row_code_of(const RowE (&row)[6]) {
+  unsigned code = RC_WET;
+  bool unit = true;
+#pragma unroll
+  for (int f = 0; f < 6; ++f) {
+    unsigned st = row[f].n >= 0 ? 1u : (row[f].a > 0.f ? 2u : 0u);
+    code |= st << (1 + 2 * f);
+    if (st && row[f].a != 1.f) unit = false;
+  }
+  if (unit) code |= RC_UNIT;
+  return code;
+}
+
 __global__ void k_row_codes(Geo g, unsigned short* __restrict__ codes) {
   KSTART();
   int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -32,15 +46,7 @@ __global__ void k_row_codes(Geo g, unsigned short* __restrict__ codes) {
   unsigned code = 0;
   if (wet3(g, i, j, k)) {
     RowE row[6]; mobile_row(g, i, j, k, row);
-    code = RC_WET;
-    bool unit = true;
-#pragma unroll
-    for (int f = 0; f < 6; ++f) {
-      unsigned st = row[f].n >= 0 ? 1u : (row[f].a > 0.f ? 2u : 0u);
-      code |= st << (1 + 2 * f);
-      if (st && row[f].a != 1.f) unit = false;
-    }
-    if (unit) code |= RC_UNIT;
+    code = row_code_of(row);
   }
   codes[c] = (unsigned short)code;
 }
@@ -899,16 +905,20 @@ __global__ void k_loop_cond(cudaGraphConditionalHandle handle, Scalars* S) {
 // Set-up reductions with the in-kernel finish.
 
 // rhs_mobile3 (delta3d_mobile.rs:215-241) with b.b (FIN_B2) when `reduce`.
+// With `codes` not null, the same pass also writes each cell's row code (k_row_codes, from the
+// same row).
 template <int MODE>
 __global__ void __launch_bounds__(TPB) k_rhs_b2(Geo g, float scale, float* __restrict__ rhs, float* __restrict__ prec,
-                                                Red red, Scalars* S, int reduce) {
+                                                Red red, Scalars* S, int reduce, unsigned short* __restrict__ codes) {
   KSTART();
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   float b = 0.f;
   if (c < g.n) {
     int i, j, k; cell_ijk(g, c, i, j, k);
-    if (!wet3(g, i, j, k)) { rhs[c] = 0.f; prec[c] = 0.f; }
-    else {
+    if (!wet3(g, i, j, k)) {
+      rhs[c] = 0.f; prec[c] = 0.f;
+      if (codes) codes[c] = 0;
+    } else {
       RowE row[6]; mobile_row(g, i, j, k, row);
       b = scale * rhs[c];
       float diag = 0.f;
@@ -922,6 +932,7 @@ __global__ void __launch_bounds__(TPB) k_rhs_b2(Geo g, float scale, float* __res
       }
       rhs[c] = b;
       prec[c] = diag > 0.f ? 1.f / (diag * g.inv) : 0.f;
+      if (codes) codes[c] = (unsigned short)row_code_of(row);
     }
   }
   if (!reduce) return;

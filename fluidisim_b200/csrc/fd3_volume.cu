@@ -619,8 +619,7 @@ int project_mobile3(fd3_volume* V, float scale, float k1, uint32_t max_iters, fd
     LAUNCH(V, k_row_codes_linear, V->n, G, V->codes);
     CK(cudaMemsetAsync(V->p, 0, (size_t)V->n * sizeof(float), V->stream));
   } else {
-    DISPATCH(V, k_rhs_b2, V->n, G, scale, V->rhs, V->prec, V->red(), V->dS, 1);
-    LAUNCH(V, k_row_codes, V->n, G, V->codes);
+    DISPATCH(V, k_rhs_b2, V->n, G, scale, V->rhs, V->prec, V->red(), V->dS, 1, V->codes);
     if (V->has_mg) prepare_multigrid(V);
     LAUNCH(V, k_zero_dry, V->n, G, V->p);
   }
@@ -1593,7 +1592,7 @@ int fd3_assemble_pressure_problem_for_trials(fd3_volume* V, const float* diverge
   TRY(check_finite_device(V, V->tmp, V->n, &ok));
   if (!ok) return FD3_ERR_NOT_FINITE;
   CK(cudaMemcpyAsync(V->rhs, V->tmp, len * 4, cudaMemcpyDeviceToDevice, V->stream));
-  DISPATCH(V, k_rhs_b2, V->n, V->geo(), scale, V->rhs, V->prec, V->red(), V->dS, 0);
+  DISPATCH(V, k_rhs_b2, V->n, V->geo(), scale, V->rhs, V->prec, V->red(), V->dS, 0, (unsigned short*)nullptr);
   CK(cudaMemcpyAsync(rhs, V->rhs, len * 4, cudaMemcpyDeviceToHost, V->stream));
   CK(cudaMemcpyAsync(prec, V->prec, len * 4, cudaMemcpyDeviceToHost, V->stream));
   return sync(V);
@@ -1605,8 +1604,7 @@ int fd3_vcycle_for_tests(fd3_volume* V, const float* x, float* z, size_t len) {
   if (!V->has_mg) return FD3_ERR_DOMAIN;
   if (len != (size_t)V->n) return FD3_ERR_SHAPE;
   CK(cudaMemsetAsync(V->rhs, 0, len * 4, V->stream));
-  DISPATCH(V, k_rhs_b2, V->n, V->geo(), 1.f, V->rhs, V->prec, V->red(), V->dS, 0);
-  LAUNCH(V, k_row_codes, V->n, V->geo(), V->codes);
+  DISPATCH(V, k_rhs_b2, V->n, V->geo(), 1.f, V->rhs, V->prec, V->red(), V->dS, 0, V->codes);
   prepare_multigrid(V);
   CK(cudaMemcpyAsync(V->res, x, len * 4, cudaMemcpyHostToDevice, V->stream));
   if (V->half()) LAUNCH_G(V, k_reset_scalars, 1, 1, V->dS, 0.f);  // FP16 storage, r unscaled (vinv = 1)

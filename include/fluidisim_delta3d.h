@@ -275,8 +275,10 @@ int fd3_residual_loss(fd3_volume* v, const float* d_z, const float* d_b, float w
 
 /* project_mobile3 with the learned FCG in front (from the current p): FCG(1) with the network as
  * the preconditioner until the reference tolerance, max_fcg iterations or a stall, then the
- * reference acceptance loop, whose multigrid PCG continues from FCG's p when needed.  report is
- * that loop's (its iterations are the fallback's); fcg_iterations and fell_back describe FCG. */
+ * reference acceptance loop.  When FCG reached the tolerance the loop starts from its p; when it
+ * stalled (or hit max_fcg), its p is discarded and the loop's multigrid PCG, the fallback, starts
+ * from the pressure the call started with.  report is that loop's (its iterations are the
+ * fallback's); fcg_iterations and fell_back describe FCG. */
 int fd3_project_learned(fd3_volume* v, fd3_unet* net, float scale, float k1, uint32_t max_iters, uint32_t max_fcg,
                         fd3_report* report, uint32_t* fcg_iterations, int* fell_back);
 
