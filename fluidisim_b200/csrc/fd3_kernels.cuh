@@ -51,6 +51,7 @@ struct Geo {
   const float* ou;        // apertures (cut only)
   const float* ov;
   const float* ow;
+  const unsigned char* act;  // sparse column set, 1 per column in the domain (null: every column)
 };
 
 // A coarse level (Level3, delta3d_multigrid.rs:37-52).
@@ -132,7 +133,38 @@ struct Red {
 // ------------------------------------------------------------------------------------------------
 // Geometry predicates (delta3d_mobile.rs:92-124)
 
-__device__ __forceinline__ bool solid3(const Geo& g, int c) { return g.cut && __ldg(g.frac + c) == 0.f; }
+// The sparse column set (delta3d_sparse.rs:256-319).  A column outside the set is solid for every
+// operator; an interior u or v face touching such a column, and every w face of one, is closed.
+// Faces on the box's boundary keep the box's treatment.
+__device__ __forceinline__ bool col_active(const Geo& g, int i, int j) {
+  return !g.act || __ldg(g.act + j * g.nx + i) != 0;
+}
+__device__ __forceinline__ bool sparse_closed_ij(const unsigned char* __restrict__ act, int nx, int ny, int axis,
+                                                 int i, int j) {
+  if (axis == 0) return i > 0 && i < nx && (__ldg(act + j * nx + i - 1) == 0 || __ldg(act + j * nx + i) == 0);
+  if (axis == 1) return j > 0 && j < ny && (__ldg(act + (j - 1) * nx + i) == 0 || __ldg(act + j * nx + i) == 0);
+  return __ldg(act + j * nx + i) == 0;
+}
+__device__ __forceinline__ bool sparse_closed3(const Geo& g, int axis, int f) {
+  int i, j;
+  if (axis == 0) { i = f % (g.nx + 1); j = (f / (g.nx + 1)) % g.ny; }
+  else if (axis == 1) { i = f % g.nx; j = (f / g.nx) % (g.ny + 1); }
+  else { const int col = f % (g.nx * g.ny); i = col % g.nx; j = col / g.nx; }
+  return sparse_closed_ij(g.act, g.nx, g.ny, axis, i, j);
+}
+// sparse_outside3 (delta3d_sparse.rs:307-319): the face of axis `axis` at column position (i, j)
+// touches no column of the set.
+__device__ __forceinline__ bool sparse_outside3(const Geo& g, int axis, int i, int j) {
+  if (!g.act) return false;
+  if (axis == 0) return !((i > 0 && col_active(g, i - 1, j)) || (i < g.nx && col_active(g, i, j)));
+  if (axis == 1) return !((j > 0 && col_active(g, i, j - 1)) || (j < g.ny && col_active(g, i, j)));
+  return !col_active(g, i, j);
+}
+
+__device__ __forceinline__ bool solid3(const Geo& g, int c) {
+  if (g.cut && __ldg(g.frac + c) == 0.f) return true;
+  return g.act && __ldg(g.act + c % (g.nx * g.ny)) == 0;
+}
 
 __device__ __forceinline__ bool wet3(const Geo& g, int i, int j, int k) {
   int c = (k * g.ny + j) * g.nx + i;
@@ -140,9 +172,17 @@ __device__ __forceinline__ bool wet3(const Geo& g, int i, int j, int k) {
   return ((float)k + 0.5f) * g.dx < __ldg(g.eta + j * g.nx + i);
 }
 
-__device__ __forceinline__ float open3(const Geo& g, int axis, int f) {
+// The cut's aperture of a face, 1 on a flat bottom.  The hot stencils read it only on a face a row
+// code marks live, which the sparse set never closes.
+__device__ __forceinline__ float aper3(const Geo& g, int axis, int f) {
   if (!g.cut) return 1.f;
   return __ldg((axis == 0 ? g.ou : (axis == 1 ? g.ov : g.ow)) + f);
+}
+
+// open3 (delta3d_mobile.rs:105-119): 0 on a face the sparse set closes, else the cut's aperture.
+__device__ __forceinline__ float open3(const Geo& g, int axis, int f) {
+  if (g.act && sparse_closed3(g, axis, f)) return 0.f;
+  return aper3(g, axis, f);
 }
 
 __device__ __forceinline__ int fu(const Geo& g, int i, int j, int k) { return (k * g.ny + j) * (g.nx + 1) + i; }
@@ -464,7 +504,7 @@ __global__ void k_coarsen_kind_level(Lev F, Lev C) {
 // Coarse apertures: mean of the 4 fine faces a coarse face covers.  `fo*` are the fine apertures
 // (nullptr: a flat fine level, every aperture 1).  fnx/fny are the fine dimensions.
 __global__ void k_coarsen_open(int fnx, int fny, const float* __restrict__ fou, const float* __restrict__ fov,
-                               const float* __restrict__ fow, Lev C) {
+                               const float* __restrict__ fow, const unsigned char* __restrict__ act, Lev C) {
   KSTART();
   int cx = C.nx, cy = C.ny, cz = C.nz;
   int nu = (cx + 1) * cy * cz, nv = cx * (cy + 1) * cz, nw = cx * cy * (cz + 1);
@@ -475,7 +515,9 @@ __global__ void k_coarsen_open(int fnx, int fny, const float* __restrict__ fou, 
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
       int dj = e & 1, dk = e >> 1;
-      s += fou ? fou[((2 * k + dk) * fny + 2 * j + dj) * (fnx + 1) + 2 * i] : 1.f;
+      float a = fou ? fou[((2 * k + dk) * fny + 2 * j + dj) * (fnx + 1) + 2 * i] : 1.f;
+      if (act && sparse_closed_ij(act, fnx, fny, 0, 2 * i, 2 * j + dj)) a = 0.f;
+      s += a;
     }
     C.ou[q] = 0.25f * s;
     return;
@@ -487,7 +529,9 @@ __global__ void k_coarsen_open(int fnx, int fny, const float* __restrict__ fou, 
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
       int di = e & 1, dk = e >> 1;
-      s += fov ? fov[((2 * k + dk) * (fny + 1) + 2 * j) * fnx + 2 * i + di] : 1.f;
+      float a = fov ? fov[((2 * k + dk) * (fny + 1) + 2 * j) * fnx + 2 * i + di] : 1.f;
+      if (act && sparse_closed_ij(act, fnx, fny, 1, 2 * i + di, 2 * j)) a = 0.f;
+      s += a;
     }
     C.ov[q] = 0.25f * s;
     return;
@@ -499,7 +543,9 @@ __global__ void k_coarsen_open(int fnx, int fny, const float* __restrict__ fou, 
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
       int di = e & 1, dj = e >> 1;
-      s += fow ? fow[((2 * k) * fny + 2 * j + dj) * fnx + 2 * i + di] : 1.f;
+      float a = fow ? fow[((2 * k) * fny + 2 * j + dj) * fnx + 2 * i + di] : 1.f;
+      if (act && sparse_closed_ij(act, fnx, fny, 2, 2 * i + di, 2 * j + dj)) a = 0.f;
+      s += a;
     }
     C.ow[q] = 0.25f * s;
   }
@@ -708,8 +754,10 @@ __global__ void k_advect(Geo g, float dt, const float* __restrict__ u, const flo
       float dn = k > 0 ? val(a, b, k - 1) : uc;
       float uz = (upv - dn) * h;
       float wc = 0.25f * (vertical(a - 1, b, k) + vertical(a, b, k) + vertical(a - 1, b, k + 1) + vertical(a, b, k + 1));
-      float rt = b + 1 < nb ? val(a, b + 1, k) : uc;
-      float lf = b > 0 ? val(a, b - 1, k) : uc;
+      // the edge of the sparse set reads as the box's edge (delta3d_mobile.rs:664-667)
+      auto outside = [&](int A, int B) { return axis == 0 ? sparse_outside3(g, 0, A, B) : sparse_outside3(g, 1, B, A); };
+      float rt = b + 1 < nb && !outside(a, b + 1) ? val(a, b + 1, k) : uc;
+      float lf = b > 0 && !outside(a, b - 1) ? val(a, b - 1, k) : uc;
       float uy = (rt - lf) * h;
       float vc = 0.25f * (transverse(a - 1, b, k) + transverse(a, b, k) + transverse(a - 1, b + 1, k) + transverse(a, b + 1, k));
       cur = uc - dt * (uc * ux + wc * uz + vc * uy);
@@ -724,13 +772,13 @@ __global__ void k_advect(Geo g, float dt, const float* __restrict__ u, const flo
   float cur = w[f];
   if (k >= 1 && k < nz && open3(g, 2, f) != 0.f) {
     float wc = w[f];
-    float rt = i + 1 < nx ? w[fw(g, i + 1, j, k)] : wc;
-    float lf = i > 0 ? w[fw(g, i - 1, j, k)] : wc;
+    float rt = i + 1 < nx && !sparse_outside3(g, 2, i + 1, j) ? w[fw(g, i + 1, j, k)] : wc;
+    float lf = i > 0 && !sparse_outside3(g, 2, i - 1, j) ? w[fw(g, i - 1, j, k)] : wc;
     float wx = (rt - lf) * h;
     float wz = (w[fw(g, i, j, k + 1)] - w[fw(g, i, j, k - 1)]) * h;
     float uc = 0.25f * (u[fu(g, i, j, k - 1)] + u[fu(g, i + 1, j, k - 1)] + u[fu(g, i, j, k)] + u[fu(g, i + 1, j, k)]);
-    float bk = j + 1 < ny ? w[fw(g, i, j + 1, k)] : wc;
-    float fr = j > 0 ? w[fw(g, i, j - 1, k)] : wc;
+    float bk = j + 1 < ny && !sparse_outside3(g, 2, i, j + 1) ? w[fw(g, i, j + 1, k)] : wc;
+    float fr = j > 0 && !sparse_outside3(g, 2, i, j - 1) ? w[fw(g, i, j - 1, k)] : wc;
     float wy = (bk - fr) * h;
     float vc = 0.25f * (v[fv(g, i, j, k - 1)] + v[fv(g, i, j + 1, k - 1)] + v[fv(g, i, j, k)] + v[fv(g, i, j + 1, k)]);
     cur = wc - dt * (uc * wx + wc * wz + vc * wy);

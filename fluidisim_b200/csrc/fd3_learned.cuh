@@ -391,7 +391,7 @@ __global__ void k_fcg_input(Geo g, const unsigned short* __restrict__ codes, con
   if (c < g.n) {
     const float rc = r[c];
     in3[3 * c] = rc;
-    in3[3 * c + 1] = (g.cut && __ldg(g.frac + c) == 0.f) ? 1.f : 0.f;
+    in3[3 * c + 1] = solid3(g, c) ? 1.f : 0.f;
     in3[3 * c + 2] = (codes[c] & RC_WET) ? 1.f : 0.f;
     rr = (double)rc * (double)rc;
   }

@@ -86,6 +86,11 @@ struct fd3_volume {
   // floors, the solid volume per column and the water it deposited
   float *sdf = nullptr, *bfrac = nullptr, *bou = nullptr, *bov = nullptr, *bow = nullptr, *bfloor = nullptr;
   float *bcol = nullptr, *bdep = nullptr;
+  // the sparse column set (Sparse3, delta3d_sparse.rs:31-44): device mask, a scratch mask of the
+  // columns leaving it, and the host copy the refusals and the published counts read
+  bool sparse = false;
+  unsigned char *act = nullptr, *act_next = nullptr;
+  std::vector<unsigned char> hact;
   // multigrid
   bool has_mg = false;
   bool linear = false;            // the current projection is the linear path's
@@ -143,6 +148,7 @@ struct fd3_volume {
     G.rest = rest;
     G.eta = eta; G.rof = rof;
     G.frac = frac; G.ou = ou; G.ov = ov; G.ow = ow;
+    G.act = sparse ? act : nullptr;
     return G;
   }
   bool ord() const { return opt.reduction == FD3_REDUCE_ORDERED_F32; }
@@ -153,7 +159,7 @@ struct fd3_volume {
   bool half() const { return opt.storage == FD3_STORAGE_F16 && paired() && mg_on(); }
   int loop_key() const {
     return (ord() ? 1 : 0) | (mg_on() ? 2 : 0) | (blocked() ? 4 : 0) | (opt.no_overlap ? 8 : 0) | (linear ? 16 : 0) |
-           (paired() ? 32 : 0) | (half() ? 64 : 0);
+           (paired() ? 32 : 0) | (half() ? 64 : 0) | (sparse ? 128 : 0);  // the captured Geo holds the set's mask
   }
   Red red() const { return Red{p64, p32, count}; }
 };
@@ -274,11 +280,13 @@ void prepare_multigrid(fd3_volume* V) {
                        (long long)C.nx * C.ny * (C.nz + 1);
     if (l == 0) {
       LAUNCH(V, k_coarsen_kind_fine, C.n, G, C);
-      LAUNCH(V, k_coarsen_open, nfaces, V->nx, V->ny, (const float*)V->ou, (const float*)V->ov, (const float*)V->ow, C);
+      LAUNCH(V, k_coarsen_open, nfaces, V->nx, V->ny, (const float*)V->ou, (const float*)V->ov, (const float*)V->ow,
+             (const unsigned char*)G.act, C);
     } else {
       Lev& F = V->levels[l - 1];
       LAUNCH(V, k_coarsen_kind_level, C.n, F, C);
-      LAUNCH(V, k_coarsen_open, nfaces, F.nx, F.ny, (const float*)F.ou, (const float*)F.ov, (const float*)F.ow, C);
+      LAUNCH(V, k_coarsen_open, nfaces, F.nx, F.ny, (const float*)F.ou, (const float*)F.ov, (const float*)F.ow,
+             (const unsigned char*)nullptr, C);
     }
     LAUNCH(V, k_level_diag, C.n, C);
     LAUNCH(V, k_level_codes, C.n, C);
@@ -729,26 +737,64 @@ __global__ void k_check_finite(long long n, const float* __restrict__ x, int* fl
   if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(flag, 1);
 }
 
-// close_walls (delta3d.rs:666-690): walls, bottom, and faces the cut closes have no velocity.
+// A face of a column whose byte in `m` equals `mark` (clear_column_faces, delta3d_sparse.rs:213-233):
+// the column's two u faces, two v faces and every w face.
+__device__ __forceinline__ bool column_face(const unsigned char* __restrict__ m, unsigned char mark, int nx, int ny,
+                                            int axis, int i, int j) {
+  if (axis == 0) return (i < nx && m[j * nx + i] == mark) || (i > 0 && m[j * nx + i - 1] == mark);
+  if (axis == 1) return (j < ny && m[j * nx + i] == mark) || (j > 0 && m[(j - 1) * nx + i] == mark);
+  return m[j * nx + i] == mark;
+}
+
+// close_walls (delta3d.rs:666-690): walls, bottom, and faces the cut closes have no velocity;
+// then close_sparse_walls (delta3d_sparse.rs:236-247): nor has any face of a column outside the
+// sparse set (g.act, 0 for those columns).
 __global__ void k_close_walls(Geo g, float* __restrict__ u, float* __restrict__ v, float* __restrict__ w) {
+  const unsigned char* out = g.act;
   int nu = (g.nx + 1) * g.ny * g.nz, nv = g.nx * (g.ny + 1) * g.nz, nw = g.nx * g.ny * (g.nz + 1);
   int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q < nu) {
-    int i = q % (g.nx + 1);
-    if (i == 0 || i == g.nx || (g.cut && g.ou[q] == 0.f)) u[q] = 0.f;
+    int i = q % (g.nx + 1), j = (q / (g.nx + 1)) % g.ny;
+    if (i == 0 || i == g.nx || (g.cut && g.ou[q] == 0.f) || (out && column_face(out, 0, g.nx, g.ny, 0, i, j))) u[q] = 0.f;
     return;
   }
   q -= nu;
   if (q < nv) {
-    int j = (q / g.nx) % (g.ny + 1);
-    if (j == 0 || j == g.ny || (g.cut && g.ov[q] == 0.f)) v[q] = 0.f;
+    int i = q % g.nx, j = (q / g.nx) % (g.ny + 1);
+    if (j == 0 || j == g.ny || (g.cut && g.ov[q] == 0.f) || (out && column_face(out, 0, g.nx, g.ny, 1, i, j))) v[q] = 0.f;
     return;
   }
   q -= nv;
   if (q < nw) {
-    int k = q / (g.nx * g.ny);
-    if (k == 0 || (g.cut && g.ow[q] == 0.f)) w[q] = 0.f;
+    int k = q / (g.nx * g.ny), col = q % (g.nx * g.ny);
+    if (k == 0 || (g.cut && g.ow[q] == 0.f) || (out && out[col] == 0)) w[q] = 0.f;
   }
+}
+
+// Columns leaving the sparse set go to rest (apply_sparse, delta3d_sparse.rs:181-210): surface,
+// roundoff, pressure and every face of the column.  `leave` marks them; vmax collects the largest
+// |velocity| cleared, as the bits of a non-negative float (ordered like the integers).
+__global__ void k_sparse_leave(Geo g, const unsigned char* __restrict__ leave, float rest, float* __restrict__ eta,
+                               float* __restrict__ rof, float* __restrict__ p, float* __restrict__ u,
+                               float* __restrict__ v, float* __restrict__ w, int* vmax) {
+  const int nx = g.nx, ny = g.ny, ncol = nx * ny;
+  const int nu = (nx + 1) * ny * g.nz, nv = nx * (ny + 1) * g.nz, nw = ncol * (g.nz + 1);
+  long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  int cleared = 0;
+  if (q < ncol) {
+    if (leave[q]) { eta[q] = rest; rof[q] = 0.f; }
+  } else if ((q -= ncol) < g.n) {
+    if (leave[q % ncol]) p[q] = 0.f;
+  } else if ((q -= g.n) < nu) {
+    int i = (int)(q % (nx + 1)), j = (int)((q / (nx + 1)) % ny);
+    if (column_face(leave, 1, nx, ny, 0, i, j)) { cleared = __float_as_int(fabsf(u[q])); u[q] = 0.f; }
+  } else if ((q -= nu) < nv) {
+    int i = (int)(q % nx), j = (int)((q / nx) % (ny + 1));
+    if (column_face(leave, 1, nx, ny, 1, i, j)) { cleared = __float_as_int(fabsf(v[q])); v[q] = 0.f; }
+  } else if ((q -= nv) < nw) {
+    if (leave[q % ncol]) { cleared = __float_as_int(fabsf(w[q])); w[q] = 0.f; }
+  }
+  if (cleared) atomicMax(vmax, cleared);
 }
 
 // Geometry copies: fractions, the three aperture families and the floors.
@@ -1310,6 +1356,19 @@ int fd3_enable_multigrid(fd3_volume* V) {
 
 int fd3_multigrid_levels(const fd3_volume* v) { return v && v->has_mg ? (int)v->levels.size() : -1; }
 
+// sparse_surface_ok (delta3d_sparse.rs:327-332): outside the set the surface is `rest`, to the bit.
+static bool sparse_surface_ok(const fd3_volume* V, const float* eta, float rest) {
+  if (!V->sparse) return true;
+  uint32_t rb;
+  std::memcpy(&rb, &rest, 4);
+  for (int c = 0; c < V->ncol; ++c) {
+    uint32_t eb;
+    std::memcpy(&eb, eta + c, 4);
+    if (!V->hact[c] && eb != rb) return false;
+  }
+  return true;
+}
+
 // delta3d_mobile.rs:9-25
 int fd3_set_free_surface(fd3_volume* V, const float* eta, size_t len, float rest) {
   if (!V || (!eta && len)) return FD3_ERR_INVALID_ARGUMENT;
@@ -1317,6 +1376,7 @@ int fd3_set_free_surface(fd3_volume* V, const float* eta, size_t len, float rest
   if (!std::isfinite(rest)) return FD3_ERR_NOT_FINITE;
   for (size_t q = 0; q < len; ++q)
     if (!std::isfinite(eta[q])) return FD3_ERR_NOT_FINITE;
+  if (!sparse_surface_ok(V, eta, rest)) return FD3_ERR_DOMAIN;  // delta3d_mobile.rs:16-19
   CK(cudaMemcpyAsync(V->eta, eta, len * sizeof(float), cudaMemcpyHostToDevice, V->stream));
   CK(cudaMemsetAsync(V->rof, 0, len * sizeof(float), V->stream));
   CK(cudaMemsetAsync(V->p, 0, (size_t)V->n * sizeof(float), V->stream));
@@ -1330,6 +1390,7 @@ int fd3_set_surface(fd3_volume* V, const float* eta, size_t len) {
   if (len != (size_t)V->ncol) return FD3_ERR_SHAPE;
   for (size_t q = 0; q < len; ++q)
     if (!std::isfinite(eta[q])) return FD3_ERR_NOT_FINITE;
+  if (!sparse_surface_ok(V, eta, V->rest)) return FD3_ERR_DOMAIN;  // delta3d.rs:621-624
   CK(cudaMemcpyAsync(V->eta, eta, len * sizeof(float), cudaMemcpyHostToDevice, V->stream));
   CK(cudaMemsetAsync(V->rof, 0, len * sizeof(float), V->stream));
   return sync(V);
@@ -1364,6 +1425,107 @@ int fd3_set_velocity_device(fd3_volume* V, const float* u, const float* vv, cons
   CK(cudaMemcpyAsync(V->vs, vv, (size_t)V->nv * 4, cudaMemcpyDeviceToDevice, V->stream));
   CK(cudaMemcpyAsync(V->ws, w, (size_t)V->nw * 4, cudaMemcpyDeviceToDevice, V->stream));
   return set_velocity_staged(V);
+}
+
+// ------------------------------------------------------------------------------- sparse sets
+// enable_sparse (delta3d_sparse.rs:105-117): the masks are reserved here, every column in the set.
+int fd3_enable_sparse(fd3_volume* V) {
+  if (!V) return FD3_ERR_INVALID_ARGUMENT;
+  if (V->sparse) return FD3_ERR_DOMAIN;
+  float *a, *b;
+  TRY(dalloc(V, &a, ((size_t)V->ncol + 3) / 4));
+  TRY(dalloc(V, &b, ((size_t)V->ncol + 3) / 4));
+  V->act = (unsigned char*)a;
+  V->act_next = (unsigned char*)b;
+  V->hact.assign(V->ncol, 1);
+  CK(cudaMemcpyAsync(V->act, V->hact.data(), V->ncol, cudaMemcpyHostToDevice, V->stream));
+  TRY(sync(V));
+  V->sparse = true;
+  return FD3_OK;
+}
+
+// apply_sparse (delta3d_sparse.rs:181-210): `next` replaces the set.  What the leaving columns
+// carried is counted on the host in the reference's column order (its f64 sum is published), then
+// one kernel puts them to rest.
+static int apply_sparse(fd3_volume* V, const std::vector<unsigned char>& next, fd3_sparse_change* out) {
+  const int nx = V->nx, ny = V->ny, ncol = V->ncol;
+  std::vector<float> e(ncol), r(ncol);
+  CK(cudaMemcpyAsync(e.data(), V->eta, (size_t)ncol * 4, cudaMemcpyDeviceToHost, V->stream));
+  CK(cudaMemcpyAsync(r.data(), V->rof, (size_t)ncol * 4, cudaMemcpyDeviceToHost, V->stream));
+  TRY(sync(V));
+  fd3_sparse_change ch{};
+  std::vector<unsigned char> leave(ncol, 0);
+  const double area = (double)V->dx * (double)V->dx;
+  for (int j = 0; j < ny; ++j)
+    for (int i = 0; i < nx; ++i) {
+      const int c = j * nx + i;
+      const bool was = V->hact[c] != 0, will = next[c] != 0;
+      if (was && !will) {
+        ++ch.deactivated;
+        leave[c] = 1;
+        const double h = ((double)e[c] - (double)r[c]) - (double)V->rest;
+        ch.volume_removed += h * area;
+        ch.height_removed = std::max(ch.height_removed, std::fabs(e[c] - V->rest));
+      } else if (!was && will) {
+        ++ch.activated;
+      }
+    }
+  if (ch.deactivated) {
+    CK(cudaMemcpyAsync(V->act_next, leave.data(), ncol, cudaMemcpyHostToDevice, V->stream));
+    CK(cudaMemsetAsync(V->dflag, 0, sizeof(int), V->stream));
+    LAUNCH(V, k_sparse_leave, (long long)ncol + V->n + V->nu + V->nv + V->nw, V->geo(),
+           (const unsigned char*)V->act_next, V->rest, V->eta, V->rof, V->p, V->u, V->v, V->w, V->dflag);
+    CK(cudaMemcpyAsync(V->hflag, V->dflag, sizeof(int), cudaMemcpyDeviceToHost, V->stream));
+  }
+  V->hact = next;
+  CK(cudaMemcpyAsync(V->act, V->hact.data(), ncol, cudaMemcpyHostToDevice, V->stream));
+  TRY(sync(V));
+  if (ch.deactivated) std::memcpy(&ch.velocity_removed, V->hflag, 4);
+  for (unsigned char a : V->hact) ch.active_columns += a != 0;
+  if (out) *out = ch;
+  return FD3_OK;
+}
+
+// set_active_columns (delta3d_sparse.rs:147-158)
+int fd3_set_active_columns(fd3_volume* V, const uint8_t* mask, size_t len, fd3_sparse_change* change) {
+  if (!V || (!mask && len)) return FD3_ERR_INVALID_ARGUMENT;
+  if (!V->sparse) return FD3_ERR_DOMAIN;
+  if (len != (size_t)V->ncol) return FD3_ERR_SHAPE;
+  std::vector<unsigned char> next(V->ncol);
+  for (int c = 0; c < V->ncol; ++c) next[c] = mask[c] != 0;
+  return apply_sparse(V, next, change);
+}
+
+// set_active_blocks (delta3d_sparse.rs:163-178): block (bi, bj) covers the columns
+// [(bi - origin_i) * 8, +8) x [(bj - origin_j) * 8, +8) of the window, clipped to it.
+int fd3_set_active_blocks(fd3_volume* V, const int32_t* blocks, size_t count, int32_t origin_i, int32_t origin_j,
+                          fd3_sparse_change* change) {
+  if (!V || (!blocks && count)) return FD3_ERR_INVALID_ARGUMENT;
+  if (!V->sparse) return FD3_ERR_DOMAIN;
+  const long long side = FD3_BLOCK, nx = V->nx, ny = V->ny;
+  std::vector<unsigned char> next(V->ncol, 0);
+  for (size_t b = 0; b < count; ++b) {
+    const long long i0 = ((long long)blocks[2 * b] - origin_i) * side, j0 = ((long long)blocks[2 * b + 1] - origin_j) * side;
+    for (long long j = std::max(j0, 0LL); j < std::min(j0 + side, ny); ++j)
+      for (long long i = std::max(i0, 0LL); i < std::min(i0 + side, nx); ++i) next[(size_t)(j * nx + i)] = 1;
+  }
+  return apply_sparse(V, next, change);
+}
+
+int fd3_active_columns(const fd3_volume* V, uint8_t* out, size_t len) {
+  if (!V || (!out && len)) return FD3_ERR_INVALID_ARGUMENT;
+  if (!V->sparse) return FD3_ERR_DOMAIN;
+  if (len != (size_t)V->ncol) return FD3_ERR_SHAPE;
+  std::memcpy(out, V->hact.data(), len);
+  return FD3_OK;
+}
+
+uint64_t fd3_sparse_cells(const fd3_volume* V) {
+  if (!V) return 0;
+  if (!V->sparse) return (uint64_t)V->n;
+  uint64_t cols = 0;
+  for (unsigned char a : V->hact) cols += a != 0;
+  return cols * (uint64_t)V->nz;
 }
 
 int fd3_reset_pressure(fd3_volume* V) {
@@ -1431,6 +1593,7 @@ int fd3_step_surface_mobile(fd3_volume* V, uint64_t duration_us, uint32_t max_it
 // tests_delta3d.rs:143-148: us = u, then project.  A refusal leaves u, v, w, p untouched.
 int fd3_project_linear(fd3_volume* V, float scale, float k1, uint32_t max_iters, fd3_report* rep) {
   if (!V || !rep) return FD3_ERR_INVALID_ARGUMENT;
+  if (V->sparse) return FD3_ERR_DOMAIN;  // the linear path does not carry a sparse set (delta3d.rs:1210-1211)
   CK(cudaMemcpyAsync(V->us, V->u, (size_t)V->nu * 4, cudaMemcpyDeviceToDevice, V->stream));
   CK(cudaMemcpyAsync(V->vs, V->v, (size_t)V->nv * 4, cudaMemcpyDeviceToDevice, V->stream));
   CK(cudaMemcpyAsync(V->ws, V->w, (size_t)V->nw * 4, cudaMemcpyDeviceToDevice, V->stream));
@@ -1448,6 +1611,7 @@ int fd3_project_linear(fd3_volume* V, float scale, float k1, uint32_t max_iters,
 
 int fd3_step_surface_linear(fd3_volume* V, uint64_t duration_us, uint32_t max_iters, fd3_report* rep) {
   if (!V || !rep) return FD3_ERR_INVALID_ARGUMENT;
+  if (V->sparse) return FD3_ERR_DOMAIN;  // delta3d.rs:1210-1211
   return step_surface_linear(V, duration_us, max_iters, rep);
 }
 

@@ -42,32 +42,32 @@ __device__ __forceinline__ float apply_code_nb(const Geo& g, unsigned code, int 
   const bool unit = code & RC_UNIT;
   unsigned st = face_state(code, 0);
   if (st) {
-    float a = unit ? 1.f : open3(g, 0, fu(g, i, j, k));
+    float a = unit ? 1.f : aper3(g, 0, fu(g, i, j, k));
     if (st == 1) acc += a * (pc - xm); else acc += a * pc * ghost_it_side(g, i, j, k, i - 1, j);
   }
   st = face_state(code, 1);
   if (st) {
-    float a = unit ? 1.f : open3(g, 0, fu(g, i + 1, j, k));
+    float a = unit ? 1.f : aper3(g, 0, fu(g, i + 1, j, k));
     if (st == 1) acc += a * (pc - xp); else acc += a * pc * ghost_it_side(g, i, j, k, i + 1, j);
   }
   st = face_state(code, 2);
   if (st) {
-    float a = unit ? 1.f : open3(g, 1, fv(g, i, j, k));
+    float a = unit ? 1.f : aper3(g, 1, fv(g, i, j, k));
     if (st == 1) acc += a * (pc - ym); else acc += a * pc * ghost_it_side(g, i, j, k, i, j - 1);
   }
   st = face_state(code, 3);
   if (st) {
-    float a = unit ? 1.f : open3(g, 1, fv(g, i, j + 1, k));
+    float a = unit ? 1.f : aper3(g, 1, fv(g, i, j + 1, k));
     if (st == 1) acc += a * (pc - yp); else acc += a * pc * ghost_it_side(g, i, j, k, i, j + 1);
   }
   st = face_state(code, 4);
   if (st) {
-    float a = unit ? 1.f : open3(g, 2, fw(g, i, j, k));
+    float a = unit ? 1.f : aper3(g, 2, fw(g, i, j, k));
     acc += a * (pc - zm);
   }
   st = face_state(code, 5);
   if (st) {
-    float a = unit ? 1.f : open3(g, 2, fw(g, i, j, k + 1));
+    float a = unit ? 1.f : aper3(g, 2, fw(g, i, j, k + 1));
     if (st == 1) acc += a * (pc - zp);
     else if (g.linear) acc += 2.f * a * pc;
     else acc += a * pc * ghost_it_up(g, i, j, k);

@@ -55,6 +55,30 @@ class _Options(C.Structure):
                 ("reserved", C.c_uint32 * 2)]
 
 
+class _SparseChange(C.Structure):
+    _fields_ = [("activated", C.c_uint64), ("deactivated", C.c_uint64), ("active_columns", C.c_uint64),
+                ("volume_removed", C.c_double), ("height_removed", C.c_float), ("velocity_removed", C.c_float)]
+
+
+@dataclass
+class SparseChange:
+    """SparseChange (delta3d_sparse.rs:85-99): what a change of the sparse column set did."""
+    activated: int
+    deactivated: int
+    active_columns: int
+    volume_removed: float
+    height_removed: float
+    velocity_removed: float
+
+    @staticmethod
+    def _from(c: _SparseChange) -> "SparseChange":
+        return SparseChange(int(c.activated), int(c.deactivated), int(c.active_columns), float(c.volume_removed),
+                            float(c.height_removed), float(c.velocity_removed))
+
+
+BLOCK = 8  # side of a block of the shared lattice, in columns (domain_blocks.rs:18)
+
+
 @dataclass
 class Report:
     """Report (delta_projection.rs:164-189)."""
@@ -115,6 +139,12 @@ def library() -> C.CDLL:
     L.fd3_project_linear.argtypes = [vp, f32, f32, u32, C.POINTER(_Report)]
     L.fd3_step_surface_linear.argtypes = [vp, u64, u32, C.POINTER(_Report)]
     L.fd3_set_precondition_cut.argtypes = [vp, C.c_int]
+    L.fd3_enable_sparse.argtypes = [vp]
+    L.fd3_set_active_columns.argtypes = [vp, vp, sz, C.POINTER(_SparseChange)]
+    L.fd3_set_active_blocks.argtypes = [vp, vp, sz, C.c_int32, C.c_int32, C.POINTER(_SparseChange)]
+    L.fd3_active_columns.argtypes = [vp, vp, sz]
+    L.fd3_sparse_cells.argtypes = [vp]
+    L.fd3_sparse_cells.restype = u64
     L.fd3_get_pressure.argtypes = [vp, fp, sz]
     L.fd3_get_velocity.argtypes = [vp, fp, sz, fp, sz, fp, sz]
     L.fd3_get_surface.argtypes = [vp, fp, fp, sz]
@@ -264,6 +294,41 @@ class Volume3:
 
     def reset_pressure(self):
         self._check(self._L.fd3_reset_pressure(self._h), "reset_pressure")
+
+    # ---- the sparse column set (delta3d_sparse.rs)
+    def enable_sparse(self):
+        """Volume3::enable_sparse (delta3d_sparse.rs:105): reserve the set, every column in it."""
+        self._check(self._L.fd3_enable_sparse(self._h), "enable_sparse")
+
+    def set_active_columns(self, mask) -> SparseChange:
+        """Volume3::set_active_columns (delta3d_sparse.rs:147): mask[j*nx + i] != 0 puts column (i, j) in
+        the set; a column that leaves goes to rest."""
+        m = np.ascontiguousarray(np.asarray(mask).reshape(-1) != 0, dtype=np.uint8)
+        ch = _SparseChange()
+        self._check(self._L.fd3_set_active_columns(self._h, m.ctypes.data, m.size, C.byref(ch)), "set_active_columns")
+        return SparseChange._from(ch)
+
+    def set_active_blocks(self, blocks, origin=(0, 0)) -> SparseChange:
+        """Volume3::set_active_blocks (delta3d_sparse.rs:163): the set from (i, j) blocks of BLOCK x BLOCK
+        columns, relative to the block `origin` whose window starts at column (0, 0)."""
+        b = np.ascontiguousarray(np.asarray(blocks, dtype=np.int32).reshape(-1, 2))
+        ch = _SparseChange()
+        self._check(self._L.fd3_set_active_blocks(self._h, b.ctypes.data, b.shape[0], int(origin[0]), int(origin[1]),
+                                                  C.byref(ch)), "set_active_blocks")
+        return SparseChange._from(ch)
+
+    def active_columns(self):
+        """Volume3::active_columns (delta3d_sparse.rs:129): one byte per column, or None without a set."""
+        out = np.empty(self.nx * self.ny, np.uint8)
+        e = self._L.fd3_active_columns(self._h, out.ctypes.data, out.size)
+        if e == 1:
+            return None
+        self._check(e, "active_columns")
+        return out
+
+    def sparse_cells(self) -> int:
+        """Volume3::sparse_cells (delta3d_sparse.rs:135)."""
+        return int(self._L.fd3_sparse_cells(self._h))
 
     # ---- steps
     def project_mobile3(self, scale, k1, max_iters=4000) -> Report:

@@ -373,3 +373,37 @@ def projection_scalars(scene: dict):
     step_surface_mobile does (delta3d_mobile.rs:838-840)."""
     dt, rho = scene["dt"], scene["rho"]
     return float(f32(-rho / dt)), float(f32(dt / rho))
+
+
+# ------------------------------------------------------------------------------------------------
+# Sparse column sets (delta3d_sparse.rs), the scenes of tests_delta3d_sparse.rs:8-36, 198-225.
+
+SPARSE_DX, SPARSE_NZ, SPARSE_REST = 0.25, 12, 2.0
+
+
+def rect_mask(nx: int, ny: int, rects) -> np.ndarray:
+    """Column mask (j*nx + i) of the union of rectangles [i0, i1) x [j0, j1)."""
+    m = np.zeros((ny, nx), np.uint8)
+    for i0, i1, j0, j1 in rects:
+        m[j0:j1, i0:i1] = 1
+    return m.ravel()
+
+
+def bumps_in(nx: int, ny: int, mask, centres, rest: float = SPARSE_REST) -> np.ndarray:
+    """Surface of a window: rest + sum of 5 cm Gaussian bumps exp(-r^2/8) (r in cells) in the set's
+    columns, exactly `rest` outside the set."""
+    mask = np.asarray(mask).reshape(-1)
+    out = np.empty(nx * ny, np.float32)
+    r = f32(rest)
+    for c in range(nx * ny):
+        if mask[c] == 0:
+            out[c] = r
+            continue
+        i, j = c % nx, c // nx
+        s = f32(0.0)
+        for cx, cy in centres:
+            x = f32(f32(i) + f32(0.5)) - f32(cx)
+            y = f32(f32(j) + f32(0.5)) - f32(cy)
+            s = f32(s + f32(f32(0.05) * expf(f32(-(f32(x * x) + f32(y * y))) / f32(8.0))))
+        out[c] = f32(r + s)
+    return out

@@ -100,6 +100,20 @@ typedef struct fd3_options {
 
 typedef struct fd3_volume fd3_volume;
 
+/* SparseChange (delta3d_sparse.rs:85-99): what a change of the sparse column set did. */
+typedef struct fd3_sparse_change {
+  uint64_t activated;       /* columns that entered the set, at rest with zero velocities */
+  uint64_t deactivated;     /* columns that left the set, put to rest */
+  uint64_t active_columns;  /* columns of the set after the change */
+  double volume_removed;    /* perturbation volume the leaving columns carried, m^3 (compensated
+                               height, summed in column order in f64) */
+  float height_removed;     /* largest |eta - rest| of a leaving column, m */
+  float velocity_removed;   /* largest |velocity| of a face set to zero, m/s */
+} fd3_sparse_change;
+
+/* Side of a block of the shared block lattice, in columns (domain_blocks.rs:18). */
+#define FD3_BLOCK 8
+
 /* Library and device. */
 const char* fd3_version(void);
 const char* fd3_last_cuda_error(void);
@@ -151,6 +165,33 @@ int fd3_set_velocity(fd3_volume* v, const float* u, size_t nu, const float* vv, 
 int fd3_set_velocity_device(fd3_volume* v, const float* d_u, const float* d_v, const float* d_w);
 /* Zero the pressure (the state set_free_surface leaves), e.g. to repeat a first projection. */
 int fd3_reset_pressure(fd3_volume* v);
+
+/* The sparse column set (delta3d_sparse.rs).  The memory stays the box (the window); a column
+ * outside the set is solid for every operator, the faces touching it are closed, and it stays at
+ * rest.  The edge of the set reads as the box's edge in the advection.  A full set is the box, bit
+ * for bit.  The linear path refuses a volume with a set (FD3_ERR_DOMAIN); set_free_surface and
+ * set_surface refuse a surface that is not `rest`, to the bit, outside the set.
+ *
+ * Volume3::enable_sparse (delta3d_sparse.rs:105): reserves the set, every column in it.
+ * FD3_ERR_DOMAIN if already reserved. */
+int fd3_enable_sparse(fd3_volume* v);
+/* Volume3::set_active_columns (delta3d_sparse.rs:147): mask[j*nx + i] != 0 puts column (i, j) in
+ * the set.  A column that leaves goes to rest (surface, roundoff, pressure, every face); what it
+ * carried is published in `change` (may be NULL).  FD3_ERR_DOMAIN without a set, FD3_ERR_SHAPE
+ * when len != nx*ny; nothing is written then.  No allocation. */
+int fd3_set_active_columns(fd3_volume* v, const uint8_t* mask, size_t len, fd3_sparse_change* change);
+/* Volume3::set_active_blocks (delta3d_sparse.rs:163): the set from blocks of FD3_BLOCK x FD3_BLOCK
+ * columns; `blocks` holds `count` (i, j) pairs of int32, and block (bi, bj) covers the columns
+ * [(bi - origin_i)*FD3_BLOCK, +FD3_BLOCK) x [(bj - origin_j)*FD3_BLOCK, +FD3_BLOCK), clipped to the
+ * window.  As fd3_set_active_columns. */
+int fd3_set_active_blocks(fd3_volume* v, const int32_t* blocks, size_t count, int32_t origin_i, int32_t origin_j,
+                          fd3_sparse_change* change);
+/* Volume3::active_columns (delta3d_sparse.rs:129): the set, one byte per column.  FD3_ERR_DOMAIN
+ * without a set. */
+int fd3_active_columns(const fd3_volume* v, uint8_t* out, size_t len);
+/* Volume3::sparse_cells (delta3d_sparse.rs:135): cells of the set's columns (every cell without
+ * a set). */
+uint64_t fd3_sparse_cells(const fd3_volume* v);
 
 /* project_mobile3 (delta3d_mobile.rs:465) of the current velocity field: us = u, then the
  * projection with `scale` (-rho/dt) and `k1` (dt/rho), as tests_delta3d.rs:389-400 does. */

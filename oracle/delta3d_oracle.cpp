@@ -749,14 +749,45 @@ struct Volume3 {
   size_t fw(size_t i, size_t j, size_t k) const { return (k * d.ny + j) * d.nx + i; }
   size_t col(size_t i, size_t j) const { return j * d.nx + i; }
 
+  // The sparse column set (delta3d_sparse.rs:31-44): one byte per column, 1 in the domain.
+  // `next_active` holds a requested set before it replaces `active`.
+  bool has_sparse = false;
+  std::vector<uint8_t> active, next_active;
+  bool column_active(size_t i, size_t j) const { return !has_sparse || active[col(i, j)] != 0; }
+  // delta3d_sparse.rs:272-277: every cell of a column outside the set is solid
+  bool sparse_solid3(size_t cc) const { return has_sparse && active[cc % (d.nx * d.ny)] == 0; }
+  // delta3d_sparse.rs:283-300: an interior u/v face touching a column outside the set, or a w face
+  // of such a column, is closed; the faces on the box's boundary keep the box's treatment
+  bool sparse_closed3(int axis, size_t f) const {
+    if (!has_sparse) return false;
+    size_t nx = d.nx, ny = d.ny;
+    if (axis == 0) {
+      size_t i = f % (nx + 1), j = (f / (nx + 1)) % ny;
+      return i > 0 && i < nx && (active[j * nx + i - 1] == 0 || active[j * nx + i] == 0);
+    }
+    if (axis == 1) {
+      size_t i = f % nx, j = (f / nx) % (ny + 1);
+      return j > 0 && j < ny && (active[(j - 1) * nx + i] == 0 || active[j * nx + i] == 0);
+    }
+    return active[f % (nx * ny)] == 0;
+  }
+  // delta3d_sparse.rs:307-319: the face of axis `axis` at (i, j) touches no column of the set
+  bool sparse_outside3(int axis, size_t i, size_t j) const {
+    if (!has_sparse) return false;
+    if (axis == 0) return !((i > 0 && column_active(i - 1, j)) || (i < d.nx && column_active(i, j)));
+    if (axis == 1) return !((j > 0 && column_active(i, j - 1)) || (j < d.ny && column_active(i, j)));
+    return !column_active(i, j);
+  }
+
   // delta3d_mobile.rs:92-124
   R height3(size_t i, size_t j) const { return eta[col(i, j)]; }
-  bool solid3(size_t cc) const { return has_cut && g.frac[cc] == 0; }
+  bool solid3(size_t cc) const { return (has_cut && g.frac[cc] == 0) || sparse_solid3(cc); }
   bool wet3(size_t i, size_t j, size_t k) const {
     if (solid3(c(i, j, k))) return false;
     return ((R)k + (R)0.5) * d.dx < height3(i, j);
   }
   R open3(int axis, size_t f) const {
+    if (sparse_closed3(axis, f)) return 0;
     if (!has_cut) return 1;
     return axis == 0 ? g.open_u[f] : (axis == 1 ? g.open_v[f] : g.open_w[f]);
   }
@@ -1293,8 +1324,10 @@ struct Volume3 {
             R dn = k > 0 ? val(a, b, k - 1) : uc;
             R uz = (upv - dn) * h;
             R wc = (R)0.25 * (vertical(a - 1, b, k) + vertical(a, b, k) + vertical(a - 1, b, k + 1) + vertical(a, b, k + 1));
-            R rt = b + 1 < nb ? val(a, b + 1, k) : uc;
-            R lf = b > 0 ? val(a, b - 1, k) : uc;
+            // the edge of the sparse set reads as the box's edge (delta3d_mobile.rs:664-667)
+            auto outside = [&](size_t A, size_t B) { return axis == 0 ? sparse_outside3(0, A, B) : sparse_outside3(1, B, A); };
+            R rt = b + 1 < nb && !outside(a, b + 1) ? val(a, b + 1, k) : uc;
+            R lf = b > 0 && !outside(a, b - 1) ? val(a, b - 1, k) : uc;
             R uy = (rt - lf) * h;
             R vc = (R)0.25 * (transverse(a - 1, b, k) + transverse(a, b, k) + transverse(a - 1, b + 1, k) + transverse(a, b + 1, k));
             R next = uc - dt * (uc * ux + wc * uz + vc * uy);
@@ -1310,13 +1343,13 @@ struct Volume3 {
           size_t f = fw(i, j, k);
           if (open3(2, f) == 0) continue;
           R wc = w[f];
-          R rt = i + 1 < nx ? w[fw(i + 1, j, k)] : wc;
-          R lf = i > 0 ? w[fw(i - 1, j, k)] : wc;
+          R rt = i + 1 < nx && !sparse_outside3(2, i + 1, j) ? w[fw(i + 1, j, k)] : wc;
+          R lf = i > 0 && !sparse_outside3(2, i - 1, j) ? w[fw(i - 1, j, k)] : wc;
           R wx = (rt - lf) * h;
           R wz = (w[fw(i, j, k + 1)] - w[fw(i, j, k - 1)]) * h;
           R uc = (R)0.25 * (u[fu(i, j, k - 1)] + u[fu(i + 1, j, k - 1)] + u[fu(i, j, k)] + u[fu(i + 1, j, k)]);
-          R bk = j + 1 < ny ? w[fw(i, j + 1, k)] : wc;
-          R fr = j > 0 ? w[fw(i, j - 1, k)] : wc;
+          R bk = j + 1 < ny && !sparse_outside3(2, i, j + 1) ? w[fw(i, j + 1, k)] : wc;
+          R fr = j > 0 && !sparse_outside3(2, i, j - 1) ? w[fw(i, j - 1, k)] : wc;
           R wy = (bk - fr) * h;
           R vc = (R)0.25 * (v[fv(i, j, k - 1)] + v[fv(i, j + 1, k - 1)] + v[fv(i, j, k)] + v[fv(i, j + 1, k)]);
           ws[f] = wc - dt * (uc * wx + wc * wz + vc * wy);
@@ -1411,6 +1444,69 @@ struct Volume3 {
       for (size_t q = 0; q < v.size(); ++q) if (g.open_v[q] == 0) v[q] = 0;
       for (size_t q = 0; q < w.size(); ++q) if (g.open_w[q] == 0) w[q] = 0;
     }
+  }
+
+  // clear_column_faces (delta3d_sparse.rs:213-233): zeroes the column's two u faces, two v faces
+  // and nz+1 w faces per layer, and returns the largest |velocity| it cleared.
+  float clear_column_faces(size_t i, size_t j) {
+    float worst = 0;
+    for (size_t k = 0; k < d.nz; ++k) {
+      for (size_t f : {fu(i, j, k), fu(i + 1, j, k)}) { worst = std::max(worst, std::fabs((float)u[f])); u[f] = 0; }
+      for (size_t f : {fv(i, j, k), fv(i, j + 1, k)}) { worst = std::max(worst, std::fabs((float)v[f])); v[f] = 0; }
+    }
+    for (size_t k = 0; k <= d.nz; ++k) { size_t f = fw(i, j, k); worst = std::max(worst, std::fabs((float)w[f])); w[f] = 0; }
+    return worst;
+  }
+
+  // close_sparse_walls (delta3d_sparse.rs:236-247)
+  void close_sparse_walls() {
+    if (!has_sparse) return;
+    for (size_t j = 0; j < d.ny; ++j)
+      for (size_t i = 0; i < d.nx; ++i)
+        if (!column_active(i, j)) clear_column_faces(i, j);
+  }
+
+  // sparse_surface_ok (delta3d_sparse.rs:327-332): outside the set the surface is `rest`, to the bit
+  bool sparse_surface_ok(const float* e, float r) const {
+    if (!has_sparse) return true;
+    uint32_t rb; std::memcpy(&rb, &r, 4);
+    for (size_t q = 0; q < active.size(); ++q) {
+      uint32_t eb; std::memcpy(&eb, &e[q], 4);
+      if (!active[q] && eb != rb) return false;
+    }
+    return true;
+  }
+
+  // apply_sparse (delta3d_sparse.rs:181-210): `next_active` replaces `active`; a column that leaves
+  // goes to rest (surface, roundoff, pressure, faces) and what it carried is counted.
+  // out: activated, deactivated, active columns, volume removed, height removed, velocity removed
+  void apply_sparse(double out[6]) {
+    size_t deact = 0, act = 0;
+    double volume = 0;
+    float height = 0, speed = 0;
+    const double area = (double)d.dx * (double)d.dx;
+    for (size_t j = 0; j < d.ny; ++j)
+      for (size_t i = 0; i < d.nx; ++i) {
+        size_t cc = col(i, j);
+        bool was = active[cc] != 0, will = next_active[cc] != 0;
+        if (was && !will) {
+          ++deact;
+          double h = ((double)(float)eta[cc] - (double)(float)eta_roundoff[cc]) - (double)(float)rest;
+          volume += h * area;
+          height = std::max(height, std::fabs((float)eta[cc] - (float)rest));
+          eta[cc] = rest;
+          eta_roundoff[cc] = 0;
+          for (size_t k = 0; k < d.nz; ++k) p[c(i, j, k)] = 0;
+          speed = std::max(speed, clear_column_faces(i, j));
+        } else if (!was && will) {
+          ++act;
+        }
+      }
+    std::swap(active, next_active);
+    size_t count = 0;
+    for (uint8_t a : active) count += a != 0;
+    out[0] = (double)act; out[1] = (double)deact; out[2] = (double)count;
+    out[3] = volume; out[4] = height; out[5] = speed;
   }
 
   // delta3d_mobile.rs:819-927
@@ -1982,6 +2078,7 @@ int od3_set_free_surface(Volume3* v, const float* eta, uint64_t len, float rest)
   if (len != v->eta.size()) return SHAPE;
   if (!std::isfinite(rest)) return NOT_FINITE;
   for (size_t q = 0; q < len; ++q) if (!std::isfinite(eta[q])) return NOT_FINITE;
+  if (!v->sparse_surface_ok(eta, rest)) return DOMAIN;  // delta3d_mobile.rs:16-19
   for (size_t q = 0; q < len; ++q) v->eta[q] = (R)eta[q];
   std::fill(v->eta_roundoff.begin(), v->eta_roundoff.end(), (R)0);
   std::fill(v->p.begin(), v->p.end(), (R)0);
@@ -1994,6 +2091,7 @@ int od3_set_surface(Volume3* v, const float* eta, uint64_t len) {
   if (!v || (!eta && len)) return INVALID;
   if (len != v->eta.size()) return SHAPE;
   for (size_t q = 0; q < len; ++q) if (!std::isfinite(eta[q])) return NOT_FINITE;
+  if (!v->sparse_surface_ok(eta, (float)v->rest)) return DOMAIN;  // delta3d.rs:621-624
   for (size_t q = 0; q < len; ++q) v->eta[q] = (R)eta[q];
   std::fill(v->eta_roundoff.begin(), v->eta_roundoff.end(), (R)0);
   return OK;
@@ -2010,6 +2108,7 @@ int od3_set_velocity(Volume3* v, const float* u, uint64_t nu, const float* vv, u
   for (size_t q = 0; q < nv; ++q) v->v[q] = (R)vv[q];
   for (size_t q = 0; q < nw; ++q) v->w[q] = (R)w[q];
   v->close_walls();
+  v->close_sparse_walls();
   return OK;
 }
 
@@ -2044,12 +2143,14 @@ int od3_refine_mobile(Volume3* v, float scale, float k1, uint32_t max_iters, dou
 // (tests_delta3d.rs:143-148).
 int od3_project_linear(Volume3* v, float scale, float k1, uint32_t max_iters, double rep[8]) {
   if (!v || !rep) return INVALID;
+  if (v->has_sparse) return DOMAIN;  // the linear path does not carry a sparse set (delta3d.rs:1210-1211)
   v->us = v->u; v->vs = v->v; v->ws = v->w;
   return v->project_linear((R)scale, (R)k1, max_iters, rep);
 }
 
 int od3_step_surface_linear(Volume3* v, uint64_t duration_us, uint32_t max_iters, double rep[8]) {
   if (!v || !rep) return INVALID;
+  if (v->has_sparse) return DOMAIN;  // delta3d.rs:1210-1211
   return v->step_surface_linear(duration_us, max_iters, rep);
 }
 
@@ -2063,6 +2164,59 @@ int od3_set_precondition_cut(Volume3* v, int on) {
 int od3_step_surface_mobile(Volume3* v, uint64_t duration_us, uint32_t max_iters, double rep[8]) {
   if (!v || !rep) return INVALID;
   return v->step_surface_mobile(duration_us, max_iters, rep);
+}
+
+// enable_sparse (delta3d_sparse.rs:105-117): every column starts in the set.
+int od3_enable_sparse(Volume3* v) {
+  if (!v) return INVALID;
+  if (v->has_sparse) return DOMAIN;
+  v->has_sparse = true;
+  v->active.assign(v->d.nx * v->d.ny, 1);
+  v->next_active.assign(v->d.nx * v->d.ny, 1);
+  return OK;
+}
+
+// set_active_columns (delta3d_sparse.rs:147-158); change[6] as apply_sparse writes it
+int od3_set_active_columns(Volume3* v, const uint8_t* mask, uint64_t len, double change[6]) {
+  if (!v || !change || (!mask && len)) return INVALID;
+  if (!v->has_sparse) return DOMAIN;
+  if (len != v->active.size()) return SHAPE;
+  for (size_t q = 0; q < len; ++q) v->next_active[q] = mask[q] != 0;
+  v->apply_sparse(change);
+  return OK;
+}
+
+// set_active_blocks (delta3d_sparse.rs:163-178): block b covers the columns
+// [(b.i - origin.i)*8, +8) x [(b.j - origin.j)*8, +8) of the window, clipped to it.
+// blocks: count (i, j) pairs.
+int od3_set_active_blocks(Volume3* v, const int32_t* blocks, uint64_t count, int32_t oi, int32_t oj, double change[6]) {
+  if (!v || !change || (!blocks && count)) return INVALID;
+  if (!v->has_sparse) return DOMAIN;
+  const long long side = 8, nx = (long long)v->d.nx, ny = (long long)v->d.ny;
+  std::fill(v->next_active.begin(), v->next_active.end(), (uint8_t)0);
+  for (uint64_t b = 0; b < count; ++b) {
+    long long i0 = ((long long)blocks[2 * b] - oi) * side, j0 = ((long long)blocks[2 * b + 1] - oj) * side;
+    for (long long j = std::max(j0, 0LL); j < std::min(j0 + side, ny); ++j)
+      for (long long i = std::max(i0, 0LL); i < std::min(i0 + side, nx); ++i) v->next_active[(size_t)(j * nx + i)] = 1;
+  }
+  v->apply_sparse(change);
+  return OK;
+}
+
+// active_columns / sparse_cells (delta3d_sparse.rs:129-141)
+int od3_active_columns(const Volume3* v, uint8_t* out, uint64_t len) {
+  if (!v || !out) return INVALID;
+  if (!v->has_sparse) return DOMAIN;
+  if (len != v->active.size()) return SHAPE;
+  std::memcpy(out, v->active.data(), len);
+  return OK;
+}
+uint64_t od3_sparse_cells(const Volume3* v) {
+  if (!v) return 0;
+  if (!v->has_sparse) return (uint64_t)v->d.nx * v->d.ny * v->d.nz;
+  uint64_t cols = 0;
+  for (uint8_t a : v->active) cols += a != 0;
+  return cols * v->d.nz;
 }
 
 int od3_last_refused_report(const Volume3* v, double rep[8]) {

@@ -98,6 +98,12 @@ def lib(real: str = "f32") -> C.CDLL:
     L.od3_set_solid_rigid.argtypes = [vp, fp, u64, fp, fp, fp]
     L.od3_step_surface_linear.argtypes = [vp, u64, u32, dp]
     L.od3_set_precondition_cut.argtypes = [vp, C.c_int]
+    L.od3_enable_sparse.argtypes = [vp]
+    L.od3_set_active_columns.argtypes = [vp, vp, u64, dp]
+    L.od3_set_active_blocks.argtypes = [vp, vp, u64, C.c_int32, C.c_int32, dp]
+    L.od3_active_columns.argtypes = [vp, vp, u64]
+    L.od3_sparse_cells.argtypes = [vp]
+    L.od3_sparse_cells.restype = u64
     _LIBS[real] = L
     return L
 
@@ -120,6 +126,20 @@ def report_dict(rep) -> dict:
     d["iterations"] = int(d["iterations"])
     d["degraded"] = bool(d["degraded"])
     d["floor"] = bool(d["floor"])
+    return d
+
+
+CHANGE_KEYS = ("activated", "deactivated", "active_columns", "volume_removed", "height_removed",
+               "velocity_removed")
+
+
+def change_dict(ch) -> dict:
+    """SparseChange (delta3d_sparse.rs:85-99) from the six doubles the oracle writes."""
+    d = dict(zip(CHANGE_KEYS, [float(x) for x in ch]))
+    for k in ("activated", "deactivated", "active_columns"):
+        d[k] = int(d[k])
+    d["height_removed"] = float(np.float32(d["height_removed"]))
+    d["velocity_removed"] = float(np.float32(d["velocity_removed"]))
     return d
 
 
@@ -254,6 +274,31 @@ class OracleVolume:
 
     def set_precondition_cut(self, on: bool):
         self._check(self.L.od3_set_precondition_cut(self.h, 1 if on else 0), "set_precondition_cut")
+
+    # The sparse column set (delta3d_sparse.rs:101-178).
+    def enable_sparse(self):
+        self._check(self.L.od3_enable_sparse(self.h), "enable_sparse")
+
+    def set_active_columns(self, mask) -> dict:
+        m = np.ascontiguousarray(np.asarray(mask) != 0, dtype=np.uint8)
+        ch = (C.c_double * 6)()
+        self._check(self.L.od3_set_active_columns(self.h, m.ctypes.data, m.size, ch), "set_active_columns")
+        return change_dict(ch)
+
+    def set_active_blocks(self, blocks, origin=(0, 0)) -> dict:
+        b = np.ascontiguousarray(np.asarray(blocks, dtype=np.int32).reshape(-1, 2))
+        ch = (C.c_double * 6)()
+        self._check(self.L.od3_set_active_blocks(self.h, b.ctypes.data, b.shape[0], int(origin[0]), int(origin[1]),
+                                                 ch), "set_active_blocks")
+        return change_dict(ch)
+
+    def active_columns(self) -> np.ndarray:
+        out = np.empty(self.nx * self.ny, np.uint8)
+        self._check(self.L.od3_active_columns(self.h, out.ctypes.data, out.size), "active_columns")
+        return out
+
+    def sparse_cells(self) -> int:
+        return int(self.L.od3_sparse_cells(self.h))
 
     def last_refused_report(self):
         rep = (C.c_double * 8)()
