@@ -26,6 +26,7 @@
 #include "fd3_cut.cuh"
 #include "fd3_zmarch2.cuh"
 #include "fd3_linear.cuh"
+#include "fd3_levels.cuh"
 
 using namespace fd3;
 
@@ -750,6 +751,7 @@ __device__ __forceinline__ bool column_face(const unsigned char* __restrict__ m,
 // then close_sparse_walls (delta3d_sparse.rs:236-247): nor has any face of a column outside the
 // sparse set (g.act, 0 for those columns).
 __global__ void k_close_walls(Geo g, float* __restrict__ u, float* __restrict__ v, float* __restrict__ w) {
+  KSTART();
   const unsigned char* out = g.act;
   int nu = (g.nx + 1) * g.ny * g.nz, nv = g.nx * (g.ny + 1) * g.nz, nw = g.nx * g.ny * (g.nz + 1);
   int q = blockIdx.x * blockDim.x + threadIdx.x;
@@ -777,6 +779,7 @@ __global__ void k_close_walls(Geo g, float* __restrict__ u, float* __restrict__ 
 __global__ void k_sparse_leave(Geo g, const unsigned char* __restrict__ leave, float rest, float* __restrict__ eta,
                                float* __restrict__ rof, float* __restrict__ p, float* __restrict__ u,
                                float* __restrict__ v, float* __restrict__ w, int* vmax) {
+  KSTART();
   const int nx = g.nx, ny = g.ny, ncol = nx * ny;
   const int nu = (nx + 1) * ny * g.nz, nv = nx * (ny + 1) * g.nz, nw = ncol * (g.nz + 1);
   long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -1526,6 +1529,49 @@ uint64_t fd3_sparse_cells(const fd3_volume* V) {
   uint64_t cols = 0;
   for (unsigned char a : V->hact) cols += a != 0;
   return cols * (uint64_t)V->nz;
+}
+
+// perturbation_volume (delta3d_balance.rs:105-113): summed on the host in column order, in f64.
+static int perturbation_volume(fd3_volume* V, double* out) {
+  std::vector<float> e(V->ncol), r(V->ncol);
+  CK(cudaMemcpyAsync(e.data(), V->eta, (size_t)V->ncol * 4, cudaMemcpyDeviceToHost, V->stream));
+  CK(cudaMemcpyAsync(r.data(), V->rof, (size_t)V->ncol * 4, cudaMemcpyDeviceToHost, V->stream));
+  TRY(sync(V));
+  const double area = (double)V->dx * (double)V->dx, rest = (double)V->rest;
+  double total = 0.0;
+  for (int c = 0; c < V->ncol; ++c) total += ((double)e[c] - (double)r[c]) - rest;
+  *out = total * area;
+  return FD3_OK;
+}
+
+int fd3_perturbation_volume(fd3_volume* V, double* out) {
+  if (!V || !out) return FD3_ERR_INVALID_ARGUMENT;
+  return perturbation_volume(V, out);
+}
+
+// resample_from (delta3d_levels.rs:43-69).  Refusal (FD3_ERR_DOMAIN) writes nothing.
+int fd3_resample_from(fd3_volume* V, fd3_volume* S, fd3_level_change* change) {
+  if (!V || !S || V == S) return FD3_ERR_INVALID_ARGUMENT;
+  if (V->device != S->device) return FD3_ERR_INVALID_ARGUMENT;
+  auto extent = [](int n, float dx) { return (double)n * (double)dx; };
+  auto same = [](double a, double b) { return std::fabs(a - b) <= 1e-6 * std::max(std::fabs(a), std::fabs(b)); };
+  auto fbits = [](float x) { uint32_t b; std::memcpy(&b, &x, 4); return b; };
+  if (!same(extent(V->nx, V->dx), extent(S->nx, S->dx)) || !same(extent(V->ny, V->dx), extent(S->ny, S->dx)) ||
+      !same(extent(V->nz, V->dx), extent(S->nz, S->dx)) || fbits(V->rest) != fbits(S->rest) ||
+      fbits(V->rho) != fbits(S->rho) || fbits(V->g) != fbits(S->g) || V->cut || S->cut)
+    return FD3_ERR_DOMAIN;
+  fd3_level_change ch{};
+  TRY(perturbation_volume(S, &ch.volume_before));  // also orders S's stream before V's launches
+  LevelSrc src{S->nx, S->ny, S->nz, S->dx, S->rest, S->eta, S->rof, S->u, S->v, S->w, S->sparse ? S->act : nullptr};
+  const int n = std::max((int)std::ceil((double)V->dx / (double)S->dx), 1);
+  LAUNCH(V, k_resample_surface, V->ncol, src, V->nx, V->ny, V->dx, V->rest,
+         (const unsigned char*)(V->sparse ? V->act : nullptr), V->eta, V->rof);
+  LAUNCH(V, k_resample_faces, (long long)V->nu + V->nv + V->nw, src, V->nx, V->ny, V->nz, n, V->u, V->v, V->w);
+  CK(cudaMemsetAsync(V->p, 0, (size_t)V->n * 4, V->stream));
+  LAUNCH(V, k_close_walls, (long long)V->nu + V->nv + V->nw, V->geo(), V->u, V->v, V->w);
+  TRY(perturbation_volume(V, &ch.volume_after));
+  if (change) *change = ch;
+  return FD3_OK;
 }
 
 int fd3_reset_pressure(fd3_volume* V) {

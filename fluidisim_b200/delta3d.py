@@ -79,6 +79,10 @@ class SparseChange:
 BLOCK = 8  # side of a block of the shared lattice, in columns (domain_blocks.rs:18)
 
 
+class _LevelChange(C.Structure):
+    _fields_ = [("volume_before", C.c_double), ("volume_after", C.c_double)]
+
+
 @dataclass
 class Report:
     """Report (delta_projection.rs:164-189)."""
@@ -145,6 +149,8 @@ def library() -> C.CDLL:
     L.fd3_active_columns.argtypes = [vp, vp, sz]
     L.fd3_sparse_cells.argtypes = [vp]
     L.fd3_sparse_cells.restype = u64
+    L.fd3_resample_from.argtypes = [vp, vp, C.POINTER(_LevelChange)]
+    L.fd3_perturbation_volume.argtypes = [vp, C.POINTER(C.c_double)]
     L.fd3_get_pressure.argtypes = [vp, fp, sz]
     L.fd3_get_velocity.argtypes = [vp, fp, sz, fp, sz, fp, sz]
     L.fd3_get_surface.argtypes = [vp, fp, fp, sz]
@@ -329,6 +335,20 @@ class Volume3:
     def sparse_cells(self) -> int:
         """Volume3::sparse_cells (delta3d_sparse.rs:135)."""
         return int(self._L.fd3_sparse_cells(self._h))
+
+    # ---- the level change (delta3d_levels.rs)
+    def resample_from(self, src: "Volume3") -> dict:
+        """Volume3::resample_from (delta3d_levels.rs:43): receive the state of `src`, the same window at
+        another dx.  Returns LevelChange as {volume_before, volume_after}."""
+        ch = _LevelChange()
+        self._check(self._L.fd3_resample_from(self._h, src._h, C.byref(ch)), "resample_from")
+        return {"volume_before": float(ch.volume_before), "volume_after": float(ch.volume_after)}
+
+    def perturbation_volume(self) -> float:
+        """Volume3::perturbation_volume (delta3d_balance.rs:105), m^3."""
+        out = C.c_double()
+        self._check(self._L.fd3_perturbation_volume(self._h, C.byref(out)), "perturbation_volume")
+        return float(out.value)
 
     # ---- steps
     def project_mobile3(self, scale, k1, max_iters=4000) -> Report:

@@ -111,6 +111,13 @@ typedef struct fd3_sparse_change {
   float velocity_removed;   /* largest |velocity| of a face set to zero, m/s */
 } fd3_sparse_change;
 
+/* LevelChange (delta3d_levels.rs:29-36): what a level change did. */
+typedef struct fd3_level_change {
+  double volume_before;  /* perturbation volume of the source, m^3 */
+  double volume_after;   /* perturbation volume of the destination, m^3: equal to roundoff, less
+                            what the destination's sparse set does not cover of the source's */
+} fd3_level_change;
+
 /* Side of a block of the shared block lattice, in columns (domain_blocks.rs:18). */
 #define FD3_BLOCK 8
 
@@ -192,6 +199,20 @@ int fd3_active_columns(const fd3_volume* v, uint8_t* out, size_t len);
 /* Volume3::sparse_cells (delta3d_sparse.rs:135): cells of the set's columns (every cell without
  * a set). */
 uint64_t fd3_sparse_cells(const fd3_volume* v);
+
+/* Volume3::resample_from (delta3d_levels.rs:43): `v` receives the state of `src`, which covers the
+ * same window at another dx (a level change).  The surface by overlap of a conservative linear
+ * reconstruction of each source column (centred slopes and the cross term; the perturbation volume
+ * is kept exactly), the velocities trilinear at each destination face's centre on the source's
+ * staggered grid, averaged over n x n sub-faces when the destination is coarser (n = ceil of the
+ * ratio), the pressure zero, walls and faces outside the destination's sparse set closed.  Either
+ * volume may carry a sparse set: the source's edge reads as the box's edge, and only the
+ * destination's set receives the state.  Both volumes on the same device.  FD3_ERR_DOMAIN, nothing
+ * written: different extent (1e-6 relative), rest, density or gravity, or a cut on either side. */
+int fd3_resample_from(fd3_volume* v, fd3_volume* src, fd3_level_change* change);
+/* Volume3::perturbation_volume (delta3d_balance.rs:105): sum over columns of the compensated height
+ * minus rest, times dx^2, in f64 and in column order. */
+int fd3_perturbation_volume(fd3_volume* v, double* out);
 
 /* project_mobile3 (delta3d_mobile.rs:465) of the current velocity field: us = u, then the
  * projection with `scale` (-rho/dt) and `k1` (dt/rho), as tests_delta3d.rs:389-400 does. */

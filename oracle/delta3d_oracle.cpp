@@ -1430,6 +1430,165 @@ struct Volume3 {
         }
   }
 
+  // perturbation_volume (delta3d_balance.rs:105-113): f64, in column order
+  double perturbation_volume() const {
+    const double area = (double)(float)d.dx * (double)(float)d.dx, r = (double)(float)rest;
+    double total = 0;
+    for (size_t q = 0; q < eta.size(); ++q) total += ((double)eta[q] - (double)eta_roundoff[q]) - r;
+    return total * area;
+  }
+
+  // ---- the level change (delta3d_levels.rs:38-292)
+  double compensated(size_t i, size_t j) const { return (double)eta[col(i, j)] - (double)eta_roundoff[col(i, j)]; }
+  // delta3d_levels.rs:76-90: centred inside, one-sided at the box's or the set's edge
+  double surface_slope(size_t i, size_t j, int axis) const {
+    size_t n = axis == 0 ? d.nx : d.ny, k = axis == 0 ? i : j;
+    if (n < 2) return 0;
+    auto at = [&](size_t m) { return axis == 0 ? compensated(m, j) : compensated(i, m); };
+    auto inside = [&](size_t m) { return axis == 0 ? column_active(m, j) : column_active(i, m); };
+    size_t lo = k > 0 && inside(k - 1) ? k - 1 : k;
+    size_t hi = k + 1 < n && inside(k + 1) ? k + 1 : k;
+    if (hi == lo) return 0;
+    return (at(hi) - at(lo)) / ((double)(hi - lo) * (double)(float)d.dx);
+  }
+  // delta3d_levels.rs:95-107
+  double surface_twist(size_t i, size_t j) const {
+    size_t nx = d.nx, ny = d.ny;
+    if (i == 0 || j == 0 || i + 1 >= nx || j + 1 >= ny) return 0;
+    if (!column_active(i - 1, j - 1) || !column_active(i + 1, j - 1) || !column_active(i - 1, j + 1) ||
+        !column_active(i + 1, j + 1))
+      return 0;
+    double dx64 = (double)(float)d.dx;
+    return (compensated(i + 1, j + 1) - compensated(i + 1, j - 1) - compensated(i - 1, j + 1) + compensated(i - 1, j - 1)) /
+           (4. * dx64 * dx64);
+  }
+  R velocity3(int axis, const size_t p[3]) const {
+    return axis == 0 ? u[fu(p[0], p[1], p[2])] : (axis == 1 ? v[fv(p[0], p[1], p[2])] : w[fw(p[0], p[1], p[2])]);
+  }
+  // staggered_at (delta3d_levels.rs:159-200): trilinear on the staggered grid, indices clamped
+  float staggered_at(int axis, const double rel[3]) const {
+    const size_t dims[3] = {d.nx + (axis == 0), d.ny + (axis == 1), d.nz + (axis == 2)};
+    const size_t cells[3] = {d.nx, d.ny, d.nz};
+    size_t base[3];
+    double frac[3];
+    for (int a = 0; a < 3; ++a) {
+      double f = rel[a] * (double)cells[a] - (a == axis ? 0. : 0.5);
+      double top = (double)(dims[a] - 1);
+      f = std::min(std::max(f, 0.), top);
+      size_t b = std::min((size_t)std::floor(f), dims[a] >= 2 ? dims[a] - 2 : 0);
+      base[a] = b;
+      frac[a] = dims[a] < 2 ? 0. : f - (double)b;
+    }
+    if (has_sparse) return (float)staggered_in_set(axis, base, frac, dims);
+    double acc = 0;
+    for (int corner = 0; corner < 8; ++corner) {
+      size_t p[3] = {base[0], base[1], base[2]};
+      double weight = 1;
+      for (int a = 0; a < 3; ++a) {
+        bool up = (corner >> a) & 1;
+        if (dims[a] < 2) { if (up) weight = 0; continue; }
+        if (up) { p[a] += 1; weight *= frac[a]; } else { weight *= 1. - frac[a]; }
+      }
+      if (weight != 0.) acc += weight * (double)(float)velocity3(axis, p);
+    }
+    return (float)acc;
+  }
+  // staggered_in_set (delta3d_levels.rs:204-245): a corner outside the set's grid takes, axis by
+  // axis, its neighbour's value inside the set
+  double staggered_in_set(int axis, const size_t base[3], const double frac[3], const size_t dims[3]) const {
+    double values[8];
+    bool outside[8];
+    for (int corner = 0; corner < 8; ++corner) {
+      size_t p[3] = {base[0], base[1], base[2]};
+      for (int a = 0; a < 3; ++a) if (((corner >> a) & 1) && dims[a] >= 2) p[a] += 1;
+      values[corner] = (double)(float)velocity3(axis, p);
+      outside[corner] = sparse_outside3(axis, p[0], p[1]);
+    }
+    for (int a = 0; a < 3; ++a) {
+      if (dims[a] < 2) continue;
+      for (int corner = 0; corner < 8; ++corner) {
+        if ((corner >> a) & 1) continue;
+        int up = corner | (1 << a);
+        if (outside[corner] && !outside[up]) { values[corner] = values[up]; outside[corner] = false; }
+        else if (outside[up] && !outside[corner]) { values[up] = values[corner]; outside[up] = false; }
+      }
+    }
+    double acc = 0;
+    for (int corner = 0; corner < 8; ++corner) {
+      double weight = 1;
+      for (int a = 0; a < 3; ++a) {
+        bool up = (corner >> a) & 1;
+        if (dims[a] < 2) { if (up) weight = 0; continue; }
+        weight *= up ? frac[a] : 1. - frac[a];
+      }
+      if (weight != 0.) acc += weight * values[corner];
+    }
+    return acc;
+  }
+  // resample_surface (delta3d_levels.rs:109-155)
+  void resample_surface(const Volume3& src) {
+    const Domain3 &dd_ = d, &ss = src.d;
+    const double dd = (double)(float)dd_.dx;
+    const double sx = (double)dd_.nx * dd / (double)ss.nx, sy = (double)dd_.ny * dd / (double)ss.ny;
+    for (size_t j = 0; j < dd_.ny; ++j) {
+      const double y0 = (double)j * dd, y1 = (double)(j + 1) * dd;
+      for (size_t i = 0; i < dd_.nx; ++i) {
+        const double x0 = (double)i * dd, x1 = (double)(i + 1) * dd;
+        double total = 0;
+        const size_t i0 = (size_t)std::floor(x0 / sx), i1 = std::min((size_t)std::ceil(x1 / sx), ss.nx);
+        const size_t j0 = (size_t)std::floor(y0 / sy), j1 = std::min((size_t)std::ceil(y1 / sy), ss.ny);
+        const size_t cc = col(i, j);
+        if (!column_active(i, j)) { eta[cc] = rest; eta_roundoff[cc] = 0; continue; }
+        for (size_t sj = j0; sj < j1; ++sj) {
+          const double ya = std::max(y0, (double)sj * sy), yb = std::min(y1, (double)(sj + 1) * sy);
+          if (yb <= ya) continue;
+          for (size_t si = i0; si < i1; ++si) {
+            const double xa = std::max(x0, (double)si * sx), xb = std::min(x1, (double)(si + 1) * sx);
+            if (xb <= xa) continue;
+            const double area = (xb - xa) * (yb - ya);
+            const double cx = 0.5 * (xa + xb) - ((double)si + 0.5) * sx, cy = 0.5 * (ya + yb) - ((double)sj + 0.5) * sy;
+            double h;
+            if (src.column_active(si, sj))
+              h = src.compensated(si, sj) + src.surface_slope(si, sj, 0) * cx + src.surface_slope(si, sj, 1) * cy +
+                  src.surface_twist(si, sj) * cx * cy;
+            else
+              h = (double)(float)src.rest;
+            total += area * h;
+          }
+        }
+        const double h = total / (dd * dd);
+        eta[cc] = (R)(float)h;
+        eta_roundoff[cc] = (R)(float)((double)(float)eta[cc] - h);
+      }
+    }
+  }
+  // resample_faces (delta3d_levels.rs:249-288)
+  void resample_faces(const Volume3& src) {
+    const size_t n = std::max((size_t)std::ceil((double)(float)d.dx / (double)(float)src.d.dx), (size_t)1);
+    const double cells[3] = {(double)d.nx, (double)d.ny, (double)d.nz};
+    for (int axis = 0; axis < 3; ++axis) {
+      const size_t dims[3] = {d.nx + (axis == 0), d.ny + (axis == 1), d.nz + (axis == 2)};
+      const int t1 = (axis + 1) % 3, t2 = (axis + 2) % 3;
+      for (size_t k = 0; k < dims[2]; ++k)
+        for (size_t j = 0; j < dims[1]; ++j)
+          for (size_t i = 0; i < dims[0]; ++i) {
+            const size_t p[3] = {i, j, k};
+            double centre[3];
+            for (int a = 0; a < 3; ++a) centre[a] = ((double)p[a] + (a == axis ? 0. : 0.5)) / cells[a];
+            double acc = 0;
+            for (size_t a = 0; a < n; ++a)
+              for (size_t b = 0; b < n; ++b) {
+                double q[3] = {centre[0], centre[1], centre[2]};
+                q[t1] += (((double)a + 0.5) / (double)n - 0.5) / cells[t1];
+                q[t2] += (((double)b + 0.5) / (double)n - 0.5) / cells[t2];
+                acc += (double)src.staggered_at(axis, q);
+              }
+            const float val = (float)(acc / (double)(n * n));
+            if (axis == 0) u[fu(i, j, k)] = val; else if (axis == 1) v[fv(i, j, k)] = val; else w[fw(i, j, k)] = val;
+          }
+    }
+  }
+
   // delta3d.rs:666-690
   void close_walls() {
     size_t nx = d.nx, ny = d.ny, nz = d.nz;
@@ -2202,6 +2361,31 @@ int od3_set_active_blocks(Volume3* v, const int32_t* blocks, uint64_t count, int
   v->apply_sparse(change);
   return OK;
 }
+
+// resample_from (delta3d_levels.rs:43-69): the state of `src`, which covers the same window at
+// another dx.  out: volume before (src), volume after (dst).
+int od3_resample_from(Volume3* v, const Volume3* src, double out[2]) {
+  if (!v || !src || !out) return INVALID;
+  const Domain3 &d = v->d, &s = src->d;
+  auto extent = [](size_t n, float dx) { return (double)n * (double)dx; };
+  auto same = [](double a, double b) { return std::fabs(a - b) <= 1e-6 * std::max(std::fabs(a), std::fabs(b)); };
+  auto fbits = [](float x) { uint32_t b; std::memcpy(&b, &x, 4); return b; };
+  if (!same(extent(d.nx, (float)d.dx), extent(s.nx, (float)s.dx)) || !same(extent(d.ny, (float)d.dx), extent(s.ny, (float)s.dx)) ||
+      !same(extent(d.nz, (float)d.dx), extent(s.nz, (float)s.dx)) || fbits((float)v->rest) != fbits((float)src->rest) ||
+      fbits((float)v->rho) != fbits((float)src->rho) || fbits((float)v->g_eff) != fbits((float)src->g_eff) ||
+      v->has_cut || src->has_cut)
+    return DOMAIN;
+  out[0] = src->perturbation_volume();
+  v->resample_surface(*src);
+  v->resample_faces(*src);
+  std::fill(v->p.begin(), v->p.end(), (R)0);
+  v->close_walls();
+  v->close_sparse_walls();
+  out[1] = v->perturbation_volume();
+  return OK;
+}
+
+double od3_perturbation_volume(const Volume3* v) { return v ? v->perturbation_volume() : 0.; }
 
 // active_columns / sparse_cells (delta3d_sparse.rs:129-141)
 int od3_active_columns(const Volume3* v, uint8_t* out, uint64_t len) {

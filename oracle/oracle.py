@@ -104,6 +104,9 @@ def lib(real: str = "f32") -> C.CDLL:
     L.od3_active_columns.argtypes = [vp, vp, u64]
     L.od3_sparse_cells.argtypes = [vp]
     L.od3_sparse_cells.restype = u64
+    L.od3_resample_from.argtypes = [vp, vp, dp]
+    L.od3_perturbation_volume.argtypes = [vp]
+    L.od3_perturbation_volume.restype = C.c_double
     _LIBS[real] = L
     return L
 
@@ -299,6 +302,15 @@ class OracleVolume:
 
     def sparse_cells(self) -> int:
         return int(self.L.od3_sparse_cells(self.h))
+
+    # The level change (delta3d_levels.rs:38-69).
+    def resample_from(self, src: "OracleVolume") -> dict:
+        out = (C.c_double * 2)()
+        self._check(self.L.od3_resample_from(self.h, src.h, out), "resample_from")
+        return {"volume_before": float(out[0]), "volume_after": float(out[1])}
+
+    def perturbation_volume(self) -> float:
+        return float(self.L.od3_perturbation_volume(self.h))
 
     def last_refused_report(self):
         rep = (C.c_double * 8)()
