@@ -786,6 +786,94 @@ __global__ void k_advect(Geo g, float dt, const float* __restrict__ u, const flo
   ws[f] = cur;
 }
 
+// The velocity of family `axis` at position p (velocity3, delta3d_coupling.rs:298-305).
+__device__ __forceinline__ float vel3(const Geo& g, const float* __restrict__ u, const float* __restrict__ v,
+                                      const float* __restrict__ w, int axis, int i, int j, int k) {
+  if (axis == 0) return u[fu(g, i, j, k)];
+  if (axis == 1) return v[fv(g, i, j, k)];
+  return w[fw(g, i, j, k)];
+}
+
+// correct_advection3 (delta3d_advection.rs:31-111) of the uncoupled step: + (dt^2/2) sum_ab V_a V_b
+// d_a d_b u on the predicted us/vs/ws, V collocated at the face (collocated3, delta3d_coupling.rs:
+// 308-328), derivatives of the velocities at the start of the step.  A direction with a neighbour
+// outside its axis's grid (the box's or the sparse set's) is left out, and so is a cross term with
+// a diagonal neighbour outside the set.  One thread per face; a face reads u, v, w and writes only
+// itself.
+__global__ void k_correct_advection(Geo g, float dt, const float* __restrict__ u, const float* __restrict__ v,
+                                    const float* __restrict__ w, float* __restrict__ us, float* __restrict__ vs,
+                                    float* __restrict__ ws) {
+  KSTART();
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int nu = (nx + 1) * ny * nz, nv = nx * (ny + 1) * nz, nw = nx * ny * (nz + 1);
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  int axis;
+  if (q < nu) axis = 0;
+  else if ((q -= nu) < nv) axis = 1;
+  else if ((q -= nv) < nw) axis = 2;
+  else return;
+  const int dims[3] = {nx, ny, nz};
+  const int end[3] = {nx + (axis == 0), ny + (axis == 1), nz + (axis == 2)};
+  const int p[3] = {q % end[0], (q / end[0]) % end[1], q / (end[0] * end[1])};
+  if (p[axis] == 0 || (axis < 2 && p[axis] == dims[axis])) return;
+  if (open3(g, axis, q) == 0.f) return;
+  auto V = [&](int a, const int r[3]) { return vel3(g, u, v, w, a, r[0], r[1], r[2]); };
+  float vel[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    float col;
+    if (a == axis) {
+      col = V(a, p);
+    } else {
+      int lo[3] = {p[0], p[1], p[2]};
+      lo[axis] -= 1;
+      int hi[3] = {lo[0], lo[1], lo[2]};
+      hi[a] += 1;
+      if (axis == 2 && p[2] == nz) {
+        col = 0.5f * (V(a, lo) + V(a, hi));
+      } else {
+        int qq[3] = {lo[0], lo[1], lo[2]}, rr[3] = {hi[0], hi[1], hi[2]};
+        qq[axis] += 1;
+        rr[axis] += 1;
+        col = a < axis ? 0.25f * (V(a, lo) + V(a, hi) + V(a, qq) + V(a, rr))
+                       : 0.25f * (V(a, lo) + V(a, qq) + V(a, hi) + V(a, rr));
+      }
+    }
+    vel[a] = 0.f + col;  // the carried background velocity is 0 on the uncoupled step
+  }
+  const float c = V(axis, p);
+  auto shifted = [&](int da, int sa, int db, int sb, int r[3]) {
+    r[0] = p[0]; r[1] = p[1]; r[2] = p[2];
+    r[da] += sa;
+    if (db >= 0) r[db] += sb;
+  };
+  auto at = [&](int da, int sa, int db, int sb) { int r[3]; shifted(da, sa, db, sb, r); return V(axis, r); };
+  auto outside = [&](int da, int sa, int db, int sb) {
+    if (!g.act) return false;
+    int r[3]; shifted(da, sa, db, sb, r);
+    return sparse_outside3(g, axis, r[0], r[1]);
+  };
+  auto inside = [&](int a) { return p[a] > 0 && p[a] + 1 < end[a] && !outside(a, 1, -1, 0) && !outside(a, -1, -1, 0); };
+  float acc = 0.f;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    if (!inside(a)) continue;
+    acc += vel[a] * vel[a] * (at(a, 1, -1, 0) - 2.f * c + at(a, -1, -1, 0));
+#pragma unroll
+    for (int b = a + 1; b < 3; ++b) {
+      if (!inside(b)) continue;
+      if (outside(a, 1, b, 1) || outside(a, 1, b, -1) || outside(a, -1, b, 1) || outside(a, -1, b, -1)) continue;
+      const float cross = at(a, 1, b, 1) - at(a, 1, b, -1) - at(a, -1, b, 1) + at(a, -1, b, -1);
+      acc += 2.f * vel[a] * vel[b] * 0.25f * cross;
+    }
+  }
+  const float scale = 0.5f * dt * dt;
+  const float term = scale * acc / (g.dx * g.dx);
+  if (axis == 0) us[q] += term;
+  else if (axis == 1) vs[q] += term;
+  else ws[q] += term;
+}
+
 // extrapolate_mobile3 (delta3d_mobile.rs:345-394): one thread per column and axis walks up the
 // column and copies the last solved face into the unsolved open faces above it.
 __global__ void k_extrapolate(Geo g, float* __restrict__ u, float* __restrict__ v, float* __restrict__ w) {

@@ -99,6 +99,7 @@ struct fd3_volume {
   // the inner loop's kernels read ghost coefficients only, so the loop graph does not depend on it.
   bool homog = false;
   bool precondition_cut = true;   // Jacobi on the linear cut path (set_precondition_cut, delta3d.rs:526)
+  bool advection_correction = false;  // the second-order advection term (delta3d_advection.rs:17-26)
   float *z = nullptr, *z2 = nullptr;
   std::vector<Lev> levels;
   Lev* dlev = nullptr;   // the level table in device memory (for the single-CTA coarse tail)
@@ -1030,6 +1031,9 @@ int step_body(fd3_volume* V, float scale, float correction, float transport, flo
   Geo G = V->geo();
   LAUNCH(V, k_advect, (long long)V->nu + V->nv + V->nw, G, advection, (const float*)V->u, (const float*)V->v,
          (const float*)V->w, V->us, V->vs, V->ws);
+  if (V->advection_correction)  // delta3d_mobile.rs:858-860
+    LAUNCH(V, k_correct_advection, (long long)V->nu + V->nv + V->nw, G, advection, (const float*)V->u,
+           (const float*)V->v, (const float*)V->w, V->us, V->vs, V->ws);
   TRY(project_mobile3(V, scale, correction, max_iters, rep));
   if (rep->degraded) {
     V->has_refused = true;
@@ -1659,6 +1663,31 @@ int fd3_step_surface_linear(fd3_volume* V, uint64_t duration_us, uint32_t max_it
   if (!V || !rep) return FD3_ERR_INVALID_ARGUMENT;
   if (V->sparse) return FD3_ERR_DOMAIN;  // delta3d.rs:1210-1211
   return step_surface_linear(V, duration_us, max_iters, rep);
+}
+
+// enable_advection_correction / advection_correction (delta3d_advection.rs:17-26)
+int fd3_enable_advection_correction(fd3_volume* V) {
+  if (!V) return FD3_ERR_INVALID_ARGUMENT;
+  V->advection_correction = true;
+  return FD3_OK;
+}
+int fd3_advection_correction(const fd3_volume* V) { return V && V->advection_correction ? 1 : 0; }
+
+// The predictor alone, as tests_delta3d.rs:2136-2160 runs it: advect_mobile3, the second-order term
+// when enabled, then u = us (no projection).
+int fd3_advect_for_tests(fd3_volume* V, float dt) {
+  if (!V) return FD3_ERR_INVALID_ARGUMENT;
+  if (!(dt > 0.f) || !std::isfinite(dt)) return FD3_ERR_NOT_FINITE;
+  Geo G = V->geo();
+  LAUNCH(V, k_advect, (long long)V->nu + V->nv + V->nw, G, dt, (const float*)V->u, (const float*)V->v,
+         (const float*)V->w, V->us, V->vs, V->ws);
+  if (V->advection_correction)
+    LAUNCH(V, k_correct_advection, (long long)V->nu + V->nv + V->nw, G, dt, (const float*)V->u, (const float*)V->v,
+           (const float*)V->w, V->us, V->vs, V->ws);
+  CK(cudaMemcpyAsync(V->u, V->us, (size_t)V->nu * 4, cudaMemcpyDeviceToDevice, V->stream));
+  CK(cudaMemcpyAsync(V->v, V->vs, (size_t)V->nv * 4, cudaMemcpyDeviceToDevice, V->stream));
+  CK(cudaMemcpyAsync(V->w, V->ws, (size_t)V->nw * 4, cudaMemcpyDeviceToDevice, V->stream));
+  return sync(V);
 }
 
 int fd3_set_precondition_cut(fd3_volume* V, int on) {

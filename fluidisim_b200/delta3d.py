@@ -151,6 +151,9 @@ def library() -> C.CDLL:
     L.fd3_sparse_cells.restype = u64
     L.fd3_resample_from.argtypes = [vp, vp, C.POINTER(_LevelChange)]
     L.fd3_perturbation_volume.argtypes = [vp, C.POINTER(C.c_double)]
+    L.fd3_enable_advection_correction.argtypes = [vp]
+    L.fd3_advection_correction.argtypes = [vp]
+    L.fd3_advect_for_tests.argtypes = [vp, f32]
     L.fd3_get_pressure.argtypes = [vp, fp, sz]
     L.fd3_get_velocity.argtypes = [vp, fp, sz, fp, sz, fp, sz]
     L.fd3_get_surface.argtypes = [vp, fp, fp, sz]
@@ -371,6 +374,18 @@ class Volume3:
         self._check(self._L.fd3_step_surface_mobile(self._h, int(duration_us), int(max_iters), C.byref(r)),
                     "step_surface_mobile")
         return Report._from(r)
+
+    def enable_advection_correction(self):
+        """Volume3::enable_advection_correction (delta3d_advection.rs:19): the second-order advection term."""
+        self._check(self._L.fd3_enable_advection_correction(self._h), "enable_advection_correction")
+
+    def advection_correction(self) -> bool:
+        return bool(self._L.fd3_advection_correction(self._h))
+
+    def advect_for_tests(self, dt):
+        """The predictor alone (tests_delta3d.rs:2136-2160): advection over dt, the second-order term when on,
+        then u = us."""
+        self._check(self._L.fd3_advect_for_tests(self._h, np.float32(dt)), "advect_for_tests")
 
     def last_refused_report(self):
         r = _Report()

@@ -225,6 +225,15 @@ int fd3_project_mobile(fd3_volume* v, float scale, float k1, uint32_t max_iters,
 int fd3_refine_mobile(fd3_volume* v, float scale, float k1, uint32_t max_iters, fd3_report* report);
 /* Volume3::step_surface_mobile (delta3d_mobile.rs:819): advect, project, extrapolate, transport. */
 int fd3_step_surface_mobile(fd3_volume* v, uint64_t duration_us, uint32_t max_iters, fd3_report* report);
+/* Volume3::enable_advection_correction (delta3d_advection.rs:19): the second-order term of the
+ * advection, + (dt^2/2) sum V_a V_b d_a d_b u on the prediction (Lax-Wendroff at constant velocity),
+ * for the mobile steps that follow.  Off by default: the step is then the reference's, bit for bit. */
+int fd3_enable_advection_correction(fd3_volume* v);
+/* Volume3::advection_correction (delta3d_advection.rs:24): 1 when the term is on. */
+int fd3_advection_correction(const fd3_volume* v);
+/* The predictor alone, as tests_delta3d.rs:2136-2160 runs it: advect_mobile3 over dt seconds, the
+ * second-order term when on, then the prediction becomes the velocity.  No projection. */
+int fd3_advect_for_tests(fd3_volume* v, float dt);
 /* No reference counterpart: many independent volumes (patches), each projected as
  * fd3_project_mobile projects it, concurrently.  Every volume keeps its own stream and device-side
  * loop; `threads` host workers (0 = up to 16) issue them, largest first.  statuses[i] and

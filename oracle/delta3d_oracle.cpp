@@ -1357,6 +1357,73 @@ struct Volume3 {
     }
   }
 
+  // collocated3 (delta3d_coupling.rs:308-328): component a at the centre of a face of axis `axis`,
+  // four neighbours (two at the top w face)
+  R collocated3(int axis, int a, const size_t p[3]) const {
+    if (a == axis) return velocity3(a, p);
+    size_t lo[3] = {p[0], p[1], p[2]};
+    lo[axis] -= 1;
+    size_t hi[3] = {lo[0], lo[1], lo[2]};
+    hi[a] += 1;
+    if (axis == 2 && p[2] == d.nz) return (R)0.5 * (velocity3(a, lo) + velocity3(a, hi));
+    size_t q[3] = {lo[0], lo[1], lo[2]}, r[3] = {hi[0], hi[1], hi[2]};
+    q[axis] += 1;
+    r[axis] += 1;
+    const size_t *b = a < axis ? hi : q, *c2 = a < axis ? q : hi;
+    return (R)0.25 * (velocity3(a, lo) + velocity3(a, b) + velocity3(a, c2) + velocity3(a, r));
+  }
+
+  // correct_advection3 (delta3d_advection.rs:31-111) of the uncoupled step: + (dt^2/2) sum
+  // V_a V_b d_a d_b u on the predicted us/vs/ws, from the velocities at the start of the step.  A
+  // direction with a neighbour outside its axis's grid (the box's or the sparse set's) is left out;
+  // so is a cross term with a diagonal neighbour outside the set.
+  bool advection_correction = false;
+  void correct_advection3(R dt) {
+    if (!advection_correction) return;
+    const size_t dims[3] = {d.nx, d.ny, d.nz};
+    const R scale = (R)0.5 * dt * dt;
+    for (int axis = 0; axis < 3; ++axis) {
+      const size_t end[3] = {d.nx + (axis == 0), d.ny + (axis == 1), d.nz + (axis == 2)};
+      for (size_t k = 0; k < end[2]; ++k)
+        for (size_t j = 0; j < end[1]; ++j)
+          for (size_t i = 0; i < end[0]; ++i) {
+            const size_t p[3] = {i, j, k};
+            if (p[axis] == 0 || (axis < 2 && p[axis] == dims[axis])) continue;
+            const size_t f = axis == 0 ? fu(i, j, k) : (axis == 1 ? fv(i, j, k) : fw(i, j, k));
+            if (open3(axis, f) == 0) continue;
+            R vel[3];
+            for (int a = 0; a < 3; ++a) vel[a] = (R)0 + collocated3(axis, a, p);
+            const R c0 = velocity3(axis, p);
+            auto shifted = [&](int da, int sa, int db, int sb, size_t out[3]) {
+              out[0] = p[0]; out[1] = p[1]; out[2] = p[2];
+              if (da >= 0) out[da] = (size_t)((long long)out[da] + sa);
+              if (db >= 0) out[db] = (size_t)((long long)out[db] + sb);
+            };
+            auto at = [&](int da, int sa, int db, int sb) { size_t q[3]; shifted(da, sa, db, sb, q); return velocity3(axis, q); };
+            auto outside = [&](int da, int sa, int db, int sb) {
+              size_t q[3]; shifted(da, sa, db, sb, q);
+              return sparse_outside3(axis, q[0], q[1]);
+            };
+            auto inside = [&](int a) {
+              return p[a] > 0 && p[a] + 1 < end[a] && !outside(a, 1, -1, 0) && !outside(a, -1, -1, 0);
+            };
+            R acc = 0;
+            for (int a = 0; a < 3; ++a) {
+              if (!inside(a)) continue;
+              acc += vel[a] * vel[a] * (at(a, 1, -1, 0) - (R)2 * c0 + at(a, -1, -1, 0));
+              for (int b = a + 1; b < 3; ++b) {
+                if (!inside(b)) continue;
+                if (outside(a, 1, b, 1) || outside(a, 1, b, -1) || outside(a, -1, b, 1) || outside(a, -1, b, -1)) continue;
+                R cross = at(a, 1, b, 1) - at(a, 1, b, -1) - at(a, -1, b, 1) + at(a, -1, b, -1);
+                acc += (R)2 * vel[a] * vel[b] * (R)0.25 * cross;
+              }
+            }
+            const R term = scale * acc / (d.dx * d.dx);
+            if (axis == 0) us[f] += term; else if (axis == 1) vs[f] += term; else ws[f] += term;
+          }
+    }
+  }
+
   // delta3d_mobile.rs:734-782
   void transport_mobile3(R transport) {
     size_t nx = d.nx, ny = d.ny, nz = d.nz;
@@ -1684,6 +1751,7 @@ struct Volume3 {
     saved_u = u; saved_v = v; saved_w = w; saved_p = p; saved_eta = eta; saved_eta_roundoff = eta_roundoff;
     int e = [&]() -> int {
       advect_mobile3(advection);
+      correct_advection3(advection);  // the second-order term, when enabled (delta3d_mobile.rs:858-860)
       int err = project_mobile3(scale, correction, max_iters, rep);
       if (err) return err;
       if (rep[2] != 0) {
@@ -2386,6 +2454,23 @@ int od3_resample_from(Volume3* v, const Volume3* src, double out[2]) {
 }
 
 double od3_perturbation_volume(const Volume3* v) { return v ? v->perturbation_volume() : 0.; }
+
+// The predictor alone, as tests_delta3d.rs:2136-2160 runs it: advect, the second-order term when
+// on, then u = us.
+int od3_advect_for_tests(Volume3* v, float dt) {
+  if (!v) return INVALID;
+  v->advect_mobile3((R)dt);
+  v->correct_advection3((R)dt);
+  v->u = v->us; v->v = v->vs; v->w = v->ws;
+  return OK;
+}
+
+// enable_advection_correction (delta3d_advection.rs:17-21)
+int od3_enable_advection_correction(Volume3* v) {
+  if (!v) return INVALID;
+  v->advection_correction = true;
+  return OK;
+}
 
 // active_columns / sparse_cells (delta3d_sparse.rs:129-141)
 int od3_active_columns(const Volume3* v, uint8_t* out, uint64_t len) {

@@ -107,6 +107,8 @@ def lib(real: str = "f32") -> C.CDLL:
     L.od3_resample_from.argtypes = [vp, vp, dp]
     L.od3_perturbation_volume.argtypes = [vp]
     L.od3_perturbation_volume.restype = C.c_double
+    L.od3_enable_advection_correction.argtypes = [vp]
+    L.od3_advect_for_tests.argtypes = [vp, f32]
     _LIBS[real] = L
     return L
 
@@ -308,6 +310,13 @@ class OracleVolume:
         out = (C.c_double * 2)()
         self._check(self.L.od3_resample_from(self.h, src.h, out), "resample_from")
         return {"volume_before": float(out[0]), "volume_after": float(out[1])}
+
+    def enable_advection_correction(self):
+        """enable_advection_correction (delta3d_advection.rs:17-21): the second-order term of the advection."""
+        self._check(self.L.od3_enable_advection_correction(self.h), "enable_advection_correction")
+
+    def advect_for_tests(self, dt):
+        self._check(self.L.od3_advect_for_tests(self.h, np.float32(dt)), "advect_for_tests")
 
     def perturbation_volume(self) -> float:
         return float(self.L.od3_perturbation_volume(self.h))

@@ -62,13 +62,17 @@ NAMES = ["eta", "roundoff", "u", "v", "w", "p"]
 
 @pytest.mark.parametrize("reduction", [REDUCE_ORDERED_F32, REDUCE_F64])
 @pytest.mark.parametrize("mg", [False, True])
-def test_a_full_set_is_the_box_at_bit(reduction, mg):
-    """Criterion 1 (tests_delta3d_sparse.rs:52-72), in both reduction modes and kernel families."""
+@pytest.mark.parametrize("correction", [False, True])
+def test_a_full_set_is_the_box_at_bit(reduction, mg, correction):
+    """Criterion 1 (tests_delta3d_sparse.rs:52-72), in both reduction modes and kernel families, with
+    and without the second-order advection term."""
     nx, ny = 24, 16
     plain, sparse = gpu(nx, ny, False, mg, reduction), gpu(nx, ny, True, mg, reduction)
     eta = scenes.bumps_in(nx, ny, np.ones(nx * ny), [(9.0, 7.0)])
     for v in (plain, sparse):
         v.set_free_surface(eta, REST)
+        if correction:
+            v.enable_advection_correction()
     assert sparse.sparse_cells() == nx * ny * NZ
     for s in range(20):
         a, b = plain.step_surface_mobile(DT_US, 20_000), sparse.step_surface_mobile(DT_US, 20_000)

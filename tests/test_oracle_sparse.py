@@ -45,13 +45,16 @@ def perturbation_volume(v):
     return total * (np.float64(np.float32(DX)) ** 2)
 
 
-def test_a_full_set_is_the_box_at_bit():
+@pytest.mark.parametrize("correction", [False, True])
+def test_a_full_set_is_the_box_at_bit(correction):
     """Criterion 1 (tests_delta3d_sparse.rs:52-72): with every column in the set, fifty mobile steps
-    are bit-identical to the steps without a set."""
+    are bit-identical to the steps without a set, with and without the second-order advection term."""
     plain, sparse = domain(24, 16, False), domain(24, 16, True)
     eta = scenes.bumps_in(24, 16, np.ones(24 * 16), [(9.0, 7.0)])
     for v in (plain, sparse):
         v.set_free_surface(eta, REST)
+        if correction:
+            v.enable_advection_correction()
     assert sparse.sparse_cells() == plain.cells
     for s in range(50):
         a, b = plain.step_surface_mobile(DT_US, 20_000), sparse.step_surface_mobile(DT_US, 20_000)
