@@ -1348,7 +1348,8 @@ int fd3_enable_multigrid(fd3_volume* V) {
       floats += tail_level_floats(V->levels[l].nx, V->levels[l].ny, V->levels[l].nz);
     if (floats * sizeof(float) <= 200 * 1024) {
       V->tail_smem_bytes = floats * sizeof(float);
-      CK(cudaFuncSetAttribute(k_coarse_tail_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)V->tail_smem_bytes));
+      // the largest size any volume may ask for: the attribute is per function, shared by every volume
+      CK(cudaFuncSetAttribute(k_coarse_tail_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     }
   }
   if (!V->levels.empty()) {
