@@ -781,15 +781,125 @@ def cpu_patches_sample(ps, budget_s: float = 20.0):
             "sample": f"the first {done} patches of the set, oracle with OpenMP (setup excluded)"}
 
 
+def run_sparse(args):
+    """A sparse set in a 256 x 256 x 32 window (37% of the columns, blocks along a curved path):
+    projections per second of the set, against the same set with every tile of the window
+    processed (what looping over the whole window costs) and against the dense window.  N > 1
+    runs replicas."""
+    import numpy as np
+    import torch
+
+    from fluidisim_b200 import build as B
+    from fluidisim_b200 import scenes
+    from fluidisim_b200.delta3d import REDUCE_F64, Volume3
+
+    rank, world, local = dist_setup(args.gpus)
+    B.build()
+    s = scenes.sparse_window(args.size)
+    scale, k1 = float(np.float32(-s["rho"] / s["dt"])), float(np.float32(s["dt"] / s["rho"]))
+    du, dv, dw = (torch.from_numpy(s[k]).cuda() for k in ("u", "v", "w"))
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.Stream()
+    rest = np.float32(s["rest"])
+
+    def volume(mask, skip):
+        v = Volume3.configure(s["nx"], s["ny"], s["nz"], s["dx"], s["rho"], s["g"])
+        v.set_options(reduction=REDUCE_F64, use_graphs=args.graphs, no_tile_skip=0 if skip else 1)
+        v.set_stream(stream.cuda_stream)
+        v.enable_multigrid()
+        v.enable_sparse()
+        v.set_active_columns(mask)
+        v.set_free_surface(np.where(mask != 0, s["eta"], rest).astype(np.float32), s["rest"])
+        return v
+
+    def timed(v, steps, clocks=None):
+        def step():
+            v.set_velocity_device(du.data_ptr(), dv.data_ptr(), dw.data_ptr())
+            v.reset_pressure()
+            return v.project_mobile3(scale, k1, 4000)
+        for _ in range(args.warmup):
+            rep = step()
+        torch.cuda.synchronize()
+        barrier(world)
+        launches0 = v.kernel_launches()
+        if clocks:
+            clocks.mark(True)
+        total = 0.0
+        for _ in range(steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            rep = step()
+            b.record(stream)
+            torch.cuda.synchronize()
+            total += a.elapsed_time(b)
+        if clocks:
+            clocks.mark(False)
+        return max_over_ranks(total, world), rep, v.kernel_launches() - launches0
+
+    full = np.ones(s["nx"] * s["ny"], np.uint8)
+    side_steps = max(10, args.steps // 3)
+    with ClockSampler(local) as clocks:
+        ms_set, rep, launches = timed(volume(s["mask"], True), args.steps, clocks)
+    ms_all_tiles, rep_all, _ = timed(volume(s["mask"], False), side_steps)
+    ms_dense, rep_dense, _ = timed(volume(full, True), side_steps)
+    if rank == 0:
+        frac = float(s["mask"].mean())
+        cpu = None
+        if world == 1 and not args.no_cpu:
+            from oracle import oracle as O
+            O.build()
+            O.set_threads(O.max_threads())
+            o = O.OracleVolume(s["nx"], s["ny"], s["nz"], s["dx"], s["rho"], s["g"])
+            o.enable_multigrid()
+            o.enable_sparse()
+            o.set_active_columns(s["mask"])
+            times = []
+            t_start = time.perf_counter()
+            while not times or (time.perf_counter() - t_start < 20.0 and len(times) < 3):
+                o.set_free_surface(np.where(s["mask"] != 0, s["eta"], rest).astype(np.float32), s["rest"])
+                o.set_velocity(s["u"], s["v"], s["w"])
+                t0 = time.perf_counter()
+                o.project_mobile(scale, k1, 4000)
+                times.append(time.perf_counter() - t0)
+            cpu = {"value": len(times) / sum(times), "unit": "projections/s", "cores": O.max_threads(), "kind": "port",
+                   "sample": f"{len(times)} projections of the same set, oracle with OpenMP (it loops over the window)"}
+        out = {
+            "impl": "b200",
+            "metric": f"sparse-set projections/s ({args.size}x{args.size}x{s['nz']} window, {100 * frac:.0f}% of the "
+                      f"columns in the set)",
+            "value": world * args.steps / (ms_set * 1e-3), "unit": "projections/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_set / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded sparse window)",
+            "config": {"workload": f"sparse_window {args.size}^2 x {s['nz']}: 8x8-column blocks within 3 blocks of a "
+                                   f"curved path, 5 cm bumps, N(0,0.3) faces; projection from p = 0",
+                       "active_fraction": frac, "iterations": rep.iterations, "parallelism": f"replicas x{world}",
+                       "l2": "256 MiB written between steps"},
+            "every_tile": {"value": world * side_steps / (ms_all_tiles * 1e-3), "iterations": rep_all.iterations,
+                           "note": "the same set, every tile of the window processed"},
+            "dense_window": {"value": world * side_steps / (ms_dense * 1e-3), "iterations": rep_dense.iterations,
+                             "note": "every column of the window in the set"},
+            "gpu_launches": launches,
+            "cpu_baseline": cpu,
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="basin", choices=["basin", "wave", "patches"],
+    ap.add_argument("--workload", default="basin", choices=["basin", "wave", "patches", "sparse"],
                     help="basin: the 128^3 box basin the metric is quoted on; wave: the 256^3 breaking wave; "
-                         "patches: the batched delta patches")
+                         "patches: the batched delta patches; sparse: a sparse set in a 256^2 x 32 window")
     ap.add_argument("--patches", type=int, default=256, help="patch count of the patches workload")
     ap.add_argument("--threads", type=int, default=0, help="host workers of fd3_project_batch (0 = up to 16)")
     ap.add_argument("--size", type=int, default=None, help="grid side (default 128 for basin, 256 for wave)")
@@ -804,8 +914,14 @@ def main():
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.size is None:
-        args.size = 256 if args.workload == "wave" else 128
-    if args.workload == "patches":
+        args.size = 256 if args.workload in ("wave", "sparse") else 128
+    if args.workload == "sparse":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the sparse-window workload has no reference arm; "
+                              "its line carries the oracle's cpu_baseline"}), flush=True)
+        else:
+            run_sparse(args)
+    elif args.workload == "patches":
         if args.impl == "reference":
             run_reference_patches(args)
         else:

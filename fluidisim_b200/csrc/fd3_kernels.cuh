@@ -52,7 +52,13 @@ struct Geo {
   const float* ov;
   const float* ow;
   const unsigned char* act;  // sparse column set, 1 per column in the domain (null: every column)
+  // per 32 x 8 tile of columns, 1 if any column of the tile is in the sparse set (null: every tile).
+  // The blocked fine kernels skip the other tiles: every cell there is solid, every vector the
+  // projection writes is 0 there (the set change zeroes them), and a skipped tile adds exactly 0 to
+  // each reduction, so skipping changes no bit.
+  const unsigned char* tiles;
 };
+constexpr int TILE_X = 32, TILE_Y = 8;
 
 // A coarse level (Level3, delta3d_multigrid.rs:37-52).
 struct Lev {

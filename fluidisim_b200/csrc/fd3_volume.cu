@@ -92,6 +92,7 @@ struct fd3_volume {
   bool sparse = false;
   unsigned char *act = nullptr, *act_next = nullptr;
   std::vector<unsigned char> hact;
+  unsigned char* tiles = nullptr;  // per 32 x 8 tile of columns: any column in the set (Geo::tiles)
   // multigrid
   bool has_mg = false;
   bool linear = false;            // the current projection is the linear path's
@@ -151,6 +152,7 @@ struct fd3_volume {
     G.eta = eta; G.rof = rof;
     G.frac = frac; G.ou = ou; G.ov = ov; G.ow = ow;
     G.act = sparse ? act : nullptr;
+    G.tiles = sparse && !opt.no_tile_skip ? tiles : nullptr;
     return G;
   }
   bool ord() const { return opt.reduction == FD3_REDUCE_ORDERED_F32; }
@@ -161,7 +163,8 @@ struct fd3_volume {
   bool half() const { return opt.storage == FD3_STORAGE_F16 && paired() && mg_on(); }
   int loop_key() const {
     return (ord() ? 1 : 0) | (mg_on() ? 2 : 0) | (blocked() ? 4 : 0) | (opt.no_overlap ? 8 : 0) | (linear ? 16 : 0) |
-           (paired() ? 32 : 0) | (half() ? 64 : 0) | (sparse ? 128 : 0);  // the captured Geo holds the set's mask
+           (paired() ? 32 : 0) | (half() ? 64 : 0) | (sparse ? 128 : 0) |  // the captured Geo holds the set's mask
+           (opt.no_tile_skip ? 256 : 0);
   }
   Red red() const { return Red{p64, p32, count}; }
 };
@@ -264,6 +267,10 @@ int pull(fd3_volume* V) {
 
 // Grid of the grid-stride update: no more blocks than groups of four cells need.
 inline int update_blocks(int n) { return std::min(UPDATE_BLOCKS, std::max(1, blocks_for((n + 3) / 4))); }
+// The sparse set for kv_update_rn's skip (four cells of a row share a 4-byte mask word when nx % 4 == 0).
+inline const unsigned char* update_mask(const fd3_volume* V) {
+  return V->sparse && !V->opt.no_tile_skip && V->nx % 4 == 0 ? V->act : nullptr;
+}
 
 #define DISPATCH(V, KERNEL, N, ...)                                                               \
   do {                                                                                           \
@@ -457,7 +464,7 @@ void iteration(fd3_volume* V, int parity) {
                       dout, V->tmp, V->red(), V->dS);
       }
       LAUNCH_G(V, kv_update_rn, update_blocks(V->n), TPB, V->n, V->p, V->res, (const float*)dout,
-               (const float*)V->tmp, V->red(), V->dS);
+               (const float*)V->tmp, V->red(), V->dS, update_mask(V), V->ncol);
     } else if (V->blocked()) {
       if (zfull(V->nx, V->ny, V->nz))
         LAUNCH_G(V, kz_dir_apply_dot<true>, zblocks(V->nx, V->ny, V->nz), ZT, G, (const unsigned short*)V->codes,
@@ -466,7 +473,7 @@ void iteration(fd3_volume* V, int parity) {
         LAUNCH_G(V, kz_dir_apply_dot<false>, zblocks(V->nx, V->ny, V->nz), ZT, G, (const unsigned short*)V->codes,
                  (const float*)V->z, (const float*)din, dout, V->tmp, V->red(), V->dS);
       LAUNCH_G(V, kv_update_rn, update_blocks(V->n), TPB, V->n, V->p, V->res, (const float*)dout,
-               (const float*)V->tmp, V->red(), V->dS);
+               (const float*)V->tmp, V->red(), V->dS, update_mask(V), V->ncol);
     } else {
       DISPATCH(V, k_dir_apply_dot, V->n, G, (const unsigned short*)V->codes, (const float*)V->z, (const float*)din, dout,
                V->tmp, V->red(), V->dS);
@@ -1289,7 +1296,8 @@ void fd3_destroy(fd3_volume* v) {
 
 int fd3_set_options(fd3_volume* v, const fd3_options* o) {
   if (!v || !o) return FD3_ERR_INVALID_ARGUMENT;
-  if (o->reduction > 1 || o->kernels > 2 || o->no_overlap > 1 || o->storage > 1) return FD3_ERR_DOMAIN;
+  if (o->reduction > 1 || o->kernels > 2 || o->no_overlap > 1 || o->storage > 1 || o->no_tile_skip > 1)
+    return FD3_ERR_DOMAIN;
   // FP16 storage runs on the paired fine kernels: f64 reductions, kernels = 0 and an even nx
   if (o->storage == FD3_STORAGE_F16 && (o->reduction != FD3_REDUCE_F64 || o->kernels != 0 || v->nx % 2 != 0))
     return FD3_ERR_DOMAIN;
@@ -1436,6 +1444,17 @@ int fd3_set_velocity_device(fd3_volume* V, const float* u, const float* vv, cons
 }
 
 // ------------------------------------------------------------------------------- sparse sets
+// Geo::tiles from the host copy of the set: 1 for a 32 x 8 tile of columns with a column in it.
+static int upload_tiles(fd3_volume* V) {
+  const int ntx = (V->nx + TILE_X - 1) / TILE_X, nty = (V->ny + TILE_Y - 1) / TILE_Y;
+  std::vector<unsigned char> t((size_t)ntx * nty, 0);
+  for (int j = 0; j < V->ny; ++j)
+    for (int i = 0; i < V->nx; ++i)
+      if (V->hact[(size_t)j * V->nx + i]) t[(size_t)(j / TILE_Y) * ntx + i / TILE_X] = 1;
+  CK(cudaMemcpyAsync(V->tiles, t.data(), t.size(), cudaMemcpyHostToDevice, V->stream));
+  return sync(V);
+}
+
 // enable_sparse (delta3d_sparse.rs:105-117): the masks are reserved here, every column in the set.
 int fd3_enable_sparse(fd3_volume* V) {
   if (!V) return FD3_ERR_INVALID_ARGUMENT;
@@ -1443,11 +1462,15 @@ int fd3_enable_sparse(fd3_volume* V) {
   float *a, *b;
   TRY(dalloc(V, &a, ((size_t)V->ncol + 3) / 4));
   TRY(dalloc(V, &b, ((size_t)V->ncol + 3) / 4));
+  const size_t ntiles = (size_t)((V->nx + TILE_X - 1) / TILE_X) * ((V->ny + TILE_Y - 1) / TILE_Y);
+  float* t;
+  TRY(dalloc(V, &t, (ntiles + 3) / 4));
   V->act = (unsigned char*)a;
   V->act_next = (unsigned char*)b;
+  V->tiles = (unsigned char*)t;
   V->hact.assign(V->ncol, 1);
   CK(cudaMemcpyAsync(V->act, V->hact.data(), V->ncol, cudaMemcpyHostToDevice, V->stream));
-  TRY(sync(V));
+  TRY(upload_tiles(V));
   V->sparse = true;
   return FD3_OK;
 }
@@ -1484,9 +1507,17 @@ static int apply_sparse(fd3_volume* V, const std::vector<unsigned char>& next, f
     LAUNCH(V, k_sparse_leave, (long long)ncol + V->n + V->nu + V->nv + V->nw, V->geo(),
            (const unsigned char*)V->act_next, V->rest, V->eta, V->rof, V->p, V->u, V->v, V->w, V->dflag);
     CK(cudaMemcpyAsync(V->hflag, V->dflag, sizeof(int), cudaMemcpyDeviceToHost, V->stream));
+    // The blocked kernels skip tiles outside the set (Geo::tiles) and rely on every vector they
+    // write being 0 there.  The work vectors are scratch of each projection and the coarse
+    // levels' of each V-cycle, so they are zeroed whole; p was zeroed in the leaving columns.
+    for (float* f : {V->res, V->dir, V->dir2, V->tmp, V->z, V->z2})
+      if (f) CK(cudaMemsetAsync(f, 0, (size_t)V->n * 4, V->stream));
+    for (Lev& L : V->levels)
+      for (float* f : {L.x, L.x2, L.r, L.t}) CK(cudaMemsetAsync(f, 0, (size_t)L.n * 4, V->stream));
   }
   V->hact = next;
   CK(cudaMemcpyAsync(V->act, V->hact.data(), ncol, cudaMemcpyHostToDevice, V->stream));
+  TRY(upload_tiles(V));
   TRY(sync(V));
   if (ch.deactivated) std::memcpy(&ch.velocity_removed, V->hflag, 4);
   for (unsigned char a : V->hact) ch.active_columns += a != 0;

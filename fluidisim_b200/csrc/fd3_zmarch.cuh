@@ -117,6 +117,7 @@ __device__ __forceinline__ void zmarch(const Geo& g, const unsigned short* __res
   __shared__ float sbuf[FD3_PLANES][ZY + 2][ZX + 2];
   const int tx = threadIdx.x % ZX, ty = threadIdx.x / ZX;
   const ZTile t = ztile(g);
+  if (g.tiles && !g.tiles[(t.j / TILE_Y) * ((g.nx + TILE_X - 1) / TILE_X) + t.i / TILE_X]) return;  // no column of the set
   const int nxny = g.nx * g.ny;
   const int base = t.j * g.nx + t.i;
   // this thread's halo duty in x and in y (at most one each)
@@ -179,6 +180,7 @@ __device__ __forceinline__ void zmarch_full(const Geo& g, const unsigned short* 
   __shared__ float sbuf[FD3_PLANES][ZY + 2][ZX + 2];
   const int tx = threadIdx.x % ZX, ty = threadIdx.x / ZX;
   const ZTile t = ztile(g);
+  if (g.tiles && !g.tiles[(t.j / TILE_Y) * ((g.nx + TILE_X - 1) / TILE_X) + t.i / TILE_X]) return;  // no column of the set
   const int nxny = g.nx * g.ny;
   const int base = t.j * g.nx + t.i;
   const int hxi = tx == 0 ? t.i - 1 : (tx == ZX - 1 ? t.i + 1 : -1);
@@ -433,9 +435,11 @@ __global__ void __launch_bounds__(ZT, FD3_ZMINB) kz_fine_restrict(Geo g, const u
 
 // p += alpha d, r -= alpha q, r.r (FIN_RN): four cells per thread with 16-byte loads, grid-stride.
 constexpr int UPDATE_BLOCKS = 592;
+// `act` (the sparse set, with nx % 4 == 0; else null): four cells of one row whose columns are all
+// outside the set are skipped (p, r, d, q are 0 there and stay 0).
 __global__ void __launch_bounds__(TPB) kv_update_rn(int n, float* __restrict__ p, float* __restrict__ r,
                                                     const float* __restrict__ d, const float* __restrict__ q, Red red,
-                                                    Scalars* S) {
+                                                    Scalars* S, const unsigned char* __restrict__ act, int ncol) {
   KSTART();
   if (!S->active) return;
   const float alpha = S->alpha;
@@ -449,6 +453,7 @@ __global__ void __launch_bounds__(TPB) kv_update_rn(int n, float* __restrict__ p
   const float4* d4 = reinterpret_cast<const float4*>(d);
   const float4* q4 = reinterpret_cast<const float4*>(q);
   for (int v = tid; v < n4; v += stride) {
+    if (act && *reinterpret_cast<const unsigned*>(act + (4 * v) % ncol) == 0u) continue;
     float4 P = p4[v], R = r4[v];
     const float4 D = d4[v], Q = q4[v];
     P.x += alpha * D.x; P.y += alpha * D.y; P.z += alpha * D.z; P.w += alpha * D.w;

@@ -75,6 +75,10 @@ __device__ __forceinline__ void zmarch2(const Geo& g, const unsigned short* __re
   __shared__ __align__(16) float sbuf[2][Z2Y + 2][Z2ROW];
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
   const ZTile2 t = ztile2<K2>(g);
+  if (g.tiles) {  // a 64 x 8 tile is two 32 x 8 tiles of the set's tile flags
+    const int ntx = (g.nx + TILE_X - 1) / TILE_X, row = (t.j / TILE_Y) * ntx, a = t.x0 / TILE_X;
+    if (!g.tiles[row + a] && (a + 1 >= ntx || !g.tiles[row + a + 1])) return;  // no column of the set
+  }
   const int nxny = g.nx * g.ny;
   const int base = t.j * g.nx + t.i0;
   // x halo: lane 0 the cell left of the tile, lane 31 the cell right of it

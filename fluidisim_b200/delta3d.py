@@ -52,7 +52,7 @@ class _Report(C.Structure):
 class _Options(C.Structure):
     _fields_ = [("reduction", C.c_uint32), ("mg_max_levels", C.c_uint32), ("use_graphs", C.c_uint32),
                 ("kernels", C.c_uint32), ("no_overlap", C.c_uint32), ("storage", C.c_uint32),
-                ("reserved", C.c_uint32 * 2)]
+                ("no_tile_skip", C.c_uint32), ("reserved", C.c_uint32 * 1)]
 
 
 class _SparseChange(C.Structure):
@@ -241,7 +241,7 @@ class Volume3:
 
     # ---- options
     def set_options(self, reduction=None, mg_max_levels=None, use_graphs=None, kernels=None, no_overlap=None,
-                    storage=None):
+                    storage=None, no_tile_skip=None):
         o = _Options()
         self._check(self._L.fd3_get_options(self._h, C.byref(o)), "get_options")
         if reduction is not None:
@@ -256,6 +256,8 @@ class Volume3:
             o.no_overlap = int(no_overlap)
         if storage is not None:
             o.storage = int(storage)
+        if no_tile_skip is not None:
+            o.no_tile_skip = int(no_tile_skip)
         self._check(self._L.fd3_set_options(self._h, C.byref(o)), "set_options")
 
     def set_stream(self, stream_ptr: int):

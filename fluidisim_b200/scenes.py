@@ -407,3 +407,31 @@ def bumps_in(nx: int, ny: int, mask, centres, rest: float = SPARSE_REST) -> np.n
             s = f32(s + f32(f32(0.05) * expf(f32(-(f32(x * x) + f32(y * y))) / f32(8.0))))
         out[c] = f32(r + s)
     return out
+
+
+def sparse_window(n: int = 256, nz: int = 32, seed: int = 6, half_width_blocks: int = 3) -> dict:
+    """A n x n x nz window at 25 cm, 4 m of water at rest, whose sparse set is the blocks of 8 x 8
+    columns within `half_width_blocks` blocks of a curved path across it (the kind of set that
+    follows a moving source).  In the set: a train of 5 cm bumps along the path and N(0, 0.3) m/s
+    face noise; outside it the surface is at rest (the faces there are closed by set_velocity)."""
+    rng = SplitMix64(seed)
+    nb = n // 8
+    blocks = np.zeros((nb, nb), np.uint8)
+    path = []
+    jj, ii = np.mgrid[0:nb, 0:nb]
+    for t in np.linspace(0.0, 1.0, 4 * nb):
+        bx = 0.15 * nb + 0.7 * nb * t
+        by = 0.5 * nb + 0.3 * nb * math.sin(2 * math.pi * t)
+        path.append((bx, by))
+        blocks |= ((np.abs(ii + 0.5 - bx) <= half_width_blocks) & (np.abs(jj + 0.5 - by) <= half_width_blocks)).astype(np.uint8)
+    mask = np.kron(blocks, np.ones((8, 8), np.uint8)).ravel()
+    dx, rest = float(f32(0.25)), float(f32(4.0))
+    centres = [(8 * bx, 8 * by) for bx, by in path[:: max(1, len(path) // 6)]]
+    j, i = np.mgrid[0:n, 0:n]
+    h = np.zeros((n, n))
+    for cx, cy in centres:
+        h += 0.05 * np.exp(-((i + 0.5 - cx) ** 2 + (j + 0.5 - cy) ** 2) / 32.0)
+    eta = np.where(mask.reshape(n, n) != 0, rest + h, rest).astype(np.float32).ravel()
+    nu, nv, nw = face_counts(n, n, nz)
+    return dict(nx=n, ny=n, nz=nz, dx=dx, rho=1000.0, g=9.81, mask=mask, eta=eta, rest=rest,
+                u=rng.normal_array(nu, 0.3), v=rng.normal_array(nv, 0.3), w=rng.normal_array(nw, 0.3), dt=0.02)

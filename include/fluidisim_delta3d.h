@@ -95,7 +95,9 @@ typedef struct fd3_options {
                              = programmatic dependent launch: the next kernel is scheduled early and
                              waits on the device (results are identical either way) */
   uint32_t storage;       /* fd3_storage of the V-cycle vectors */
-  uint32_t reserved[2];
+  uint32_t no_tile_skip;  /* 1 = the blocked fine kernels process the tiles of columns outside the
+                             sparse set too; 0 (default) = they skip them (results are identical) */
+  uint32_t reserved[1];
 } fd3_options;
 
 typedef struct fd3_volume fd3_volume;

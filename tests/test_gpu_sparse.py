@@ -231,3 +231,34 @@ def test_a_sparse_set_over_a_cut_lake_matches_the_oracle():
     assert a["iterations"] == b.iterations
     for x, y, name in zip([*o.velocity(), o.pressure()], [*d.velocity(), d.pressure()], ["u", "v", "w", "p"]):
         assert_bits(x, y, name)
+
+
+@pytest.mark.parametrize("kernels", [0, 2])
+def test_skipping_the_tiles_outside_the_set_changes_no_bit(kernels):
+    """The blocked fine kernels skip the 32 x 8 (64 x 8 paired) column tiles with no column of the set.
+    Against the same volume processing every tile: every field bit for bit, through steps, a set
+    change that empties tiles and one that refills them."""
+    nx, ny = 128, 64
+    vols = []
+    for skip in (0, 1):
+        d = Volume3.configure(nx, ny, NZ, DX, 1000.0, 9.81)
+        d.set_options(reduction=REDUCE_F64, kernels=kernels, no_tile_skip=skip)
+        d.set_free_surface(np.full(nx * ny, REST, np.float32), REST)
+        d.enable_multigrid()
+        d.enable_sparse()
+        vols.append(d)
+    masks = [scenes.rect_mask(nx, ny, [(0, 40, 0, 24), (70, 128, 30, 64)]),
+             scenes.rect_mask(nx, ny, [(0, 40, 0, 24), (70, 100, 30, 64)]),
+             scenes.rect_mask(nx, ny, [(0, 128, 0, 24), (70, 128, 30, 64)])]
+    first = True
+    for mask in masks:
+        for d in vols:
+            d.set_active_columns(mask)
+            if first:
+                d.set_free_surface(scenes.bumps_in(nx, ny, mask, [(20.0, 12.0), (90.0, 45.0)]), REST)
+        first = False
+        for s in range(8):
+            a, b = (d.step_surface_mobile(DT_US, 20_000) for d in vols)
+            assert a.iterations == b.iterations, s
+        for x, y, name in zip(fields(vols[0]), fields(vols[1]), NAMES):
+            assert_bits(x, y, name)
