@@ -466,6 +466,70 @@ def learned_fcg_measure(args, s, vol_plain_p, stream):
     }
 
 
+def parts_measure(args, s, stream):
+    """The other parts of the path on the same 128^3 scene, each timed with CUDA events on the
+    volume's stream after warm-up: a whole mobile step (advection, projection, extrapolation,
+    transport), the same with the second-order advection term, a re-cut of the moving solid, and a
+    level change of the flat-bottomed state to half the resolution."""
+    import numpy as np
+    import torch
+
+    from fluidisim_b200.delta3d import REDUCE_F64, Volume3
+
+    def timed(fn, n):
+        fn()
+        torch.cuda.synchronize()
+        total = 0.0
+        out = None
+        for _ in range(n):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            out = fn()
+            b.record(stream)
+            torch.cuda.synchronize()
+            total += a.elapsed_time(b)
+        return total / n, out
+
+    def volume(correction=False):
+        v = Volume3.configure_with_solid(s["nx"], s["ny"], s["nz"], s["dx"], s["rho"], s["g"], s["bottom"], s["solid"])
+        v.set_options(reduction=REDUCE_F64, use_graphs=args.graphs)
+        v.set_stream(stream.cuda_stream)
+        v.enable_multigrid()
+        v.set_free_surface(s["eta"], s["rest"])
+        v.set_velocity(s["u"], s["v"], s["w"])
+        if correction:
+            v.enable_advection_correction()
+        return v
+
+    out = {}
+    dt_us = int(round(s["dt"] * 1e6))
+    for key, corr in (("mobile_step", False), ("mobile_step_second_order", True)):
+        v = volume(corr)
+        its = []
+        ms, _ = timed(lambda: its.append(v.step_surface_mobile(dt_us, 4000).iterations), 10)
+        out[key] = {"ms": ms, "iterations_mean": float(np.mean(its)), "dt_us": dt_us}
+        v.close()
+    v = volume()
+    ms, _ = timed(lambda: v.set_solid_rigid(s["solid"], (0.1, 0.0, 0.0), (0.0, 0.0, 0.2),
+                                             (0.5 * s["nx"] * s["dx"], 0.5 * s["ny"] * s["dx"], 0.3 * s["nz"] * s["dx"])), 10)
+    out["set_solid_rigid"] = {"ms": ms, "note": "re-cut of the 16 boxes from the kept base, wall velocities, displaced water"}
+    v.close()
+    n = s["nx"]
+    fine = Volume3.configure(n, n, n, s["dx"], s["rho"], s["g"])
+    coarse = Volume3.configure(n // 2, n // 2, n // 2, float(np.float32(2 * s["dx"])), s["rho"], s["g"])
+    for x in (fine, coarse):
+        x.set_stream(stream.cuda_stream)
+    fine.set_free_surface(s["eta"], s["rest"])
+    coarse.set_free_surface(np.full((n // 2) ** 2, s["rest"], np.float32), s["rest"])
+    fine.set_velocity(s["u"], s["v"], s["w"])
+    ms, ch = timed(lambda: coarse.resample_from(fine), 10)
+    out["resample_from"] = {"ms": ms, "case": f"{n}^3 -> {n // 2}^3, flat bottom",
+                            "volume_error_m3": ch["volume_after"] - ch["volume_before"]}
+    fine.close()
+    coarse.close()
+    return out
+
+
 def run_b200(args):
     import numpy as np
     import torch
@@ -606,6 +670,7 @@ def run_b200(args):
         mixed_line, p16 = mixed_measure(args, s, stream, flush, plain_p.astype(np.float64), ms_per_step)
     if world == 1 and args.learned:
         learned_line = learned_fcg_measure(args, s, plain_p, stream)
+    parts_line = parts_measure(args, s, stream) if (world == 1 and args.parts) else None
 
     if rank == 0:
         cpu = cpu_baseline_sample(args.workload, args.size) if (world == 1 and not args.no_cpu) else None
@@ -635,6 +700,7 @@ def run_b200(args):
             "clocks": clocks.summary(),
             "learned_fcg": learned_line,
             "mixed_precision": mixed_line,
+            "parts": parts_line,
         }
         print(json.dumps(out), flush=True)
     vol.close()
@@ -907,6 +973,8 @@ def main():
     ap.add_argument("--learned", type=int, default=1,
                     help="1: also train the learned preconditioner and time learned-FCG projections (N=1 only)")
     ap.add_argument("--mixed", type=int, default=1, help="1: also time the FP16-storage V-cycle on the same scene")
+    ap.add_argument("--parts", type=int, default=1,
+                    help="1: also time a mobile step, the second-order advection, a solid re-cut and a level change")
     ap.add_argument("--train-samples", type=int, default=20000,
                     help="training samples of the learned preconditioner (20,000 at 64^3, as config 4 asks)")
     ap.add_argument("--graphs", type=int, default=1,
