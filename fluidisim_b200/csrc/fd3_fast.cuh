@@ -507,88 +507,173 @@ __device__ __forceinline__ float level_x1(const Lev& L, int n) {
   return dg > 0.f ? 0.f + OMEGA * (Store<T>::ld(as<T>(L.r), n) - 0.f) / dg : 0.f;
 }
 
+// The small coarse levels' passes are latency-bound: a pass is one dependent chain of loads per
+// thread.  There (SPEC) every load a cell may need is issued before its row code (and the loop's
+// gate) arrive: the
+// six neighbours' operands at indices clamped to the grid (a neighbour outside the grid has face
+// state 0 and its value is never used), then the gate is checked before anything is stored.  A
+// plain row sums the preloaded values with level_row_code's masked sum; any other row goes through
+// level_row_code itself.  The arithmetic, and so every bit, is that of level_row_code.
+struct Nb6 {
+  float xm, xp, ym, yp, zm, zp;
+};
+// P(n, i, j, k): the operand at cell n = (i, j, k).
+template <class P>
+__device__ __forceinline__ Nb6 level_nb(const Lev& L, int i, int j, int k, int c, const P& p) {
+  const int nxny = L.nx * L.ny;
+  const bool xl = i > 0, xr = i + 1 < L.nx, yl = j > 0, yr = j + 1 < L.ny, zl = k > 0, zr = k + 1 < L.nz;
+  Nb6 b;
+  b.xm = p(xl ? c - 1 : c, xl ? i - 1 : i, j, k);
+  b.xp = p(xr ? c + 1 : c, xr ? i + 1 : i, j, k);
+  b.ym = p(yl ? c - L.nx : c, i, yl ? j - 1 : j, k);
+  b.yp = p(yr ? c + L.nx : c, i, yr ? j + 1 : j, k);
+  b.zm = p(zl ? c - nxny : c, i, j, zl ? k - 1 : k);
+  b.zp = p(zr ? c + nxny : c, i, j, zr ? k + 1 : k);
+  return b;
+}
+// The row sum from preloaded neighbours (plain rows) or level_row_code with the operand source q.
+template <class Q>
+__device__ __forceinline__ float level_row_nb(const Lev& L, unsigned code, int i, int j, int k, int c, float pc,
+                                              const Nb6& b, const Q& q) {
+  if (!rc_plain(code)) return level_row_code(L, code, i, j, k, c, q);
+  float acc = 0.f;
+  acc += (code & (1u << 1)) ? pc - b.xm : 0.f;
+  acc += (code & (1u << 3)) ? pc - b.xp : 0.f;
+  acc += (code & (1u << 5)) ? pc - b.ym : 0.f;
+  acc += (code & (1u << 7)) ? pc - b.yp : 0.f;
+  acc += (code & (1u << 9)) ? pc - b.zm : 0.f;
+  acc += (code & (1u << 11)) ? pc - b.zp : 0.f;
+  return acc * L.inv;
+}
+__device__ __forceinline__ void level_ijk(const Lev& L, int c, int& i, int& j, int& k) {
+  i = c % L.nx;
+  const int t = c / L.nx;
+  j = t % L.ny;
+  k = t / L.ny;
+}
+
 // The two pre-sweeps of a coarse level from x = 0, written to L.x (smooth3 twice after fill(0)).
-template <class T>
+template <class T, bool SPEC>
 __global__ void __launch_bounds__(TPB) k_level_pre(Lev L, const Scalars* S, int gate) {
   KSTART();
-  if (gate && !S->active) return;
+  if (!SPEC && gate && !S->active) return;
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= L.n) return;
   auto X1 = [&](int n) { return level_x1<T>(L, n); };
-  float dg = L.diag[c];
+  auto X1c = [&](int n, int, int, int) { return level_x1<T>(L, n); };
+  int i, j, k;
+  level_ijk(L, c, i, j, k);
+  const unsigned code = L.code[c];
+  const float dg = L.diag[c];
+  const float rc = Store<T>::ld(as<T>(L.r), c);
   float xc = X1(c);
-  if (dg > 0.f) {
-    int i = c % L.nx, t = c / L.nx, j = t % L.ny, k = t / L.ny;
-    xc += OMEGA * (Store<T>::ld(as<T>(L.r), c) - level_row_code(L, L.code[c], i, j, k, c, X1)) / dg;
+  if (SPEC) {
+    const Nb6 b = level_nb(L, i, j, k, c, X1c);
+    if (gate && !S->active) return;
+    if (dg > 0.f) xc += OMEGA * (rc - level_row_nb(L, code, i, j, k, c, xc, b, X1)) / dg;
+  } else if (dg > 0.f) {
+    xc += OMEGA * (rc - level_row_code(L, code, i, j, k, c, X1)) / dg;
   }
   Store<T>::st(as<T>(L.x), c, xc);
 }
 
 // t = r - L x on every cell of a coarse level (0 on inactive rows), the restriction's operand.
-template <class T>
+template <class T, bool SPEC>
 __global__ void __launch_bounds__(TPB) k_level_resid(Lev L, const Scalars* S, int gate) {
   KSTART();
-  if (gate && !S->active) return;
+  if (!SPEC && gate && !S->active) return;
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= L.n) return;
-  unsigned code = L.code[c];
+  const LoadT<T> X{as<T>(L.x)};
+  auto Xc = [&](int n, int, int, int) { return X(n); };
+  int i, j, k;
+  level_ijk(L, c, i, j, k);
+  const unsigned code = L.code[c];
+  const float rc = Store<T>::ld(as<T>(L.r), c);
+  const float pc = X(c);
   float lx = 0.f;
-  if (code & RC_WET) {
-    int i = c % L.nx, t = c / L.nx, j = t % L.ny, k = t / L.ny;
-    lx = level_row_code(L, code, i, j, k, c, LoadT<T>{as<T>(L.x)});
+  if (SPEC) {
+    const Nb6 b = level_nb(L, i, j, k, c, Xc);
+    if (gate && !S->active) return;
+    if (code & RC_WET) lx = level_row_nb(L, code, i, j, k, c, pc, b, X);
+  } else if (code & RC_WET) {
+    lx = level_row_code(L, code, i, j, k, c, X);
   }
-  Store<T>::st(as<T>(L.t), c, Store<T>::ld(as<T>(L.r), c) - lx);
+  Store<T>::st(as<T>(L.t), c, rc - lx);
 }
 
 // C.r = mean of the 8 children of F.t, in the reference's CHILDREN order (restrict3).
 template <class T>
 __global__ void __launch_bounds__(TPB) k_level_sum8(Lev F, Lev C, const Scalars* S, int gate) {
   KSTART();
-  if (gate && !S->active) return;
   int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= C.n) return;
   int ci = q % C.nx, t = q / C.nx, cj = t % C.ny, ck = t / C.ny;
-  float s = 0.f;
+  float v[8];
 #pragma unroll
   for (int e = 0; e < 8; ++e) {
     int i = 2 * ci + (e & 1), j = 2 * cj + ((e >> 1) & 1), k = 2 * ck + (e >> 2);
-    s += Store<T>::ld(as<T>(F.t), (k * F.ny + j) * F.nx + i);
+    v[e] = Store<T>::ld(as<T>(F.t), (k * F.ny + j) * F.nx + i);
   }
+  if (gate && !S->active) return;
+  float s = 0.f;
+#pragma unroll
+  for (int e = 0; e < 8; ++e) s += v[e];
   Store<T>::st(as<T>(C.r), q, 0.125f * s);
 }
 
 // Prolongation from C (x += parent) fused with the first post-sweep, L.x -> L.x2.
-template <class T>
+template <class T, bool SPEC>
 __global__ void __launch_bounds__(TPB) k_level_post1(Lev L, Lev C, const Scalars* S, int gate) {
   KSTART();
-  if (gate && !S->active) return;
+  if (!SPEC && gate && !S->active) return;
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= L.n) return;
-  auto XP = [&](int n) {
-    int i = n % L.nx, t = n / L.nx, j = t % L.ny, k = t / L.ny;
+  auto XPc = [&](int n, int i, int j, int k) {
     return Store<T>::ld(as<T>(L.x), n) + Store<T>::ld(as<T>(C.x), ((k >> 1) * C.ny + (j >> 1)) * C.nx + (i >> 1));
   };
-  float dg = L.diag[c];
-  float xc = XP(c);
-  if (dg > 0.f) {
-    int i = c % L.nx, t = c / L.nx, j = t % L.ny, k = t / L.ny;
-    xc += OMEGA * (Store<T>::ld(as<T>(L.r), c) - level_row_code(L, L.code[c], i, j, k, c, XP)) / dg;
+  auto XP = [&](int n) {
+    int i, j, k;
+    level_ijk(L, n, i, j, k);
+    return XPc(n, i, j, k);
+  };
+  int i, j, k;
+  level_ijk(L, c, i, j, k);
+  const unsigned code = L.code[c];
+  const float dg = L.diag[c];
+  const float rc = Store<T>::ld(as<T>(L.r), c);
+  float xc = XPc(c, i, j, k);
+  if (SPEC) {
+    const Nb6 b = level_nb(L, i, j, k, c, XPc);
+    if (gate && !S->active) return;
+    if (dg > 0.f) xc += OMEGA * (rc - level_row_nb(L, code, i, j, k, c, xc, b, XP)) / dg;
+  } else if (dg > 0.f) {
+    xc += OMEGA * (rc - level_row_code(L, code, i, j, k, c, XP)) / dg;
   }
   Store<T>::st(as<T>(L.x2), c, xc);
 }
 
 // The second post-sweep, L.x2 -> L.x.
-template <class T>
+template <class T, bool SPEC>
 __global__ void __launch_bounds__(TPB) k_level_post2(Lev L, const Scalars* S, int gate) {
   KSTART();
-  if (gate && !S->active) return;
+  if (!SPEC && gate && !S->active) return;
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= L.n) return;
-  float dg = L.diag[c];
-  float xc = Store<T>::ld(as<T>(L.x2), c);
-  if (dg > 0.f) {
-    int i = c % L.nx, t = c / L.nx, j = t % L.ny, k = t / L.ny;
-    xc += OMEGA * (Store<T>::ld(as<T>(L.r), c) - level_row_code(L, L.code[c], i, j, k, c, LoadT<T>{as<T>(L.x2)})) / dg;
+  const LoadT<T> X{as<T>(L.x2)};
+  auto Xc = [&](int n, int, int, int) { return X(n); };
+  int i, j, k;
+  level_ijk(L, c, i, j, k);
+  const unsigned code = L.code[c];
+  const float dg = L.diag[c];
+  const float rc = Store<T>::ld(as<T>(L.r), c);
+  float xc = X(c);
+  if (SPEC) {
+    const Nb6 b = level_nb(L, i, j, k, c, Xc);
+    if (gate && !S->active) return;
+    if (dg > 0.f) xc += OMEGA * (rc - level_row_nb(L, code, i, j, k, c, xc, b, X)) / dg;
+  } else if (dg > 0.f) {
+    xc += OMEGA * (rc - level_row_code(L, code, i, j, k, c, X)) / dg;
   }
   Store<T>::st(as<T>(L.x), c, xc);
 }

@@ -55,6 +55,14 @@ int cuda_fail(cudaError_t e, const char* what, int line) {
 
 inline int blocks_for(long long n) { return (int)((n + TPB - 1) / TPB); }
 
+// Coarse levels of at most this many cells issue their passes' loads before the row code and the
+// gate (the latency-bound levels: measured 2% faster at 128^3, 1% slower on the 128^3 level of a
+// 256^3 volume, which is throughput-bound).
+#ifndef FD3_SPEC_MAX
+#define FD3_SPEC_MAX 262144
+#endif
+constexpr int SPEC_MAX_CELLS = FD3_SPEC_MAX;
+
 // Coarse levels of at most this many cells are solved together by one CTA (k_coarse_tail).
 constexpr int TAIL_MAX_CELLS = 512;
 
@@ -320,8 +328,13 @@ void coarse_cycle_t(fd3_volume* V, int gate) {
         LAUNCH(V, k_level_sweep_c<T>, L.n, L, (const float*)((s % 2 == 0) ? L.x : L.x2), (s % 2 == 0) ? L.x2 : L.x,
                s == 0 ? 1 : 0, S, gate);
     } else {
-      LAUNCH(V, k_level_pre<T>, L.n, L, S, gate);
-      LAUNCH(V, k_level_resid<T>, L.n, L, S, gate);
+      if (L.n <= SPEC_MAX_CELLS) {
+        launch_grid(V, "k_level_pre", blocks_for(L.n), TPB, k_level_pre<T, true>, L, S, gate);
+        launch_grid(V, "k_level_resid", blocks_for(L.n), TPB, k_level_resid<T, true>, L, S, gate);
+      } else {
+        launch_grid(V, "k_level_pre", blocks_for(L.n), TPB, k_level_pre<T, false>, L, S, gate);
+        launch_grid(V, "k_level_resid", blocks_for(L.n), TPB, k_level_resid<T, false>, L, S, gate);
+      }
       LAUNCH(V, k_level_sum8<T>, Ls[l + 1].n, L, Ls[l + 1], S, gate);
     }
   }
@@ -335,8 +348,13 @@ void coarse_cycle_t(fd3_volume* V, int gate) {
       LAUNCH_G(V, k_coarse_tail, 1, TAIL_THREADS, (const Lev*)V->dlev, first_tail, last, S, gate);
   }
   for (int l = std::min(first_tail, last) - 1; l >= 0; --l) {
-    LAUNCH(V, k_level_post1<T>, Ls[l].n, Ls[l], Ls[l + 1], S, gate);
-    LAUNCH(V, k_level_post2<T>, Ls[l].n, Ls[l], S, gate);
+    if (Ls[l].n <= SPEC_MAX_CELLS) {
+      launch_grid(V, "k_level_post1", blocks_for(Ls[l].n), TPB, k_level_post1<T, true>, Ls[l], Ls[l + 1], S, gate);
+      launch_grid(V, "k_level_post2", blocks_for(Ls[l].n), TPB, k_level_post2<T, true>, Ls[l], S, gate);
+    } else {
+      launch_grid(V, "k_level_post1", blocks_for(Ls[l].n), TPB, k_level_post1<T, false>, Ls[l], Ls[l + 1], S, gate);
+      launch_grid(V, "k_level_post2", blocks_for(Ls[l].n), TPB, k_level_post2<T, false>, Ls[l], S, gate);
+    }
   }
 }
 void coarse_cycle(fd3_volume* V, int gate) {
