@@ -752,6 +752,7 @@ def run_patches(args):
     torch.cuda.synchronize()
     barrier(world)
     ms = []
+    launches0 = sum(v.kernel_launches() for v in vols)
     with ClockSampler(local) as clocks:
         clocks.mark(True)
         for _ in range(args.steps):
@@ -762,6 +763,7 @@ def run_patches(args):
             torch.cuda.synchronize()
             ms.append(a.elapsed_time(b))
         clocks.mark(False)
+    launches = sum(v.kernel_launches() for v in vols) - launches0
     assert all(x == 0 for x in st), st
     ms_total = max_over_ranks(sum(ms), world)
     my_ci = sum(p["nx"] * p["ny"] * p["nz"] * r.iterations for p, r in zip(mine, reps))
@@ -790,6 +792,7 @@ def run_patches(args):
                        "iterations_rank0": {"min": min(its), "max": max(its), "mean": float(np.mean(its))},
                        "l2": "inputs restored each step; the patch set exceeds L2"},
             "cells_iterations_per_s": args.steps * ci / (ms_total * 1e-3),
+            "gpu_launches": launches,
             "cpu_baseline": cpu,
             "clocks": clocks.summary(),
         }
