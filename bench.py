@@ -65,7 +65,6 @@ BYTES_PER_CELL = {
     # set-up and checks, once per projection
     "k_residual_c": 2 + 4 * 3,                 # code, p, rhs, res
     "k_rhs_b2": 4 * 3 + GEOM + 2,              # rhs read+write, prec, geometry, row code
-    "k_row_codes": GEOM + 2,
     "k_divergence": 4 * 3 + 4 + GEOM,          # three face families in, rhs out
 }
 

@@ -38,18 +38,6 @@ __device__ __forceinline__ unsigned row_code_of(const RowE (&row)[6]) {
   return code;
 }
 
-__global__ void k_row_codes(Geo g, unsigned short* __restrict__ codes) {
-  KSTART();
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= g.n) return;
-  int i, j, k; cell_ijk(g, c, i, j, k);
-  unsigned code = 0;
-  if (wet3(g, i, j, k)) {
-    RowE row[6]; mobile_row(g, i, j, k, row);
-    code = row_code_of(row);
-  }
-  codes[c] = (unsigned short)code;
-}
 
 // 1/max(theta, 1e-3) of ghost_side3 and ghost_up3 (delta3d_mobile.rs:126-147).
 __device__ __forceinline__ float ghost_it_side(const Geo& g, int i, int j, int k, int x, int y) {
@@ -990,8 +978,8 @@ __global__ void k_loop_cond(cudaGraphConditionalHandle handle, Scalars* S) {
 // Set-up reductions with the in-kernel finish.
 
 // rhs_mobile3 (delta3d_mobile.rs:215-241) with b.b (FIN_B2) when `reduce`.
-// With `codes` not null, the same pass also writes each cell's row code (k_row_codes, from the
-// same row).
+// With `codes` not null, the same pass also writes each cell's row code (row_code_of the same
+// row; 0 for a dry cell).
 template <int MODE>
 __global__ void __launch_bounds__(TPB) k_rhs_b2(Geo g, float scale, float* __restrict__ rhs, float* __restrict__ prec,
                                                 Red red, Scalars* S, int reduce, unsigned short* __restrict__ codes) {
