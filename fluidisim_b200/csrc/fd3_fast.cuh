@@ -610,6 +610,47 @@ __global__ void __launch_bounds__(TPB) k_level_sum8(Lev F, Lev C, const Scalars*
   Store<T>::st(as<T>(C.r), q, 0.125f * s);
 }
 
+// k_level_resid and k_level_sum8 in one pass, with one thread per fine cell as k_level_resid has:
+// the eight threads of a coarse cell (consecutive lanes, child e = lane % 8 in the reference's
+// CHILDREN order) each evaluate one child's t = r - L x, rounded through the storage type as the
+// stored t would be, and the first of them sums the eight in order (restrict3).
+template <class T, bool SPEC>
+__global__ void __launch_bounds__(TPB) k_level_restrict8(Lev F, Lev C, const Scalars* S, int gate) {
+  KSTART();
+  if (!SPEC && gate && !S->active) return;
+  const int q8 = blockIdx.x * blockDim.x + threadIdx.x;
+  const int q = q8 >> 3, e = q8 & 7;
+  const bool own = q < C.n;
+  float tv = 0.f;
+  unsigned code = 0u;
+  int i = 0, j = 0, k = 0, c = 0;
+  float rc = 0.f, pc = 0.f;
+  const LoadT<T> X{as<T>(F.x)};
+  if (own) {
+    const int ci = q % C.nx, t = q / C.nx, cj = t % C.ny, ck = t / C.ny;
+    i = 2 * ci + (e & 1);
+    j = 2 * cj + ((e >> 1) & 1);
+    k = 2 * ck + (e >> 2);
+    c = (k * F.ny + j) * F.nx + i;
+    code = F.code[c];
+    rc = Store<T>::ld(as<T>(F.r), c);
+    pc = X(c);
+  }
+  if (SPEC) {
+    Nb6 b{};
+    if (own) b = level_nb(F, i, j, k, c, [&](int n, int, int, int) { return X(n); });
+    if (gate && !S->active) return;
+    if (own) tv = Store<T>::rt(rc - ((code & RC_WET) ? level_row_nb(F, code, i, j, k, c, pc, b, X) : 0.f));
+  } else if (own) {
+    tv = Store<T>::rt(rc - ((code & RC_WET) ? level_row_code(F, code, i, j, k, c, X) : 0.f));
+  }
+  const int lane0 = threadIdx.x & 24;  // first lane of the eight
+  float sum = 0.f;
+#pragma unroll
+  for (int a = 0; a < 8; ++a) sum += __shfl_sync(0xffffffffu, tv, lane0 + a);
+  if (own && e == 0) Store<T>::st(as<T>(C.r), q, 0.125f * sum);
+}
+
 // Prolongation from C (x += parent) fused with the first post-sweep, L.x -> L.x2.
 template <class T, bool SPEC>
 __global__ void __launch_bounds__(TPB) k_level_post1(Lev L, Lev C, const Scalars* S, int gate) {

@@ -56,8 +56,9 @@ int cuda_fail(cudaError_t e, const char* what, int line) {
 inline int blocks_for(long long n) { return (int)((n + TPB - 1) / TPB); }
 
 // Coarse levels of at most this many cells issue their passes' loads before the row code and the
-// gate (the latency-bound levels: measured 2% faster at 128^3, 1% slower on the 128^3 level of a
-// 256^3 volume, which is throughput-bound).
+// gate, and restrict their residual in the same pass that computes it (k_level_restrict8).  These
+// are the latency-bound levels: measured 2% and 1.4% faster at 128^3; the loads ahead of the code
+// were 1% slower on the throughput-bound 128^3 level of a 256^3 volume.
 #ifndef FD3_SPEC_MAX
 #define FD3_SPEC_MAX 262144
 #endif
@@ -328,14 +329,15 @@ void coarse_cycle_t(fd3_volume* V, int gate) {
         LAUNCH(V, k_level_sweep_c<T>, L.n, L, (const float*)((s % 2 == 0) ? L.x : L.x2), (s % 2 == 0) ? L.x2 : L.x,
                s == 0 ? 1 : 0, S, gate);
     } else {
+      const long long n8 = 8LL * Ls[l + 1].n;  // one thread per child of each next-level cell
       if (L.n <= SPEC_MAX_CELLS) {
         launch_grid(V, "k_level_pre", blocks_for(L.n), TPB, k_level_pre<T, true>, L, S, gate);
-        launch_grid(V, "k_level_resid", blocks_for(L.n), TPB, k_level_resid<T, true>, L, S, gate);
+        launch_grid(V, "k_level_restrict8", blocks_for(n8), TPB, k_level_restrict8<T, true>, L, Ls[l + 1], S, gate);
       } else {
         launch_grid(V, "k_level_pre", blocks_for(L.n), TPB, k_level_pre<T, false>, L, S, gate);
         launch_grid(V, "k_level_resid", blocks_for(L.n), TPB, k_level_resid<T, false>, L, S, gate);
+        LAUNCH(V, k_level_sum8<T>, Ls[l + 1].n, L, Ls[l + 1], S, gate);
       }
-      LAUNCH(V, k_level_sum8<T>, Ls[l + 1].n, L, Ls[l + 1], S, gate);
     }
   }
   if (first_tail <= last) {
