@@ -868,20 +868,20 @@ __device__ __forceinline__ TailRow tail_row(const Lev& L, int c) {
 #pragma unroll
   for (int f = 0; f < 6; ++f) w.a[f] = 0.f;
   if (c >= L.n) return w;
-  w.code = L.code[c];
-  w.diag = L.diag[c];
+  // the six apertures are loaded with the code, not after it: every face index of a cell is valid
   const int i = c % L.nx, t = c / L.nx, j = t % L.ny, k = t / L.ny;
-  const bool unit = w.code & RC_UNIT;
   const int fi[6] = {(k * L.ny + j) * (L.nx + 1) + i, (k * L.ny + j) * (L.nx + 1) + i + 1,
                      (k * (L.ny + 1) + j) * L.nx + i, (k * (L.ny + 1) + j + 1) * L.nx + i,
                      (k * L.ny + j) * L.nx + i, ((k + 1) * L.ny + j) * L.nx + i};
+  float ap[6];
 #pragma unroll
-  for (int f = 0; f < 6; ++f) {
-    if (face_state(w.code, f)) {
-      const float* ap = f < 2 ? L.ou : (f < 4 ? L.ov : L.ow);
-      w.a[f] = unit ? 1.f : ap[fi[f]];
-    }
-  }
+  for (int f = 0; f < 6; ++f) ap[f] = (f < 2 ? L.ou : (f < 4 ? L.ov : L.ow))[fi[f]];
+  w.code = L.code[c];
+  w.diag = L.diag[c];
+  const bool unit = w.code & RC_UNIT;
+#pragma unroll
+  for (int f = 0; f < 6; ++f)
+    if (face_state(w.code, f)) w.a[f] = unit ? 1.f : ap[f];
   return w;
 }
 
@@ -900,28 +900,32 @@ __device__ __forceinline__ float tail_rowsum(const TailRow& w, int c, int nx, in
   return acc * inv;
 }
 
+// The tail's levels, passed by value: the kernel reads them from its parameters, not memory.
+struct TailLevs {
+  Lev L[TAIL_REG_LEVELS];
+};
+
 template <class ST>
-__global__ void __launch_bounds__(TAIL_REG_THREADS) k_coarse_tail_reg(const Lev* __restrict__ T, int first, int last,
-                                                                     const Scalars* S, int gate) {
+__global__ void __launch_bounds__(TAIL_REG_THREADS) k_coarse_tail_reg(const TailLevs Ls_, int nl, const Scalars* S,
+                                                                     int gate) {
   KSTART();
-  if (gate && !S->active) return;
   // per level: XA, XB (sweep ping-pong), XF (final x of the level), R (right-hand side)
   __shared__ float XA[TAIL_REG_LEVELS][TAIL_REG_THREADS];
   __shared__ float XB[TAIL_REG_LEVELS][TAIL_REG_THREADS];
   __shared__ float XF[TAIL_REG_LEVELS][TAIL_REG_THREADS];
   __shared__ float R[TAIL_REG_LEVELS][TAIL_REG_THREADS];
-  __shared__ Lev Ls[TAIL_REG_LEVELS];
+  const Lev (&Ls)[TAIL_REG_LEVELS] = Ls_.L;
   const int c = threadIdx.x;
-  const int nl = last - first + 1;
-  if (c < nl) Ls[c] = T[first + c];
-  __syncthreads();
-  // every row of every level, and the right-hand side of the first, in one round of loads
+  // every row of every level, and the right-hand side of the first, in one round of loads issued
+  // before the loop's gate is read (the gate is checked before anything is written to memory)
   TailRow w[TAIL_REG_LEVELS];
 #pragma unroll
   for (int l = 0; l < TAIL_REG_LEVELS; ++l) {
     if (l < nl) w[l] = tail_row(Ls[l], c);
   }
-  if (c < Ls[0].n) R[0][c] = Store<ST>::ld(as<ST>(Ls[0].r), c);
+  const float r0 = c < Ls[0].n ? Store<ST>::ld(as<ST>(Ls[0].r), c) : 0.f;
+  if (gate && !S->active) return;
+  if (c < Ls[0].n) R[0][c] = r0;
   __syncthreads();
   // descent
 #pragma unroll

@@ -341,8 +341,11 @@ void coarse_cycle_t(fd3_volume* V, int gate) {
     }
   }
   if (first_tail <= last) {
-    if (V->tail_reg)
-      LAUNCH_G(V, k_coarse_tail_reg<T>, 1, TAIL_REG_THREADS, (const Lev*)V->dlev, first_tail, last, S, gate);
+    if (V->tail_reg) {
+      TailLevs tl{};
+      for (int l = first_tail; l <= last; ++l) tl.L[l - first_tail] = Ls[l];
+      LAUNCH_G(V, k_coarse_tail_reg<T>, 1, TAIL_REG_THREADS, tl, last - first_tail + 1, S, gate);
+    }
     else if (V->tail_smem_bytes > 0)
       launch_grid_smem(V, "k_coarse_tail_smem", 1, TAIL_THREADS, V->tail_smem_bytes, k_coarse_tail_smem,
                        (const Lev*)V->dlev, first_tail, last, S, gate);
