@@ -707,6 +707,79 @@ __global__ void __launch_bounds__(TPB) k_level_post2(Lev L, const Scalars* S, in
   Store<T>::st(as<T>(L.x), c, xc);
 }
 
+// k_level_post2 of the coarser level C fused into k_level_post1 of L: the eight threads of a C
+// cell (consecutive lanes, child e = lane % 8) are its eight children in L.  Lanes 0..6 evaluate
+// C's second post-sweep at the cell and at its six neighbours (the parents of the children's
+// stencil points), with k_level_post2's expression, rounded through the storage type as the stored
+// C.x would be; the warp shares the seven values; each child then sweeps its own row with
+// k_level_post1's expression.  C.x is never stored: only this pass would read it.
+template <class T>
+__global__ void __launch_bounds__(TPB) k_level_post21(Lev L, Lev C, const Scalars* S, int gate) {
+  KSTART();
+  const int q8 = blockIdx.x * blockDim.x + threadIdx.x;
+  const int q = q8 >> 3, e = q8 & 7;
+  const bool own = q < C.n;
+  const int ci = own ? q % C.nx : 0, cj = own ? (q / C.nx) % C.ny : 0, ck = own ? q / (C.nx * C.ny) : 0;
+  // the C cell this lane sweeps: 0 the parent, 1..6 its x-, x+, y-, y+, z-, z+ neighbours
+  int pi = ci, pj = cj, pk = ck;
+  if (e == 1) pi -= 1; else if (e == 2) pi += 1; else if (e == 3) pj -= 1;
+  else if (e == 4) pj += 1; else if (e == 5) pk -= 1; else if (e == 6) pk += 1;
+  const bool psweep = own && e < 7 && pi >= 0 && pi < C.nx && pj >= 0 && pj < C.ny && pk >= 0 && pk < C.nz;
+  const LoadT<T> X2{as<T>(C.x2)};
+  unsigned pcode = 0u;
+  float pdg = 0.f, pr = 0.f, px2 = 0.f;
+  Nb6 pb{};
+  int pc = 0;
+  if (psweep) {
+    pc = (pk * C.ny + pj) * C.nx + pi;
+    pcode = C.code[pc];
+    pdg = C.diag[pc];
+    pr = Store<T>::ld(as<T>(C.r), pc);
+    px2 = X2(pc);
+    pb = level_nb(C, pi, pj, pk, pc, [&](int n, int, int, int) { return X2(n); });
+  }
+  // the child's own row
+  const int i = 2 * ci + (e & 1), j = 2 * cj + ((e >> 1) & 1), k = 2 * ck + (e >> 2);
+  const int c = (k * L.ny + j) * L.nx + i;
+  const LoadT<T> X{as<T>(L.x)};
+  unsigned code = 0u;
+  float dg = 0.f, rc = 0.f, xc0 = 0.f;
+  Nb6 b{};
+  if (own) {
+    code = L.code[c];
+    dg = L.diag[c];
+    rc = Store<T>::ld(as<T>(L.r), c);
+    xc0 = X(c);
+    b = level_nb(L, i, j, k, c, [&](int n, int, int, int) { return X(n); });
+  }
+  if (gate && !S->active) return;
+  float xp = px2;  // C's final x at the lane's cell (k_level_post2)
+  if (psweep && pdg > 0.f) xp += OMEGA * (pr - level_row_nb(C, pcode, pi, pj, pk, pc, px2, pb, X2)) / pdg;
+  xp = Store<T>::rt(xp);
+  const int lane0 = threadIdx.x & 24;
+  float par[7];
+#pragma unroll
+  for (int a = 0; a < 7; ++a) par[a] = __shfl_sync(0xffffffffu, xp, lane0 + a);
+  if (!own) return;
+  // x + the parent's x at the child and its six neighbours (a neighbour across the parent's face
+  // has the parent's neighbour as its parent)
+  const float own_p = par[0];
+  const float pxm = (e & 1) ? own_p : par[1], pxp = (e & 1) ? par[2] : own_p;
+  const float pym = ((e >> 1) & 1) ? own_p : par[3], pyp = ((e >> 1) & 1) ? par[4] : own_p;
+  const float pzm = (e >> 2) ? own_p : par[5], pzp = (e >> 2) ? par[6] : own_p;
+  const float xc = xc0 + own_p;
+  Nb6 v;
+  v.xm = b.xm + pxm; v.xp = b.xp + pxp; v.ym = b.ym + pym; v.yp = b.yp + pyp; v.zm = b.zm + pzm; v.zp = b.zp + pzp;
+  const int nxny = L.nx * L.ny;
+  auto XP = [&](int n) {
+    return n == c ? xc : n == c - 1 ? v.xm : n == c + 1 ? v.xp : n == c - L.nx ? v.ym : n == c + L.nx ? v.yp
+         : n == c - nxny ? v.zm : v.zp;
+  };
+  float out = xc;
+  if (dg > 0.f) out += OMEGA * (rc - level_row_nb(L, code, i, j, k, c, xc, v, XP)) / dg;
+  Store<T>::st(as<T>(L.x2), c, out);
+}
+
 // One damped Jacobi sweep from codes (a large coarsest level's 8 sweeps); zero_in: from x = 0.
 template <class T>
 __global__ void __launch_bounds__(TPB) k_level_sweep_c(Lev L, const float* __restrict__ xin_, float* __restrict__ xout_,

@@ -352,10 +352,19 @@ void coarse_cycle_t(fd3_volume* V, int gate) {
     else
       LAUNCH_G(V, k_coarse_tail, 1, TAIL_THREADS, (const Lev*)V->dlev, first_tail, last, S, gate);
   }
-  for (int l = std::min(first_tail, last) - 1; l >= 0; --l) {
+  // Level l's second post-sweep is folded into level l - 1's first (k_level_post21) when both are
+  // small, level l is no tail level, and level l - 1 exists.
+  const int top = std::min(first_tail, last) - 1;
+  auto fused = [&](int l) { return l >= 0 && l + 1 <= top && Ls[l].n <= SPEC_MAX_CELLS; };
+  for (int l = top; l >= 0; --l) {
     if (Ls[l].n <= SPEC_MAX_CELLS) {
-      launch_grid(V, "k_level_post1", blocks_for(Ls[l].n), TPB, k_level_post1<T, true>, Ls[l], Ls[l + 1], S, gate);
-      launch_grid(V, "k_level_post2", blocks_for(Ls[l].n), TPB, k_level_post2<T, true>, Ls[l], S, gate);
+      if (fused(l))
+        launch_grid(V, "k_level_post21", blocks_for(8LL * Ls[l + 1].n), TPB, k_level_post21<T>, Ls[l], Ls[l + 1], S,
+                    gate);
+      else
+        launch_grid(V, "k_level_post1", blocks_for(Ls[l].n), TPB, k_level_post1<T, true>, Ls[l], Ls[l + 1], S, gate);
+      if (!fused(l - 1))
+        launch_grid(V, "k_level_post2", blocks_for(Ls[l].n), TPB, k_level_post2<T, true>, Ls[l], S, gate);
     } else {
       launch_grid(V, "k_level_post1", blocks_for(Ls[l].n), TPB, k_level_post1<T, false>, Ls[l], Ls[l + 1], S, gate);
       launch_grid(V, "k_level_post2", blocks_for(Ls[l].n), TPB, k_level_post2<T, false>, Ls[l], S, gate);
