@@ -126,6 +126,86 @@ struct LoadT {
 };
 
 // ------------------------------------------------------------------------------------------------
+// The outer loop's metrics from the projection's row codes (the surface is the one the codes were
+// built for), instead of rebuilding each row from the geometry.
+
+// divergence_mobile3 (delta3d_mobile.rs:398-433): max |div u| over the wet rows and over the
+// plain ones (no surface ghost: no face state 2), into S->fmax[0] and [1].
+__global__ void k_div_metric_c(Geo g, const unsigned short* __restrict__ codes, const float* __restrict__ u,
+                               const float* __restrict__ v, const float* __restrict__ w, Scalars* S) {
+  KSTART();
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  float all = 0.f, plain = 0.f;
+  if (c < g.n) {
+    const unsigned code = codes[c];
+    if (code & RC_WET) {
+      int i, j, k; cell_ijk(g, c, i, j, k);
+      float dv;
+      if (g.cut) {
+        float fl = __ldg(g.ou + fu(g, i, j, k)) * u[fu(g, i, j, k)];
+        float fr = __ldg(g.ou + fu(g, i + 1, j, k)) * u[fu(g, i + 1, j, k)];
+        float ff = __ldg(g.ov + fv(g, i, j, k)) * v[fv(g, i, j, k)];
+        float fk = __ldg(g.ov + fv(g, i, j + 1, k)) * v[fv(g, i, j + 1, k)];
+        float fb = __ldg(g.ow + fw(g, i, j, k)) * w[fw(g, i, j, k)];
+        float ft = __ldg(g.ow + fw(g, i, j, k + 1)) * w[fw(g, i, j, k + 1)];
+        dv = ((fr - fl + ft - fb) + (fk - ff)) / g.dx;
+      } else {
+        float fl = u[fu(g, i, j, k)], fr = u[fu(g, i + 1, j, k)];
+        float ff = v[fv(g, i, j, k)], fk = v[fv(g, i, j + 1, k)];
+        float fb = w[fw(g, i, j, k)], ft = w[fw(g, i, j, k + 1)];
+        dv = ((fr - fl + ft - fb) + (fk - ff)) / g.dx;
+      }
+      const float d = fabsf(dv);
+      all = d;
+      if (!(code & RC_GHOSTS)) plain = d;
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    all = fmaxf(all, __shfl_down_sync(0xffffffffu, all, o));
+    plain = fmaxf(plain, __shfl_down_sync(0xffffffffu, plain, o));
+  }
+  if ((threadIdx.x & 31) == 0) { atomic_fmax_nonneg(&S->fmax[0], all); atomic_fmax_nonneg(&S->fmax[1], plain); }
+}
+
+// backward_error_mobile3 (delta3d_mobile.rs:243-271): max |r_i| / (|b| + |A||p|)_i over the wet
+// rows into S->fmax[3].  A row's apertures and ghost coefficients are the ones apply_code uses.
+__global__ void k_backward_error_c(Geo g, const unsigned short* __restrict__ codes, const float* __restrict__ p,
+                                   const float* __restrict__ rhs, const float* __restrict__ res, Scalars* S) {
+  KSTART();
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  float worst = 0.f;
+  if (c < g.n) {
+    const unsigned code = codes[c];
+    if (code & RC_WET) {
+      int i, j, k; cell_ijk(g, c, i, j, k);
+      const int nxny = g.nx * g.ny;
+      const bool unit = code & RC_UNIT;
+      const float pc = fabsf(p[c]);
+      float acc = 0.f;
+      auto face = [&](int f, int axis, int fi, int m, int x, int y) {
+        const unsigned st = face_state(code, f);
+        if (!st) return;
+        const float a = unit ? 1.f : aper3(g, axis, fi);
+        if (st == 1) acc += a * (pc + fabsf(p[m]));
+        else acc += a * pc * (f == 5 ? ghost_it_up(g, i, j, k) : ghost_it_side(g, i, j, k, x, y));
+      };
+      face(0, 0, fu(g, i, j, k), c - 1, i - 1, j);
+      face(1, 0, fu(g, i + 1, j, k), c + 1, i + 1, j);
+      face(2, 1, fv(g, i, j, k), c - g.nx, i, j - 1);
+      face(3, 1, fv(g, i, j + 1, k), c + g.nx, i, j + 1);
+      face(4, 2, fw(g, i, j, k), c - nxny, i, j);
+      face(5, 2, fw(g, i, j, k + 1), c + nxny, i, j);
+      const float scale = fabsf(rhs[c]) + acc * g.inv;
+      if (scale > 0.f) worst = fabsf(res[c]) / scale;
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) worst = fmaxf(worst, __shfl_down_sync(0xffffffffu, worst, o));
+  if ((threadIdx.x & 31) == 0) atomic_fmax_nonneg(&S->fmax[3], worst);
+}
+
+// ------------------------------------------------------------------------------------------------
 // Reductions finished in the kernel that produces them: each block leaves its partial(s), the last
 // block to arrive (a counter) merges them in a fixed order and applies the PCG scalar step.
 

@@ -612,49 +612,6 @@ __device__ __forceinline__ void atomic_fmax_nonneg(float* addr, float v) {
   atomicMax(reinterpret_cast<int*>(addr), __float_as_int(v));
 }
 
-// divergence_mobile3 (delta3d_mobile.rs:398-433): max |div u| over wet rows (all) and over rows
-// without a surface ghost (plain).  S->fmax[0] = all, [1] = plain.
-__global__ void k_div_metric(Geo g, const float* __restrict__ u, const float* __restrict__ v,
-                             const float* __restrict__ w, Scalars* S) {
-  KSTART();
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
-  float all = 0.f, plain = 0.f;
-  if (c < g.n) {
-    int i, j, k; cell_ijk(g, c, i, j, k);
-    if (wet3(g, i, j, k)) {
-      float dv;
-      if (g.cut) {
-        float fl = __ldg(g.ou + fu(g, i, j, k)) * u[fu(g, i, j, k)];
-        float fr = __ldg(g.ou + fu(g, i + 1, j, k)) * u[fu(g, i + 1, j, k)];
-        float ff = __ldg(g.ov + fv(g, i, j, k)) * v[fv(g, i, j, k)];
-        float fk = __ldg(g.ov + fv(g, i, j + 1, k)) * v[fv(g, i, j + 1, k)];
-        float fb = __ldg(g.ow + fw(g, i, j, k)) * w[fw(g, i, j, k)];
-        float ft = __ldg(g.ow + fw(g, i, j, k + 1)) * w[fw(g, i, j, k + 1)];
-        dv = ((fr - fl + ft - fb) + (fk - ff)) / g.dx;
-      } else {
-        float fl = u[fu(g, i, j, k)], fr = u[fu(g, i + 1, j, k)];
-        float ff = v[fv(g, i, j, k)], fk = v[fv(g, i, j + 1, k)];
-        float fb = w[fw(g, i, j, k)], ft = w[fw(g, i, j, k + 1)];
-        dv = ((fr - fl + ft - fb) + (fk - ff)) / g.dx;
-      }
-      float d = fabsf(dv);
-      all = d;
-      RowE row[6]; mobile_row(g, i, j, k, row);
-      bool ghost = false;
-#pragma unroll
-      for (int f = 0; f < 6; ++f) ghost = ghost || (row[f].n < 0 && row[f].a > 0.f);
-      if (!ghost) plain = d;
-    }
-  }
-  // warp max then one atomic per warp
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    all = fmaxf(all, __shfl_down_sync(0xffffffffu, all, o));
-    plain = fmaxf(plain, __shfl_down_sync(0xffffffffu, plain, o));
-  }
-  if ((threadIdx.x & 31) == 0) { atomic_fmax_nonneg(&S->fmax[0], all); atomic_fmax_nonneg(&S->fmax[1], plain); }
-}
-
 // max |x| over an array into S->fmax[slot].
 __global__ void k_maxabs(int n, const float* __restrict__ x, Scalars* S, int slot) {
   KSTART();
@@ -663,32 +620,6 @@ __global__ void k_maxabs(int n, const float* __restrict__ x, Scalars* S, int slo
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_down_sync(0xffffffffu, m, o));
   if ((threadIdx.x & 31) == 0) atomic_fmax_nonneg(&S->fmax[slot], m);
-}
-
-// backward_error_mobile3 (delta3d_mobile.rs:243-271) into S->fmax[3].
-__global__ void k_backward_error(Geo g, const float* __restrict__ p, const float* __restrict__ rhs,
-                                 const float* __restrict__ res, Scalars* S) {
-  KSTART();
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
-  float worst = 0.f;
-  if (c < g.n) {
-    int i, j, k; cell_ijk(g, c, i, j, k);
-    if (wet3(g, i, j, k)) {
-      RowE row[6]; mobile_row(g, i, j, k, row);
-      float pc = fabsf(p[c]);
-      float acc = 0.f;
-#pragma unroll
-      for (int f = 0; f < 6; ++f) {
-        if (row[f].n >= 0) acc += row[f].a * (pc + fabsf(p[row[f].n]));
-        else if (row[f].a > 0.f) acc += row[f].a * pc * row[f].it;
-      }
-      float scale = fabsf(rhs[c]) + acc * g.inv;
-      if (scale > 0.f) worst = fabsf(res[c]) / scale;
-    }
-  }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) worst = fmaxf(worst, __shfl_down_sync(0xffffffffu, worst, o));
-  if ((threadIdx.x & 31) == 0) atomic_fmax_nonneg(&S->fmax[3], worst);
 }
 
 // Fingerprint of the exact bits of p for cycle detection (the role of fingerprint,
