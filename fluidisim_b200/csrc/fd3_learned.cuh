@@ -737,8 +737,7 @@ int fd3_project_learned(fd3_volume* V, fd3_unet* N, float scale, float k1, uint3
   TRY(assemble_device(V, scale));
   Geo G = V->geo();
   LAUNCH(V, k_zero_dry, V->n, G, V->p);
-  DISPATCH(V, k_residual_c, V->n, G, (const unsigned short*)V->codes, (const float*)V->p, (const float*)V->rhs, V->res,
-           V->red(), V->dS, (int)FIN_RR0);
+  residual(V, (int)FIN_RR0);
   uint32_t it = 0;
   int stalled = 0;
   int e = fcg(V, N, max_fcg, 0.5, &it, &stalled);

@@ -597,13 +597,31 @@ void correct(fd3_volume* V, float k1) {
 // the true residual, the corrected field and its divergence metric (delta3d_mobile.rs:398-433),
 // the backward error (:243-271) and the fingerprint of p.  Correcting before knowing whether the
 // solve is accepted is harmless: us is untouched and every exit corrects from it again or restores
+// res = rhs - A p with res.res (FIN_RR0 or FIN_ACTUAL): on the paired march where the loop runs on
+// it (f64 reductions), else one cell per thread (the ordered mode's chunk order).
+void residual(fd3_volume* V, int op) {
+  Geo G = V->geo();
+  if (V->paired()) {
+    const int k2 = pick_k2(V->nx, V->ny, V->nz);
+    const int zb = zblocks2(V->nx, V->ny, V->nz, k2);
+    if (k2 == 8)
+      launch_grid(V, "kx_residual<8>", zb, Z2T, kx_residual<8>, G, (const unsigned short*)V->codes, (const float*)V->p,
+                  (const float*)V->rhs, V->res, V->red(), V->dS, op);
+    else
+      launch_grid(V, "kx_residual<4>", zb, Z2T, kx_residual<4>, G, (const unsigned short*)V->codes, (const float*)V->p,
+                  (const float*)V->rhs, V->res, V->red(), V->dS, op);
+    return;
+  }
+  DISPATCH(V, k_residual_c, V->n, G, (const unsigned short*)V->codes, (const float*)V->p, (const float*)V->rhs, V->res,
+           V->red(), V->dS, op);
+}
+
 // u.  One synchronisation.
 struct Checks { double actual, all, plain; float be; unsigned long long hash; int status; };
 
 int outer_checks(fd3_volume* V, float k1, Checks* out) {
   Geo G = V->geo();
-  DISPATCH(V, k_residual_c, V->n, G, (const unsigned short*)V->codes, (const float*)V->p, (const float*)V->rhs, V->res,
-           V->red(), V->dS, (int)FIN_ACTUAL);
+  residual(V, (int)FIN_ACTUAL);
   if (V->linear) {
     LAUNCH(V, k_correct_linear_uv, (long long)V->nu + V->nv, G, k1, (const float*)V->p, (const float*)V->us,
            (const float*)V->vs, V->u, V->v);
@@ -674,8 +692,7 @@ int project_mobile3(fd3_volume* V, float scale, float k1, uint32_t max_iters, fd
     if (V->has_mg) prepare_multigrid(V);
     LAUNCH(V, k_zero_dry, V->n, G, V->p);
   }
-  DISPATCH(V, k_residual_c, V->n, G, (const unsigned short*)V->codes, (const float*)V->p, (const float*)V->rhs, V->res,
-           V->red(), V->dS, (int)FIN_RR0);
+  residual(V, (int)FIN_RR0);
   TRY(pull(V));
   if (V->hS->status) return V->hS->status;
   const double b2 = V->hS->b2;

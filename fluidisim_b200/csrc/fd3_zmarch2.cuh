@@ -244,6 +244,23 @@ struct L2LoadR {  // operand x, with r carried for the epilogue
   __device__ __forceinline__ float hv(const Halo& h) const { return h.v; }
 };
 
+// res = rhs - A p with res.res (FIN_RR0 or FIN_ACTUAL): k_residual_c on the paired march.
+template <int K2>
+__global__ void __launch_bounds__(Z2T, FD3_ZMINB2) kx_residual(Geo g, const unsigned short* __restrict__ codes,
+                                                             const float* __restrict__ p, const float* __restrict__ rhs,
+                                                             float* __restrict__ res, Red red, Scalars* S, int op) {
+  KSTART();
+  L2LoadR<float> ld{p, rhs};
+  double acc = 0.0;
+  zmarch2<K2>(g, codes, ld, [&](int c, const L2LoadR<float>::Raw2& o, float2, float a0, float a1) {
+    const float r0 = o.r.x - a0, r1 = o.r.y - a1;
+    st2(res, c, r0, r1);
+    acc += (double)r0 * (double)r0;
+    acc += (double)r1 * (double)r1;
+  });
+  zreduce_finish(acc, red, S, op);
+}
+
 // d = z (+ beta d); q = A d; d.q; alpha (FIN_DQ).
 template <int K2, class T>
 __global__ void __launch_bounds__(Z2T, FD3_ZMINB2) kx_dir_apply_dot(Geo g, const unsigned short* __restrict__ codes,
