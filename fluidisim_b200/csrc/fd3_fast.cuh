@@ -1177,10 +1177,11 @@ __global__ void k_loop_cond(cudaGraphConditionalHandle handle, Scalars* S) {
 
 // rhs_mobile3 (delta3d_mobile.rs:215-241) with b.b (FIN_B2) when `reduce`.
 // With `codes` not null, the same pass also writes each cell's row code (row_code_of the same
-// row; 0 for a dry cell).
+// row; 0 for a dry cell); with `pdry` not null it zeroes that pressure on the dry cells.
 template <int MODE>
 __global__ void __launch_bounds__(TPB) k_rhs_b2(Geo g, float scale, float* __restrict__ rhs, float* __restrict__ prec,
-                                                Red red, Scalars* S, int reduce, unsigned short* __restrict__ codes) {
+                                                Red red, Scalars* S, int reduce, unsigned short* __restrict__ codes,
+                                                float* __restrict__ pdry) {
   KSTART();
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   float b = 0.f;
@@ -1189,6 +1190,7 @@ __global__ void __launch_bounds__(TPB) k_rhs_b2(Geo g, float scale, float* __res
     if (!wet3(g, i, j, k)) {
       rhs[c] = 0.f; prec[c] = 0.f;
       if (codes) codes[c] = 0;
+      if (pdry) pdry[c] = 0.f;
     } else {
       RowE row[6]; mobile_row(g, i, j, k, row);
       b = scale * rhs[c];

@@ -612,11 +612,28 @@ __device__ __forceinline__ void atomic_fmax_nonneg(float* addr, float v) {
   atomicMax(reinterpret_cast<int*>(addr), __float_as_int(v));
 }
 
-// max |x| over an array into S->fmax[slot].
-__global__ void k_maxabs(int n, const float* __restrict__ x, Scalars* S, int slot) {
+// max |x| over the three face families into S->fmax[slot] (one launch, 16-byte loads; each array
+// starts on a 16-byte boundary).
+__global__ void k_maxabs3(const float* __restrict__ u, int nu, const float* __restrict__ v, int nv,
+                          const float* __restrict__ w, int nw, Scalars* S, int slot) {
   KSTART();
+  const int stride = gridDim.x * blockDim.x, tid = blockIdx.x * blockDim.x + threadIdx.x;
   float m = 0.f;
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) m = fmaxf(m, fabsf(x[q]));
+  auto scan = [&](const float* __restrict__ x, int n) {
+    const int n4 = n / 4;
+    const float4* x4 = reinterpret_cast<const float4*>(x);
+    for (int q = tid; q < n4; q += stride) {
+      const float4 a = x4[q];
+      m = fmaxf(m, fabsf(a.x));
+      m = fmaxf(m, fabsf(a.y));
+      m = fmaxf(m, fabsf(a.z));
+      m = fmaxf(m, fabsf(a.w));
+    }
+    for (int q = 4 * n4 + tid; q < n; q += stride) m = fmaxf(m, fabsf(x[q]));
+  };
+  scan(u, nu);
+  scan(v, nv);
+  scan(w, nw);
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_down_sync(0xffffffffu, m, o));
   if ((threadIdx.x & 31) == 0) atomic_fmax_nonneg(&S->fmax[slot], m);

@@ -609,7 +609,7 @@ int assemble_device(fd3_volume* V, float scale) {
   CK(cudaMemcpyAsync(V->ws, V->w, (size_t)V->nw * 4, cudaMemcpyDeviceToDevice, V->stream));
   LAUNCH_G(V, k_reset_scalars, 1, 1, V->dS, vscale_k(V));
   LAUNCH(V, k_divergence, V->n, G, (const float*)V->us, (const float*)V->vs, (const float*)V->ws, V->rhs);
-  DISPATCH(V, k_rhs_b2, V->n, G, scale, V->rhs, V->prec, V->red(), V->dS, 1, V->codes);
+  DISPATCH(V, k_rhs_b2, V->n, G, scale, V->rhs, V->prec, V->red(), V->dS, 1, V->codes, (float*)nullptr);
   return FD3_OK;
 }
 

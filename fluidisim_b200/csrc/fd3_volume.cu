@@ -633,9 +633,8 @@ int outer_checks(fd3_volume* V, float k1, Checks* out) {
   if (V->linear) LAUNCH(V, k_div_metric_linear, V->n, G, (const float*)V->u, (const float*)V->v, (const float*)V->w, V->dS);
   else LAUNCH(V, k_div_metric_c, V->n, G, (const unsigned short*)V->codes, (const float*)V->u, (const float*)V->v,
               (const float*)V->w, V->dS);
-  LAUNCH_G(V, k_maxabs, 592, TPB, V->nu, (const float*)V->u, V->dS, 2);
-  LAUNCH_G(V, k_maxabs, 592, TPB, V->nv, (const float*)V->v, V->dS, 2);
-  LAUNCH_G(V, k_maxabs, 592, TPB, V->nw, (const float*)V->w, V->dS, 2);
+  LAUNCH_G(V, k_maxabs3, 8 * 148, TPB, (const float*)V->u, V->nu, (const float*)V->v, V->nv, (const float*)V->w,
+           V->nw, V->dS, 2);
   if (V->linear)
     LAUNCH(V, k_backward_error_linear, V->n, G, (const float*)V->p, (const float*)V->rhs, (const float*)V->res, V->dS);
   else
@@ -688,9 +687,9 @@ int project_mobile3(fd3_volume* V, float scale, float k1, uint32_t max_iters, fd
     LAUNCH(V, k_row_codes_linear, V->n, G, V->codes);
     CK(cudaMemsetAsync(V->p, 0, (size_t)V->n * sizeof(float), V->stream));
   } else {
-    DISPATCH(V, k_rhs_b2, V->n, G, scale, V->rhs, V->prec, V->red(), V->dS, 1, V->codes);
+    // the assembly also zeroes p on the dry cells (delta3d_mobile.rs:486-495)
+    DISPATCH(V, k_rhs_b2, V->n, G, scale, V->rhs, V->prec, V->red(), V->dS, 1, V->codes, V->p);
     if (V->has_mg) prepare_multigrid(V);
-    LAUNCH(V, k_zero_dry, V->n, G, V->p);
   }
   residual(V, (int)FIN_RR0);
   TRY(pull(V));
@@ -1914,7 +1913,8 @@ int fd3_assemble_pressure_problem_for_trials(fd3_volume* V, const float* diverge
   TRY(check_finite_device(V, V->tmp, V->n, &ok));
   if (!ok) return FD3_ERR_NOT_FINITE;
   CK(cudaMemcpyAsync(V->rhs, V->tmp, len * 4, cudaMemcpyDeviceToDevice, V->stream));
-  DISPATCH(V, k_rhs_b2, V->n, V->geo(), scale, V->rhs, V->prec, V->red(), V->dS, 0, (unsigned short*)nullptr);
+  DISPATCH(V, k_rhs_b2, V->n, V->geo(), scale, V->rhs, V->prec, V->red(), V->dS, 0, (unsigned short*)nullptr,
+           (float*)nullptr);
   CK(cudaMemcpyAsync(rhs, V->rhs, len * 4, cudaMemcpyDeviceToHost, V->stream));
   CK(cudaMemcpyAsync(prec, V->prec, len * 4, cudaMemcpyDeviceToHost, V->stream));
   return sync(V);
@@ -1926,7 +1926,7 @@ int fd3_vcycle_for_tests(fd3_volume* V, const float* x, float* z, size_t len) {
   if (!V->has_mg) return FD3_ERR_DOMAIN;
   if (len != (size_t)V->n) return FD3_ERR_SHAPE;
   CK(cudaMemsetAsync(V->rhs, 0, len * 4, V->stream));
-  DISPATCH(V, k_rhs_b2, V->n, V->geo(), 1.f, V->rhs, V->prec, V->red(), V->dS, 0, V->codes);
+  DISPATCH(V, k_rhs_b2, V->n, V->geo(), 1.f, V->rhs, V->prec, V->red(), V->dS, 0, V->codes, (float*)nullptr);
   prepare_multigrid(V);
   CK(cudaMemcpyAsync(V->res, x, len * 4, cudaMemcpyHostToDevice, V->stream));
   if (V->half()) LAUNCH_G(V, k_reset_scalars, 1, 1, V->dS, 0.f);  // FP16 storage, r unscaled (vinv = 1)
