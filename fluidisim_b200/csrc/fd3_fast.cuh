@@ -168,6 +168,65 @@ __global__ void k_div_metric_c(Geo g, const unsigned short* __restrict__ codes, 
   if ((threadIdx.x & 31) == 0) { atomic_fmax_nonneg(&S->fmax[0], all); atomic_fmax_nonneg(&S->fmax[1], plain); }
 }
 
+// correct_mobile3 (delta3d_mobile.rs:284-343) from the row codes.  A u or v face between cells l
+// and r is corrected when r's row has it live (state 1: both wet, the gradient; state 2: l is air,
+// r's ghost) or, r being dry, when l's row has it as a ghost (r is air, l's ghost).  Those are
+// exactly the faces the reference corrects: open, neither cell solid, at least one wet.  A w face
+// is corrected when the row of the cell below has it live.  Ghost coefficients and values are the
+// reference's (ghost_side3, ghost_up3).
+__global__ void k_correct_uv_c(Geo g, const unsigned short* __restrict__ codes, float k1, const float* __restrict__ p,
+                               const float* __restrict__ us, const float* __restrict__ vs, float* __restrict__ u,
+                               float* __restrict__ v) {
+  KSTART();
+  const int nu = (g.nx + 1) * g.ny * g.nz, nv = g.nx * (g.ny + 1) * g.nz;
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  int axis, f, i, j, k;
+  if (q < nu) { axis = 0; f = q; i = f % (g.nx + 1); int t = f / (g.nx + 1); j = t % g.ny; k = t / g.ny; }
+  else if (q < nu + nv) { axis = 1; f = q - nu; i = f % g.nx; int t = f / g.nx; j = t % (g.ny + 1); k = t / (g.ny + 1); }
+  else return;
+  float val = axis == 0 ? us[f] : vs[f];
+  const bool interior = axis == 0 ? (i > 0 && i < g.nx) : (j > 0 && j < g.ny);
+  if (interior) {
+    const int x = axis == 0 ? i - 1 : i, y = axis == 0 ? j : j - 1;
+    const int l = (k * g.ny + y) * g.nx + x, r = (k * g.ny + j) * g.nx + i;
+    const unsigned cr = codes[r];
+    const unsigned sr = face_state(cr, axis == 0 ? 0 : 2);  // r's face toward l
+    if (sr == 1) {
+      val -= k1 * (p[r] - p[l]) / g.dx;
+    } else if (sr == 2) {
+      float a, b; ghost_side3(g, i, j, k, x, y, a, b);
+      val -= k1 * (p[r] - b) * a / g.dx;
+    } else if (!(cr & RC_WET) && face_state(codes[l], axis == 0 ? 1 : 3) == 2) {  // l's face toward r
+      float a, b; ghost_side3(g, x, y, k, i, j, a, b);
+      val -= k1 * (b - p[l]) * a / g.dx;
+    }
+  }
+  if (axis == 0) u[f] = val; else v[f] = val;
+}
+
+__global__ void k_correct_w_c(Geo g, const unsigned short* __restrict__ codes, float k1, const float* __restrict__ p,
+                              const float* __restrict__ ws, float* __restrict__ w) {
+  KSTART();
+  const int nw = g.nx * g.ny * (g.nz + 1);
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= nw) return;
+  const int nxny = g.nx * g.ny;
+  const int k = f / nxny;
+  float val = ws[f];
+  if (k >= 1) {
+    const int below = f - nxny;
+    const unsigned st = face_state(codes[below], 5);  // the face above the cell below
+    if (st == 1) {
+      val -= k1 * (p[below + nxny] - p[below]) / g.dx;
+    } else if (st == 2) {
+      const int col = f % nxny, i = col % g.nx, j = col / g.nx;
+      float a, b; ghost_up3(g, i, j, k - 1, a, b);
+      val -= k1 * (b - p[below]) * a / g.dx;
+    }
+  }
+  w[f] = val;
+}
+
 // backward_error_mobile3 (delta3d_mobile.rs:243-271): max |r_i| / (|b| + |A||p|)_i over the wet
 // rows into S->fmax[3].  A row's apertures and ghost coefficients are the ones apply_code uses.
 __global__ void k_backward_error_c(Geo g, const unsigned short* __restrict__ codes, const float* __restrict__ p,

@@ -560,52 +560,6 @@ __global__ void k_coarsen_open(int fnx, int fny, const float* __restrict__ fou, 
 // ------------------------------------------------------------------------------------------------
 // Correction and diagnostics
 
-// correct_mobile3 (delta3d_mobile.rs:284-343): u = us - change on every u face (axis 0), v face
-// (axis 1); untouched faces copy the prediction.
-__global__ void k_correct_uv(Geo g, float k1, const float* __restrict__ p, const float* __restrict__ us,
-                             const float* __restrict__ vs, float* __restrict__ u, float* __restrict__ v) {
-  KSTART();
-  int nu = (g.nx + 1) * g.ny * g.nz, nv = g.nx * (g.ny + 1) * g.nz;
-  int q = blockIdx.x * blockDim.x + threadIdx.x;
-  int axis, f, i, j, k;
-  if (q < nu) { axis = 0; f = q; i = f % (g.nx + 1); int t = f / (g.nx + 1); j = t % g.ny; k = t / g.ny; }
-  else if (q < nu + nv) { axis = 1; f = q - nu; i = f % g.nx; int t = f / g.nx; j = t % (g.ny + 1); k = t / (g.ny + 1); }
-  else return;
-  float val = axis == 0 ? us[f] : vs[f];
-  bool interior = axis == 0 ? (i > 0 && i < g.nx) : (j > 0 && j < g.ny);
-  if (interior) {
-    int x = axis == 0 ? i - 1 : i, y = axis == 0 ? j : j - 1;
-    int l = (k * g.ny + y) * g.nx + x, r = (k * g.ny + j) * g.nx + i;
-    if (!(open3(g, axis, f) == 0.f || solid3(g, l) || solid3(g, r))) {
-      bool wl = wet3(g, x, y, k), wr = wet3(g, i, j, k);
-      if (wl || wr) {
-        float change;
-        if (wl && wr) change = k1 * (p[r] - p[l]) / g.dx;
-        else if (wl) { float a, b; ghost_side3(g, x, y, k, i, j, a, b); change = k1 * (b - p[l]) * a / g.dx; }
-        else { float a, b; ghost_side3(g, i, j, k, x, y, a, b); change = k1 * (p[r] - b) * a / g.dx; }
-        val -= change;
-      }
-    }
-  }
-  if (axis == 0) u[f] = val; else v[f] = val;
-}
-
-__global__ void k_correct_w(Geo g, float k1, const float* __restrict__ p, const float* __restrict__ ws,
-                            float* __restrict__ w) {
-  KSTART();
-  int nw = g.nx * g.ny * (g.nz + 1);
-  int f = blockIdx.x * blockDim.x + threadIdx.x;
-  if (f >= nw) return;
-  int i = f % g.nx, t = f / g.nx, j = t % g.ny, k = t / g.ny;
-  float val = ws[f];
-  if (k >= 1 && open3(g, 2, f) != 0.f && wet3(g, i, j, k - 1)) {
-    int below = ((k - 1) * g.ny + j) * g.nx + i;
-    if (k < g.nz && wet3(g, i, j, k)) val -= k1 * (p[below + g.nx * g.ny] - p[below]) / g.dx;
-    else { float a, b; ghost_up3(g, i, j, k - 1, a, b); val -= k1 * (b - p[below]) * a / g.dx; }
-  }
-  w[f] = val;
-}
-
 // Order-independent float max of non-negative values (NaN-free inputs compare as their bits).
 __device__ __forceinline__ void atomic_fmax_nonneg(float* addr, float v) {
   if (!(v > 0.f)) return;  // +0 initial value; NaN is ignored, as Rust's f32::max does

@@ -589,8 +589,9 @@ __global__ void k_reset_diag(Scalars* S, int mask) {
 
 void correct(fd3_volume* V, float k1) {
   Geo G = V->geo();
-  LAUNCH(V, k_correct_uv, (long long)V->nu + V->nv, G, k1, (const float*)V->p, (const float*)V->us, (const float*)V->vs, V->u, V->v);
-  LAUNCH(V, k_correct_w, V->nw, G, k1, (const float*)V->p, (const float*)V->ws, V->w);
+  LAUNCH(V, k_correct_uv_c, (long long)V->nu + V->nv, G, (const unsigned short*)V->codes, k1, (const float*)V->p,
+         (const float*)V->us, (const float*)V->vs, V->u, V->v);
+  LAUNCH(V, k_correct_w_c, V->nw, G, (const unsigned short*)V->codes, k1, (const float*)V->p, (const float*)V->ws, V->w);
 }
 
 // The checks that end or restart the outer loop (delta3d_mobile.rs:547-585), launched together:
