@@ -9,3 +9,9 @@ if ROOT not in sys.path:
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (runs the sm_100a library)")
     config.addinivalue_line("markers", "slow: a CPU test of more than a few seconds")
+
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+if GOLDEN not in sys.path:
+    sys.path.insert(0, GOLDEN)
+

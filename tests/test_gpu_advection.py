@@ -7,6 +7,7 @@ mode; and the four-cell mode of tests_delta3d.rs:2182-2193 must stop growing.
 import numpy as np
 import pytest
 
+import golden_cases as G
 from fluidisim_b200 import scenes
 from fluidisim_b200.delta3d import REDUCE_ORDERED_F32, Volume3
 from oracle import oracle as O
@@ -101,5 +102,7 @@ def test_second_order_advection_stops_the_ftcs_growth():
             c += x * np.cos(np.pi / 2 * i)
         return float(np.hypot(s, c)) / (1e-3 * 32 / 2)
     ftcs, corrected = growth(False), growth(True)
-    assert 5 < ftcs < 10, ftcs
-    assert corrected < 0.5, corrected
+    want = G.known_answers()["advection_four_cell_mode"]
+    lo, hi = want["ftcs_growth_between"]
+    assert lo < ftcs < hi, ftcs
+    assert corrected < want["corrected_growth_below"], corrected

@@ -8,6 +8,7 @@ projection must reach the reference's acceptance (relative residual <= 1e-6, pla
 import numpy as np
 import pytest
 
+import golden_cases as G
 from fluidisim_b200 import scenes
 from fluidisim_b200.delta3d import REDUCE_F64, REDUCE_ORDERED_F32, Delta3dError, Volume3
 from oracle import oracle as O
@@ -137,7 +138,8 @@ def test_s385_first_step_matches_the_oracle(nx, bump, reduction):
     o, d, s = s385_pair(nx, bump, reduction=reduction)
     ro = o.step_surface_mobile(s["dt_us"], 20000)
     rd = d.step_surface_mobile(s["dt_us"], 20000)
-    assert rd.iterations == {32: 9, 64: 10}[nx] or reduction == REDUCE_F64
+    published = G.known_answers()["s385_multigrid_iterations"]["bump" if bump else "flat"][str(nx)]
+    assert rd.iterations == published or reduction == REDUCE_F64
     _compare_projection(o, d, ro, rd, reduction == REDUCE_ORDERED_F32)
     if reduction == REDUCE_ORDERED_F32:
         for a, b in zip(o.surface(), d.surface_and_roundoff()):

@@ -4,6 +4,7 @@ The reference's criterion (tests_delta3d.rs:2132-2193): the centred explicit pre
 four-cell mode (Courant 0.264: x7.4 over 60 steps); with the term the mode no longer grows
 (|G|^2 = 1 - C^2 + C^4, x0.13).  The term is off by default.
 """
+import golden_cases as G
 import numpy as np
 
 from oracle import oracle as O
@@ -41,5 +42,7 @@ def growth(corrected, steps):
 
 def test_second_order_advection_stops_the_ftcs_growth():
     ftcs, corrected = growth(False, 60), growth(True, 60)
-    assert 5 < ftcs < 10, ftcs
-    assert corrected < 0.5, corrected
+    want = G.known_answers()["advection_four_cell_mode"]
+    lo, hi = want["ftcs_growth_between"]
+    assert lo < ftcs < hi, ftcs
+    assert corrected < want["corrected_growth_below"], corrected

@@ -9,6 +9,7 @@ import math
 import numpy as np
 import pytest
 
+import golden_cases as G
 from fluidisim_b200 import scenes
 from oracle import oracle as O
 
@@ -29,24 +30,23 @@ def s324_step(nx, bump, jacobi):
     return r, q
 
 
+_KA = G.known_answers()
+
+
 # FACES-COUPEES-3D-S324.md:136 (S326, Jacobi) and :85 (S324, no preconditioner)
-@pytest.mark.parametrize("nx,jacobi,iters,flux", [
-    (32, True, 117, 9.144646532e-4),
-    (64, True, 220, 9.169151446e-4),
-    (32, False, 222, 9.144646e-4),
-    (64, False, 645, 9.169173e-4),
-])
-def test_cut_bump_step_matches_the_published_bench(nx, jacobi, iters, flux):
+@pytest.mark.parametrize("nx,jacobi,iters,flux,digits", [
+    (r["nx"], r["jacobi"], r["iterations"], r["flux"], r["digits"]) for r in _KA["s324_cut_bump_linear"]["rows"]])
+def test_cut_bump_step_matches_the_published_bench(nx, jacobi, iters, flux, digits):
     r, q = s324_step(nx, True, jacobi)
     assert r["iterations"] == iters
-    digits = 10 if jacobi else 7
     assert round(q, digits + 3) == pytest.approx(flux, rel=0.5 * 10 ** (1 - digits))
     assert not r["degraded"] and r["divergence"] <= 1e-5
 
 
 # FACES-COUPEES-3D-S324.md:85: the smooth bottom without y, no preconditioner, 95 / 179 iterations;
 # its flux per unit width 2.2524960e-4 / 2.2584836e-4 m^2/s (width 4 m).
-@pytest.mark.parametrize("nx,iters,flux_per_width", [(32, 95, 2.2524960e-4), (64, 179, 2.2584836e-4)])
+@pytest.mark.parametrize("nx,iters,flux_per_width", [
+    (r["nx"], r["iterations"], r["flux_per_width"]) for r in _KA["s324_smooth_bottom_linear"]["rows"]])
 def test_smooth_bottom_witness_matches_the_published_bench(nx, iters, flux_per_width):
     r, q = s324_step(nx, False, False)
     assert r["iterations"] == iters
@@ -75,9 +75,10 @@ def test_oblique_standing_wave_follows_its_scheme():
         ph = big * t
         e_scheme = max(e_scheme, float(np.max(np.abs(hn - w["a"] * w["mode"] * (math.cos(ph) + beta * math.sin(ph)))))
                        / w["a"])
-    assert round(100 * e_cont, 4) == 2.3165
-    assert round(100 * e_scheme, 4) == 0.0046
-    assert round(its / steps, 1) == 17.9
+    want = _KA["s295_oblique_standing_wave"]
+    assert round(100 * e_cont, 4) == want["error_vs_continuous_percent"]
+    assert round(100 * e_scheme, 4) == want["error_vs_scheme_percent"]
+    assert round(its / steps, 1) == want["mean_iterations"]
 
 
 @pytest.mark.parametrize("shape", [(8, 6, 5), (12, 1, 7), (5, 9, 4)])
