@@ -130,15 +130,23 @@ struct LoadT {
 // built for), instead of rebuilding each row from the geometry.
 
 // divergence_mobile3 (delta3d_mobile.rs:398-433): max |div u| over the wet rows and over the
-// plain ones (no surface ghost: no face state 2), into S->fmax[0] and [1].
+// plain ones (no surface ghost: no face state 2), into S->fmax[0] and [1].  Each thread takes
+// METRIC_CELLS cells, a block's cells apart, and the block merges its maxima by one atomic each.
 __global__ void k_div_metric_c(Geo g, const unsigned short* __restrict__ codes, const float* __restrict__ u,
                                const float* __restrict__ v, const float* __restrict__ w, Scalars* S) {
   KSTART();
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
   float all = 0.f, plain = 0.f;
-  if (c < g.n) {
-    const unsigned code = codes[c];
-    if (code & RC_WET) {
+  const int c0 = blockIdx.x * (METRIC_CELLS * blockDim.x) + threadIdx.x;
+  unsigned code[METRIC_CELLS];
+#pragma unroll
+  for (int q = 0; q < METRIC_CELLS; ++q) {
+    const int c = c0 + q * blockDim.x;
+    code[q] = c < g.n ? codes[c] : 0u;
+  }
+#pragma unroll
+  for (int q = 0; q < METRIC_CELLS; ++q) {
+    if (code[q] & RC_WET) {
+      const int c = c0 + q * blockDim.x;
       int i, j, k; cell_ijk(g, c, i, j, k);
       float dv;
       if (g.cut) {
@@ -156,16 +164,11 @@ __global__ void k_div_metric_c(Geo g, const unsigned short* __restrict__ codes, 
         dv = ((fr - fl + ft - fb) + (fk - ff)) / g.dx;
       }
       const float d = fabsf(dv);
-      all = d;
-      if (!(code & RC_GHOSTS)) plain = d;
+      all = fmaxf(all, d);
+      if (!(code[q] & RC_GHOSTS)) plain = fmaxf(plain, d);
     }
   }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    all = fmaxf(all, __shfl_down_sync(0xffffffffu, all, o));
-    plain = fmaxf(plain, __shfl_down_sync(0xffffffffu, plain, o));
-  }
-  if ((threadIdx.x & 31) == 0) { atomic_fmax_nonneg(&S->fmax[0], all); atomic_fmax_nonneg(&S->fmax[1], plain); }
+  block_fmax2_atomic(all, plain, &S->fmax[0], &S->fmax[1]);
 }
 
 // correct_mobile3 (delta3d_mobile.rs:284-343) from the row codes.  A u or v face between cells l
@@ -229,14 +232,23 @@ __global__ void k_correct_w_c(Geo g, const unsigned short* __restrict__ codes, f
 
 // backward_error_mobile3 (delta3d_mobile.rs:243-271): max |r_i| / (|b| + |A||p|)_i over the wet
 // rows into S->fmax[3].  A row's apertures and ghost coefficients are the ones apply_code uses.
+// Each thread takes METRIC_CELLS cells, a block's cells apart; one atomic per block.
 __global__ void k_backward_error_c(Geo g, const unsigned short* __restrict__ codes, const float* __restrict__ p,
                                    const float* __restrict__ rhs, const float* __restrict__ res, Scalars* S) {
   KSTART();
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
   float worst = 0.f;
-  if (c < g.n) {
-    const unsigned code = codes[c];
+  const int c0 = blockIdx.x * (METRIC_CELLS * blockDim.x) + threadIdx.x;
+  unsigned codev[METRIC_CELLS];
+#pragma unroll
+  for (int q = 0; q < METRIC_CELLS; ++q) {
+    const int c = c0 + q * blockDim.x;
+    codev[q] = c < g.n ? codes[c] : 0u;
+  }
+#pragma unroll
+  for (int q = 0; q < METRIC_CELLS; ++q) {
+    const unsigned code = codev[q];
     if (code & RC_WET) {
+      const int c = c0 + q * blockDim.x;
       int i, j, k; cell_ijk(g, c, i, j, k);
       const int nxny = g.nx * g.ny;
       const bool unit = code & RC_UNIT;
@@ -256,12 +268,10 @@ __global__ void k_backward_error_c(Geo g, const unsigned short* __restrict__ cod
       face(4, 2, fw(g, i, j, k), c - nxny, i, j);
       face(5, 2, fw(g, i, j, k + 1), c + nxny, i, j);
       const float scale = fabsf(rhs[c]) + acc * g.inv;
-      if (scale > 0.f) worst = fabsf(res[c]) / scale;
+      if (scale > 0.f) worst = fmaxf(worst, fabsf(res[c]) / scale);
     }
   }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) worst = fmaxf(worst, __shfl_down_sync(0xffffffffu, worst, o));
-  if ((threadIdx.x & 31) == 0) atomic_fmax_nonneg(&S->fmax[3], worst);
+  block_fmax2_atomic(worst, 0.f, &S->fmax[3], nullptr);
 }
 
 // ------------------------------------------------------------------------------------------------

@@ -566,6 +566,39 @@ __device__ __forceinline__ void atomic_fmax_nonneg(float* addr, float v) {
   atomicMax(reinterpret_cast<int*>(addr), __float_as_int(v));
 }
 
+// The block's maxima of two nonnegative values (warp shuffles, then the warps' maxima through
+// shared memory) merged into addr0 / addr1 by thread 0: one atomic per block and value.  Atomics on
+// one address serialise in L2, so a metric over millions of cells keeps them to one per block.
+// Every thread of the block calls it (it holds a barrier).  NaN is ignored, as fmaxf does.
+__device__ __forceinline__ void block_fmax2_atomic(float a, float b, float* addr0, float* addr1) {
+  __shared__ float pa[32], pb[32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    a = fmaxf(a, __shfl_down_sync(0xffffffffu, a, o));
+    b = fmaxf(b, __shfl_down_sync(0xffffffffu, b, o));
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) { pa[wid] = a; pb[wid] = b; }
+  __syncthreads();
+  if (wid == 0) {
+    const bool on = lane < (int)(blockDim.x >> 5);
+    a = on ? pa[lane] : 0.f;
+    b = on ? pb[lane] : 0.f;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      a = fmaxf(a, __shfl_down_sync(0xffffffffu, a, o));
+      b = fmaxf(b, __shfl_down_sync(0xffffffffu, b, o));
+    }
+    if (lane == 0) {
+      if (addr0) atomic_fmax_nonneg(addr0, a);
+      if (addr1) atomic_fmax_nonneg(addr1, b);
+    }
+  }
+}
+
+// Cells per thread of the max-metric kernels (a block covers METRIC_CELLS * blockDim.x cells).
+constexpr int METRIC_CELLS = 4;
+
 // max |x| over the three face families into S->fmax[slot] (one launch, 16-byte loads; each array
 // starts on a 16-byte boundary).
 __global__ void k_maxabs3(const float* __restrict__ u, int nu, const float* __restrict__ v, int nv,
@@ -588,9 +621,7 @@ __global__ void k_maxabs3(const float* __restrict__ u, int nu, const float* __re
   scan(u, nu);
   scan(v, nv);
   scan(w, nw);
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_down_sync(0xffffffffu, m, o));
-  if ((threadIdx.x & 31) == 0) atomic_fmax_nonneg(&S->fmax[slot], m);
+  block_fmax2_atomic(m, 0.f, &S->fmax[slot], nullptr);
 }
 
 // Fingerprint of the exact bits of p for cycle detection (the role of fingerprint,

@@ -178,9 +178,7 @@ __global__ void k_div_metric_linear(Geo g, const float* __restrict__ u, const fl
     }
     d = fabsf(dv);
   }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) d = fmaxf(d, __shfl_down_sync(0xffffffffu, d, o));
-  if ((threadIdx.x & 31) == 0) { atomic_fmax_nonneg(&S->fmax[0], d); atomic_fmax_nonneg(&S->fmax[1], d); }
+  block_fmax2_atomic(d, d, &S->fmax[0], &S->fmax[1]);
 }
 
 // backward_error (delta3d.rs:881-907) and backward_error_cut (:909-945) into S->fmax[3].
@@ -215,9 +213,7 @@ __global__ void k_backward_error_linear(Geo g, const float* __restrict__ p, cons
     float scale = fabsf(rhs[c]) + acc * g.inv;
     if (scale > 0.f) worst = fabsf(res[c]) / scale;
   }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) worst = fmaxf(worst, __shfl_down_sync(0xffffffffu, worst, o));
-  if ((threadIdx.x & 31) == 0) atomic_fmax_nonneg(&S->fmax[3], worst);
+  block_fmax2_atomic(worst, 0.f, &S->fmax[3], nullptr);
 }
 
 // The heights carried by the column fluxes (delta3d.rs:1305-1336): each column sums its four side

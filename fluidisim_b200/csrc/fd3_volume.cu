@@ -632,15 +632,15 @@ int outer_checks(fd3_volume* V, float k1, Checks* out) {
   }
   LAUNCH_G(V, k_reset_diag, 1, 1, V->dS, 7);
   if (V->linear) LAUNCH(V, k_div_metric_linear, V->n, G, (const float*)V->u, (const float*)V->v, (const float*)V->w, V->dS);
-  else LAUNCH(V, k_div_metric_c, V->n, G, (const unsigned short*)V->codes, (const float*)V->u, (const float*)V->v,
-              (const float*)V->w, V->dS);
+  else LAUNCH(V, k_div_metric_c, ((long long)V->n + METRIC_CELLS - 1) / METRIC_CELLS, G,
+              (const unsigned short*)V->codes, (const float*)V->u, (const float*)V->v, (const float*)V->w, V->dS);
   LAUNCH_G(V, k_maxabs3, 8 * 148, TPB, (const float*)V->u, V->nu, (const float*)V->v, V->nv, (const float*)V->w,
            V->nw, V->dS, 2);
   if (V->linear)
     LAUNCH(V, k_backward_error_linear, V->n, G, (const float*)V->p, (const float*)V->rhs, (const float*)V->res, V->dS);
   else
-    LAUNCH(V, k_backward_error_c, V->n, G, (const unsigned short*)V->codes, (const float*)V->p, (const float*)V->rhs,
-           (const float*)V->res, V->dS);
+    LAUNCH(V, k_backward_error_c, ((long long)V->n + METRIC_CELLS - 1) / METRIC_CELLS, G,
+           (const unsigned short*)V->codes, (const float*)V->p, (const float*)V->rhs, (const float*)V->res, V->dS);
   LAUNCH_G(V, k_hash, 592, TPB, V->n, (const float*)V->p, V->dS);
   TRY(pull(V));
   const Scalars* S = V->hS;
