@@ -39,6 +39,18 @@ enum Mode { RED_F64 = 0, RED_ORD = 1 };
   } while (0)
 
 // Fine-level geometry, passed by value to every fine kernel.
+// The rigid motion of a solid: translation v, rotation w (rad/s) about c.
+struct Rigid {
+  float v[3], w[3], c[3];
+};
+// wall_velocity (delta3d.rs:75-82): component `axis` of v + w x (x - c).
+__device__ __forceinline__ float wall_velocity(const Rigid& R, int axis, float x0, float x1, float x2) {
+  const float r0 = x0 - R.c[0], r1 = x1 - R.c[1], r2 = x2 - R.c[2];
+  if (axis == 0) return R.v[0] + (R.w[1] * r2 - R.w[2] * r1);
+  if (axis == 1) return R.v[1] + (R.w[2] * r0 - R.w[0] * r2);
+  return R.v[2] + (R.w[0] * r1 - R.w[1] * r0);
+}
+
 struct Geo {
   int nx, ny, nz, n;
   int cut;                // 0: flat bottom (every aperture 1, nothing solid)
@@ -57,6 +69,14 @@ struct Geo {
   // projection writes is 0 there (the set change zeroes them), and a skipped tile adds exactly 0 to
   // each reduction, so skipping changes no bit.
   const unsigned char* tiles;
+  // A solid set in motion by set_solid_rigid: wall = 1 in translation, 2 in rotation, 0 at rest or
+  // without a solid.  The divergence then adds the flux of the parts of the faces the solid covers
+  // (base apertures bou/bov/bow, the bottom-only cut, minus the apertures).
+  int wall;
+  Rigid rig;
+  const float* bou;
+  const float* bov;
+  const float* bow;
 };
 constexpr int TILE_X = 32, TILE_Y = 8;
 
@@ -194,6 +214,30 @@ __device__ __forceinline__ float open3(const Geo& g, int axis, int f) {
 __device__ __forceinline__ int fu(const Geo& g, int i, int j, int k) { return (k * g.ny + j) * (g.nx + 1) + i; }
 __device__ __forceinline__ int fv(const Geo& g, int i, int j, int k) { return (k * (g.ny + 1) + j) * g.nx + i; }
 __device__ __forceinline__ int fw(const Geo& g, int i, int j, int k) { return (k * g.ny + j) * g.nx + i; }
+
+// divergence_cut's moving-wall term (delta3d.rs:824-852), for g.wall != 0: in rotation, each face
+// part the solid covers moves at the wall's velocity at the face centre; in translation, at the
+// solid's velocity.  The caller adds it to the cell's divergence.
+__device__ __forceinline__ float wall_flux(const Geo& g, int i, int j, int k) {
+  const int ul = fu(g, i, j, k), ur = fu(g, i + 1, j, k), vl = fv(g, i, j, k), vr = fv(g, i, j + 1, k);
+  const int wl = fw(g, i, j, k), wr = fw(g, i, j, k + 1);
+  const float cul = __ldg(g.bou + ul) - __ldg(g.ou + ul), cur = __ldg(g.bou + ur) - __ldg(g.ou + ur);
+  const float cvl = __ldg(g.bov + vl) - __ldg(g.ov + vl), cvr = __ldg(g.bov + vr) - __ldg(g.ov + vr);
+  const float cwl = __ldg(g.bow + wl) - __ldg(g.ow + wl), cwr = __ldg(g.bow + wr) - __ldg(g.ow + wr);
+  const float dx = g.dx;
+  if (g.wall == 2) {
+    const float xc = ((float)i + 0.5f) * dx, yc = ((float)j + 0.5f) * dx, zc = ((float)k + 0.5f) * dx;
+    const float x0 = (float)i * dx, x1 = (float)(i + 1) * dx;
+    const float y0 = (float)j * dx, y1 = (float)(j + 1) * dx;
+    const float z0 = (float)k * dx, z1 = (float)(k + 1) * dx;
+    const float fx = cur * wall_velocity(g.rig, 0, x1, yc, zc) - cul * wall_velocity(g.rig, 0, x0, yc, zc);
+    const float fy = cvr * wall_velocity(g.rig, 1, xc, y1, zc) - cvl * wall_velocity(g.rig, 1, xc, y0, zc);
+    const float fz = cwr * wall_velocity(g.rig, 2, xc, yc, z1) - cwl * wall_velocity(g.rig, 2, xc, yc, z0);
+    return (fx + fy + fz) / dx;
+  }
+  const float x = cur - cul, y = cvr - cvl, z = cwr - cwl;
+  return (g.rig.v[0] * x + g.rig.v[1] * y + g.rig.v[2] * z) / dx;
+}
 
 // ghost_up3 (delta3d_mobile.rs:126-134)
 __device__ __forceinline__ void ghost_up3(const Geo& g, int i, int j, int k, float& it, float& value) {
@@ -335,7 +379,9 @@ __global__ void k_divergence(Geo g, const float* __restrict__ u, const float* __
     float fk = __ldg(g.ov + fv(g, i, j + 1, k)) * v[fv(g, i, j + 1, k)];
     float fb = __ldg(g.ow + fw(g, i, j, k)) * w[fw(g, i, j, k)];
     float ft = __ldg(g.ow + fw(g, i, j, k + 1)) * w[fw(g, i, j, k + 1)];
-    out[c] = ((fr - fl + ft - fb) + (fk - ff)) / g.dx;
+    float d = ((fr - fl + ft - fb) + (fk - ff)) / g.dx;
+    if (g.wall) d = d + wall_flux(g, i, j, k);
+    out[c] = d;
   } else {
     float fl = u[fu(g, i, j, k)], fr = u[fu(g, i + 1, j, k)];
     float ff = v[fv(g, i, j, k)], fk = v[fv(g, i, j + 1, k)];

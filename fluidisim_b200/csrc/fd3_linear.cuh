@@ -169,6 +169,7 @@ __global__ void k_div_metric_linear(Geo g, const float* __restrict__ u, const fl
         float fb = __ldg(g.ow + fw(g, i, j, k)) * w[fw(g, i, j, k)];
         float ft = __ldg(g.ow + fw(g, i, j, k + 1)) * w[fw(g, i, j, k + 1)];
         dv = ((fr - fl + ft - fb) + (fk - ff)) / g.dx;
+        if (g.wall) dv = dv + wall_flux(g, i, j, k);
       }
     } else {
       float fl = u[fu(g, i, j, k)], fr = u[fu(g, i + 1, j, k)];

@@ -95,6 +95,10 @@ struct fd3_volume {
   // cut is redone from when the solid moves (Base3, delta3d_cut.rs:53-80): fractions, apertures,
   // floors, the solid volume per column and the water it deposited
   float *sdf = nullptr, *bfrac = nullptr, *bou = nullptr, *bov = nullptr, *bow = nullptr, *bfloor = nullptr;
+  // the solid's rigid motion from the last set_solid_rigid (delta3d.rs:408-410): wall = 2 when it
+  // rotates, 1 when it only translates, 0 at rest (Geo::wall)
+  Rigid motion{};
+  int wall = 0;
   float *bcol = nullptr, *bdep = nullptr;
   // the sparse column set (Sparse3, delta3d_sparse.rs:31-44): device mask, a scratch mask of the
   // columns leaving it, and the host copy the refusals and the published counts read
@@ -162,6 +166,9 @@ struct fd3_volume {
     G.frac = frac; G.ou = ou; G.ov = ov; G.ow = ow;
     G.act = sparse ? act : nullptr;
     G.tiles = sparse && !opt.no_tile_skip ? tiles : nullptr;
+    G.wall = wall;
+    G.rig = motion;
+    G.bou = bou; G.bov = bov; G.bow = bow;
     return G;
   }
   bool ord() const { return opt.reduction == FD3_REDUCE_ORDERED_F32; }
@@ -883,18 +890,6 @@ __global__ void k_solid_columns(int nx, int ny, int nz, float dx, const float* _
   out[c] = (float)(s * (d * d * d));
 }
 
-// The rigid motion of a solid: translation v, rotation w (rad/s) about c.
-struct Rigid {
-  float v[3], w[3], c[3];
-};
-// wall_velocity (delta3d.rs:75-82): component `axis` of v + w x (x - c).
-__device__ __forceinline__ float wall_velocity(const Rigid& R, int axis, float x0, float x1, float x2) {
-  const float r0 = x0 - R.c[0], r1 = x1 - R.c[1], r2 = x2 - R.c[2];
-  if (axis == 0) return R.v[0] + (R.w[1] * r2 - R.w[2] * r1);
-  if (axis == 1) return R.v[1] + (R.w[2] * r0 - R.w[0] * r2);
-  return R.v[2] + (R.w[0] * r1 - R.w[1] * r0);
-}
-
 // delta3d.rs:412-441: a face the new cut closes loses its velocity; a face it opens starts at the
 // wall's velocity at the face centre.
 __global__ void k_wall_faces(int nx, int ny, int nz, float dx, const float* __restrict__ ou, const float* __restrict__ ov,
@@ -1322,6 +1317,10 @@ int fd3_set_solid_rigid(fd3_volume* V, const float* solid, size_t len, const flo
   LAUNCH(V, k_seal_isolated, V->n, C);
   Rigid R;
   for (int a = 0; a < 3; ++a) { R.v[a] = velocity[a]; R.w[a] = angular[a]; R.c[a] = center[a]; }
+  V->motion = R;
+  const bool spins = angular[0] != 0.f || angular[1] != 0.f || angular[2] != 0.f;
+  const bool moves = velocity[0] != 0.f || velocity[1] != 0.f || velocity[2] != 0.f;
+  V->wall = spins ? 2 : (moves ? 1 : 0);
   LAUNCH(V, k_wall_faces, (long long)V->nu + V->nv + V->nw, V->nx, V->ny, V->nz, V->dx, (const float*)V->ou,
          (const float*)V->ov, (const float*)V->ow, (const float*)V->sv_u, (const float*)V->sv_v,
          (const float*)V->sv_w, V->u, V->v, V->w, R);

@@ -175,7 +175,17 @@ struct Cut3 {
   bool has_base = false;
   Base3 base;
   bool piercing = false;
+  // the solid's rigid motion, set by set_solid_rigid (delta3d_cut.rs:42-46; delta3d.rs:408-410)
+  float solid_velocity[3] = {0.f, 0.f, 0.f}, solid_angular[3] = {0.f, 0.f, 0.f}, solid_center[3] = {0.f, 0.f, 0.f};
 };
+
+// delta3d.rs:75-82: the axis component of the rigid wall velocity V + W x (x - c) at x.
+static R wall_velocity(const float vel[3], const float ang[3], const float cen[3], int axis, R x0, R x1, R x2) {
+  R r0 = x0 - (R)cen[0], r1 = x1 - (R)cen[1], r2 = x2 - (R)cen[2];
+  if (axis == 0) return (R)vel[0] + ((R)ang[1] * r2 - (R)ang[2] * r1);
+  if (axis == 1) return (R)vel[1] + ((R)ang[2] * r0 - (R)ang[0] * r2);
+  return (R)vel[2] + ((R)ang[0] * r1 - (R)ang[1] * r0);
+}
 
 // delta3d_cut.rs:85-110
 std::vector<R> corners(const Domain3& d, const R* bottom) {
@@ -985,9 +995,45 @@ struct Volume3 {
     }
   }
 
-  // delta3d.rs:747-763 and 806-855 (a solid at rest: the moving-wall terms are zero)
+  // The flux of a moving solid through the parts of a cell's faces that it covers (base aperture
+  // minus aperture): in rotation, at the wall's velocity at each face centre; in translation, at
+  // the solid's velocity (delta3d.rs:824-852).  Zero terms are not added: a solid at rest, or a
+  // volume without the bottom-only base, leaves the divergence as it is.
+  bool wall_moves() const {
+    if (!has_cut || !g.has_base) return false;
+    for (int a = 0; a < 3; ++a)
+      if (g.solid_angular[a] != 0.f || g.solid_velocity[a] != 0.f) return true;
+    return false;
+  }
+  R wall_flux(size_t i, size_t j, size_t k) const {
+    const Base3& b = g.base;
+    const R dx = d.dx;
+    auto cu = [&](size_t f) { return b.open_u[f] - g.open_u[f]; };
+    auto cv = [&](size_t f) { return b.open_v[f] - g.open_v[f]; };
+    auto cw = [&](size_t f) { return b.open_w[f] - g.open_w[f]; };
+    if (g.solid_angular[0] != 0.f || g.solid_angular[1] != 0.f || g.solid_angular[2] != 0.f) {
+      auto pw = [&](int axis, R x0, R x1, R x2) {
+        return wall_velocity(g.solid_velocity, g.solid_angular, g.solid_center, axis, x0, x1, x2);
+      };
+      const R xc = ((R)i + (R)0.5) * dx, yc = ((R)j + (R)0.5) * dx, zc = ((R)k + (R)0.5) * dx;
+      const R x0 = (R)i * dx, x1 = (R)(i + 1) * dx;
+      const R y0 = (R)j * dx, y1 = (R)(j + 1) * dx;
+      const R z0 = (R)k * dx, z1 = (R)(k + 1) * dx;
+      const R fx = cu(fu(i + 1, j, k)) * pw(0, x1, yc, zc) - cu(fu(i, j, k)) * pw(0, x0, yc, zc);
+      const R fy = cv(fv(i, j + 1, k)) * pw(1, xc, y1, zc) - cv(fv(i, j, k)) * pw(1, xc, y0, zc);
+      const R fz = cw(fw(i, j, k + 1)) * pw(2, xc, yc, z1) - cw(fw(i, j, k)) * pw(2, xc, yc, z0);
+      return (fx + fy + fz) / dx;
+    }
+    const R x = cu(fu(i + 1, j, k)) - cu(fu(i, j, k));
+    const R y = cv(fv(i, j + 1, k)) - cv(fv(i, j, k));
+    const R z = cw(fw(i, j, k + 1)) - cw(fw(i, j, k));
+    return ((R)g.solid_velocity[0] * x + (R)g.solid_velocity[1] * y + (R)g.solid_velocity[2] * z) / dx;
+  }
+
+  // delta3d.rs:747-763 and 806-855
   void divergence(const R* uu, const R* vv, const R* ww, R* out) const {
     R dx = d.dx;
+    const bool moving = wall_moves();
     for_cells([&](size_t i, size_t j, size_t k) {
       size_t cc = c(i, j, k);
       if (has_cut) {
@@ -999,6 +1045,7 @@ struct Volume3 {
         R fb = g.open_w[fw(i, j, k)] * ww[fw(i, j, k)];
         R ft = g.open_w[fw(i, j, k + 1)] * ww[fw(i, j, k + 1)];
         out[cc] = ((fr - fl + ft - fb) + (fk - ff)) / dx;
+        if (moving) out[cc] += wall_flux(i, j, k);
       } else {
         R fl = uu[fu(i, j, k)], fr = uu[fu(i + 1, j, k)];
         R ff = vv[fv(i, j, k)], fk = vv[fv(i, j + 1, k)];
@@ -2211,14 +2258,6 @@ int od3_configure_with_solid(const od3_domain* dom, float rho, float g, const fl
   return OK;
 }
 
-// delta3d.rs:75-82: the axis component of the rigid wall velocity V + W x (x - c) at x.
-static R wall_velocity(const float vel[3], const float ang[3], const float cen[3], int axis, R x0, R x1, R x2) {
-  R r0 = x0 - (R)cen[0], r1 = x1 - (R)cen[1], r2 = x2 - (R)cen[2];
-  if (axis == 0) return (R)vel[0] + ((R)ang[1] * r2 - (R)ang[2] * r1);
-  if (axis == 1) return (R)vel[1] + ((R)ang[2] * r0 - (R)ang[0] * r2);
-  return (R)vel[2] + ((R)ang[0] * r1 - (R)ang[1] * r0);
-}
-
 // set_solid_rigid (delta3d.rs:382-509): the solid moved as a rigid body.  The cut is redone from
 // the bottom-only base; a face that opens takes the wall's normal velocity at its centre, a face
 // that closes loses its own; the solid volume a column gains raises its surface (compensated f32
@@ -2242,6 +2281,11 @@ int od3_set_solid_rigid(Volume3* v, const float* solid, uint64_t len, const floa
   v->saved_u = g.open_u; v->saved_v = g.open_v; v->saved_w = g.open_w;
   g.frac = base.frac; g.open_u = base.open_u; g.open_v = base.open_v; g.open_w = base.open_w; g.floor = base.floor;
   add_solid(g, d, solid);
+  for (int a = 0; a < 3; ++a) {
+    g.solid_velocity[a] = vel[a];
+    g.solid_angular[a] = ang[a];
+    g.solid_center[a] = cen[a];
+  }
   const R dx = d.dx;
   for (size_t k = 0; k < nz; ++k) {
     for (size_t j = 0; j < ny; ++j)
