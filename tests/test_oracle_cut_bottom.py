@@ -170,3 +170,14 @@ def test_a_surface_too_close_to_the_cut_bottom_is_refused():
     w = volume(NX, NY, NZ, DX, np.full(NX * NY, 0.3, np.float32))
     w.set_free_surface(np.full(NX * NY, 1.4, np.float32), 1.4)
     w.step_surface_mobile(2000, 4000)
+
+
+@pytest.mark.parametrize("bottom,kind", [(np.full(23, 0.3, np.float32), "Shape"),
+                                         (np.full(24, -0.1, np.float32), "NotFinite"),
+                                         (np.full(24, 2.5, np.float32), "NotFinite")])
+def test_a_bottom_it_cannot_hold_is_refused(bottom, kind):
+    """tests_delta3d.rs:871-891: 6 x 4 x 5 cells of 0.5 m (z0 = 2.5 m): a bottom of the wrong size
+    (Shape), below 0 or at the lid (NotFinite, the reference's code for a height outside [0, z0[)."""
+    with pytest.raises(O.OracleError) as e:
+        volume(6, 4, 5, 0.5, bottom)
+    assert e.value.kind == kind
