@@ -708,12 +708,6 @@ def run_b200(args):
         dist.destroy_process_group()
 
 
-def snake_owner(k: int, world: int) -> int:
-    """Rank of the k-th patch in decreasing cost: 0, 1, ..., w-1, w-1, ..., 0, 0, 1, ..."""
-    q, r = divmod(k, world)
-    return r if q % 2 == 0 else world - 1 - r
-
-
 def run_patches(args):
     """Batched patches: every rank projects its share of the seeded patch set (dealt by decreasing
     size) through fd3_project_batch, after the autotuner has picked the options per size class.
@@ -728,8 +722,7 @@ def run_patches(args):
     B.build()
     ps = batch.patch_scenes(args.patches, seed=3)
     cells = [p["nx"] * p["ny"] * p["nz"] for p in ps]
-    order = sorted(range(len(ps)), key=lambda i: -cells[i])
-    mine = [ps[i] for k, i in enumerate(order) if snake_owner(k, world) == rank]
+    mine = [ps[i] for i in batch.deal(cells, world, rank)]
     tuned = batch.autotune(batch.by_class(mine))
     vols, inputs, sk = [], [], []
     for p in mine:
@@ -764,14 +757,8 @@ def run_patches(args):
         clocks.mark(False)
     launches = sum(v.kernel_launches() for v in vols) - launches0
     assert all(x == 0 for x in st), st
-    ms_total = max_over_ranks(sum(ms), world)
     my_ci = sum(p["nx"] * p["ny"] * p["nz"] * r.iterations for p, r in zip(mine, reps))
-    ci = my_ci
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([float(my_ci)], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t)
-        ci = float(t.item())
+    ms_total, ci = batch.reduce_totals(sum(ms), my_ci, world, device="cuda")
     its = [r.iterations for r in reps]
     if rank == 0:
         cpu = None

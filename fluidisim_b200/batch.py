@@ -143,6 +143,34 @@ def autotune(scenes_by_class: dict, repeats: int = 3, timer=None) -> dict:
     return out
 
 
+def snake_owner(k: int, world: int) -> int:
+    """Rank of the k-th patch in decreasing cost: 0, 1, ..., w-1, w-1, ..., 0, 0, 1, ..."""
+    q, r = divmod(k, world)
+    return r if q % 2 == 0 else world - 1 - r
+
+
+def deal(cells, world: int, rank: int) -> list:
+    """The indices of the patches rank `rank` projects: patches sorted by decreasing cell count
+    (ties by index) and dealt in snake order, so each rank gets every patch once and the ranks'
+    cell loads differ by at most one patch.  No data moves between ranks."""
+    order = sorted(range(len(cells)), key=lambda i: (-cells[i], i))
+    return [i for k, i in enumerate(order) if snake_owner(k, world) == rank]
+
+
+def reduce_totals(ms: float, cells_iterations: float, world: int, device="cpu"):
+    """The two collectives of the sharded patch run: the slowest rank's device time (max) and the
+    cells x iterations of all ranks (sum).  One rank returns its own values unchanged."""
+    if world == 1:
+        return float(ms), float(cells_iterations)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    c = torch.tensor([float(cells_iterations)], dtype=torch.float64, device=device)
+    dist.all_reduce(c, op=dist.ReduceOp.SUM)
+    return float(t.item()), float(c.item())
+
+
 def by_class(scene_list) -> dict:
     out = {name: [] for name, _, _ in SIZE_CLASSES}
     for s in scene_list:

@@ -2008,11 +2008,23 @@ constexpr int kMaxDevices = 64;
 std::mutex g_noalloc_mutex;
 void* g_noalloc_addr[kMaxDevices] = {};
 
-// The device address of g_noalloc_scratch on the current device, looked up once per device (in
-// host code the symbol is only a host-side stand-in, not a device address).
-int noalloc_scratch(NoAllocScratch* out) {
-  int dev = 0;
-  CK(cudaGetDevice(&dev));
+// Makes `dev` the calling thread's current device for one scope and restores the previous one.
+struct ScopedDevice {
+  int prev = -1;
+  cudaError_t err = cudaSuccess;
+  explicit ScopedDevice(int dev) {
+    err = cudaGetDevice(&prev);
+    if (err == cudaSuccess && prev != dev) err = cudaSetDevice(dev);
+    else if (err == cudaSuccess) prev = -1;  // already current: nothing to restore
+  }
+  ~ScopedDevice() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+// The device address of g_noalloc_scratch on device `dev` (which must be current), looked up once
+// per device: in host code the symbol is only a host-side stand-in, not a device address.
+int noalloc_scratch(int dev, NoAllocScratch* out) {
   if (dev < 0 || dev >= kMaxDevices) return FD3_ERR_NO_DEVICE;
   std::lock_guard<std::mutex> lock(g_noalloc_mutex);
   if (!g_noalloc_addr[dev]) {
@@ -2098,8 +2110,12 @@ extern "C" int fd3_assemble_pressure_problem_noalloc(fd3_volume* V, const float*
   if (len != (size_t)V->n) return FD3_ERR_DOMAIN;
   if (len > (size_t)kNoAllocMaxCells) return FD3_ERR_SCRATCH_LIMIT;
   if (!std::isfinite(scale)) return FD3_ERR_NOT_FINITE;
+  // the volume's device is made current for the call (and the caller's restored on return), so the
+  // scratch looked up, the memset and the launch all belong to the device the volume lives on
+  ScopedDevice on(V->device);
+  if (on.err != cudaSuccess) return cuda_fail(on.err, "cudaSetDevice", __LINE__);
   NoAllocScratch sc;
-  TRY(noalloc_scratch(&sc));
+  TRY(noalloc_scratch(V->device, &sc));
   // the counter, the flag and the sum start at zero on every call (the array keeps the last call's
   // contents); the partials are all overwritten
   CK(cudaMemsetAsync(sc.counter, 0, 24, V->stream));

@@ -272,20 +272,23 @@ int fd3_apply_pressure_operator_for_trials(fd3_volume* v, const float* p, float*
 int fd3_assemble_pressure_problem_for_trials(fd3_volume* v, const float* divergence, float scale,
                                              float* rhs, float* prec, size_t len);
 /* The pressure-problem assembly for callers that cannot allocate device memory when they call:
- * e.g. a host whose memory arena is sealed once set up (the reference's own rule: nothing is
- * allocated after `seal()`), or a real-time loop where a cudaMalloc would stall the frame.
- * No counterpart in the reference (its trial hook above allocates nothing either, but this
- * library's version stages through the volume's work buffers).  Device pointers in and out:
- * d_divergence (len cells) -> d_rhs and d_prec, as rhs_mobile3 (delta3d_mobile.rs:215-241)
- * computes them, plus |rhs|^2 in f64 written to *rhs_norm2 (host).  The volume's own buffers
- * are not touched.
- * It allocates nothing: its scratch is a static device array of 128 KiB + 256 B in this library
- * (held on every GPU that loads it until exit), so volumes above 4,194,304 cells are refused with
- * FD3_ERR_SCRATCH_LIMIT.  The first call on a device looks the scratch's device address up
- * (cudaGetSymbolAddress) and should come before any stream capture.  All calls share the one
- * scratch array: calls that overlap on the GPU (other streams, other threads) race; each call
- * clears the parts that must start at zero.  A non-finite divergence gives FD3_ERR_NOT_FINITE
- * (the outputs are then written anyway). */
+ * a host whose memory arena is sealed once it is set up, or a real-time loop in which a cudaMalloc
+ * would stall a frame.  It has no counterpart in the reference.
+ * Inputs and outputs are device pointers of `len` cells on the volume's device: d_divergence in;
+ * d_rhs (the right-hand side: scale times the divergence plus the surface-ghost terms of each wet
+ * row, 0 on dry cells) and d_prec (1 / the row's diagonal, 0 on dry cells) out; |rhs|^2 in f64
+ * written to *rhs_norm2 (host memory).  The volume's own buffers are not touched.
+ * Ordering: the call runs on the volume's stream (fd3_set_stream) and does not wait for the
+ * caller's other streams, so work that writes d_divergence must be complete before the call; the
+ * call synchronises the volume's stream before it returns.  The volume's device is made current
+ * for the call and the caller's current device is restored.
+ * It allocates nothing: its scratch is a static device array of 128 KiB + 256 B in this library,
+ * held on every GPU that loads it until the process exits, so volumes above 4,194,304 cells are
+ * refused with FD3_ERR_SCRATCH_LIMIT.  The first call on a device looks the scratch's device
+ * address up (cudaGetSymbolAddress) and should come before any stream capture.  All calls share
+ * the one scratch array and it keeps the last call's contents: each call clears the parts that
+ * must start at zero, and calls that overlap on the GPU (other streams, other threads) race.
+ * A non-finite divergence gives FD3_ERR_NOT_FINITE (the outputs are then written anyway). */
 int fd3_assemble_pressure_problem_noalloc(fd3_volume* v, const float* d_divergence, float scale, float* d_rhs,
                                           float* d_prec, size_t len, double* rhs_norm2);
 /* v_cycle3 (delta3d_multigrid.rs:393) on `x`, set up as tests_delta3d.rs:1840-1873 does
