@@ -52,6 +52,13 @@ BYTES_PER_CELL = {
     "kx_fine_restrict": 2 + 4 + 4 + 0.5,
     "kx_fine_post1": 2 + 4 + 4 + 4 + 0.5 + 4,
     "kx_fine_post2_rz": 2 + 4 + 4 + 4 + 4,
+    # the same passes with four cells per thread (f64 mode, the default when nx % 4 == 0, f32 storage)
+    "kq_dir_apply_dot": 2 + 4 + 4 + 4 + 4,
+    "kq_fine_pre": 2 + 4 + 4 + 4,
+    "kq_fine_restrict": 2 + 4 + 4 + 0.5,
+    "kq_fine_post1": 2 + 4 + 4 + 4 + 0.5 + 4,
+    "kq_fine_post2_rz": 2 + 4 + 4 + 4 + 4,
+    "kq_residual": 2 + 4 * 3,
     # one-cell-per-thread kernels (ordered mode, and f64 mode with kernels = 1)
     "k_dir_apply_dot": 2 + 4 + 4 + 4 + 4,
     "k_update_rn": 4 * 6,
@@ -91,33 +98,85 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi samples of the SM clock and throttle reasons, kept only for the timed region.
+    """SM clock and clock-event reasons sampled DURING the timed region.
 
-    The sampler starts before the warm-up (nvidia-smi needs about half a second to produce its
-    first line); `mark(True)` / `mark(False)` bracket the timed region and only lines that arrive
-    between the two marks are summarised."""
+    NVML is polled from a thread every `period` seconds (2 ms by default), so even a timed region
+    of tens of milliseconds gets samples; the GPU is found by its PCI bus id (NVML numbers GPUs
+    without CUDA_VISIBLE_DEVICES).  Without NVML the sampler falls back to `nvidia-smi -lms 100`.
+    `mark(True)` / `mark(False)` bracket the timed region; only samples taken between the two marks
+    are summarised.  Reading clocks changes no GPU setting."""
 
     FIELDS = "clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown," \
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown," \
              "clocks_event_reasons.sw_power_cap"
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
-    def __init__(self, index: int):
+    def __init__(self, index: int, period: float = 0.002):
         self.index = index
+        self.period = period
         self.proc = None
-        self.lines = []
+        self.nvml = None
+        self.handle = None
+        self.lines = []     # nvidia-smi: (t, csv line)
+        self.samples = []   # NVML: (t, sm_mhz, max_mhz, power_w, reasons)
         self.t0 = None
         self.t1 = None
+        self.stop = threading.Event()
+        self.source = "none"
+
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        self.nvml = pynvml
+        try:
+            import torch
+            pr = torch.cuda.get_device_properties(self.index)
+            bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+            return pynvml.nvmlDeviceGetHandleByPciBusId(bus.encode())
+        except Exception:
+            return pynvml.nvmlDeviceGetHandleByIndex(self.index)
 
     def __enter__(self):
+        try:
+            self.handle = self._nvml_handle()
+            self.source = "nvml"
+            self.thread = threading.Thread(target=self._poll, daemon=True)
+            self.thread.start()
+            return self
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100",
                  "-i", str(self.index)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.source = "nvidia-smi"
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
         except Exception:
             self.proc = None
         return self
+
+    def _poll(self):
+        n = self.nvml
+        bits = [n.nvmlClocksEventReasonHwSlowdown, n.nvmlClocksEventReasonHwThermalSlowdown,
+                n.nvmlClocksEventReasonSwThermalSlowdown, n.nvmlClocksEventReasonSwPowerCap]
+        try:
+            smax = float(n.nvmlDeviceGetMaxClockInfo(self.handle, n.NVML_CLOCK_SM))
+        except Exception:
+            smax = float("nan")
+        while not self.stop.is_set():
+            try:
+                sm = float(n.nvmlDeviceGetClockInfo(self.handle, n.NVML_CLOCK_SM))
+                reasons = int(n.nvmlDeviceGetCurrentClocksEventReasons(self.handle))
+                try:
+                    power = n.nvmlDeviceGetPowerUsage(self.handle) / 1000.0
+                except Exception:
+                    power = float("nan")
+                active = {name for name, b in zip(self.NAMES, bits) if reasons & b}
+                self.samples.append((time.monotonic(), sm, smax, power, active))
+            except Exception:
+                pass
+            self.stop.wait(self.period)
 
     def _read(self):
         for line in self.proc.stdout:
@@ -130,18 +189,30 @@ class ClockSampler:
             self.t1 = time.monotonic()
 
     def __exit__(self, *exc):
+        self.stop.set()
         if self.proc:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except Exception:
                 self.proc.kill()
+        if self.nvml is not None:
+            try:
+                self.thread.join(timeout=2)
+                self.nvml.nvmlShutdown()
+            except Exception:
+                pass
 
     def summary(self):
         sm, smax, power, reasons = [], [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         t0 = self.t0 if self.t0 is not None else float("-inf")
         t1 = self.t1 if self.t1 is not None else float("inf")
+        for t, a, b, pw, active in self.samples:
+            if t0 <= t <= t1:
+                sm.append(a)
+                smax.append(b)
+                power.append(pw)
+                reasons |= active
         for t, line in self.lines:
             if not (t0 <= t <= t1):
                 continue
@@ -154,13 +225,13 @@ class ClockSampler:
                 power.append(float(parts[2]))
             except ValueError:
                 continue
-            for name, val in zip(names, parts[3:7]):
+            for name, val in zip(self.NAMES, parts[3:7]):
                 if val.lower().startswith("active"):
                     reasons.add(name)
         if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0, "source": self.source}
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
-                "power_w_max": max(power), "samples": len(sm)}
+                "power_w_max": max(power), "samples": len(sm), "source": self.source}
 
 
 def dist_setup(gpus: int):
@@ -208,6 +279,11 @@ WORKLOAD_NAMES = {
 }
 
 
+def workload_label(workload: str, size: int) -> str:
+    """The workload name both arms print (the same scene, solver recipe and stopping rule)."""
+    return WORKLOAD_NAMES[workload].format(n=size) + ": multigrid-PCG projection (reference V-cycle recipe)"
+
+
 def run_reference(args):
     """The reference arm: the CPU oracle (a restatement of the reference's Rust projection, whose own
     toolchain is absent here) on the host cores, same scene, metric and unit."""
@@ -246,8 +322,7 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": "projections/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": f"synthetic (seeded {args.workload} scene)",
-        "config": {"workload": WORKLOAD_NAMES[args.workload].format(n=args.size)
-                   + ": multigrid-PCG projection (reference recipe)",
+        "config": {"workload": workload_label(args.workload, args.size),
                    "cells": s["nx"] * s["ny"] * s["nz"], "solver": "mgpcg", "iterations": rep["iterations"],
                    "rel_residual": rep["residual"], "parallelism": "host threads"},
         "cpu_baseline": {"value": value, "unit": "projections/s", "cores": threads, "kind": "port",
@@ -278,8 +353,18 @@ def cpu_baseline_sample(workload: str, size: int, budget_s: float = 20.0):
         v.project_mobile(scale, k1, 4000)
         times.append(time.perf_counter() - t0)
     ms = 1e3 * sum(times) / len(times)
+    # the reference's own semantics: one thread (its reductions are serial by design)
+    O.set_threads(1)
+    v.set_velocity(s["u"], s["v"], s["w"])
+    v.set_free_surface(s["eta"], s["rest"])
+    t0 = time.perf_counter()
+    v.project_mobile(scale, k1, 4000)
+    one = time.perf_counter() - t0
+    O.set_threads(threads)
     return {"value": 1e3 / ms, "unit": "projections/s", "cores": threads, "kind": "port",
-            "sample": f"{len(times)} full {size}^3 {workload} projections (same scene), oracle with OpenMP"}
+            "sample": f"{len(times)} full {size}^3 {workload} projections (same scene), oracle with OpenMP",
+            "single_thread": {"value": 1.0 / one, "unit": "projections/s", "cores": 1,
+                              "sample": f"1 full {size}^3 {workload} projection, oracle on one thread"}}
 
 
 def fp64_pressure_check(workload: str, size: int, pressures: dict, max_cells: int = 128 ** 3):
@@ -543,7 +628,7 @@ def run_b200(args):
     scale, k1 = scenes.projection_scalars(s)
     stream = torch.cuda.Stream()
     vol = Volume3.configure_with_solid(s["nx"], s["ny"], s["nz"], s["dx"], s["rho"], s["g"], s["bottom"], s["solid"])
-    vol.set_options(reduction=REDUCE_F64, use_graphs=args.graphs)
+    vol.set_options(reduction=REDUCE_F64, use_graphs=args.graphs, kernels=args.kernels)
     vol.set_stream(stream.cuda_stream)
     vol.enable_multigrid()
     vol.set_free_surface(s["eta"], s["rest"])
@@ -566,7 +651,7 @@ def run_b200(args):
         for _ in range(args.warmup):
             rep = step()
         torch.cuda.synchronize()
-        while time.monotonic() - t_warm < 1.0:   # let nvidia-smi produce its first lines
+        while clocks.source == "nvidia-smi" and time.monotonic() - t_warm < 1.0:  # its first lines
             rep = step()
             torch.cuda.synchronize()
         barrier(world)
@@ -680,8 +765,7 @@ def run_b200(args):
             "impl": "b200", "metric": METRIC, "value": value, "unit": "projections/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": f"synthetic (seeded {args.workload} scene)",
-            "config": {"workload": WORKLOAD_NAMES[args.workload].format(n=args.size)
-                       + ": multigrid-PCG projection (reference V-cycle recipe)",
+            "config": {"workload": workload_label(args.workload, args.size),
                        "cells": cells, "solver": "mgpcg", "reduction": "f64", "iterations": rep.iterations,
                        "rel_residual": rep.residual, "divergence_plain": rep.divergence_plain,
                        "l2": "flushed between steps (256 MiB write outside the timed events)",
@@ -693,6 +777,9 @@ def run_b200(args):
                          "share_of_step": ms / total_prof if total_prof else None},
             "kernels": {n: {"launches": c, "ms_per_step": round(m / prof_steps, 5)}
                         for n, c, m in sorted(prof, key=lambda e: -e[2])[:14]},
+            "kernels_source": f"an instrumented replay of {prof_steps} steps right after the timed region: the "
+                              "loop driven from the host without its CUDA graph, CUDA events around every launch "
+                              "(the kernel table and roofline.avg_launch_ms come from it)",
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "projections/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,
@@ -966,6 +1053,9 @@ def main():
                     help="1: also time a mobile step, the second-order advection, a solid re-cut and a level change")
     ap.add_argument("--train-samples", type=int, default=20000,
                     help="training samples of the learned preconditioner (20,000 at 64^3, as config 4 asks)")
+    ap.add_argument("--kernels", type=int, default=0,
+                    help="fine-level kernel family (fd3_options.kernels): 0 the default (four cells per thread when "
+                         "nx % 4 == 0), 3 two cells per thread, 2 one cell per thread in the same blocking")
     ap.add_argument("--graphs", type=int, default=1,
                     help="1: the inner loop as a CUDA graph with a WHILE node; 0: host-driven (for ncu launch lists)")
     args = ap.parse_args()

@@ -19,12 +19,13 @@
 #include <new>
 #include <string>
 #include <thread>
+#include <type_traits>
 #include <utility>
 #include <vector>
 
 #include "../../include/fluidisim_delta3d.h"
 #include "fd3_cut.cuh"
-#include "fd3_zmarch2.cuh"
+#include "fd3_zmarch4.cuh"
 #include "fd3_linear.cuh"
 #include "fd3_levels.cuh"
 
@@ -173,14 +174,16 @@ struct fd3_volume {
   }
   bool ord() const { return opt.reduction == FD3_REDUCE_ORDERED_F32; }
   bool blocked() const { return !ord() && opt.kernels != 1; }
-  bool paired() const { return blocked() && opt.kernels == 0 && nx % 2 == 0; }
+  bool paired() const { return blocked() && (opt.kernels == 0 || opt.kernels == 3) && nx % 2 == 0; }
+  // four cells per thread: the default family for an nx divisible by 4 with f32 storage
+  bool quad() const { return paired() && opt.kernels == 0 && nx % 4 == 0 && opt.storage != FD3_STORAGE_F16; }
   bool mg_on() const { return has_mg && !linear; }  // the linear path has no multigrid
   // FP16 storage of the V-cycle vectors (fd3_set_options accepts it only with the paired kernels)
   bool half() const { return opt.storage == FD3_STORAGE_F16 && paired() && mg_on(); }
   int loop_key() const {
     return (ord() ? 1 : 0) | (mg_on() ? 2 : 0) | (blocked() ? 4 : 0) | (opt.no_overlap ? 8 : 0) | (linear ? 16 : 0) |
            (paired() ? 32 : 0) | (half() ? 64 : 0) | (sparse ? 128 : 0) |  // the captured Geo holds the set's mask
-           (opt.no_tile_skip ? 256 : 0);
+           (opt.no_tile_skip ? 256 : 0) | (quad() ? 512 : 0);
   }
   Red red() const { return Red{p64, p32, count}; }
 };
@@ -413,6 +416,44 @@ void paired_vcycle(fd3_volume* V, int gate, int op) {
   else paired_vcycle<K2, float>(V, gate, op);
 }
 
+// The tiling of the four-cells-per-thread kernels: QX lanes per row (a tile 4 QX cells wide, 256 /
+// QX rows), K4 layers per CTA (8 when that still gives two waves of CTAs at two per SM, else 4).
+template <int N>
+using IC = std::integral_constant<int, N>;
+inline int quad_qx(int nx) { return nx >= 128 ? 32 : 16; }
+template <class F>
+void quad_dispatch(const fd3_volume* V, F f) {
+  const bool wide = quad_qx(V->nx) == 32;
+  const int k8 = wide ? zblocks4<32>(V->nx, V->ny, V->nz, 8) : zblocks4<16>(V->nx, V->ny, V->nz, 8);
+  const bool deep = k8 >= 2 * 2 * 148;
+  if (wide) { if (deep) f(IC<32>{}, IC<8>{}); else f(IC<32>{}, IC<4>{}); }
+  else { if (deep) f(IC<16>{}, IC<8>{}); else f(IC<16>{}, IC<4>{}); }
+}
+
+// The fine passes of the V-cycle with the four-cells-per-thread kernels (f32 storage).
+void quad_vcycle(fd3_volume* V, int gate, int op) {
+  quad_dispatch(V, [&](auto qx, auto k4) {
+    constexpr int QX = decltype(qx)::value, K4 = decltype(k4)::value;
+    Geo G = V->geo();
+    const Scalars* S = V->dS;
+    const bool levels = !V->levels.empty();
+    Lev L0 = levels ? V->levels[0] : Lev{};
+    const unsigned short* codes = V->codes;
+    const int zb = zblocks4<QX>(V->nx, V->ny, V->nz, K4);
+    launch_grid(V, "kq_fine_pre", zb, Z4T, kq_fine_pre<QX, K4>, G, codes, (const float*)V->prec,
+                (const float*)V->res, V->z, S, gate);
+    if (levels) {
+      launch_grid(V, "kq_fine_restrict", zb, Z4T, kq_fine_restrict<QX, K4>, G, codes, (const float*)V->res,
+                  (const float*)V->z, L0, S, gate);
+      coarse_cycle(V, gate);
+    }
+    launch_grid(V, "kq_fine_post1", zb, Z4T, kq_fine_post1<QX, K4>, G, codes, (const float*)V->prec,
+                (const float*)V->res, (const float*)V->z, L0, levels ? 1 : 0, V->z2, S, gate);
+    launch_grid(V, "kq_fine_post2_rz", zb, Z4T, kq_fine_post2_rz<QX, K4>, G, codes, (const float*)V->prec,
+                (const float*)V->res, (const float*)V->z2, V->z, V->red(), V->dS, gate, op);
+  });
+}
+
 // v_cycle3 (delta3d_multigrid.rs:393-429) with res.z at its end (op FIN_RZ_PRIME or FIN_RZ_ITER);
 // z = M^-1 res is left in V->z.
 void vcycle(fd3_volume* V, int gate, int op) {
@@ -421,6 +462,10 @@ void vcycle(fd3_volume* V, int gate, int op) {
   const bool levels = !V->levels.empty();
   Lev L0 = levels ? V->levels[0] : Lev{};
   const unsigned short* codes = V->codes;
+  if (V->quad()) {  // 2.5-D blocked kernels, four cells per thread (f64 reductions, f32 storage)
+    quad_vcycle(V, gate, op);
+    return;
+  }
   if (V->paired()) {  // 2.5-D blocked kernels, two cells per thread (f64 reductions)
     if (pick_k2(V->nx, V->ny, V->nz) == 8) paired_vcycle<8>(V, gate, op);
     else paired_vcycle<4>(V, gate, op);
@@ -481,7 +526,16 @@ void iteration(fd3_volume* V, int parity) {
   if (V->mg_on()) {
     float* din = parity ? V->dir2 : V->dir;
     float* dout = parity ? V->dir : V->dir2;
-    if (V->paired()) {
+    if (V->quad()) {
+      quad_dispatch(V, [&](auto qx, auto k4) {
+        constexpr int QX = decltype(qx)::value, K4 = decltype(k4)::value;
+        launch_grid(V, "kq_dir_apply_dot", zblocks4<QX>(V->nx, V->ny, V->nz, K4), Z4T, kq_dir_apply_dot<QX, K4>, G,
+                    (const unsigned short*)V->codes, (const float*)V->z, (const float*)din, dout, V->tmp, V->red(),
+                    V->dS);
+      });
+      LAUNCH_G(V, kv_update_rn, update_blocks(V->n), TPB, V->n, V->p, V->res, (const float*)dout,
+               (const float*)V->tmp, V->red(), V->dS, update_mask(V), V->ncol);
+    } else if (V->paired()) {
       const int k2 = pick_k2(V->nx, V->ny, V->nz);
       const int zb = zblocks2(V->nx, V->ny, V->nz, k2);
       const unsigned short* codes = V->codes;
@@ -609,6 +663,15 @@ void correct(fd3_volume* V, float k1) {
 // it (f64 reductions), else one cell per thread (the ordered mode's chunk order).
 void residual(fd3_volume* V, int op) {
   Geo G = V->geo();
+  if (V->quad()) {
+    quad_dispatch(V, [&](auto qx, auto k4) {
+      constexpr int QX = decltype(qx)::value, K4 = decltype(k4)::value;
+      launch_grid(V, "kq_residual", zblocks4<QX>(V->nx, V->ny, V->nz, K4), Z4T, kq_residual<QX, K4>, G,
+                  (const unsigned short*)V->codes, (const float*)V->p, (const float*)V->rhs, V->res, V->red(), V->dS,
+                  op);
+    });
+    return;
+  }
   if (V->paired()) {
     const int k2 = pick_k2(V->nx, V->ny, V->nz);
     const int zb = zblocks2(V->nx, V->ny, V->nz, k2);
@@ -1346,10 +1409,11 @@ void fd3_destroy(fd3_volume* v) {
 
 int fd3_set_options(fd3_volume* v, const fd3_options* o) {
   if (!v || !o) return FD3_ERR_INVALID_ARGUMENT;
-  if (o->reduction > 1 || o->kernels > 2 || o->no_overlap > 1 || o->storage > 1 || o->no_tile_skip > 1)
+  if (o->reduction > 1 || o->kernels > 3 || o->no_overlap > 1 || o->storage > 1 || o->no_tile_skip > 1)
     return FD3_ERR_DOMAIN;
-  // FP16 storage runs on the paired fine kernels: f64 reductions, kernels = 0 and an even nx
-  if (o->storage == FD3_STORAGE_F16 && (o->reduction != FD3_REDUCE_F64 || o->kernels != 0 || v->nx % 2 != 0))
+  // FP16 storage runs on the paired fine kernels: f64 reductions, kernels = 0 or 3 and an even nx
+  if (o->storage == FD3_STORAGE_F16 &&
+      (o->reduction != FD3_REDUCE_F64 || (o->kernels != 0 && o->kernels != 3) || v->nx % 2 != 0))
     return FD3_ERR_DOMAIN;
   v->opt = *o;
   return FD3_OK;

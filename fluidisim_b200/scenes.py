@@ -207,30 +207,40 @@ def scheme_frequency(kx: float, ky: float, dx: float, nz: int, g: float, dt: flo
 # ----------------------------------------------------------------------------------------------
 # Signed distances at the nodes, (nx+1)(ny+1)(nz+1) x-fastest, negative inside (delta3d.rs:322-327).
 
-def _node_grid(nx, ny, nz, dx):
+def _node_axes(nx, ny, nz, dx):
+    """Node coordinates per axis, shaped to broadcast over the (z, y, x) node grid."""
     d = float(f32(dx))
-    z, y, x = np.meshgrid(np.arange(nz + 1) * d, np.arange(ny + 1) * d, np.arange(nx + 1) * d, indexing="ij")
-    return x, y, z
+    return (np.arange(nx + 1)[None, None, :] * d, np.arange(ny + 1)[None, :, None] * d,
+            np.arange(nz + 1)[:, None, None] * d)
 
 
 def spheres_sdf(nx, ny, nz, dx, centres, radii) -> np.ndarray:
-    """Union of spheres (centres, radii in metres), as the sphere nodes of tests_delta3d.rs:1161-1179."""
-    x, y, z = _node_grid(nx, ny, nz, dx)
-    out = np.full(x.shape, np.inf)
+    """Union of spheres (centres, radii in metres), as the sphere nodes of tests_delta3d.rs:1161-1179.
+    Each sphere's distance is evaluated by broadcasting the three axes, one z layer block at a time
+    (the same f64 operations, node by node, as on a full mesh grid)."""
+    x, y, z = _node_axes(nx, ny, nz, dx)
+    out = np.full((nz + 1, ny + 1, nx + 1), np.inf)
     for (cx, cy, cz), r in zip(centres, radii):
-        out = np.minimum(out, np.sqrt((x - cx) ** 2 + (y - cy) ** 2 + (z - cz) ** 2) - r)
+        xy = (x - cx) ** 2 + (y - cy) ** 2
+        for k0 in range(0, nz + 1, 16):
+            zz = z[k0:k0 + 16]
+            np.minimum(out[k0:k0 + 16], np.sqrt(xy + (zz - cz) ** 2) - r, out=out[k0:k0 + 16])
     return out.astype(np.float32).ravel()
 
 
 def boxes_sdf(nx, ny, nz, dx, centres, halves) -> np.ndarray:
     """Union of boxes (centre, half sizes in metres), the box distance of tests_delta3d.rs:1332-1350."""
-    x, y, z = _node_grid(nx, ny, nz, dx)
-    out = np.full(x.shape, np.inf)
+    x, y, z = _node_axes(nx, ny, nz, dx)
+    out = np.full((nz + 1, ny + 1, nx + 1), np.inf)
     for c, h in zip(centres, halves):
-        q = [np.abs(x - c[0]) - h[0], np.abs(y - c[1]) - h[1], np.abs(z - c[2]) - h[2]]
-        outside = np.sqrt(sum(np.maximum(a, 0.0) ** 2 for a in q))
-        inside = np.minimum(np.maximum(np.maximum(q[0], q[1]), q[2]), 0.0)
-        out = np.minimum(out, outside + inside)
+        qx, qy = np.abs(x - c[0]) - h[0], np.abs(y - c[1]) - h[1]
+        sx, sy = np.maximum(qx, 0.0) ** 2, np.maximum(qy, 0.0) ** 2
+        mxy = np.maximum(qx, qy)
+        for k0 in range(0, nz + 1, 16):
+            qz = np.abs(z[k0:k0 + 16] - c[2]) - h[2]
+            outside = np.sqrt(0 + sx + sy + np.maximum(qz, 0.0) ** 2)
+            inside = np.minimum(np.maximum(mxy, qz), 0.0)
+            np.minimum(out[k0:k0 + 16], outside + inside, out=out[k0:k0 + 16])
     return out.astype(np.float32).ravel()
 
 

@@ -79,7 +79,8 @@ typedef enum fd3_reduction { FD3_REDUCE_F64 = 0, FD3_REDUCE_ORDERED_F32 = 1 } fd
  *                   the FP16 range whatever the pressure scale; PCG is unchanged by that positive
  *                   scale.  The reference's outer loop (true residual, restart from b - A p,
  *                   delta3d_mobile.rs:547-588) is the defect correction that restores the 1e-6
- *                   tolerance.  Needs FD3_REDUCE_F64, kernels = 0 and an even nx. */
+ *                   tolerance.  Needs FD3_REDUCE_F64, kernels = 0 or 3 and an even nx (it runs
+ *                   on the two-cells-per-thread kernels). */
 typedef enum fd3_storage { FD3_STORAGE_F32 = 0, FD3_STORAGE_F16 = 1 } fd3_storage;
 
 typedef struct fd3_options {
@@ -87,10 +88,12 @@ typedef struct fd3_options {
   uint32_t mg_max_levels; /* coarse levels kept by fd3_enable_multigrid; 0 = every level the
                              reference's coarsening rule allows (delta3d_multigrid.rs:73-88) */
   uint32_t use_graphs;    /* 1 = run the inner PCG loop as a CUDA graph with a WHILE node */
-  uint32_t kernels;       /* fine-level kernels in f64 mode: 0 = 2.5-D blocked with two cells per thread
-                             (default; one cell per thread when nx is odd), 1 = one cell per thread
-                             (the family the ordered mode always uses), 2 = 2.5-D blocked with one
-                             cell per thread */
+  uint32_t kernels;       /* fine-level kernels in f64 mode: 0 = 2.5-D blocked, four cells per thread
+                             when nx % 4 == 0 and the storage is f32, else two cells per thread (one
+                             when nx is odd) (default); 1 = one cell per thread (the family the
+                             ordered mode always uses); 2 = 2.5-D blocked with one cell per thread;
+                             3 = 2.5-D blocked with two cells per thread.  Every family gives the same
+                             cell values; only the order of the f64 partial sums differs */
   uint32_t no_overlap;    /* 1 = launch each kernel only after the previous one completes; 0 (default)
                              = programmatic dependent launch: the next kernel is scheduled early and
                              waits on the device (results are identical either way) */

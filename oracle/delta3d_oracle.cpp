@@ -69,7 +69,12 @@ int g_threads = 1;
 // Smoother of the V-cycle: 0 = the reference's damped Jacobi (delta3d_multigrid.rs:28, 290-299);
 // 1 = red-black Gauss-Seidel (omega = 1), pre-sweeps red then black, post-sweeps black then red,
 // the coarsest level's sweeps forward then backward, so the preconditioner stays symmetric.
+// 0: damped Jacobi everywhere (the reference); 1: red-black Gauss-Seidel on every level;
+// 2: red-black on the fine level only, Jacobi on the coarse levels; 3: the converse
 int g_smoother = 0;
+bool rb_fine() { return g_smoother == 1 || g_smoother == 2; }
+bool rb_coarse() { return g_smoother == 1 || g_smoother == 3; }
+int g_transfer = 0;  // 0: the reference's 8-child mean and injection; 1: trilinear (restrict3_tri)
 
 // Storage of the V-cycle vectors.  0 = the reference's f32.  1 = the B200 library's mixed-precision
 // mode (no reference counterpart): the V-cycle runs on r / sigma, sigma = rms(r over all cells) *
@@ -638,8 +643,11 @@ void coarsen3(size_t nx, size_t ny, OpenF open, KindF kind, Level3& L) {
   row_sums(L, nullptr, L.diag.data());
 }
 
+void restrict3_tri(size_t nx, size_t ny, const R* fine, Level3& L);
+
 // delta3d_multigrid.rs:258-272
 void restrict3(size_t nx, size_t ny, const R* fine, Level3& L) {
+  if (g_transfer == 1) { restrict3_tri(nx, ny, fine, L); return; }
   size_t cx = L.nx, cy = L.ny, cz = L.nz;
 #pragma omp parallel for schedule(static) num_threads(g_threads) if (cx * cy * cz > 32768)
   for (long long kk = 0; kk < (long long)cz; ++kk) {
@@ -654,8 +662,71 @@ void restrict3(size_t nx, size_t ny, const R* fine, Level3& L) {
   }
 }
 
+// An alternative grid transfer for experiments, not the reference's (od3_set_transfer(1)):
+// cell-centred trilinear prolongation (weights 3/4, 1/4 per axis) that interpolates from active
+// coarse cells, takes air cells (kind < 0) as the value 0 and renormalises its weights over the
+// cells that are not solid or outside the level; and its adjoint restriction scaled by 1/8 (full
+// weighting in the bulk, where every coarse cell's weights sum to 8 over the fine cells).  The coarse operators
+// stay the reference's rediscretised ones.
+// The trilinear weights of fine cell (i, j, k) over its 8 candidate coarse cells, 0 where the coarse
+// cell is outside the level or not active; returns their count and fills idx / w (renormalised).
+int tri_weights(const Level3& L, size_t i, size_t j, size_t k, size_t idx[8], R w[8]) {
+  long I = (long)(i / 2), J = (long)(j / 2), K = (long)(k / 2);
+  long Io = (i & 1) ? I + 1 : I - 1, Jo = (j & 1) ? J + 1 : J - 1, Ko = (k & 1) ? K + 1 : K - 1;
+  const long xs[2] = {I, Io}, ys[2] = {J, Jo}, zs[2] = {K, Ko};
+  const R wt[2] = {(R)0.75, (R)0.25};
+  int n = 0;
+  R sum = 0;
+  for (int c = 0; c < 2; ++c)
+    for (int b = 0; b < 2; ++b)
+      for (int a = 0; a < 2; ++a) {
+        long x = xs[a], y = ys[b], z = zs[c];
+        if (x < 0 || y < 0 || z < 0 || x >= (long)L.nx || y >= (long)L.ny || z >= (long)L.nz) continue;
+        size_t cc = L.c((size_t)x, (size_t)y, (size_t)z);
+        if (L.kind[cc] == 0) continue;       // solid: no value, renormalise over the rest
+        R wq = wt[a] * wt[b] * wt[c];
+        sum += wq;
+        if (L.kind[cc] < 0) continue;        // air: the value 0 (Dirichlet), weight kept in the sum
+        idx[n] = cc;
+        w[n] = wq;
+        ++n;
+      }
+  for (int q = 0; q < n; ++q) w[q] = w[q] / sum;
+  return n;
+}
+
+void restrict3_tri(size_t nx, size_t ny, const R* fine, Level3& L) {
+  std::fill(L.r.begin(), L.r.end(), (R)0);
+  size_t nz = 2 * L.nz;
+  size_t idx[8];
+  R w[8];
+  for (size_t k = 0; k < nz; ++k)
+    for (size_t j = 0; j < ny; ++j)
+      for (size_t i = 0; i < nx; ++i) {
+        R t = fine[(k * ny + j) * nx + i];
+        int n = tri_weights(L, i, j, k, idx, w);
+        for (int q = 0; q < n; ++q) L.r[idx[q]] += w[q] * t;
+      }
+  for (auto& x : L.r) x = (R)0.125 * x;
+}
+
+void prolong_add3_tri(size_t nx, size_t ny, R* fine, const Level3& L) {
+  size_t nz = 2 * L.nz;
+  size_t idx[8];
+  R w[8];
+  for (size_t k = 0; k < nz; ++k)
+    for (size_t j = 0; j < ny; ++j)
+      for (size_t i = 0; i < nx; ++i) {
+        int n = tri_weights(L, i, j, k, idx, w);
+        R v = 0;
+        for (int q = 0; q < n; ++q) v += w[q] * L.x[idx[q]];
+        fine[(k * ny + j) * nx + i] += v;
+      }
+}
+
 // delta3d_multigrid.rs:275-287
 void prolong_add3(size_t nx, size_t ny, R* fine, const Level3& L) {
+  if (g_transfer == 1) { prolong_add3_tri(nx, ny, fine, L); return; }
   size_t cx = L.nx, cy = L.ny, cz = L.nz;
 #pragma omp parallel for schedule(static) num_threads(g_threads) if (cx * cy * cz > 32768)
   for (long long kk = 0; kk < (long long)cz; ++kk) {
@@ -692,7 +763,7 @@ void smooth3_rb(Level3& L, int color) {
 // `count` smoothing sweeps of a coarse level; `forward` orders each sweep red then black.
 void smooth_level(Level3& L, int count, bool forward) {
   for (int s = 0; s < count; ++s) {
-    if (g_smoother == 0) { smooth3(L); continue; }
+    if (!rb_coarse()) { smooth3(L); continue; }
     smooth3_rb(L, forward ? 0 : 1);
     smooth3_rb(L, forward ? 1 : 0);
   }
@@ -708,7 +779,7 @@ void coarse_cycle3(std::vector<Level3>& levels) {
     std::fill(L.x.begin(), L.x.end(), (R)0);
     if (g_storage && big(l) && l == last) {
       for (int s = 0; s < sweeps; ++s) { smooth_level(L, 1, true); round16(L.x); }
-    } else if (g_smoother == 0 || l < last) {
+    } else if (!rb_coarse() || l < last) {
       smooth_level(L, sweeps, true);
       if (big(l)) round16(L.x);
     } else { smooth_level(L, sweeps / 2, true); smooth_level(L, sweeps / 2, false); }
@@ -1166,7 +1237,7 @@ struct Volume3 {
     }
     // one fine sweep: Jacobi (the reference) or a red-black half sweep pair in the given order
     auto fine_sweep = [&](bool forward) {
-      if (g_smoother == 0) {
+      if (!rb_fine()) {
         apply_mobile3(mg.z.data(), mg.t.data());
         for (size_t q = 0; q < cells; ++q)
           if (prec[q] > 0) mg.z[q] += SMOOTH_DAMPING_3D * prec[q] * (rv[q] - mg.t[q]);
@@ -2193,7 +2264,8 @@ struct od3_domain { uint64_t nx, ny, nz; float dx; };
 
 int od3_real_bytes(void) { return (int)sizeof(R); }
 void od3_set_threads(int n) { g_threads = n > 0 ? n : 1; }
-void od3_set_smoother(int s) { g_smoother = s == 1 ? 1 : 0; }
+void od3_set_smoother(int s) { g_smoother = (s >= 0 && s <= 3) ? s : 0; }
+void od3_set_transfer(int t) { g_transfer = t == 1 ? 1 : 0; }
 void od3_set_storage(int s) { g_storage = s == 1 ? 1 : 0; }
 double od3_take_zmax(void) { double z = g_zmax; g_zmax = 0; return z; }
 int od3_max_threads(void) {

@@ -89,6 +89,8 @@ def lib(real: str = "f32") -> C.CDLL:
     L.od3_max_threads.restype = C.c_int
     L.od3_set_smoother.argtypes = [C.c_int]
     L.od3_set_smoother.restype = None
+    L.od3_set_transfer.argtypes = [C.c_int]
+    L.od3_set_transfer.restype = None
     L.od3_set_storage.argtypes = [C.c_int]
     L.od3_set_storage.restype = None
     L.od3_take_zmax.argtypes = []
@@ -150,6 +152,19 @@ def change_dict(ch) -> dict:
 
 def set_threads(n: int, real: str = "f32") -> None:
     lib(real).od3_set_threads(int(n))
+
+
+def set_smoother(smoother: int, real: str = "f32") -> None:
+    """0: damped Jacobi on every level, the reference's (omega = 6/7); 1: red-black Gauss-Seidel on
+    every level, red first going down and black first coming up (a symmetric V-cycle); 2: red-black
+    on the fine level only; 3: red-black on the coarse levels only."""
+    lib(real).od3_set_smoother(int(smoother))
+
+
+def set_transfer(transfer: int, real: str = "f32") -> None:
+    """0: the reference's 8-child mean and injection; 1: trilinear prolongation from the active coarse
+    cells (renormalised) and its adjoint restriction (full weighting)."""
+    lib(real).od3_set_transfer(int(transfer))
 
 
 def set_storage(storage: int, real: str = "f32") -> None:

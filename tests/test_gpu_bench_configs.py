@@ -1,0 +1,136 @@
+"""Parity of the DEFAULT product path at the scenes the bench measures, through the C ABI.
+
+The default path is what `bench.py` times: f32 storage, FP64 dots/alpha/beta/true residual
+(`FD3_REDUCE_F64`), the 2.5-D paired fine kernels, the reference's V-cycle recipe.  Each case is
+checked against the reference's own CPU projection (the f32 oracle, a restatement of
+project_mobile3, code/water-core/src/delta3d_mobile.rs:465-609) as tests_delta3d.rs:389-400 does:
+
+- the reference's acceptance: relative residual <= 1e-6, plain divergence <= 1e-5, not degraded;
+- the iteration count within +-1 of the oracle's;
+- pressure L-inf difference <= 1e-5 relative to the oracle's L-inf;
+- and, where an FP64 oracle solve (relative residual 1e-12) is affordable, the default path's error
+  against it, bounded by the reference's own f32 projection's error (both are the algebraic error
+  of stopping at a relative residual of 1e-6, so neither is bounded by a fixed 1e-5 on its own).
+
+Ordered-f32 mode (the reference's reduction order) is also run on the 64^3 sphere lake and must be
+bit-identical to the oracle.
+"""
+import numpy as np
+import pytest
+
+from fluidisim_b200 import batch, scenes
+from fluidisim_b200.delta3d import REDUCE_F64, REDUCE_ORDERED_F32, Volume3
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+P_TOL = 1e-5        # pressure L-inf difference to the f32 oracle, relative to its L-inf
+ERR_FACTOR = 1.5    # the default path's FP64 error may exceed the reference f32 projection's by this factor
+ERR_FLOOR = 1e-6    # ... plus this absolute allowance (relative to the FP64 pressure's L-inf)
+
+
+def device(s, reduction=REDUCE_F64, **opts):
+    d = Volume3.configure_with_solid(s["nx"], s["ny"], s["nz"], s["dx"], s["rho"], s["g"], s["bottom"], s["solid"])
+    d.set_options(reduction=reduction, **opts)
+    d.enable_multigrid()
+    d.set_free_surface(s["eta"], s["rest"])
+    d.set_velocity(s["u"], s["v"], s["w"])
+    return d
+
+
+def oracle_run(s, real="f32"):
+    O.build()
+    O.set_threads(O.max_threads(real), real)
+    o = O.OracleVolume(s["nx"], s["ny"], s["nz"], s["dx"], s["rho"], s["g"], bottom=s["bottom"], solid=s["solid"],
+                       real=real)
+    o.enable_multigrid()
+    o.set_free_surface(s["eta"], s["rest"])
+    o.set_velocity(s["u"], s["v"], s["w"])
+    if real == "f64":
+        o.set_tolerance(1e-24)
+    scale, k1 = scenes.projection_scalars(s)
+    rep = o.project_mobile(scale, k1, 4000)
+    return rep, o
+
+
+def check_default_path(s, fp64=True):
+    scale, k1 = scenes.projection_scalars(s)
+    d = device(s)
+    r = d.project_mobile3(scale, k1, 4000)
+    p = d.pressure().astype(np.float64)
+    u, v, w = d.velocity()
+    d.close()
+    ro, o = oracle_run(s)
+    po = o.pressure().astype(np.float64)
+    # the reference's acceptance
+    assert not r.degraded and r.residual <= 1e-6 and r.divergence_plain <= 1e-5, r
+    assert abs(r.iterations - ro["iterations"]) <= 1, (r.iterations, ro["iterations"])
+    pmax = np.abs(po).max()
+    assert pmax > 0
+    dp = np.abs(p - po).max() / pmax
+    assert dp <= P_TOL, dp
+    # the projected faces: the same correction from nearly the same pressure
+    uo, vo, wo = o.velocity()
+    umax = max(np.abs(uo).max(), np.abs(vo).max(), np.abs(wo).max())
+    for a, b in ((u, uo), (v, vo), (w, wo)):
+        assert np.abs(a.astype(np.float64) - b).max() <= 1e-4 * umax
+    out = {"iterations": r.iterations, "oracle_iterations": ro["iterations"], "dp_vs_f32_oracle": dp}
+    if fp64:
+        _, o64 = oracle_run(s, "f64")
+        p64 = o64.pressure().astype(np.float64)
+        m64 = np.abs(p64).max()
+        err_gpu = np.abs(p - p64).max() / m64
+        err_ref = np.abs(po - p64).max() / m64
+        out.update(err_gpu_vs_fp64=err_gpu, err_reference_f32_vs_fp64=err_ref)
+        assert err_gpu <= ERR_FACTOR * err_ref + ERR_FLOOR, out
+    return out
+
+
+def test_config1_sphere_lake_64_default_path():
+    """64^3, 8 solid spheres (seed 1), lower half liquid, faces U[-1,1] (the learned part's scenes too)."""
+    out = check_default_path(scenes.sphere_lake(64))
+    print(out)
+
+
+def test_config2_box_basin_128_default_path():
+    """The bench's own scene: 128^3 basin, 16 boxes, sinusoidal surface, curl background + noise."""
+    out = check_default_path(scenes.box_basin(128))
+    print(out)
+
+
+def test_config1_sphere_lake_64_ordered_mode_is_bit_identical():
+    s = scenes.sphere_lake(64)
+    scale, k1 = scenes.projection_scalars(s)
+    d = device(s, reduction=REDUCE_ORDERED_F32)
+    r = d.project_mobile3(scale, k1, 4000)
+    ro, o = oracle_run(s)
+    assert r.as_dict() == ro, (r, ro)
+    assert np.array_equal(d.pressure().view(np.uint32), o.pressure().view(np.uint32))
+    for a, b in zip(d.velocity(), o.velocity()):
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    d.close()
+
+
+def test_non_cubic_patches_against_the_oracle():
+    """Three non-cubic patches of the batched workload, projected together by fd3_project_batch, each
+    against the oracle's projection of the same patch."""
+    ps = [p for p in batch.patch_scenes(24, seed=3, hi=64) if len({p["nx"], p["ny"], p["nz"]}) == 3][:3]
+    assert len(ps) == 3
+    vols = [batch.configure(p) for p in ps]
+    sk = [scenes.projection_scalars(p) for p in ps]
+    reps, st = batch.project_batch(vols, [a for a, _ in sk], [b for _, b in sk], threads=3)
+    assert st == [0, 0, 0]
+    for p, v, r in zip(ps, vols, reps):
+        assert not r.degraded and r.residual <= 1e-6 and r.divergence_plain <= 1e-5, r
+        ro, o = oracle_run(p)
+        assert abs(r.iterations - ro["iterations"]) <= 1, (p["nx"], p["ny"], p["nz"], r.iterations, ro["iterations"])
+        po = o.pressure().astype(np.float64)
+        assert np.abs(v.pressure() - po).max() <= P_TOL * np.abs(po).max()
+        v.close()
+
+
+def test_config5_breaking_wave_256_default_path():
+    """256^3 (16.8M cells): the breaking wave with 32 obstacles, against the f32 oracle (about half a
+    minute of OpenMP on the host).  The FP64 solve is skipped at this size."""
+    out = check_default_path(scenes.breaking_wave(256), fp64=False)
+    print(out)
