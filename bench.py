@@ -537,6 +537,7 @@ def learned_fcg_measure(args, s, vol_plain_p, stream):
     dp = float(np.max(np.abs(p - vol_plain_p)) / max(np.max(np.abs(vol_plain_p)), 1e-30))
     inet.close()
     lv.close()
+    args._learned_params = params
     return {
         "metric_value": K / (sum(ms) * 1e-3), "unit": "projections/s", "ms_per_projection": sum(ms) / K,
         "fcg_iterations": rep.fcg_iterations, "fallback_mg_iterations": rep.report.iterations,
@@ -548,6 +549,108 @@ def learned_fcg_measure(args, s, vol_plain_p, stream):
                      "loss_first": float(np.mean(losses[:3])), "loss_last": float(np.mean(losses[-3:]))},
         "validation_64": val,
     }
+
+
+def wave_measure(args, stream, flush):
+    """The 256^3 breaking wave (16.8M cells, inputs far above L2), three solvers on the same scene:
+    FP32-storage MGPCG (the default path), FP16-storage MGPCG and learned FCG with the network the
+    learned leg trained at 64^3, inferred at 256^3.  Each: ms per projection (CUDA events on the
+    solver's stream, device-resident inputs), iterations, the fraction of projections that fell
+    back to MGPCG, and the HBM roofline of the solver's dominant kernel (algorithmic bytes of a
+    launch / its event-timed duration in an instrumented replay / measured peak)."""
+    import numpy as np
+    import torch
+
+    from fluidisim_b200 import learned, scenes
+    from fluidisim_b200.delta3d import REDUCE_F64, STORAGE_F16, STORAGE_F32, Volume3
+    s = make_scene("wave", 256)
+    scale, k1 = scenes.projection_scalars(s)
+    cells = s["nx"] * s["ny"] * s["nz"]
+    du, dv, dw = (torch.from_numpy(s[k]).cuda() for k in ("u", "v", "w"))
+    peak, peak_kind = peaks()
+    steps = max(3, min(args.steps, 10))
+    out = {"workload": WORKLOAD_NAMES["wave"].format(n=256), "cells": cells, "steps": steps,
+           "l2": "inputs far above L2 (about 0.8 GB of fields); 256 MiB written between steps"}
+
+    def volume(storage):
+        v = Volume3.configure_with_solid(s["nx"], s["ny"], s["nz"], s["dx"], s["rho"], s["g"], s["bottom"], s["solid"])
+        v.set_options(reduction=REDUCE_F64, use_graphs=args.graphs, storage=storage)
+        v.set_stream(stream.cuda_stream)
+        v.enable_multigrid()
+        v.set_free_surface(s["eta"], s["rest"])
+        return v
+
+    def timed(step):
+        for _ in range(2):
+            step()
+        torch.cuda.synchronize()
+        ms, reps = [], []
+        for _ in range(steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            reps.append(step())
+            b.record(stream)
+            torch.cuda.synchronize()
+            ms.append(a.elapsed_time(b))
+        return sum(ms) / steps, reps
+
+    def roofline(v, step):
+        v.set_options(use_graphs=0)
+        v.profile(True)
+        for _ in range(2):
+            step()
+        torch.cuda.synchronize()
+        prof = merge_templates(v.profile_entries())
+        v.profile(False)
+        v.set_options(use_graphs=args.graphs)
+        known = [(n, c, m) for n, c, m in prof if n in BYTES_PER_CELL and BYTES_PER_CELL[n] >= 8]
+        name, count, msum = max(known, key=lambda e: e[2])
+        avg = msum / count
+        ach = BYTES_PER_CELL[name] * cells / (avg * 1e-3) / 1e9
+        return {"bound": "hbm", "kernel": name, "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                "peak_source": peak_kind, "avg_launch_ms": avg,
+                "timing": "instrumented replay of 2 projections without the loop graph"}
+
+    pressures = {}
+    for key, storage in (("fp32_mgpcg", STORAGE_F32), ("fp16_mgpcg", STORAGE_F16)):
+        v = volume(storage)
+
+        def step(v=v):
+            v.set_velocity_device(du.data_ptr(), dv.data_ptr(), dw.data_ptr())
+            v.reset_pressure()
+            return v.project_mobile3(scale, k1, 4000)
+        ms, reps = timed(step)
+        r = reps[-1]
+        out[key] = {"ms_per_projection": ms, "projections_per_s": 1e3 / ms, "iterations": r.iterations,
+                    "rel_residual": r.residual, "divergence_plain": r.divergence_plain, "fallback_rate": None,
+                    "roofline": roofline(v, step)}
+        pressures[key] = v.pressure().astype(np.float64)
+        v.close()
+    pm = np.abs(pressures["fp32_mgpcg"]).max()
+    out["fp16_mgpcg"]["pressure_linf_rel_vs_fp32"] = float(np.abs(pressures["fp16_mgpcg"] - pressures["fp32_mgpcg"]).max() / pm)
+    params = getattr(args, "_learned_params", None)
+    if params is not None:
+        v = volume(STORAGE_F32)
+        net = learned.UNet(1, s["nz"], s["ny"], s["nx"])
+        net.set_params(params)
+
+        def lstep():
+            v.set_velocity_device(du.data_ptr(), dv.data_ptr(), dw.data_ptr())
+            v.reset_pressure()
+            return learned.project_learned(v, net, scale, k1, 4000, 100)
+        ms, reps = timed(lstep)
+        r = reps[-1]
+        out["learned_fcg"] = {"ms_per_projection": ms, "projections_per_s": 1e3 / ms,
+                              "fcg_iterations": r.fcg_iterations, "fallback_mg_iterations": r.report.iterations,
+                              "fallback_rate": float(np.mean([x.fell_back for x in reps])),
+                              "rel_residual": r.report.residual, "divergence_plain": r.report.divergence_plain,
+                              "pressure_linf_rel_vs_fp32": float(np.abs(v.pressure() - pressures["fp32_mgpcg"]).max() / pm),
+                              "speedup_vs_fp32_mgpcg": out["fp32_mgpcg"]["ms_per_projection"] / ms}
+        net.close()
+        v.close()
+    return out
 
 
 def parts_measure(args, s, stream):
@@ -755,6 +858,7 @@ def run_b200(args):
     if world == 1 and args.learned:
         learned_line = learned_fcg_measure(args, s, plain_p, stream)
     parts_line = parts_measure(args, s, stream) if (world == 1 and args.parts) else None
+    wave_line = wave_measure(args, stream, flush) if (world == 1 and args.wave and args.workload == "basin") else None
 
     if rank == 0:
         cpu = cpu_baseline_sample(args.workload, args.size) if (world == 1 and not args.no_cpu) else None
@@ -787,6 +891,7 @@ def run_b200(args):
             "learned_fcg": learned_line,
             "mixed_precision": mixed_line,
             "parts": parts_line,
+            "wave_256": wave_line,
         }
         print(json.dumps(out), flush=True)
     vol.close()
@@ -797,8 +902,11 @@ def run_b200(args):
 
 def run_patches(args):
     """Batched patches: every rank projects its share of the seeded patch set (dealt by decreasing
-    size) through fd3_project_batch, after the autotuner has picked the options per size class.
-    No data-path collective: only the timing max and a count reduction."""
+    size) in ONE persistent launch per step (fd3_batch_project: thread-block clusters as independent
+    solvers, each taking its share of the patches, largest first), the cluster size chosen by timing
+    the whole set.  Inputs stay resident in HBM and are copied in by the launch.  The earlier path
+    (fd3_project_batch: per-patch loop graphs from host workers) is timed beside it.  No data-path
+    collective: only the timing max and a count reduction."""
     import numpy as np
     import torch
 
@@ -810,28 +918,43 @@ def run_patches(args):
     ps = batch.patch_scenes(args.patches, seed=3)
     cells = [p["nx"] * p["ny"] * p["nz"] for p in ps]
     mine = [ps[i] for i in batch.deal(cells, world, rank)]
-    tuned = batch.autotune(batch.by_class(mine))
-    vols, inputs, sk = [], [], []
-    for p in mine:
-        t = tuned[batch.size_class(p["nx"] * p["ny"] * p["nz"])]
-        vols.append(batch.configure(p, t.kernels, t.levels))
-        inputs.append(tuple(torch.from_numpy(p[k]).cuda() for k in ("u", "v", "w")))
-        sk.append(scenes.projection_scalars(p))
-    torch.cuda.synchronize()
+    vols = [batch.configure(p) for p in mine]
+    inputs = [tuple(torch.from_numpy(p[k]).cuda() for k in ("u", "v", "w")) for p in mine]
+    ptrs = [tuple(t.data_ptr() for t in x) for x in inputs]
+    sk = [scenes.projection_scalars(p) for p in mine]
     scales, k1s = [a for a, _ in sk], [b for _, b in sk]
+    torch.cuda.synchronize()
+
+    def timed_set(fn, reps):
+        out, best = None, float("inf")
+        for _ in range(reps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            out = fn()
+            b.record()
+            torch.cuda.synchronize()
+            best = min(best, a.elapsed_time(b))
+        return best, out
+
+    # the cluster size: the whole set timed with each (best of 3 after one warm-up)
+    tuning = {}
+    for cs in (1, 2, 4, 8):
+        pb = batch.PersistentBatch(vols, cluster_size=cs)
+        ms_cs, _ = timed_set(lambda: pb.project(scales, k1s, reset_pressure=True, inputs=ptrs), 4)
+        tuning[cs] = {"ms": round(ms_cs, 3), "clusters": pb.clusters}
+        pb.close()
+    best_cs = min(tuning, key=lambda c: tuning[c]["ms"])
+    pb = batch.PersistentBatch(vols, cluster_size=best_cs)
 
     def step():
-        for v, (du, dv, dw) in zip(vols, inputs):
-            v.set_velocity_device(du.data_ptr(), dv.data_ptr(), dw.data_ptr())
-            v.reset_pressure()
-        return batch.project_batch(vols, scales, k1s, threads=args.threads)
+        return pb.project(scales, k1s, reset_pressure=True, inputs=ptrs)
 
     for _ in range(args.warmup):
         reps, st = step()
     torch.cuda.synchronize()
     barrier(world)
     ms = []
-    launches0 = sum(v.kernel_launches() for v in vols)
+    launches0 = pb.kernel_launches()
     with ClockSampler(local) as clocks:
         clocks.mark(True)
         for _ in range(args.steps):
@@ -842,11 +965,33 @@ def run_patches(args):
             torch.cuda.synchronize()
             ms.append(a.elapsed_time(b))
         clocks.mark(False)
-    launches = sum(v.kernel_launches() for v in vols) - launches0
+    launches = pb.kernel_launches() - launches0
     assert all(x == 0 for x in st), st
+    assert all(not r.degraded and r.residual <= 1e-6 for r in reps)
     my_ci = sum(p["nx"] * p["ny"] * p["nz"] * r.iterations for p, r in zip(mine, reps))
     ms_total, ci = batch.reduce_totals(sum(ms), my_ci, world, device="cuda")
     its = [r.iterations for r in reps]
+    pb.close()
+    # the per-patch path on the same volumes: host workers issuing each patch's loop graph
+    streams_line = None
+    if world == 1 and args.streams:
+        tuned = batch.autotune(batch.by_class(mine))
+
+        def sstep():
+            for v, (du, dv, dw) in zip(vols, inputs):
+                v.set_velocity_device(du.data_ptr(), dv.data_ptr(), dw.data_ptr())
+                v.reset_pressure()
+            return batch.project_batch(vols, scales, k1s, threads=args.threads)
+        sstep()
+        ms_s = []
+        for _ in range(max(3, min(args.steps, 10))):
+            m_, _ = timed_set(sstep, 1)
+            ms_s.append(m_)
+        streams_line = {"value": len(ps) / (np.mean(ms_s) * 1e-3), "unit": "patches/s", "ms_per_step": float(np.mean(ms_s)),
+                        "note": "fd3_project_batch: every patch its own stream and device-side loop graph, issued by "
+                                "host workers; inputs set through set_velocity_device per patch",
+                        "autotuned": {k: {"kernels": v.kernels, "mg_max_levels": v.levels, "ms": round(v.ms, 3)}
+                                      for k, v in tuned.items()}}
     if rank == 0:
         cpu = None
         if world == 1 and not args.no_cpu:
@@ -858,14 +1003,15 @@ def run_patches(args):
             "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded patch set)",
             "config": {"workload": f"{args.patches} patches: sides log-uniform in [16,96] rounded to 8, spheres "
-                                   f"5-15% of cells, fill U[0.3,0.8], faces U[-1,1]; one fd3_project_batch per step",
+                                   f"5-15% of cells, fill U[0.3,0.8], faces U[-1,1]; one persistent launch per step",
                        "cells_total": sum(cells), "parallelism": f"patches sharded x{world}",
-                       "autotuned": {k: {"kernels": v.kernels, "mg_max_levels": v.levels, "ms": round(v.ms, 3)}
-                                     for k, v in tuned.items()},
+                       "autotuned": {"cluster_size": best_cs, "candidates": tuning,
+                                     "threads_per_cta": 1024, "mg_depth": "every level (the reference's hierarchy)"},
                        "iterations_rank0": {"min": min(its), "max": max(its), "mean": float(np.mean(its))},
-                       "l2": "inputs restored each step; the patch set exceeds L2"},
+                       "l2": "inputs restored each step by the launch; the patch set exceeds L2"},
             "cells_iterations_per_s": args.steps * ci / (ms_total * 1e-3),
             "gpu_launches": launches,
+            "streams_path": streams_line,
             "cpu_baseline": cpu,
             "clocks": clocks.summary(),
         }
@@ -1044,6 +1190,8 @@ def main():
                          "patches: the batched delta patches; sparse: a sparse set in a 256^2 x 32 window")
     ap.add_argument("--patches", type=int, default=256, help="patch count of the patches workload")
     ap.add_argument("--threads", type=int, default=0, help="host workers of fd3_project_batch (0 = up to 16)")
+    ap.add_argument("--streams", type=int, default=1,
+                    help="patches workload: 1 also times the per-patch stream path (fd3_project_batch) beside it")
     ap.add_argument("--size", type=int, default=None, help="grid side (default 128 for basin, 256 for wave)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--learned", type=int, default=1,
@@ -1051,6 +1199,9 @@ def main():
     ap.add_argument("--mixed", type=int, default=1, help="1: also time the FP16-storage V-cycle on the same scene")
     ap.add_argument("--parts", type=int, default=1,
                     help="1: also time a mobile step, the second-order advection, a solid re-cut and a level change")
+    ap.add_argument("--wave", type=int, default=1,
+                    help="1: also compare FP32 MGPCG, FP16-storage MGPCG and learned FCG on the 256^3 breaking wave "
+                         "(N=1, basin workload only)")
     ap.add_argument("--train-samples", type=int, default=20000,
                     help="training samples of the learned preconditioner (20,000 at 64^3, as config 4 asks)")
     ap.add_argument("--kernels", type=int, default=0,

@@ -26,6 +26,15 @@ def _bind(L):
         L.fd3_project_batch.argtypes = [C.POINTER(C.c_void_p), C.c_size_t, C.POINTER(C.c_float),
                                         C.POINTER(C.c_float), C.c_uint32, C.c_int, C.POINTER(_Report),
                                         C.POINTER(C.c_int)]
+        vpp = C.POINTER(C.c_void_p)
+        L.fd3_batch_create.argtypes = [vpp, C.c_size_t, C.c_int, C.POINTER(C.c_void_p)]
+        L.fd3_batch_destroy.argtypes = [C.c_void_p]
+        L.fd3_batch_destroy.restype = None
+        L.fd3_batch_clusters.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        L.fd3_batch_kernel_launches.argtypes = [C.c_void_p]
+        L.fd3_batch_kernel_launches.restype = C.c_uint64
+        L.fd3_batch_project.argtypes = [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_uint32, C.c_int,
+                                        vpp, vpp, vpp, C.POINTER(_Report), C.POINTER(C.c_int)]
         L._batch_bound = True
     return L
 
@@ -105,6 +114,61 @@ def project_batch(volumes, scales, k1s, max_iters: int = 4000, threads: int = 0)
     if e:
         raise Delta3dError(e, "fd3_project_batch")
     return [Report._from(reps[i]) for i in range(n)], [int(st[i]) for i in range(n)]
+
+
+class PersistentBatch:
+    """fd3_batch: the volumes projected by one persistent kernel launch (thread-block clusters as
+    independent solvers, each taking its share of the volumes, largest first).  Create once (all
+    allocations happen there), project many times; close before the volumes."""
+
+    def __init__(self, volumes, cluster_size: int = 4):
+        self.vols = list(volumes)
+        L = _bind(library())
+        self._L = L
+        arr = (C.c_void_p * len(self.vols))(*[v._h.value for v in self.vols])
+        h = C.c_void_p()
+        e = L.fd3_batch_create(arr, len(self.vols), int(cluster_size), C.byref(h))
+        if e:
+            raise Delta3dError(e, "fd3_batch_create", L.fd3_last_cuda_error().decode() if e >= 100 else "")
+        self._h = h
+        n, cs = C.c_int(), C.c_int()
+        L.fd3_batch_clusters(h, C.byref(n), C.byref(cs))
+        self.clusters, self.cluster_size = n.value, cs.value
+
+    def project(self, scales, k1s, max_iters: int = 4000, reset_pressure: bool = False, inputs=None):
+        """Returns (reports, statuses).  inputs: None, or per volume a (u, v, w) of device pointers
+        copied into the volume's velocity first."""
+        n = len(self.vols)
+        sc = np.ascontiguousarray(scales, np.float32)
+        kk = np.ascontiguousarray(k1s, np.float32)
+        reps = (_Report * n)()
+        st = (C.c_int * n)()
+        if inputs is not None:
+            iu = (C.c_void_p * n)(*[x[0] for x in inputs])
+            iv = (C.c_void_p * n)(*[x[1] for x in inputs])
+            iw = (C.c_void_p * n)(*[x[2] for x in inputs])
+        else:
+            iu = iv = iw = None
+        e = self._L.fd3_batch_project(self._h, sc.ctypes.data_as(C.POINTER(C.c_float)),
+                                      kk.ctypes.data_as(C.POINTER(C.c_float)), int(max_iters),
+                                      1 if reset_pressure else 0, iu, iv, iw, reps, st)
+        if e:
+            raise Delta3dError(e, "fd3_batch_project", self._L.fd3_last_cuda_error().decode() if e >= 100 else "")
+        return [Report._from(reps[i]) for i in range(n)], [int(st[i]) for i in range(n)]
+
+    def kernel_launches(self) -> int:
+        return int(self._L.fd3_batch_kernel_launches(self._h))
+
+    def close(self):
+        if self._h:
+            self._L.fd3_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 @dataclass

@@ -129,6 +129,34 @@ struct LoadT {
 // The outer loop's metrics from the projection's row codes (the surface is the one the codes were
 // built for), instead of rebuilding each row from the geometry.
 
+// One cell of divergence_mobile3 (delta3d_mobile.rs:398-433): |div u| of a wet row into the
+// maximum over all wet rows and, without a surface ghost (no face state 2), over the plain ones.
+__device__ __forceinline__ void div_metric_cell(const Geo& g, unsigned code, const float* __restrict__ u,
+                                                const float* __restrict__ v, const float* __restrict__ w, int c,
+                                                float& all, float& plain) {
+  if (!(code & RC_WET)) return;
+  int i, j, k; cell_ijk(g, c, i, j, k);
+  float dv;
+  if (g.cut) {
+    float fl = __ldg(g.ou + fu(g, i, j, k)) * u[fu(g, i, j, k)];
+    float fr = __ldg(g.ou + fu(g, i + 1, j, k)) * u[fu(g, i + 1, j, k)];
+    float ff = __ldg(g.ov + fv(g, i, j, k)) * v[fv(g, i, j, k)];
+    float fk = __ldg(g.ov + fv(g, i, j + 1, k)) * v[fv(g, i, j + 1, k)];
+    float fb = __ldg(g.ow + fw(g, i, j, k)) * w[fw(g, i, j, k)];
+    float ft = __ldg(g.ow + fw(g, i, j, k + 1)) * w[fw(g, i, j, k + 1)];
+    dv = ((fr - fl + ft - fb) + (fk - ff)) / g.dx;
+    if (g.wall) dv = dv + wall_flux(g, i, j, k);
+  } else {
+    float fl = u[fu(g, i, j, k)], fr = u[fu(g, i + 1, j, k)];
+    float ff = v[fv(g, i, j, k)], fk = v[fv(g, i, j + 1, k)];
+    float fb = w[fw(g, i, j, k)], ft = w[fw(g, i, j, k + 1)];
+    dv = ((fr - fl + ft - fb) + (fk - ff)) / g.dx;
+  }
+  const float d = fabsf(dv);
+  all = fmaxf(all, d);
+  if (!(code & RC_GHOSTS)) plain = fmaxf(plain, d);
+}
+
 // divergence_mobile3 (delta3d_mobile.rs:398-433): max |div u| over the wet rows and over the
 // plain ones (no surface ghost: no face state 2), into S->fmax[0] and [1].  Each thread takes
 // METRIC_CELLS cells, a block's cells apart, and the block merges its maxima by one atomic each.
@@ -144,31 +172,7 @@ __global__ void k_div_metric_c(Geo g, const unsigned short* __restrict__ codes, 
     code[q] = c < g.n ? codes[c] : 0u;
   }
 #pragma unroll
-  for (int q = 0; q < METRIC_CELLS; ++q) {
-    if (code[q] & RC_WET) {
-      const int c = c0 + q * blockDim.x;
-      int i, j, k; cell_ijk(g, c, i, j, k);
-      float dv;
-      if (g.cut) {
-        float fl = __ldg(g.ou + fu(g, i, j, k)) * u[fu(g, i, j, k)];
-        float fr = __ldg(g.ou + fu(g, i + 1, j, k)) * u[fu(g, i + 1, j, k)];
-        float ff = __ldg(g.ov + fv(g, i, j, k)) * v[fv(g, i, j, k)];
-        float fk = __ldg(g.ov + fv(g, i, j + 1, k)) * v[fv(g, i, j + 1, k)];
-        float fb = __ldg(g.ow + fw(g, i, j, k)) * w[fw(g, i, j, k)];
-        float ft = __ldg(g.ow + fw(g, i, j, k + 1)) * w[fw(g, i, j, k + 1)];
-        dv = ((fr - fl + ft - fb) + (fk - ff)) / g.dx;
-        if (g.wall) dv = dv + wall_flux(g, i, j, k);
-      } else {
-        float fl = u[fu(g, i, j, k)], fr = u[fu(g, i + 1, j, k)];
-        float ff = v[fv(g, i, j, k)], fk = v[fv(g, i, j + 1, k)];
-        float fb = w[fw(g, i, j, k)], ft = w[fw(g, i, j, k + 1)];
-        dv = ((fr - fl + ft - fb) + (fk - ff)) / g.dx;
-      }
-      const float d = fabsf(dv);
-      all = fmaxf(all, d);
-      if (!(code[q] & RC_GHOSTS)) plain = fmaxf(plain, d);
-    }
-  }
+  for (int q = 0; q < METRIC_CELLS; ++q) div_metric_cell(g, code[q], u, v, w, c0 + q * blockDim.x, all, plain);
   block_fmax2_atomic(all, plain, &S->fmax[0], &S->fmax[1]);
 }
 
@@ -178,12 +182,11 @@ __global__ void k_div_metric_c(Geo g, const unsigned short* __restrict__ codes, 
 // exactly the faces the reference corrects: open, neither cell solid, at least one wet.  A w face
 // is corrected when the row of the cell below has it live.  Ghost coefficients and values are the
 // reference's (ghost_side3, ghost_up3).
-__global__ void k_correct_uv_c(Geo g, const unsigned short* __restrict__ codes, float k1, const float* __restrict__ p,
-                               const float* __restrict__ us, const float* __restrict__ vs, float* __restrict__ u,
-                               float* __restrict__ v) {
-  KSTART();
+__device__ __forceinline__ void correct_uv_at(const Geo& g, const unsigned short* __restrict__ codes, float k1,
+                                              const float* __restrict__ p, const float* __restrict__ us,
+                                              const float* __restrict__ vs, float* __restrict__ u,
+                                              float* __restrict__ v, int q) {
   const int nu = (g.nx + 1) * g.ny * g.nz, nv = g.nx * (g.ny + 1) * g.nz;
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
   int axis, f, i, j, k;
   if (q < nu) { axis = 0; f = q; i = f % (g.nx + 1); int t = f / (g.nx + 1); j = t % g.ny; k = t / g.ny; }
   else if (q < nu + nv) { axis = 1; f = q - nu; i = f % g.nx; int t = f / g.nx; j = t % (g.ny + 1); k = t / (g.ny + 1); }
@@ -207,12 +210,17 @@ __global__ void k_correct_uv_c(Geo g, const unsigned short* __restrict__ codes, 
   }
   if (axis == 0) u[f] = val; else v[f] = val;
 }
-
-__global__ void k_correct_w_c(Geo g, const unsigned short* __restrict__ codes, float k1, const float* __restrict__ p,
-                              const float* __restrict__ ws, float* __restrict__ w) {
+__global__ void k_correct_uv_c(Geo g, const unsigned short* __restrict__ codes, float k1, const float* __restrict__ p,
+                               const float* __restrict__ us, const float* __restrict__ vs, float* __restrict__ u,
+                               float* __restrict__ v) {
   KSTART();
+  correct_uv_at(g, codes, k1, p, us, vs, u, v, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+__device__ __forceinline__ void correct_w_at(const Geo& g, const unsigned short* __restrict__ codes, float k1,
+                                             const float* __restrict__ p, const float* __restrict__ ws,
+                                             float* __restrict__ w, int f) {
   const int nw = g.nx * g.ny * (g.nz + 1);
-  const int f = blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= nw) return;
   const int nxny = g.nx * g.ny;
   const int k = f / nxny;
@@ -230,6 +238,39 @@ __global__ void k_correct_w_c(Geo g, const unsigned short* __restrict__ codes, f
   }
   w[f] = val;
 }
+__global__ void k_correct_w_c(Geo g, const unsigned short* __restrict__ codes, float k1, const float* __restrict__ p,
+                              const float* __restrict__ ws, float* __restrict__ w) {
+  KSTART();
+  correct_w_at(g, codes, k1, p, ws, w, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// One row of backward_error_mobile3 (delta3d_mobile.rs:243-271): |r_i| / (|b| + |A||p|)_i of a wet
+// row (0 for a dry row or a zero scale).  The apertures and ghost coefficients are apply_code's.
+__device__ __forceinline__ float backward_error_cell(const Geo& g, unsigned code, const float* __restrict__ p,
+                                                     const float* __restrict__ rhs, const float* __restrict__ res,
+                                                     int c) {
+  if (!(code & RC_WET)) return 0.f;
+  int i, j, k; cell_ijk(g, c, i, j, k);
+  const int nxny = g.nx * g.ny;
+  const bool unit = code & RC_UNIT;
+  const float pc = fabsf(p[c]);
+  float acc = 0.f;
+  auto face = [&](int f, int axis, int fi, int m, int x, int y) {
+    const unsigned st = face_state(code, f);
+    if (!st) return;
+    const float a = unit ? 1.f : aper3(g, axis, fi);
+    if (st == 1) acc += a * (pc + fabsf(p[m]));
+    else acc += a * pc * (f == 5 ? ghost_it_up(g, i, j, k) : ghost_it_side(g, i, j, k, x, y));
+  };
+  face(0, 0, fu(g, i, j, k), c - 1, i - 1, j);
+  face(1, 0, fu(g, i + 1, j, k), c + 1, i + 1, j);
+  face(2, 1, fv(g, i, j, k), c - g.nx, i, j - 1);
+  face(3, 1, fv(g, i, j + 1, k), c + g.nx, i, j + 1);
+  face(4, 2, fw(g, i, j, k), c - nxny, i, j);
+  face(5, 2, fw(g, i, j, k + 1), c + nxny, i, j);
+  const float scale = fabsf(rhs[c]) + acc * g.inv;
+  return scale > 0.f ? fabsf(res[c]) / scale : 0.f;
+}
 
 // backward_error_mobile3 (delta3d_mobile.rs:243-271): max |r_i| / (|b| + |A||p|)_i over the wet
 // rows into S->fmax[3].  A row's apertures and ghost coefficients are the ones apply_code uses.
@@ -246,32 +287,7 @@ __global__ void k_backward_error_c(Geo g, const unsigned short* __restrict__ cod
     codev[q] = c < g.n ? codes[c] : 0u;
   }
 #pragma unroll
-  for (int q = 0; q < METRIC_CELLS; ++q) {
-    const unsigned code = codev[q];
-    if (code & RC_WET) {
-      const int c = c0 + q * blockDim.x;
-      int i, j, k; cell_ijk(g, c, i, j, k);
-      const int nxny = g.nx * g.ny;
-      const bool unit = code & RC_UNIT;
-      const float pc = fabsf(p[c]);
-      float acc = 0.f;
-      auto face = [&](int f, int axis, int fi, int m, int x, int y) {
-        const unsigned st = face_state(code, f);
-        if (!st) return;
-        const float a = unit ? 1.f : aper3(g, axis, fi);
-        if (st == 1) acc += a * (pc + fabsf(p[m]));
-        else acc += a * pc * (f == 5 ? ghost_it_up(g, i, j, k) : ghost_it_side(g, i, j, k, x, y));
-      };
-      face(0, 0, fu(g, i, j, k), c - 1, i - 1, j);
-      face(1, 0, fu(g, i + 1, j, k), c + 1, i + 1, j);
-      face(2, 1, fv(g, i, j, k), c - g.nx, i, j - 1);
-      face(3, 1, fv(g, i, j + 1, k), c + g.nx, i, j + 1);
-      face(4, 2, fw(g, i, j, k), c - nxny, i, j);
-      face(5, 2, fw(g, i, j, k + 1), c + nxny, i, j);
-      const float scale = fabsf(rhs[c]) + acc * g.inv;
-      if (scale > 0.f) worst = fmaxf(worst, fabsf(res[c]) / scale);
-    }
-  }
+  for (int q = 0; q < METRIC_CELLS; ++q) worst = fmaxf(worst, backward_error_cell(g, codev[q], p, rhs, res, c0 + q * blockDim.x));
   block_fmax2_atomic(worst, 0.f, &S->fmax[3], nullptr);
 }
 
@@ -571,10 +587,7 @@ __device__ __forceinline__ float level_row_f(const Lev& L, int i, int j, int k, 
 // Row codes of a coarse level (row_sums, delta3d_multigrid.rs:216-255), once per projection after
 // coarsen3: bit 0 active (kind > 0); per face 0 nothing, 1 active neighbour (a (pc - p_m)),
 // 2 Dirichlet (an air neighbour or the top of the domain: 2 a pc); bit 13 every live aperture is 1.
-__global__ void k_level_codes(Lev L) {
-  KSTART();
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= L.n) return;
+__device__ __forceinline__ unsigned level_codes_at(const Lev& L, int c) {
   unsigned code = 0;
   if (L.kind[c] > 0.f) {
     int i = c % L.nx, t = c / L.nx, j = t % L.ny, k = t / L.ny;
@@ -602,7 +615,13 @@ __global__ void k_level_codes(Lev L) {
     face(5, L.ow[((k + 1) * L.ny + j) * L.nx + i], k + 1 < L.nz, c + nxny, true);
     if (unit) code |= RC_UNIT;
   }
-  L.code[c] = (unsigned short)code;
+  return code;
+}
+__global__ void k_level_codes(Lev L) {
+  KSTART();
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= L.n) return;
+  L.code[c] = (unsigned short)level_codes_at(L, c);
 }
 
 // One row of row_sums (with p) from its code: the same terms, in the same order, as level_row_f.
@@ -956,8 +975,16 @@ __global__ void __launch_bounds__(TPB) k_level_sweep_c(Lev L, const float* __res
 // to the block after the barrier).  levels[first].r is already restricted; leaves levels[first].x.
 constexpr int TAIL_THREADS = 1024;
 
-__device__ __forceinline__ void tail_sweep(const Lev& L, const float* xin, float* xout, bool zero_in) {
-  for (int c = threadIdx.x; c < L.n; c += blockDim.x) {
+// The threads of one CTA as a team: rank, size and barrier of the tail's strided phases.
+struct BlockTeam {
+  __device__ __forceinline__ int rank() const { return threadIdx.x; }
+  __device__ __forceinline__ int size() const { return blockDim.x; }
+  __device__ __forceinline__ void sync() const { __syncthreads(); }
+};
+
+template <class Team>
+__device__ __forceinline__ void tail_sweep_t(const Team& tm, const Lev& L, const float* xin, float* xout, bool zero_in) {
+  for (int c = tm.rank(); c < L.n; c += tm.size()) {
     float dg = L.diag[c];
     if (zero_in) { xout[c] = dg > 0.f ? 0.f + OMEGA * (L.r[c] - 0.f) / dg : 0.f; continue; }
     float xc = xin[c];
@@ -967,19 +994,23 @@ __device__ __forceinline__ void tail_sweep(const Lev& L, const float* xin, float
     }
     xout[c] = xc;
   }
-  __syncthreads();
+  tm.sync();
+}
+__device__ __forceinline__ void tail_sweep(const Lev& L, const float* xin, float* xout, bool zero_in) {
+  tail_sweep_t(BlockTeam{}, L, xin, xout, zero_in);
 }
 
 // coarse_cycle3 (delta3d_multigrid.rs:303-332) over levels first..last of Ls, in one block.
-__device__ __forceinline__ void tail_run(const Lev* Ls, int first, int last) {
+template <class Team>
+__device__ __forceinline__ void tail_run_t(const Team& tm, const Lev* Ls, int first, int last) {
   for (int l = first; l <= last; ++l) {
     const Lev L = Ls[l];
     const int sweeps = l == last ? 8 : 2;  // COARSE_SWEEPS_3D, PRE_SWEEPS_3D
     for (int s = 0; s < sweeps; ++s)
-      tail_sweep(L, (s % 2 == 0) ? L.x : L.x2, (s % 2 == 0) ? L.x2 : L.x, s == 0);
+      tail_sweep_t(tm, L, (s % 2 == 0) ? L.x : L.x2, (s % 2 == 0) ? L.x2 : L.x, s == 0);
     if (l < last) {
       const Lev C = Ls[l + 1];
-      for (int q = threadIdx.x; q < C.n; q += blockDim.x) {
+      for (int q = tm.rank(); q < C.n; q += tm.size()) {
         int ci = q % C.nx, t = q / C.nx, cj = t % C.ny, ck = t / C.ny;
         float s = 0.f;
 #pragma unroll
@@ -991,20 +1022,23 @@ __device__ __forceinline__ void tail_run(const Lev* Ls, int first, int last) {
         }
         C.r[q] = 0.125f * s;
       }
-      __syncthreads();
+      tm.sync();
     }
   }
   for (int l = last - 1; l >= first; --l) {
     const Lev L = Ls[l];
     const Lev C = Ls[l + 1];
-    for (int c = threadIdx.x; c < L.n; c += blockDim.x) {
+    for (int c = tm.rank(); c < L.n; c += tm.size()) {
       int i = c % L.nx, t = c / L.nx, j = t % L.ny, k = t / L.ny;
       L.x[c] += C.x[((k >> 1) * C.ny + (j >> 1)) * C.nx + (i >> 1)];
     }
-    __syncthreads();
-    tail_sweep(L, L.x, L.x2, false);
-    tail_sweep(L, L.x2, L.x, false);
+    tm.sync();
+    tail_sweep_t(tm, L, L.x, L.x2, false);
+    tail_sweep_t(tm, L, L.x2, L.x, false);
   }
+}
+__device__ __forceinline__ void tail_run(const Lev* Ls, int first, int last) {
+  tail_run_t(BlockTeam{}, Ls, first, last);
 }
 
 // The levels in global memory (fallback when they do not fit in shared memory).
@@ -1245,6 +1279,35 @@ __global__ void k_loop_cond(cudaGraphConditionalHandle handle, Scalars* S) {
 // ------------------------------------------------------------------------------------------------
 // Set-up reductions with the in-kernel finish.
 
+// One row of rhs_mobile3 (delta3d_mobile.rs:215-241): rhs and prec of cell c (the divergence in
+// rhs is replaced by the right-hand side), its row code into codes and p = 0 on a dry cell when
+// those are not null; returns b.
+__device__ __forceinline__ float rhs_b2_at(const Geo& g, float scale, float* __restrict__ rhs, float* __restrict__ prec,
+                                           unsigned short* __restrict__ codes, float* __restrict__ pdry, int c) {
+  int i, j, k; cell_ijk(g, c, i, j, k);
+  if (!wet3(g, i, j, k)) {
+    rhs[c] = 0.f; prec[c] = 0.f;
+    if (codes) codes[c] = 0;
+    if (pdry) pdry[c] = 0.f;
+    return 0.f;
+  }
+  RowE row[6]; mobile_row(g, i, j, k, row);
+  float b = scale * rhs[c];
+  float diag = 0.f;
+#pragma unroll
+  for (int f = 0; f < 6; ++f) {
+    if (row[f].n >= 0) diag += row[f].a;
+    else if (row[f].a > 0.f) {
+      diag += row[f].a * row[f].it;
+      b += row[f].a * row[f].val * row[f].it * g.inv;
+    }
+  }
+  rhs[c] = b;
+  prec[c] = diag > 0.f ? 1.f / (diag * g.inv) : 0.f;
+  if (codes) codes[c] = (unsigned short)row_code_of(row);
+  return b;
+}
+
 // rhs_mobile3 (delta3d_mobile.rs:215-241) with b.b (FIN_B2) when `reduce`.
 // With `codes` not null, the same pass also writes each cell's row code (row_code_of the same
 // row; 0 for a dry cell); with `pdry` not null it zeroes that pressure on the dry cells.
@@ -1254,30 +1317,7 @@ __global__ void __launch_bounds__(TPB) k_rhs_b2(Geo g, float scale, float* __res
                                                 float* __restrict__ pdry) {
   KSTART();
   int c = blockIdx.x * blockDim.x + threadIdx.x;
-  float b = 0.f;
-  if (c < g.n) {
-    int i, j, k; cell_ijk(g, c, i, j, k);
-    if (!wet3(g, i, j, k)) {
-      rhs[c] = 0.f; prec[c] = 0.f;
-      if (codes) codes[c] = 0;
-      if (pdry) pdry[c] = 0.f;
-    } else {
-      RowE row[6]; mobile_row(g, i, j, k, row);
-      b = scale * rhs[c];
-      float diag = 0.f;
-#pragma unroll
-      for (int f = 0; f < 6; ++f) {
-        if (row[f].n >= 0) diag += row[f].a;
-        else if (row[f].a > 0.f) {
-          diag += row[f].a * row[f].it;
-          b += row[f].a * row[f].val * row[f].it * g.inv;
-        }
-      }
-      rhs[c] = b;
-      prec[c] = diag > 0.f ? 1.f / (diag * g.inv) : 0.f;
-      if (codes) codes[c] = (unsigned short)row_code_of(row);
-    }
-  }
+  const float b = c < g.n ? rhs_b2_at(g, scale, rhs, prec, codes, pdry, c) : 0.f;
   if (!reduce) return;
   if (__syncthreads_or(c < g.n && b != 0.f) && threadIdx.x == 0) atomicOr(&S->any_nonzero, 1);
   reduce_finish<MODE>(Acc<MODE>::prod(b, b), c, g.n, red, S, FIN_B2);

@@ -364,15 +364,12 @@ __device__ __forceinline__ void flag_nonzero(bool nz, Scalars* S) {
 // ------------------------------------------------------------------------------------------------
 // Assembly
 
-// divergence / divergence_cut (delta3d.rs:747-763, 806-855), a solid at rest.
-__global__ void k_divergence(Geo g, const float* __restrict__ u, const float* __restrict__ v,
-                             const float* __restrict__ w, float* __restrict__ out) {
-  KSTART();
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= g.n) return;
+// divergence / divergence_cut (delta3d.rs:747-763, 806-855) of cell c, a solid at rest.
+__device__ __forceinline__ float divergence_at(const Geo& g, const float* __restrict__ u,
+                                               const float* __restrict__ v, const float* __restrict__ w, int c) {
   int i, j, k; cell_ijk(g, c, i, j, k);
   if (g.cut) {
-    if (__ldg(g.frac + c) == 0.f) { out[c] = 0.f; return; }
+    if (__ldg(g.frac + c) == 0.f) return 0.f;
     float fl = __ldg(g.ou + fu(g, i, j, k)) * u[fu(g, i, j, k)];
     float fr = __ldg(g.ou + fu(g, i + 1, j, k)) * u[fu(g, i + 1, j, k)];
     float ff = __ldg(g.ov + fv(g, i, j, k)) * v[fv(g, i, j, k)];
@@ -381,13 +378,19 @@ __global__ void k_divergence(Geo g, const float* __restrict__ u, const float* __
     float ft = __ldg(g.ow + fw(g, i, j, k + 1)) * w[fw(g, i, j, k + 1)];
     float d = ((fr - fl + ft - fb) + (fk - ff)) / g.dx;
     if (g.wall) d = d + wall_flux(g, i, j, k);
-    out[c] = d;
-  } else {
-    float fl = u[fu(g, i, j, k)], fr = u[fu(g, i + 1, j, k)];
-    float ff = v[fv(g, i, j, k)], fk = v[fv(g, i, j + 1, k)];
-    float fb = w[fw(g, i, j, k)], ft = w[fw(g, i, j, k + 1)];
-    out[c] = ((fr - fl + ft - fb) + (fk - ff)) / g.dx;
+    return d;
   }
+  float fl = u[fu(g, i, j, k)], fr = u[fu(g, i + 1, j, k)];
+  float ff = v[fv(g, i, j, k)], fk = v[fv(g, i, j + 1, k)];
+  float fb = w[fw(g, i, j, k)], ft = w[fw(g, i, j, k + 1)];
+  return ((fr - fl + ft - fb) + (fk - ff)) / g.dx;
+}
+__global__ void k_divergence(Geo g, const float* __restrict__ u, const float* __restrict__ v,
+                             const float* __restrict__ w, float* __restrict__ out) {
+  KSTART();
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= g.n) return;
+  out[c] = divergence_at(g, u, v, w, c);
 }
 
 // p = 0 on dry cells (delta3d_mobile.rs:485-494).
@@ -450,12 +453,9 @@ __device__ __forceinline__ float level_row(const Lev& L, int i, int j, int k, in
 }
 
 // The diagonal: row_sums with p absent (delta3d_multigrid.rs:205, 236-241).
-__global__ void k_level_diag(Lev L) {
-  KSTART();
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= L.n) return;
+__device__ __forceinline__ float level_diag_at(const Lev& L, int c) {
   int i = c % L.nx, t = c / L.nx, j = t % L.ny, k = t / L.ny;
-  if (L.kind[c] <= 0.f) { L.diag[c] = 0.f; return; }
+  if (L.kind[c] <= 0.f) return 0.f;
   float acc = 0.f;
   const int nxny = L.nx * L.ny;
   auto face = [&](float a, bool has, int m, bool top) {
@@ -474,7 +474,13 @@ __global__ void k_level_diag(Lev L) {
   face(L.ov[(k * (L.ny + 1) + j + 1) * L.nx + i], j + 1 < L.ny, c + L.nx, false);
   face(L.ow[(k * L.ny + j) * L.nx + i], k > 0, c - nxny, false);
   face(L.ow[((k + 1) * L.ny + j) * L.nx + i], k + 1 < L.nz, c + nxny, true);
-  L.diag[c] = acc * L.inv;
+  return acc * L.inv;
+}
+__global__ void k_level_diag(Lev L) {
+  KSTART();
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= L.n) return;
+  L.diag[c] = level_diag_at(L, c);
 }
 
 // Damped Jacobi sweep (smooth3): xout = xin + w (r - L xin) / diag where diag > 0.  zero_in = 1
@@ -520,10 +526,7 @@ __global__ void k_level_restrict(Lev F, Lev C, const Scalars* S, int gate) {
 // ------------------------------------------------------------------------------------------------
 // coarsen3 (delta3d_multigrid.rs:141-206) and fine_kind3 (:357-367)
 
-__global__ void k_coarsen_kind_fine(Geo g, Lev C) {
-  KSTART();
-  int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= C.n) return;
+__device__ __forceinline__ float coarsen_kind_fine_at(const Geo& g, const Lev& C, int q) {
   int ci = q % C.nx, t = q / C.nx, cj = t % C.ny, ck = t / C.ny;
   bool active = false, air = false;
 #pragma unroll
@@ -534,13 +537,16 @@ __global__ void k_coarsen_kind_fine(Geo g, Lev C) {
     if (v > 0.f) active = true;
     else if (v < 0.f) air = true;
   }
-  C.kind[q] = active ? 1.f : (air ? -1.f : 0.f);
+  return active ? 1.f : (air ? -1.f : 0.f);
 }
-
-__global__ void k_coarsen_kind_level(Lev F, Lev C) {
+__global__ void k_coarsen_kind_fine(Geo g, Lev C) {
   KSTART();
   int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= C.n) return;
+  C.kind[q] = coarsen_kind_fine_at(g, C, q);
+}
+
+__device__ __forceinline__ float coarsen_kind_level_at(const Lev& F, const Lev& C, int q) {
   int ci = q % C.nx, t = q / C.nx, cj = t % C.ny, ck = t / C.ny;
   bool active = false, air = false;
 #pragma unroll
@@ -550,17 +556,22 @@ __global__ void k_coarsen_kind_level(Lev F, Lev C) {
     if (v > 0.f) active = true;
     else if (v < 0.f) air = true;
   }
-  C.kind[q] = active ? 1.f : (air ? -1.f : 0.f);
+  return active ? 1.f : (air ? -1.f : 0.f);
+}
+__global__ void k_coarsen_kind_level(Lev F, Lev C) {
+  KSTART();
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= C.n) return;
+  C.kind[q] = coarsen_kind_level_at(F, C, q);
 }
 
 // Coarse apertures: mean of the 4 fine faces a coarse face covers.  `fo*` are the fine apertures
 // (nullptr: a flat fine level, every aperture 1).  fnx/fny are the fine dimensions.
-__global__ void k_coarsen_open(int fnx, int fny, const float* __restrict__ fou, const float* __restrict__ fov,
-                               const float* __restrict__ fow, const unsigned char* __restrict__ act, Lev C) {
-  KSTART();
+__device__ __forceinline__ void coarsen_open_at(int fnx, int fny, const float* __restrict__ fou,
+                                                const float* __restrict__ fov, const float* __restrict__ fow,
+                                                const unsigned char* __restrict__ act, const Lev& C, int q) {
   int cx = C.nx, cy = C.ny, cz = C.nz;
   int nu = (cx + 1) * cy * cz, nv = cx * (cy + 1) * cz, nw = cx * cy * (cz + 1);
-  int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q < nu) {
     int i = q % (cx + 1), t = q / (cx + 1), j = t % cy, k = t / cy;
     float s = 0.f;
@@ -601,6 +612,11 @@ __global__ void k_coarsen_open(int fnx, int fny, const float* __restrict__ fou, 
     }
     C.ow[q] = 0.25f * s;
   }
+}
+__global__ void k_coarsen_open(int fnx, int fny, const float* __restrict__ fou, const float* __restrict__ fov,
+                               const float* __restrict__ fow, const unsigned char* __restrict__ act, Lev C) {
+  KSTART();
+  coarsen_open_at(fnx, fny, fou, fov, fow, act, C, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -679,11 +695,13 @@ __device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
   z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
   return z ^ (z >> 31);
 }
+__device__ __forceinline__ unsigned long long hash_at(const float* __restrict__ p, int q) {
+  return mix64(((unsigned long long)(unsigned)__float_as_int(p[q]) << 32 | (unsigned)q) + 0x9E3779B97F4A7C15ull);
+}
 __global__ void k_hash(int n, const float* __restrict__ p, Scalars* S) {
   KSTART();
   unsigned long long h = 0;
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x)
-    h += mix64(((unsigned long long)(unsigned)__float_as_int(p[q]) << 32 | (unsigned)q) + 0x9E3779B97F4A7C15ull);
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) h += hash_at(p, q);
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) h += __shfl_down_sync(0xffffffffu, h, o);
   if ((threadIdx.x & 31) == 0) atomicAdd(&S->hash, h);

@@ -41,6 +41,9 @@ struct fd3_unet {
   std::vector<void*> allocations;
   unsigned long long launches = 0;
   int conv_tc = 1;        // 1: convolutions on tcgen05 (k_conv_tc), 0: on mma.sync (k_conv)
+  // how FCG uses the network: 0 = M(r) = the network's approximation of A^-1 r; 1 = M(r) = V(r) plus
+  // the network's approximation of A^-1 (r - A V(r)), V the multigrid V-cycle
+  int mode = 0;
   int* dflag = nullptr;   // set by k_conv_tc when a bounded wait ran out
 };
 
@@ -413,6 +416,41 @@ __global__ void k_fcg_zdots(int n, const unsigned short* __restrict__ codes, flo
   block_add(zr, dots + 5);
 }
 
+// rho = r - A z on the wet rows (the residual a V-cycle z = V(r) leaves), |rho|^2 into dots[3].
+__global__ void k_vres(Geo g, const unsigned short* __restrict__ codes, const float* __restrict__ r,
+                       const float* __restrict__ z, float* __restrict__ rho, double* dots) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  double rr = 0.0;
+  if (c < g.n) {
+    const unsigned code = codes[c];
+    float v = 0.f;
+    if (code & RC_WET) {
+      int i, j, k;
+      cell_ijk(g, c, i, j, k);
+      v = r[c] - apply_code(g, code, i, j, k, c, Load{z});
+    }
+    rho[c] = v;
+    rr = (double)v * (double)v;
+  }
+  block_add(rr, dots + 3);
+}
+
+// The hybrid preconditioner's output: z = y + z_mg on the wet rows (0 elsewhere), then z.q and z.r.
+__global__ void k_fcg_zdots_add(int n, const unsigned short* __restrict__ codes, float* __restrict__ z,
+                                const float* __restrict__ zmg, const float* __restrict__ q,
+                                const float* __restrict__ r, double* dots) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  double zq = 0.0, zr = 0.0;
+  if (c < n) {
+    float zc = (codes[c] & RC_WET) ? z[c] + zmg[c] : 0.f;
+    z[c] = zc;
+    zq = (double)zc * (double)q[c];
+    zr = (double)zc * (double)r[c];
+  }
+  block_add(zq, dots + 4);
+  block_add(zr, dots + 5);
+}
+
 // d = z + beta d
 __global__ void k_fcg_dir(int n, float beta, const float* __restrict__ z, float* __restrict__ d) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -632,13 +670,27 @@ int fcg(fd3_volume* V, fd3_unet* N, uint32_t max_fcg, double stall, uint32_t* it
   double dq_prev = 0;
   cudaStream_t net_stream = N->stream;
   N->stream = V->stream;
+  const bool hybrid = N->mode == 1;
   auto precondition = [&](double rnorm2) -> int {
     CK(cudaMemsetAsync(V->fsc, 0, 8 * sizeof(double), V->stream));
-    LAUNCH(V, k_fcg_input, V->n, G, codes, (const float*)V->res, V->fin, V->fsc);
+    const float* net_in = V->res;
+    if (hybrid) {  // z_mg = V(r) in V->z, then the network sees the residual it leaves
+      vcycle(V, 0, FIN_RZ_PRIME);
+      LAUNCH(V, k_vres, V->n, G, codes, (const float*)V->res, (const float*)V->z, V->fz, V->fsc);
+      TRY(pull_dots(V));
+      rnorm2 = V->hfsc[3];
+      CK(cudaMemsetAsync(V->fsc, 0, 8 * sizeof(double), V->stream));
+      net_in = V->fz;
+    }
+    LAUNCH(V, k_fcg_input, V->n, G, codes, net_in, V->fin, V->fsc);
     const float s = (float)std::sqrt(std::max(rnorm2, 1e-300) / (double)V->n);
     const float inv = 1.f / s, outs = s * dx2;
     TRY(fd3_unet_forward(N, 1, V->nz, V->ny, V->nx, V->fin, &inv, &outs, V->fz));
-    LAUNCH(V, k_fcg_zdots, V->n, V->n, codes, V->fz, (const float*)V->tmp, (const float*)V->res, V->fsc);
+    if (hybrid)
+      LAUNCH(V, k_fcg_zdots_add, V->n, V->n, codes, V->fz, (const float*)V->z, (const float*)V->tmp,
+             (const float*)V->res, V->fsc);
+    else
+      LAUNCH(V, k_fcg_zdots, V->n, V->n, codes, V->fz, (const float*)V->tmp, (const float*)V->res, V->fsc);
     return FD3_OK;
   };
   int e = [&]() -> int {
@@ -703,6 +755,26 @@ int fd3_apply_device(fd3_volume* V, const float* d_x, float* d_out) {
   return sync(V);
 }
 
+int fd3_unet_set_mode(fd3_unet* N, int mode) {
+  if (!N || mode < 0 || mode > 1) return FD3_ERR_INVALID_ARGUMENT;
+  N->mode = mode;
+  return FD3_OK;
+}
+
+int fd3_vcycle_residual_device(fd3_volume* V, const float* d_r, float* d_rho, double* rho2) {
+  if (!V || !d_r || !d_rho) return FD3_ERR_INVALID_ARGUMENT;
+  if (!V->has_mg || V->levels.empty()) return FD3_ERR_DOMAIN;
+  prepare_multigrid(V);
+  CK(cudaMemcpyAsync(V->res, d_r, (size_t)V->n * 4, cudaMemcpyDeviceToDevice, V->stream));
+  vcycle(V, 0, FIN_RZ_PRIME);
+  CK(cudaMemsetAsync(V->fsc, 0, 8 * sizeof(double), V->stream));
+  LAUNCH(V, k_vres, V->n, V->geo(), (const unsigned short*)V->codes, (const float*)V->res, (const float*)V->z, d_rho,
+         V->fsc);
+  TRY(pull_dots(V));
+  if (rho2) *rho2 = V->hfsc[3];
+  return FD3_OK;
+}
+
 int fd3_learned_input(fd3_volume* V, const float* d_r, float* d_in3, double* rr) {
   if (!V || !d_r || !d_in3) return FD3_ERR_INVALID_ARGUMENT;
   CK(cudaMemsetAsync(V->fsc, 0, 8 * sizeof(double), V->stream));
@@ -735,6 +807,10 @@ int fd3_project_learned(fd3_volume* V, fd3_unet* N, float scale, float k1, uint3
   TRY(attach_learned(V));
   CK(cudaMemcpyAsync(V->sv_p, V->p, (size_t)V->n * 4, cudaMemcpyDeviceToDevice, V->stream));
   TRY(assemble_device(V, scale));
+  if (N->mode == 1) {
+    if (!V->has_mg || V->levels.empty()) return FD3_ERR_DOMAIN;
+    prepare_multigrid(V);
+  }
   Geo G = V->geo();
   LAUNCH(V, k_zero_dry, V->n, G, V->p);
   residual(V, (int)FIN_RR0);

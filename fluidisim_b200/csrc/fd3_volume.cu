@@ -26,6 +26,7 @@
 #include "../../include/fluidisim_delta3d.h"
 #include "fd3_cut.cuh"
 #include "fd3_zmarch4.cuh"
+#include "fd3_batch.cuh"
 #include "fd3_linear.cuh"
 #include "fd3_levels.cuh"
 
@@ -56,6 +57,21 @@ int cuda_fail(cudaError_t e, const char* what, int line) {
 
 inline int blocks_for(long long n) { return (int)((n + TPB - 1) / TPB); }
 
+// Makes `dev` the calling thread's current device for one scope and restores the previous one.
+struct ScopedDevice {
+  int prev = -1;
+  cudaError_t err = cudaSuccess;
+  explicit ScopedDevice(int dev) {
+    err = cudaGetDevice(&prev);
+    if (err == cudaSuccess && prev != dev) err = cudaSetDevice(dev);
+    else if (err == cudaSuccess) prev = -1;  // already current: nothing to restore
+  }
+  ~ScopedDevice() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+
 // Coarse levels of at most this many cells issue their passes' loads before the row code and the
 // gate, and restrict their residual in the same pass that computes it (k_level_restrict8).  These
 // are the latency-bound levels: measured 2% and 1.4% faster at 128^3; the loads ahead of the code
@@ -71,8 +87,10 @@ constexpr int TAIL_MAX_CELLS = 512;
 // PROJECTION_DIVERGENCE_TOLERANCE (delta_projection.rs:192)
 constexpr double kDivTol = 1e-5;
 // gamma_8 and gamma_10 of u = 2^-24 (delta_projection.rs:200-203, delta3d.rs:69-72)
-const float kRoundoff2D = 8.0f * (1.0f / 16777216.0f) / (1.0f - 8.0f * (1.0f / 16777216.0f));
-const float kRoundoff3D = 10.0f * (1.0f / 16777216.0f) / (1.0f - 10.0f * (1.0f / 16777216.0f));
+constexpr float kRoundoff2D = 8.0f * (1.0f / 16777216.0f) / (1.0f - 8.0f * (1.0f / 16777216.0f));
+constexpr float kRoundoff3D = 10.0f * (1.0f / 16777216.0f) / (1.0f - 10.0f * (1.0f / 16777216.0f));
+static_assert(kRoundoff2D == BATCH_ROUNDOFF_2D && kRoundoff3D == BATCH_ROUNDOFF_3D && kDivTol == BATCH_DIV_TOL,
+              "the persistent batch shares the outer loop's constants");
 
 }  // namespace
 
@@ -1877,6 +1895,198 @@ int fd3_project_batch(fd3_volume* const* vols, size_t count, const float* scales
   return FD3_OK;
 }
 
+}  // extern "C"
+
+// ------------------------------------------------------------------------- the persistent batch
+struct fd3_batch {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int cluster = 0, clusters = 0;
+  std::vector<fd3_volume*> vols;
+  std::vector<cudaEvent_t> ready;  // one per volume: its stream's work before the launch
+  BatchPatch* hp = nullptr;        // pinned: the patch table, refreshed per call
+  BatchResult* hres = nullptr;     // pinned
+  BatchPatch* dp = nullptr;
+  BatchResult* dres = nullptr;
+  int *dorder = nullptr, *dstart = nullptr;
+  std::vector<int> order, start;
+  unsigned long long launches = 0;
+};
+
+namespace {
+
+void batch_release(fd3_batch* B) {
+  if (B->stream) cudaStreamSynchronize(B->stream);
+  for (cudaEvent_t e : B->ready) cudaEventDestroy(e);
+  if (B->hp) cudaFreeHost(B->hp);
+  if (B->hres) cudaFreeHost(B->hres);
+  if (B->dp) cudaFree(B->dp);
+  if (B->dres) cudaFree(B->dres);
+  if (B->dorder) cudaFree(B->dorder);
+  if (B->dstart) cudaFree(B->dstart);
+  if (B->stream) cudaStreamDestroy(B->stream);
+}
+
+cudaLaunchConfig_t batch_config(fd3_batch* B, cudaLaunchAttribute* attr, int clusters) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3((unsigned)(clusters * B->cluster));
+  cfg.blockDim = dim3(BATCH_THREADS);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = B->stream;
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = (unsigned)B->cluster;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cfg;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fd3_batch_create(fd3_volume* const* vols, size_t count, int cluster_size, fd3_batch** out) {
+  if (!out || !vols || !count) return FD3_ERR_INVALID_ARGUMENT;
+  if (cluster_size != 1 && cluster_size != 2 && cluster_size != 4 && cluster_size != 8) return FD3_ERR_INVALID_ARGUMENT;
+  std::vector<const fd3_volume*> seen(vols, vols + count);
+  for (const fd3_volume* V : seen) {
+    if (!V) return FD3_ERR_INVALID_ARGUMENT;
+    if (V->device != vols[0]->device) return FD3_ERR_INVALID_ARGUMENT;
+    // the batched projection: f64 reductions, f32 storage, the mobile rows with multigrid
+    if (!V->has_mg || V->ord() || V->opt.storage != FD3_STORAGE_F32) return FD3_ERR_DOMAIN;
+  }
+  std::sort(seen.begin(), seen.end());
+  if (std::adjacent_find(seen.begin(), seen.end()) != seen.end()) return FD3_ERR_INVALID_ARGUMENT;
+  fd3_batch* B = new (std::nothrow) fd3_batch();
+  if (!B) return FD3_ERR_OUT_OF_MEMORY;
+  B->device = vols[0]->device;
+  B->cluster = cluster_size;
+  B->vols.assign(vols, vols + count);
+  ScopedDevice on(B->device);
+  auto fail = [&](int e) { batch_release(B); delete B; return e; };
+  if (on.err != cudaSuccess) return fail(cuda_fail(on.err, "cudaSetDevice", __LINE__));
+  cudaError_t e = cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return fail(cuda_fail(e, "cudaStreamCreateWithFlags", __LINE__));
+  // clusters resident at once: the patches are dealt to that many solvers
+  cudaLaunchAttribute attr[1];
+  cudaLaunchConfig_t cfg = batch_config(B, attr, 1);
+  int active = 0;
+  e = cudaOccupancyMaxActiveClusters(&active, k_batch_project, &cfg);
+  if (e != cudaSuccess || active <= 0) return fail(cuda_fail(e != cudaSuccess ? e : cudaErrorInvalidConfiguration,
+                                                             "cudaOccupancyMaxActiveClusters", __LINE__));
+  B->clusters = (int)std::min<size_t>((size_t)active, count);
+  // largest patch first to the least loaded cluster (cells as the cost)
+  std::vector<int> idx(count);
+  for (size_t i = 0; i < count; ++i) idx[i] = (int)i;
+  std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return vols[a]->n > vols[b]->n; });
+  std::vector<std::vector<int>> lists(B->clusters);
+  std::vector<long long> load(B->clusters, 0);
+  for (int i : idx) {
+    int c = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+    lists[c].push_back(i);
+    load[c] += vols[i]->n;
+  }
+  B->start.push_back(0);
+  for (auto& l : lists) {
+    B->order.insert(B->order.end(), l.begin(), l.end());
+    B->start.push_back((int)B->order.size());
+  }
+  if ((e = cudaMallocHost(&B->hp, count * sizeof(BatchPatch))) != cudaSuccess ||
+      (e = cudaMallocHost(&B->hres, count * sizeof(BatchResult))) != cudaSuccess ||
+      (e = cudaMalloc(&B->dp, count * sizeof(BatchPatch))) != cudaSuccess ||
+      (e = cudaMalloc(&B->dres, count * sizeof(BatchResult))) != cudaSuccess ||
+      (e = cudaMalloc(&B->dorder, count * sizeof(int))) != cudaSuccess ||
+      (e = cudaMalloc(&B->dstart, B->start.size() * sizeof(int))) != cudaSuccess)
+    return fail(cuda_fail(e, "batch allocation", __LINE__));
+  e = cudaMemcpyAsync(B->dorder, B->order.data(), count * sizeof(int), cudaMemcpyHostToDevice, B->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(B->dstart, B->start.data(), B->start.size() * sizeof(int), cudaMemcpyHostToDevice, B->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(B->stream);
+  if (e != cudaSuccess) return fail(cuda_fail(e, "batch tables", __LINE__));
+  B->ready.resize(count, nullptr);
+  for (size_t i = 0; i < count; ++i)
+    if ((e = cudaEventCreateWithFlags(&B->ready[i], cudaEventDisableTiming)) != cudaSuccess)
+      return fail(cuda_fail(e, "cudaEventCreateWithFlags", __LINE__));
+  *out = B;
+  return FD3_OK;
+}
+
+void fd3_batch_destroy(fd3_batch* B) {
+  if (!B) return;
+  ScopedDevice on(B->device);
+  batch_release(B);
+  delete B;
+}
+
+int fd3_batch_clusters(const fd3_batch* B, int* clusters, int* cluster_size) {
+  if (!B) return FD3_ERR_INVALID_ARGUMENT;
+  if (clusters) *clusters = B->clusters;
+  if (cluster_size) *cluster_size = B->cluster;
+  return FD3_OK;
+}
+
+uint64_t fd3_batch_kernel_launches(const fd3_batch* B) { return B ? B->launches : 0; }
+
+int fd3_batch_project(fd3_batch* B, const float* scales, const float* k1s, uint32_t max_iters, int reset_pressure,
+                      const float* const* in_u, const float* const* in_v, const float* const* in_w,
+                      fd3_report* reports, int* statuses) {
+  if (!B || !scales || !k1s || !reports || !statuses) return FD3_ERR_INVALID_ARGUMENT;
+  const size_t count = B->vols.size();
+  if ((in_u || in_v || in_w) && !(in_u && in_v && in_w)) return FD3_ERR_INVALID_ARGUMENT;
+  ScopedDevice on(B->device);
+  if (on.err != cudaSuccess) return cuda_fail(on.err, "cudaSetDevice", __LINE__);
+  for (size_t i = 0; i < count; ++i) {
+    fd3_volume* V = B->vols[i];
+    if (!std::isfinite(scales[i]) || !std::isfinite(k1s[i])) return FD3_ERR_NOT_FINITE;
+    V->linear = false;
+    BatchPatch& P = B->hp[i];
+    P.g = V->geo();
+    P.codes = V->codes;
+    P.u = V->u; P.v = V->v; P.w = V->w; P.us = V->us; P.vs = V->vs; P.ws = V->ws;
+    P.p = V->p; P.sv_p = V->sv_p; P.rhs = V->rhs; P.prec = V->prec; P.res = V->res;
+    P.sv_u = V->sv_u; P.sv_v = V->sv_v; P.sv_w = V->sv_w;
+    P.dir = V->dir; P.dir2 = V->dir2; P.q = V->tmp; P.z = V->z; P.z2 = V->z2;
+    P.in_u = in_u ? in_u[i] : nullptr;
+    P.in_v = in_v ? in_v[i] : nullptr;
+    P.in_w = in_w ? in_w[i] : nullptr;
+    P.lev = V->dlev;
+    P.nlev = (int)V->levels.size();
+    P.nu = V->nu; P.nv = V->nv; P.nw = V->nw;
+    P.scale = scales[i]; P.k1 = k1s[i];
+    P.max_iters = max_iters;
+    P.flat2d = V->ny == 1 ? 1 : 0;
+    P.reset_p = reset_pressure ? 1 : 0;
+    P.S = V->dS;
+    // the volume's earlier work (on its own stream) comes before the launch
+    CK(cudaEventRecord(B->ready[i], V->stream));
+    CK(cudaStreamWaitEvent(B->stream, B->ready[i], 0));
+  }
+  CK(cudaMemcpyAsync(B->dp, B->hp, count * sizeof(BatchPatch), cudaMemcpyHostToDevice, B->stream));
+  cudaLaunchAttribute attr[1];
+  cudaLaunchConfig_t cfg = batch_config(B, attr, B->clusters);
+  CK(cudaLaunchKernelEx(&cfg, k_batch_project, (const BatchPatch*)B->dp, (const int*)B->dorder,
+                        (const int*)B->dstart, B->dres));
+  B->launches++;
+  CK(cudaMemcpyAsync(B->hres, B->dres, count * sizeof(BatchResult), cudaMemcpyDeviceToHost, B->stream));
+  CK(cudaStreamSynchronize(B->stream));
+  for (size_t i = 0; i < count; ++i) {
+    const BatchResult& R = B->hres[i];
+    statuses[i] = R.status;
+    fd3_report& rep = reports[i];
+    memset(&rep, 0, sizeof rep);
+    if (R.status) continue;
+    rep.iterations = R.iterations;
+    rep.degraded = (uint8_t)R.degraded;
+    rep.residual = R.residual;
+    rep.divergence = R.divergence;
+    rep.floor = (uint8_t)R.floor_stop;
+    rep.backward_error = R.backward_error;
+    rep.divergence_plain = R.divergence_plain;
+  }
+  return FD3_OK;
+}
+
 int fd3_last_refused_report(const fd3_volume* V, fd3_report* rep) {
   if (!V || !rep) return FD3_ERR_INVALID_ARGUMENT;
   if (!V->has_refused) return FD3_ERR_DOMAIN;
@@ -2072,19 +2282,6 @@ constexpr int kMaxDevices = 64;
 std::mutex g_noalloc_mutex;
 void* g_noalloc_addr[kMaxDevices] = {};
 
-// Makes `dev` the calling thread's current device for one scope and restores the previous one.
-struct ScopedDevice {
-  int prev = -1;
-  cudaError_t err = cudaSuccess;
-  explicit ScopedDevice(int dev) {
-    err = cudaGetDevice(&prev);
-    if (err == cudaSuccess && prev != dev) err = cudaSetDevice(dev);
-    else if (err == cudaSuccess) prev = -1;  // already current: nothing to restore
-  }
-  ~ScopedDevice() {
-    if (prev >= 0) cudaSetDevice(prev);
-  }
-};
 
 // The device address of g_noalloc_scratch on device `dev` (which must be current), looked up once
 // per device: in host code the symbol is only a host-side stand-in, not a device address.

@@ -64,6 +64,8 @@ def _bind(L: C.CDLL) -> C.CDLL:
     L.fd3_problem_device.argtypes = [vp, C.POINTER(vp), C.POINTER(vp)]
     L.fd3_apply_device.argtypes = [vp, vp, vp]
     L.fd3_learned_input.argtypes = [vp, vp, vp, C.POINTER(C.c_double)]
+    L.fd3_unet_set_mode.argtypes = [vp, i32]
+    L.fd3_vcycle_residual_device.argtypes = [vp, vp, vp, C.POINTER(C.c_double)]
     L.fd3_residual_loss.argtypes = [vp, vp, vp, f32, vp, C.POINTER(C.c_double)]
     L.fd3_project_learned.argtypes = [vp, vp, f32, f32, u32, u32, C.POINTER(_Report), C.POINTER(u32),
                                       C.POINTER(i32)]
@@ -145,6 +147,15 @@ class UNet:
     def kernel_launches(self) -> int:
         return int(self._L.fd3_unet_kernel_launches(self._h))
 
+    def set_mode(self, mode: int):
+        """How project_learned uses the network: MODE_NET (the preconditioner is the network) or
+        MODE_VCYCLE_PLUS_NET (the V-cycle plus the network's correction of the residual it leaves)."""
+        self._check(self._L.fd3_unet_set_mode(self._h, int(mode)), "set_mode")
+
+
+MODE_NET = 0
+MODE_VCYCLE_PLUS_NET = 1
+
 
 # ------------------------------------------------------------------- the volume's learned hooks
 def assemble_device(vol: Volume3, scale: float):
@@ -170,6 +181,15 @@ def learned_input(vol: Volume3, d_r: int, d_in3: int) -> float:
     L = _bind(vol._L)
     rr = C.c_double()
     vol._check(L.fd3_learned_input(vol._h, C.c_void_p(d_r), C.c_void_p(d_in3), C.byref(rr)), "learned_input")
+    return rr.value
+
+
+def vcycle_residual(vol: Volume3, d_r: int, d_rho: int) -> float:
+    """rho = r - A V(r), the residual a multigrid V-cycle leaves (d_rho may be d_r); returns |rho|^2."""
+    L = _bind(vol._L)
+    rr = C.c_double()
+    vol._check(L.fd3_vcycle_residual_device(vol._h, C.c_void_p(d_r), C.c_void_p(d_rho), C.byref(rr)),
+               "vcycle_residual")
     return rr.value
 
 
@@ -203,11 +223,13 @@ def project_learned(vol: Volume3, net: UNet, scale: float, k1: float, max_iters:
 # ------------------------------------------------------------------------------------ training
 class Trainer:
     """Trains `net` on right-hand sides assembled by the library from `volumes` (one geometry each,
-    all of the same shape) with seeded random face velocities U[-1, 1], in batches.
+    all of the same shape) with seeded random face velocities U[-1, 1], in batches.  With
+    samples="vcycle" each sample is instead the residual a V-cycle leaves of such a right-hand
+    side, r - A V(r): what the network corrects in MODE_VCYCLE_PLUS_NET.
 
     Device buffers are torch tensors (memory only); every computation is a library kernel."""
 
-    def __init__(self, net: UNet, volumes, scale: float, batch: int, seed: int = 0):
+    def __init__(self, net: UNet, volumes, scale: float, batch: int, seed: int = 0, samples: str = "rhs"):
         import torch
         self.torch = torch
         self.net, self.vols, self.scale, self.batch = net, list(volumes), scale, batch
@@ -223,6 +245,9 @@ class Trainer:
         self.gen.manual_seed(seed)
         self.dx2 = float(np.float32(v0.dx) ** 2)
         self.samples = 0
+        if samples not in ("rhs", "vcycle"):
+            raise ValueError(samples)
+        self.kind = samples
 
     def _sample(self, k: int, vol: Volume3):
         """Random velocity on vol, its rhs into slot k of the batch, the input into x."""
@@ -238,6 +263,9 @@ class Trainer:
         bk = self.b[k * n:(k + 1) * n]
         t.cuda.synchronize()
         bk.copy_(_as_tensor(rhs, n))
+        if self.kind == "vcycle":
+            t.cuda.synchronize()
+            vcycle_residual(vol, bk.data_ptr(), bk.data_ptr())
         rr = learned_input(vol, bk.data_ptr(), self.x[3 * k * n:3 * (k + 1) * n].data_ptr())
         return rr
 

@@ -246,6 +246,31 @@ int fd3_advect_for_tests(fd3_volume* v, float dt);
  * pointer, or one volume listed twice). */
 int fd3_project_batch(fd3_volume* const* volumes, size_t count, const float* scales, const float* k1s,
                       uint32_t max_iters, int threads, fd3_report* reports, int* statuses);
+/* The persistent batch (no reference counterpart): many volumes (patches) projected by ONE kernel
+ * launch.  Thread-block clusters of `cluster_size` CTAs (1, 2, 4 or 8) of 1024 threads are
+ * independent solvers; the volumes are dealt, largest first, to the least loaded of the clusters
+ * that fit the GPU at once, and each cluster runs its volumes' whole project_mobile3 (assembly,
+ * hierarchy, multigrid PCG, outer checks, report) on the device, one volume after another.
+ * fd3_batch_create validates and prepares (all of its allocations happen here): every volume on
+ * the same device, listed once, with multigrid, f64 reductions and f32 storage (FD3_ERR_DOMAIN
+ * otherwise).  The batch holds pointers into the volumes: destroy it before them.  Calls on one
+ * batch are not thread-safe. */
+typedef struct fd3_batch fd3_batch;
+int fd3_batch_create(fd3_volume* const* volumes, size_t count, int cluster_size, fd3_batch** out);
+void fd3_batch_destroy(fd3_batch* batch);
+/* The clusters the volumes were dealt to and their size. */
+int fd3_batch_clusters(const fd3_batch* batch, int* clusters, int* cluster_size);
+uint64_t fd3_batch_kernel_launches(const fd3_batch* batch);
+/* Projects every volume of the batch as fd3_project_mobile does (us = u), in one launch on the
+ * batch's own stream, after each volume's stream has finished its earlier work; returns when all
+ * are done.  reset_pressure = 1 starts every volume from p = 0 (fd3_reset_pressure).  in_u, in_v,
+ * in_w (all or none; device pointers per volume, of the face counts) are copied into the volumes'
+ * velocities first.  statuses[i] is volume i's result (FD3_OK, FD3_ERR_NOT_FINITE for a
+ * non-finite input, ...); a refused volume keeps u, v, w and p as they were.  reports[i] is its
+ * Report.  Allocates nothing. */
+int fd3_batch_project(fd3_batch* batch, const float* scales, const float* k1s, uint32_t max_iters, int reset_pressure,
+                      const float* const* in_u, const float* const* in_v, const float* const* in_w,
+                      fd3_report* reports, int* statuses);
 /* Volume3::last_refused_report (delta3d_mobile.rs:982); FD3_ERR_DOMAIN when none. */
 int fd3_last_refused_report(const fd3_volume* v, fd3_report* report);
 
@@ -350,6 +375,15 @@ int fd3_assemble_device(fd3_volume* v, float scale);
 int fd3_problem_device(fd3_volume* v, float** d_rhs, const unsigned short** d_codes);
 int fd3_apply_device(fd3_volume* v, const float* d_x, float* d_out);
 int fd3_learned_input(fd3_volume* v, const float* d_r, float* d_in3, double* rr);
+/* How fd3_project_learned uses the network (no reference counterpart): 0 (default) = FCG's
+ * preconditioner is the network alone; 1 = the multigrid V-cycle plus the network's approximation
+ * of A^-1 applied to the residual the V-cycle leaves (a network trained on such residuals, see
+ * fd3_vcycle_residual_device).  Mode 1 needs a volume with multigrid. */
+int fd3_unet_set_mode(fd3_unet* net, int mode);
+/* The residual a V-cycle leaves: rho = r - A V(r) for a device vector r of the last assembly's
+ * problem (fd3_assemble_device), |rho|^2 into *rho2 (may be NULL).  Uses the volume's work buffers;
+ * d_rho may equal d_r.  FD3_ERR_DOMAIN without multigrid.  No reference counterpart. */
+int fd3_vcycle_residual_device(fd3_volume* v, const float* d_r, float* d_rho, double* rho2);
 int fd3_residual_loss(fd3_volume* v, const float* d_z, const float* d_b, float weight, float* d_grad, double* loss);
 
 /* project_mobile3 with the learned FCG in front (from the current p): FCG(1) with the network as
