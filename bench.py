@@ -1205,8 +1205,9 @@ def main():
     ap.add_argument("--train-samples", type=int, default=20000,
                     help="training samples of the learned preconditioner (20,000 at 64^3, as config 4 asks)")
     ap.add_argument("--kernels", type=int, default=0,
-                    help="fine-level kernel family (fd3_options.kernels): 0 the default (four cells per thread when "
-                         "nx % 4 == 0), 3 two cells per thread, 2 one cell per thread in the same blocking")
+                    help="fine-level kernel family (fd3_options.kernels): 0 the default (four cells per thread from "
+                         "2^23 cells, else two), 3 two cells per thread, 4 four cells per thread, 2 one cell per "
+                         "thread in the same blocking")
     ap.add_argument("--graphs", type=int, default=1,
                     help="1: the inner loop as a CUDA graph with a WHILE node; 0: host-driven (for ncu launch lists)")
     args = ap.parse_args()

@@ -81,6 +81,9 @@ struct ScopedDevice {
 #endif
 constexpr int SPEC_MAX_CELLS = FD3_SPEC_MAX;
 
+// Volumes from this many cells run the four-cells-per-thread fine kernels by default (kernels = 0).
+constexpr long long kQuadMinCells = 1LL << 23;
+
 // Coarse levels of at most this many cells are solved together by one CTA (k_coarse_tail).
 constexpr int TAIL_MAX_CELLS = 512;
 
@@ -192,9 +195,15 @@ struct fd3_volume {
   }
   bool ord() const { return opt.reduction == FD3_REDUCE_ORDERED_F32; }
   bool blocked() const { return !ord() && opt.kernels != 1; }
-  bool paired() const { return blocked() && (opt.kernels == 0 || opt.kernels == 3) && nx % 2 == 0; }
-  // four cells per thread: the default family for an nx divisible by 4 with f32 storage
-  bool quad() const { return paired() && opt.kernels == 0 && nx % 4 == 0 && opt.storage != FD3_STORAGE_F16; }
+  bool paired() const { return blocked() && (opt.kernels == 0 || opt.kernels == 3 || opt.kernels == 4) && nx % 2 == 0; }
+  // four cells per thread: with f32 storage and nx % 4 == 0, chosen explicitly (kernels = 4) or by
+  // default on volumes of at least kQuadMinCells, where the passes stream from HBM (measured: 256^3
+  // 20.9 against 21.5 ms per projection; at 128^3, where the working set sits in L2 and the passes
+  // are latency-bound, two cells per thread is faster, 3.20 against 3.47 ms)
+  bool quad() const {
+    if (!blocked() || nx % 4 != 0 || opt.storage == FD3_STORAGE_F16) return false;
+    return opt.kernels == 4 || (opt.kernels == 0 && (long long)n >= kQuadMinCells);
+  }
   bool mg_on() const { return has_mg && !linear; }  // the linear path has no multigrid
   // FP16 storage of the V-cycle vectors (fd3_set_options accepts it only with the paired kernels)
   bool half() const { return opt.storage == FD3_STORAGE_F16 && paired() && mg_on(); }
@@ -1427,8 +1436,9 @@ void fd3_destroy(fd3_volume* v) {
 
 int fd3_set_options(fd3_volume* v, const fd3_options* o) {
   if (!v || !o) return FD3_ERR_INVALID_ARGUMENT;
-  if (o->reduction > 1 || o->kernels > 3 || o->no_overlap > 1 || o->storage > 1 || o->no_tile_skip > 1)
+  if (o->reduction > 1 || o->kernels > 4 || o->no_overlap > 1 || o->storage > 1 || o->no_tile_skip > 1)
     return FD3_ERR_DOMAIN;
+  if (o->kernels == 4 && (v->nx % 4 != 0 || o->storage == FD3_STORAGE_F16)) return FD3_ERR_DOMAIN;
   // FP16 storage runs on the paired fine kernels: f64 reductions, kernels = 0 or 3 and an even nx
   if (o->storage == FD3_STORAGE_F16 &&
       (o->reduction != FD3_REDUCE_F64 || (o->kernels != 0 && o->kernels != 3) || v->nx % 2 != 0))

@@ -18,8 +18,14 @@
 
 namespace fd3 {
 
+// Resident CTAs per SM the register budget is cut for: 2 (up to 128 registers) for the passes that
+// carry three raw operand arrays per layer, 3 (up to 85) for the lighter direction and restriction
+// passes, which fit without spilling and gain from the occupancy (measured at 256^3).
 #ifndef FD3_ZMINB4
 #define FD3_ZMINB4 2
+#endif
+#ifndef FD3_ZMINB4_LIGHT
+#define FD3_ZMINB4_LIGHT 3
 #endif
 constexpr int Z4T = 256;
 
@@ -319,7 +325,7 @@ __global__ void __launch_bounds__(Z4T, FD3_ZMINB4) kq_residual(Geo g, const unsi
 
 // d = z (+ beta d); q = A d; d.q; alpha (FIN_DQ).
 template <int QX, int K4>
-__global__ void __launch_bounds__(Z4T, FD3_ZMINB4) kq_dir_apply_dot(Geo g, const unsigned short* __restrict__ codes,
+__global__ void __launch_bounds__(Z4T, FD3_ZMINB4_LIGHT) kq_dir_apply_dot(Geo g, const unsigned short* __restrict__ codes,
                                                                   const float* __restrict__ z,
                                                                   const float* __restrict__ din, float* __restrict__ dout,
                                                                   float* __restrict__ q, Red red, Scalars* S) {
@@ -386,7 +392,7 @@ __global__ void __launch_bounds__(Z4T, FD3_ZMINB4) kq_fine_post2_rz(Geo g, const
 // sum each coarse cell's eight children, in the reference's CHILDREN order, from the two layers
 // kept in shared memory.  Needs even ny, nz (the coarsening rule guarantees them) and even K4.
 template <int QX, int K4>
-__global__ void __launch_bounds__(Z4T, FD3_ZMINB4) kq_fine_restrict(Geo g, const unsigned short* __restrict__ codes,
+__global__ void __launch_bounds__(Z4T, FD3_ZMINB4_LIGHT) kq_fine_restrict(Geo g, const unsigned short* __restrict__ codes,
                                                                   const float* __restrict__ r,
                                                                   const float* __restrict__ z, Lev L, const Scalars* S,
                                                                   int gate) {

@@ -1,5 +1,5 @@
-"""The four-cells-per-thread fine kernels (the default family when nx % 4 == 0) against the other
-families and the oracle, through the C ABI.
+"""The four-cells-per-thread fine kernels (fd3_options.kernels = 4; the default family on volumes of
+2^23 cells or more) against the other families and the oracle, through the C ABI.
 
 Every family evaluates each cell with the same f32 expressions in the same order, so a V-cycle
 (which holds no reduction) gives the same bits whichever family runs it, and the same bits as the
@@ -58,7 +58,7 @@ def test_vcycle_bits_are_the_same_in_every_family_and_the_oracle(shape):
     s = lake(*shape)
     x = scenes.noise(s["nx"] * s["ny"] * s["nz"], 5)
     zs = {}
-    for kernels in (0, 1, 2, 3):
+    for kernels in (0, 1, 2, 3, 4):
         d = device(s, kernels)
         zs[kernels] = d.vcycle_for_tests(x)
         d.close()
@@ -77,21 +77,21 @@ def test_projection_matches_the_two_cell_family(shape):
     s = lake(*shape)
     scale, k1 = scenes.projection_scalars(s)
     out = {}
-    for kernels in (0, 3):
+    for kernels in (4, 3):
         d = device(s, kernels)
         r = d.project_mobile3(scale, k1, 4000)
         out[kernels] = (r, d.pressure().astype(np.float64))
         d.close()
-    (r4, p4), (r2, p2) = out[0], out[3]
+    (r4, p4), (r2, p2) = out[4], out[3]
     assert not r4.degraded and r4.residual <= 1e-6 and r4.divergence_plain <= 1e-5, r4
     assert abs(r4.iterations - r2.iterations) <= 1
     assert np.abs(p4 - p2).max() <= 1e-5 * np.abs(p2).max()
 
 
 def test_quad_family_through_a_batch_of_patches():
-    """Patches whose nx is a multiple of 4 and of 8: the batched entry point on the default family."""
+    """Patches whose nx is a multiple of 4 and of 8: the batched entry point on the four-cell family."""
     ps = batch.patch_scenes(6, seed=11, hi=48)
-    vols = [batch.configure(p) for p in ps]
+    vols = [batch.configure(p, kernels=4) for p in ps]
     sk = [scenes.projection_scalars(p) for p in ps]
     reps, st = batch.project_batch(vols, [a for a, _ in sk], [b for _, b in sk], threads=3)
     assert st == [0] * len(ps)
