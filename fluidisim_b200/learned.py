@@ -298,3 +298,32 @@ def _as_tensor(ptr: int, n: int):
     class _Blob:
         __cuda_array_interface__ = {"shape": (n,), "typestr": "<f4", "data": (ptr, False), "version": 3}
     return torch.as_tensor(_Blob(), device="cuda")
+
+
+def _forward_case(argv=None):
+    """`python -m fluidisim_b200.learned forward [batch] [n] [repeat]`: U-Net forward passes of
+    `batch` samples of n^3 cells (He-initialised weights, random input), a small case for a
+    profiler's capture of the convolutions."""
+    import sys
+
+    import torch
+    args = list(sys.argv[1:] if argv is None else argv)
+    if not args or args[0] != "forward":
+        raise SystemExit("usage: python -m fluidisim_b200.learned forward [batch] [n] [repeat]")
+    batch = int(args[1]) if len(args) > 1 else 4
+    n = int(args[2]) if len(args) > 2 else 64
+    repeat = int(args[3]) if len(args) > 3 else 3
+    net = UNet(batch, n, n, n)
+    net.set_params(init_params(0))
+    x = torch.randn(batch * n ** 3 * 3, device="cuda")
+    y = torch.empty(batch * n ** 3, device="cuda")
+    for _ in range(repeat):
+        net.forward(batch, n, n, n, x.data_ptr(), 1.0, 1.0, y.data_ptr())
+    net.sync()
+    print("forward ok", float(y.abs().max()))
+    net.close()
+
+
+if __name__ == "__main__":
+    _forward_case()
+
