@@ -32,6 +32,13 @@ sys.path.insert(0, ROOT)
 
 METRIC = "128³ projections/s at rel. residual 1e-6: learned-FCG vs plain MGPCG, 1 B200"
 
+
+def metric_for(workload: str, size: int) -> str:
+    """The headline metric for the 128^3 basin; the same wording for the other single-volume scenes."""
+    if workload == "basin" and size == 128:
+        return METRIC
+    return f"{size}³ {workload} projections/s at rel. residual 1e-6: plain MGPCG, 1 B200"
+
 # Algorithmic bytes per cell of each fine-level kernel (f32 fields): every distinct array a pass
 # must touch, counted once (stencil neighbours are not re-counted).  The hot kernels read the
 # 2-byte row code of the projection; apertures are read only at cut faces and column heights
@@ -319,7 +326,8 @@ def run_reference(args):
     ms = 1e3 * sum(times) / len(times)
     value = 1e3 / ms
     out = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": "projections/s", "n_gpus": args.gpus,
+        "impl": "reference", "metric": metric_for(args.workload, args.size), "value": value, "unit": "projections/s",
+        "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": f"synthetic (seeded {args.workload} scene)",
         "config": {"workload": workload_label(args.workload, args.size),
@@ -443,7 +451,11 @@ def mixed_measure(args, s, stream, flush, p_f32, ms_f32):
     return {"storage": "fp16 V-cycle vectors (fine z, coarse x, r), f32 arithmetic; f32 CG vectors; f64 dots, "
                        "alpha/beta and true residual; outer loop restarts from b - A p (defect correction)",
             "value": 1e3 / ms, "unit": "projections/s", "ms_per_step": ms, "steps": steps,
-            "speedup_vs_f32_storage": ms_f32 / ms, "iterations": rep.iterations, "rel_residual": rep.residual,
+            "speedup_vs_f32_storage": ms_f32 / ms,
+            "note": "slower than f32 storage here and on the 256^3 wave (wave_256.fp16_mgpcg): the 128^3 passes are "
+                    "latency-bound, so halving the bytes of the V-cycle vectors saves nothing, and the rounding "
+                    "costs iterations; built, tested and off by default",
+            "iterations": rep.iterations, "rel_residual": rep.residual,
             "divergence_plain": rep.divergence_plain, "degraded": bool(rep.degraded),
             "pressure_linf_rel_vs_f32_storage": float(np.abs(p16.astype(np.float64) - p_f32).max() / pmax)}, p16
 
@@ -609,9 +621,16 @@ def wave_measure(args, stream, flush):
         name, count, msum = max(known, key=lambda e: e[2])
         avg = msum / count
         ach = BYTES_PER_CELL[name] * cells / (avg * 1e-3) / 1e9
+        traffic = None
+        tf = os.path.join(ROOT, "profiles", "traffic_wave_256.txt")
+        if os.path.exists(tf):
+            for line in open(tf):
+                parts = line.split()
+                if len(parts) == 2 and not line.startswith("#") and parts[0] == name:
+                    traffic = float(parts[1])
         return {"bound": "hbm", "kernel": name, "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
-                "peak_source": peak_kind, "avg_launch_ms": avg,
-                "timing": "instrumented replay of 2 projections without the loop graph"}
+                "peak_source": peak_kind, "avg_launch_ms": avg, "alg_bytes_per_launch": BYTES_PER_CELL[name] * cells,
+                "traffic": traffic, "timing": "instrumented replay of 2 projections without the loop graph"}
 
     pressures = {}
     for key, storage in (("fp32_mgpcg", STORAGE_F32), ("fp16_mgpcg", STORAGE_F16)):
@@ -866,7 +885,8 @@ def run_b200(args):
             mixed_line["fp64_check"] = fp64_pressure_check(args.workload, args.size,
                                                            {"f32_storage": plain_p, "fp16_storage": p16})
         out = {
-            "impl": "b200", "metric": METRIC, "value": value, "unit": "projections/s", "n_gpus": world,
+            "impl": "b200", "metric": metric_for(args.workload, args.size), "value": value, "unit": "projections/s",
+            "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": f"synthetic (seeded {args.workload} scene)",
             "config": {"workload": workload_label(args.workload, args.size),

@@ -40,9 +40,12 @@ constexpr int TC_LEAD = 8;       // zero cells before the block (the lowest tap 
 constexpr int TC_TAIL = 128;     // zero cells after it (the last tile's rows past the block)
 constexpr unsigned TC_SPIN_LIMIT = 1u << 26;
 
-// Rows per CTA for rows of X cells: as many as keep BY (X + 1) <= 128 * TC_MAX_TILES.
-__host__ __device__ inline int tc_rows(int X, int Y) {
-  int by = (128 * TC_MAX_TILES) / (X + 1);
+// Rows per CTA for rows of X cells: as many as keep BY (X + 1) <= 128 * tiles, where tiles is the
+// requested budget of M tiles, raised to what one row needs.
+__host__ __device__ inline int tc_rows(int X, int Y, int tiles = TC_MAX_TILES) {
+  const int need = (X + 1 + 127) / 128;
+  if (tiles < need) tiles = need;
+  int by = (128 * tiles) / (X + 1);
   if (by < 1) by = 1;
   return by < Y ? by : Y;
 }

@@ -1000,10 +1000,14 @@ __device__ __forceinline__ void tail_sweep(const Lev& L, const float* xin, float
   tail_sweep_t(BlockTeam{}, L, xin, xout, zero_in);
 }
 
-// coarse_cycle3 (delta3d_multigrid.rs:303-332) over levels first..last of Ls, in one block.
+// coarse_cycle3 (delta3d_multigrid.rs:303-332) over levels first..last of Ls, in two halves: the way
+// down (tail_down_t: the pre-sweeps of levels first..stop-1, eight sweeps on the coarsest, and each
+// level's residual restricted to the next one while l < last) and the way up (tail_up_t:
+// prolongation from level l + 1 and two post-sweeps, for l = from .. first).  A team can run a
+// part of the hierarchy and another team the rest, in that order.
 template <class Team>
-__device__ __forceinline__ void tail_run_t(const Team& tm, const Lev* Ls, int first, int last) {
-  for (int l = first; l <= last; ++l) {
+__device__ __forceinline__ void tail_down_t(const Team& tm, const Lev* Ls, int first, int stop, int last) {
+  for (int l = first; l < stop; ++l) {
     const Lev L = Ls[l];
     const int sweeps = l == last ? 8 : 2;  // COARSE_SWEEPS_3D, PRE_SWEEPS_3D
     for (int s = 0; s < sweeps; ++s)
@@ -1025,7 +1029,10 @@ __device__ __forceinline__ void tail_run_t(const Team& tm, const Lev* Ls, int fi
       tm.sync();
     }
   }
-  for (int l = last - 1; l >= first; --l) {
+}
+template <class Team>
+__device__ __forceinline__ void tail_up_t(const Team& tm, const Lev* Ls, int first, int from) {
+  for (int l = from; l >= first; --l) {
     const Lev L = Ls[l];
     const Lev C = Ls[l + 1];
     for (int c = tm.rank(); c < L.n; c += tm.size()) {
@@ -1036,6 +1043,11 @@ __device__ __forceinline__ void tail_run_t(const Team& tm, const Lev* Ls, int fi
     tail_sweep_t(tm, L, L.x, L.x2, false);
     tail_sweep_t(tm, L, L.x2, L.x, false);
   }
+}
+template <class Team>
+__device__ __forceinline__ void tail_run_t(const Team& tm, const Lev* Ls, int first, int last) {
+  tail_down_t(tm, Ls, first, last + 1, last);
+  tail_up_t(tm, Ls, first, last - 1);
 }
 __device__ __forceinline__ void tail_run(const Lev* Ls, int first, int last) {
   tail_run_t(BlockTeam{}, Ls, first, last);

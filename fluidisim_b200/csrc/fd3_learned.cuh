@@ -41,6 +41,7 @@ struct fd3_unet {
   std::vector<void*> allocations;
   unsigned long long launches = 0;
   int conv_tc = 1;        // 1: convolutions on tcgen05 (k_conv_tc), 0: on mma.sync (k_conv)
+  int conv_tiles = TC_MAX_TILES;  // budget of 128-row M tiles per CTA of k_conv_tc (fewer: smaller CTAs)
   // how FCG uses the network: 0 = M(r) = the network's approximation of A^-1 r; 1 = M(r) = V(r) plus
   // the network's approximation of A^-1 (r - A V(r)), V the multigrid V-cycle
   int mode = 0;
@@ -87,7 +88,7 @@ template <int CI, int CO, int E>
 int conv_tc_launch(fd3_unet* N, Dims d, const __nv_bfloat16* in, const __nv_bfloat16* w, const float* bias,
                    __nv_bfloat16* out, float* out32) {
   static unsigned attr_set = 0;  // devices on which the limit was raised
-  const int BY = tc_rows(d.X, d.Y), NTM = tc_tiles(d.X, BY);
+  const int BY = tc_rows(d.X, d.Y, N->conv_tiles), NTM = tc_tiles(d.X, BY);
   if (NTM > TC_MAX_TILES) return FD3_ERR_SHAPE;
   const size_t smem = tc_smem_bytes(d.X, BY, CO);
   if (smem > 227 * 1024) return FD3_ERR_SHAPE;
@@ -596,6 +597,12 @@ int fd3_unet_sync(fd3_unet* N) {
 int fd3_unet_set_conv_kernels(fd3_unet* N, int tc) {
   if (!N || (tc != 0 && tc != 1)) return FD3_ERR_INVALID_ARGUMENT;
   N->conv_tc = tc;
+  return FD3_OK;
+}
+
+int fd3_unet_set_conv_tiles(fd3_unet* N, int tiles) {
+  if (!N || tiles < 1 || tiles > TC_MAX_TILES) return FD3_ERR_INVALID_ARGUMENT;
+  N->conv_tiles = tiles;
   return FD3_OK;
 }
 

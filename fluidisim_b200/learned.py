@@ -58,6 +58,7 @@ def _bind(L: C.CDLL) -> C.CDLL:
     L.fd3_unet_adam.argtypes = [vp, f32, f32, f32, f32]
     L.fd3_unet_sync.argtypes = [vp]
     L.fd3_unet_set_conv_kernels.argtypes = [vp, i32]
+    L.fd3_unet_set_conv_tiles.argtypes = [vp, i32]
     L.fd3_unet_kernel_launches.argtypes = [vp]
     L.fd3_unet_kernel_launches.restype = C.c_uint64
     L.fd3_assemble_device.argtypes = [vp, f32]
@@ -143,6 +144,10 @@ class UNet:
     def set_conv_kernels(self, tcgen05: bool):
         """True: convolutions on tcgen05.mma (default); False: on mma.sync (for cross-checks)."""
         self._check(self._L.fd3_unet_set_conv_kernels(self._h, 1 if tcgen05 else 0), "set_conv_kernels")
+
+    def set_conv_tiles(self, tiles: int):
+        """Budget of 128-row output tiles per CTA of the tcgen05 convolutions (1..5, default 5)."""
+        self._check(self._L.fd3_unet_set_conv_tiles(self._h, int(tiles)), "set_conv_tiles")
 
     def kernel_launches(self) -> int:
         return int(self._L.fd3_unet_kernel_launches(self._h))

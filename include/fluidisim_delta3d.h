@@ -368,6 +368,9 @@ int fd3_unet_sync(fd3_unet* net);
 /* Convolution kernels of the network: 1 = tcgen05.mma with tensor-memory accumulators (default),
  * 0 = mma.sync m16n8k16 (the earlier tensor-core path, kept to cross-check the first). */
 int fd3_unet_set_conv_kernels(fd3_unet* net, int tcgen05);
+/* Budget of 128-row output tiles per CTA of the tcgen05 convolutions, 1..5 (default 5; raised to
+ * what one row of the layer needs): fewer tiles make smaller CTAs, more of them per SM. */
+int fd3_unet_set_conv_tiles(fd3_unet* net, int tiles);
 uint64_t fd3_unet_kernel_launches(const fd3_unet* net);
 
 /* Device-side hooks of a training loop, on a volume: the rhs and row codes of project_mobile3 for
