@@ -30,7 +30,10 @@ namespace fd3 {
 constexpr float BATCH_ROUNDOFF_2D = 8.0f * (1.0f / 16777216.0f) / (1.0f - 8.0f * (1.0f / 16777216.0f));
 constexpr float BATCH_ROUNDOFF_3D = 10.0f * (1.0f / 16777216.0f) / (1.0f - 10.0f * (1.0f / 16777216.0f));
 constexpr double BATCH_DIV_TOL = 1e-5;  // PROJECTION_DIVERGENCE_TOLERANCE (delta_projection.rs:192)
-constexpr int BATCH_THREADS = 1024;
+#ifndef FD3_BATCH_THREADS
+#define FD3_BATCH_THREADS 1024
+#endif
+constexpr int BATCH_THREADS = FD3_BATCH_THREADS;  // threads of a CTA (one CTA per SM)
 
 // One patch of a batch: its geometry and every device buffer its projection touches.
 struct BatchPatch {

@@ -3,11 +3,12 @@
 // hooks a training loop needs (assembly, operator, residual loss), and the flexible conjugate
 // gradient that uses the network as its preconditioner (fd3_project_learned).
 //
-// Included by fd3_volume.cu after the volume driver: it uses the driver's launch helpers.
+// Included by fd3_volume.cu after the volume host code: it uses its launch helpers.
 #pragma once
 
 #include "fd3_conv_dw.cuh"
 #include "fd3_conv_tc.cuh"
+#include "fd3_conv_tp.cuh"
 #include "fd3_unet.cuh"
 
 using namespace fd3u;
@@ -104,13 +105,54 @@ int conv_tc_launch(fd3_unet* N, Dims d, const __nv_bfloat16* in, const __nv_bflo
   return FD3_OK;
 }
 
-// The convolution for the (CIN, COUT, epilogue) triples the network uses: k_conv_tc (tcgen05), or
-// k_conv (mma.sync) when N->conv_tc is 0.
+// k_conv_tp: the pipelined tcgen05 convolution, persistent over the work tiles, one CTA per SM.
+// The M-tile budget keeps two accumulators within the 512 columns of tensor memory and at least
+// two stage slots within the shared memory; FD3_ERR_SHAPE, before anything is launched, when no
+// budget does (the caller then runs k_conv_tc).
+template <int CI, int CO, int E>
+int conv_tp_launch(fd3_unet* N, Dims d, const __nv_bfloat16* in, const __nv_bfloat16* w, const float* bias,
+                   __nv_bfloat16* out, float* out32) {
+  static unsigned attr_set = 0;
+  static int sms = 0;
+  if (!sms) CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, N->device));
+  const size_t budget = 227 * 1024 - TP_CTRL_BYTES;
+  int tiles = std::min(N->conv_tiles, 256 / CO);
+  int BY = 0, NTM = 0, S = 0;
+  for (; tiles >= 1; --tiles) {
+    BY = tc_rows(d.X, d.Y, tiles);
+    NTM = tc_tiles(d.X, BY);
+    if (NTM > TC_MAX_TILES || 2 * NTM * CO > 512) continue;
+    S = (int)std::min<size_t>(TP_MAX_STAGES, budget / tp_stage_bytes(d.X, BY, CO));
+    if (S >= 2) break;
+  }
+  if (tiles < 1) return FD3_ERR_SHAPE;
+  if (N->device < 32 && !(attr_set & (1u << N->device))) {
+    CK(cudaFuncSetAttribute(k_conv_tp<CI, CO, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+    attr_set |= 1u << N->device;
+  }
+  const long long W = (long long)d.B * d.Z * ((d.Y + BY - 1) / BY);
+  const int grid = (int)std::min<long long>(W, sms);
+  const size_t smem = TP_CTRL_BYTES + (size_t)S * tp_stage_bytes(d.X, BY, CO);
+  k_conv_tp<CI, CO, E><<<dim3((unsigned)grid), TP_THREADS, smem, N->stream>>>(d, BY, NTM, S, (int)W, in, w, bias, out,
+                                                                            out32, N->dflag);
+  N->launches++;
+  CK(cudaGetLastError());
+  return FD3_OK;
+}
+
+// The convolution for the (CIN, COUT, epilogue) triples the network uses: k_conv_tp (tcgen05,
+// pipelined; N->conv_tc 2), k_conv_tc (tcgen05, one phase at a time; 1) or k_conv (mma.sync; 0).
 int conv_fwd(fd3_unet* N, Dims d, int cin, int cout, int epi, const __nv_bfloat16* in, const __nv_bfloat16* w,
              const float* bias, __nv_bfloat16* out, float* out32) {
   if (N->conv_tc) {
-#define FD3_CONV_TC(CI, CO, E) \
-  if (cin == CI && cout == CO && epi == E) return conv_tc_launch<CI, CO, E>(N, d, in, w, bias, out, out32);
+#define FD3_CONV_TC(CI, CO, E)                                                                          \
+  if (cin == CI && cout == CO && epi == E) {                                                           \
+    if (N->conv_tc == 2) {                                                                             \
+      const int e_ = conv_tp_launch<CI, CO, E>(N, d, in, w, bias, out, out32);                         \
+      if (e_ != FD3_ERR_SHAPE) return e_;                                                              \
+    }                                                                                                  \
+    return conv_tc_launch<CI, CO, E>(N, d, in, w, bias, out, out32);                                   \
+  }
     FD3_CONV_TC(16, 16, EPI_BIAS_RELU)
     FD3_CONV_TC(16, 32, EPI_BIAS_RELU)
     FD3_CONV_TC(32, 64, EPI_BIAS_RELU)
@@ -595,7 +637,7 @@ int fd3_unet_sync(fd3_unet* N) {
 }
 
 int fd3_unet_set_conv_kernels(fd3_unet* N, int tc) {
-  if (!N || (tc != 0 && tc != 1)) return FD3_ERR_INVALID_ARGUMENT;
+  if (!N || tc < 0 || tc > 2) return FD3_ERR_INVALID_ARGUMENT;
   N->conv_tc = tc;
   return FD3_OK;
 }

@@ -141,9 +141,10 @@ class UNet:
     def sync(self):
         self._check(self._L.fd3_unet_sync(self._h), "sync")
 
-    def set_conv_kernels(self, tcgen05: bool):
-        """True: convolutions on tcgen05.mma (default); False: on mma.sync (for cross-checks)."""
-        self._check(self._L.fd3_unet_set_conv_kernels(self._h, 1 if tcgen05 else 0), "set_conv_kernels")
+    def set_conv_kernels(self, tcgen05):
+        """True or 1: convolutions on tcgen05.mma, one phase at a time (default); 2: the pipelined
+        tcgen05 kernel (the same bits); False or 0: on mma.sync (for cross-checks)."""
+        self._check(self._L.fd3_unet_set_conv_kernels(self._h, int(tcgen05)), "set_conv_kernels")
 
     def set_conv_tiles(self, tiles: int):
         """Budget of 128-row output tiles per CTA of the tcgen05 convolutions (1..5, default 5)."""

@@ -365,8 +365,11 @@ int fd3_unet_backward(fd3_unet* net, const float* d_gout);
 /* Adam step on the accumulated gradient (consumed). */
 int fd3_unet_adam(fd3_unet* net, float lr, float beta1, float beta2, float eps);
 int fd3_unet_sync(fd3_unet* net);
-/* Convolution kernels of the network: 1 = tcgen05.mma with tensor-memory accumulators (default),
- * 0 = mma.sync m16n8k16 (the earlier tensor-core path, kept to cross-check the first). */
+/* Convolution kernels of the network: 1 = tcgen05.mma with tensor-memory accumulators, one phase at
+ * a time per CTA (default); 2 = the same MMAs as a warp-specialised pipeline (producer warps staging
+ * a ring of shared-memory slots, one MMA-issuing thread, epilogue warps draining one of two
+ * tensor-memory accumulators while the other fills; the same bits as 1); 0 = mma.sync m16n8k16
+ * (the earlier tensor-core path, kept to cross-check). */
 int fd3_unet_set_conv_kernels(fd3_unet* net, int tcgen05);
 /* Budget of 128-row output tiles per CTA of the tcgen05 convolutions, 1..5 (default 5; raised to
  * what one row of the layer needs): fewer tiles make smaller CTAs, more of them per SM. */

@@ -148,3 +148,36 @@ def test_tcgen05_convolutions_match_mma_sync(shape, batch):
         n = 27 * cout * cin
         assert rel(out[True][1][off:off + n], out[False][1][off:off + n]) < 2e-2, name
         off += n + cout
+
+
+@pytest.mark.parametrize("tiles", [5, 3])
+@pytest.mark.parametrize("shape,batch", [((4, 8, 128), 1), ((8, 16, 64), 2), ((8, 8, 256), 1), ((16, 16, 16), 4)])
+def test_pipelined_convolutions_give_the_same_bits(shape, batch, tiles):
+    """The warp-specialised tcgen05 convolutions (set_conv_kernels(2)) against the one-phase-at-a-time
+    ones: the same MMAs in the same order, so the forward output and every parameter gradient
+    (whose data-gradient convolutions run on the same kernels) have the same bits.  Rows of 256
+    cells leave no room for two stage slots of the wide layers: those layers fall back."""
+    Z, Y, X = shape
+    rng = np.random.default_rng(13)
+    flat = learned.init_params(7) + (0.02 * rng.standard_normal(learned.param_count())).astype(np.float32)
+    cells = Z * Y * X
+    x = rng.standard_normal((batch, cells, 3)).astype(np.float32)
+    x[..., 1:] = (x[..., 1:] > 0).astype(np.float32)
+    gy = rng.standard_normal(batch * cells).astype(np.float32)
+    out = {}
+    for mode in (1, 2):
+        net = learned.UNet(batch, Z, Y, X)
+        net.set_conv_kernels(mode)
+        net.set_conv_tiles(tiles)
+        net.set_params(flat)
+        dx = torch.from_numpy(x.ravel()).cuda()
+        dy = torch.empty(batch * cells, dtype=torch.float32, device="cuda")
+        dg = torch.from_numpy(gy).cuda()
+        for _ in range(2):  # twice: the second call reuses the persistent CTAs' barriers from a fresh launch
+            net.forward(batch, Z, Y, X, dx.data_ptr(), 1.0, 1.0, dy.data_ptr())
+        net.backward(dg.data_ptr())
+        net.sync()
+        out[mode] = (dy.cpu().numpy(), net.grads())
+        net.close()
+    assert np.array_equal(out[1][0].view(np.uint32), out[2][0].view(np.uint32))
+    assert np.array_equal(out[1][1].view(np.uint32), out[2][1].view(np.uint32))
