@@ -307,26 +307,44 @@ def _as_tensor(ptr: int, n: int):
 
 
 def _forward_case(argv=None):
-    """`python -m fluidisim_b200.learned forward [batch] [n] [repeat]`: U-Net forward passes of
-    `batch` samples of n^3 cells (He-initialised weights, random input), a small case for a
-    profiler's capture of the convolutions."""
+    """`python -m fluidisim_b200.learned forward [batch] [n] [repeat] [kernels] [tiles]`: U-Net
+    forward passes of `batch` samples of n^3 cells (He-initialised weights, random input) on the
+    convolution kernels `kernels` (0 mma.sync, 1 one-phase tcgen05, 2 pipelined tcgen05) with
+    `tiles` 128-row tiles per CTA; prints the best CUDA-event time of one forward. Also a small
+    case for a profiler's capture of the convolutions."""
+    import json
     import sys
 
     import torch
     args = list(sys.argv[1:] if argv is None else argv)
     if not args or args[0] != "forward":
-        raise SystemExit("usage: python -m fluidisim_b200.learned forward [batch] [n] [repeat]")
+        raise SystemExit("usage: python -m fluidisim_b200.learned forward "
+                         "[batch] [n] [repeat] [kernels] [tiles]")
     batch = int(args[1]) if len(args) > 1 else 4
     n = int(args[2]) if len(args) > 2 else 64
     repeat = int(args[3]) if len(args) > 3 else 3
+    kernels = int(args[4]) if len(args) > 4 else 1
+    tiles = int(args[5]) if len(args) > 5 else 5
     net = UNet(batch, n, n, n)
     net.set_params(init_params(0))
+    net.set_conv_kernels(kernels)
+    net.set_conv_tiles(tiles)
     x = torch.randn(batch * n ** 3 * 3, device="cuda")
     y = torch.empty(batch * n ** 3, device="cuda")
+    stream = torch.cuda.Stream()
+    net.set_stream(stream.cuda_stream)  # the events below see the launches
+    torch.cuda.synchronize()
+    best = float("inf")
     for _ in range(repeat):
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
         net.forward(batch, n, n, n, x.data_ptr(), 1.0, 1.0, y.data_ptr())
-    net.sync()
-    print("forward ok", float(y.abs().max()))
+        b.record(stream)
+        net.sync()
+        best = min(best, a.elapsed_time(b))
+    print(json.dumps({"batch": batch, "n": n, "kernels": kernels, "tiles": tiles,
+                      "forward_ms": round(best, 3), "max_abs": float(y.abs().max())}))
     net.close()
 
 
