@@ -666,11 +666,11 @@ __device__ __forceinline__ float level_x1(const Lev& L, int n) {
 
 // The small coarse levels' passes are latency-bound: a pass is one dependent chain of loads per
 // thread.  There (SPEC) every load a cell may need is issued before its row code (and the loop's
-// gate) arrive: the
-// six neighbours' operands at indices clamped to the grid (a neighbour outside the grid has face
-// state 0 and its value is never used), then the gate is checked before anything is stored.  A
-// plain row sums the preloaded values with level_row_code's masked sum; any other row goes through
-// level_row_code itself.  The arithmetic, and so every bit, is that of level_row_code.
+// gate) arrive: the six neighbours' operands at indices clamped to the grid (a neighbour outside
+// the grid has face state 0 and its value is never used) and the six apertures; then the gate is
+// checked before anything is stored.  The row is then summed without branches (level_row_sel):
+// in a latency-bound pass a warp whose rows take different branches pays for each divergent path
+// and its reconvergence in series, which cost more than the selects.
 struct Nb6 {
   float xm, xp, ym, yp, zm, zp;
 };
@@ -688,19 +688,46 @@ __device__ __forceinline__ Nb6 level_nb(const Lev& L, int i, int j, int k, int c
   b.zp = p(zr ? c + nxny : c, i, j, zr ? k + 1 : k);
   return b;
 }
-// The row sum from preloaded neighbours (plain rows) or level_row_code with the operand source q.
-template <class Q>
-__device__ __forceinline__ float level_row_nb(const Lev& L, unsigned code, int i, int j, int k, int c, float pc,
-                                              const Nb6& b, const Q& q) {
-  if (!rc_plain(code)) return level_row_code(L, code, i, j, k, c, q);
+// The six apertures of a coarse cell's faces, loaded whatever its row code (every face index of a
+// cell is valid), so that they are in flight with the code.
+struct Ap6 {
+  float a[6];
+};
+__device__ __forceinline__ Ap6 level_ap6(const Lev& L, int i, int j, int k) {
+  Ap6 o;
+  o.a[0] = L.ou[(k * L.ny + j) * (L.nx + 1) + i];
+  o.a[1] = L.ou[(k * L.ny + j) * (L.nx + 1) + i + 1];
+  o.a[2] = L.ov[(k * (L.ny + 1) + j) * L.nx + i];
+  o.a[3] = L.ov[(k * (L.ny + 1) + j + 1) * L.nx + i];
+  o.a[4] = L.ow[(k * L.ny + j) * L.nx + i];
+  o.a[5] = L.ow[((k + 1) * L.ny + j) * L.nx + i];
+  return o;
+}
+// level_row_code of any row from preloaded neighbours and apertures, without branches: each face
+// adds a (pc - x) (fluid neighbour), 2 a pc (Dirichlet face) or +0 (no face), selected by its state.
+// Adding +0 changes no partial sum (the sum starts at +0 and is never -0), so the bits are those of
+// level_row_code, which skips the missing faces; a plain row's a is exactly 1.
+__device__ __forceinline__ float level_row_sel(const Lev& L, unsigned code, float pc, const Nb6& b, const Ap6& ap) {
+  const bool unit = code & RC_UNIT;
+  const float v[6] = {b.xm, b.xp, b.ym, b.yp, b.zm, b.zp};
   float acc = 0.f;
-  acc += (code & (1u << 1)) ? pc - b.xm : 0.f;
-  acc += (code & (1u << 3)) ? pc - b.xp : 0.f;
-  acc += (code & (1u << 5)) ? pc - b.ym : 0.f;
-  acc += (code & (1u << 7)) ? pc - b.yp : 0.f;
-  acc += (code & (1u << 9)) ? pc - b.zm : 0.f;
-  acc += (code & (1u << 11)) ? pc - b.zp : 0.f;
+#pragma unroll
+  for (int f = 0; f < 6; ++f) {
+    const unsigned st = face_state(code, f);
+    const float a = unit ? 1.f : ap.a[f];
+    const float t1 = a * (pc - v[f]);
+    const float t2 = 2.f * a * pc;
+    acc += st == 1u ? t1 : (st == 2u ? t2 : 0.f);
+  }
   return acc * L.inv;
+}
+// One damped Jacobi update x + w (r - row) / diag where diag > 0, x itself elsewhere, with the
+// division done by every lane and the result selected: the bits of the guarded update.  Used by the
+// one-CTA tail, whose phases are one warp's dependent chain; in the level kernels, whose dry cells
+// come in whole warps, the guarded division measured faster.
+__device__ __forceinline__ float jacobi_sel(float x, float r, float row, float dg) {
+  const float y = x + OMEGA * (r - row) / (dg > 0.f ? dg : 1.f);
+  return dg > 0.f ? y : x;
 }
 __device__ __forceinline__ void level_ijk(const Lev& L, int c, int& i, int& j, int& k) {
   i = c % L.nx;
@@ -725,9 +752,10 @@ __global__ void __launch_bounds__(TPB) k_level_pre(Lev L, const Scalars* S, int 
   const float rc = Store<T>::ld(as<T>(L.r), c);
   float xc = X1(c);
   if (SPEC) {
+    const Ap6 ap = level_ap6(L, i, j, k);
     const Nb6 b = level_nb(L, i, j, k, c, X1c);
     if (gate && !S->active) return;
-    if (dg > 0.f) xc += OMEGA * (rc - level_row_nb(L, code, i, j, k, c, xc, b, X1)) / dg;
+    if (dg > 0.f) xc += OMEGA * (rc - level_row_sel(L, code, xc, b, ap)) / dg;
   } else if (dg > 0.f) {
     xc += OMEGA * (rc - level_row_code(L, code, i, j, k, c, X1)) / dg;
   }
@@ -750,9 +778,10 @@ __global__ void __launch_bounds__(TPB) k_level_resid(Lev L, const Scalars* S, in
   const float pc = X(c);
   float lx = 0.f;
   if (SPEC) {
+    const Ap6 ap = level_ap6(L, i, j, k);
     const Nb6 b = level_nb(L, i, j, k, c, Xc);
     if (gate && !S->active) return;
-    if (code & RC_WET) lx = level_row_nb(L, code, i, j, k, c, pc, b, X);
+    if (code & RC_WET) lx = level_row_sel(L, code, pc, b, ap);
   } else if (code & RC_WET) {
     lx = level_row_code(L, code, i, j, k, c, X);
   }
@@ -807,9 +836,13 @@ __global__ void __launch_bounds__(TPB) k_level_restrict8(Lev F, Lev C, const Sca
   }
   if (SPEC) {
     Nb6 b{};
-    if (own) b = level_nb(F, i, j, k, c, [&](int n, int, int, int) { return X(n); });
+    Ap6 ap{};
+    if (own) {
+      ap = level_ap6(F, i, j, k);
+      b = level_nb(F, i, j, k, c, [&](int n, int, int, int) { return X(n); });
+    }
     if (gate && !S->active) return;
-    if (own) tv = Store<T>::rt(rc - ((code & RC_WET) ? level_row_nb(F, code, i, j, k, c, pc, b, X) : 0.f));
+    if (own) tv = Store<T>::rt(rc - ((code & RC_WET) ? level_row_sel(F, code, pc, b, ap) : 0.f));
   } else if (own) {
     tv = Store<T>::rt(rc - ((code & RC_WET) ? level_row_code(F, code, i, j, k, c, X) : 0.f));
   }
@@ -842,9 +875,10 @@ __global__ void __launch_bounds__(TPB) k_level_post1(Lev L, Lev C, const Scalars
   const float rc = Store<T>::ld(as<T>(L.r), c);
   float xc = XPc(c, i, j, k);
   if (SPEC) {
+    const Ap6 ap = level_ap6(L, i, j, k);
     const Nb6 b = level_nb(L, i, j, k, c, XPc);
     if (gate && !S->active) return;
-    if (dg > 0.f) xc += OMEGA * (rc - level_row_nb(L, code, i, j, k, c, xc, b, XP)) / dg;
+    if (dg > 0.f) xc += OMEGA * (rc - level_row_sel(L, code, xc, b, ap)) / dg;
   } else if (dg > 0.f) {
     xc += OMEGA * (rc - level_row_code(L, code, i, j, k, c, XP)) / dg;
   }
@@ -867,9 +901,10 @@ __global__ void __launch_bounds__(TPB) k_level_post2(Lev L, const Scalars* S, in
   const float rc = Store<T>::ld(as<T>(L.r), c);
   float xc = X(c);
   if (SPEC) {
+    const Ap6 ap = level_ap6(L, i, j, k);
     const Nb6 b = level_nb(L, i, j, k, c, Xc);
     if (gate && !S->active) return;
-    if (dg > 0.f) xc += OMEGA * (rc - level_row_nb(L, code, i, j, k, c, xc, b, X)) / dg;
+    if (dg > 0.f) xc += OMEGA * (rc - level_row_sel(L, code, xc, b, ap)) / dg;
   } else if (dg > 0.f) {
     xc += OMEGA * (rc - level_row_code(L, code, i, j, k, c, X)) / dg;
   }
@@ -898,6 +933,7 @@ __global__ void __launch_bounds__(TPB) k_level_post21(Lev L, Lev C, const Scalar
   unsigned pcode = 0u;
   float pdg = 0.f, pr = 0.f, px2 = 0.f;
   Nb6 pb{};
+  Ap6 pap{};
   int pc = 0;
   if (psweep) {
     pc = (pk * C.ny + pj) * C.nx + pi;
@@ -906,6 +942,7 @@ __global__ void __launch_bounds__(TPB) k_level_post21(Lev L, Lev C, const Scalar
     pr = Store<T>::ld(as<T>(C.r), pc);
     px2 = X2(pc);
     pb = level_nb(C, pi, pj, pk, pc, [&](int n, int, int, int) { return X2(n); });
+    pap = level_ap6(C, pi, pj, pk);
   }
   // the child's own row
   const int i = 2 * ci + (e & 1), j = 2 * cj + ((e >> 1) & 1), k = 2 * ck + (e >> 2);
@@ -914,16 +951,18 @@ __global__ void __launch_bounds__(TPB) k_level_post21(Lev L, Lev C, const Scalar
   unsigned code = 0u;
   float dg = 0.f, rc = 0.f, xc0 = 0.f;
   Nb6 b{};
+  Ap6 ap{};
   if (own) {
     code = L.code[c];
     dg = L.diag[c];
     rc = Store<T>::ld(as<T>(L.r), c);
     xc0 = X(c);
     b = level_nb(L, i, j, k, c, [&](int n, int, int, int) { return X(n); });
+    ap = level_ap6(L, i, j, k);
   }
   if (gate && !S->active) return;
   float xp = px2;  // C's final x at the lane's cell (k_level_post2)
-  if (psweep && pdg > 0.f) xp += OMEGA * (pr - level_row_nb(C, pcode, pi, pj, pk, pc, px2, pb, X2)) / pdg;
+  if (psweep && pdg > 0.f) xp += OMEGA * (pr - level_row_sel(C, pcode, px2, pb, pap)) / pdg;
   xp = Store<T>::rt(xp);
   const int lane0 = threadIdx.x & 24;
   float par[7];
@@ -945,7 +984,7 @@ __global__ void __launch_bounds__(TPB) k_level_post21(Lev L, Lev C, const Scalar
          : n == c - nxny ? v.zm : v.zp;
   };
   float out = xc;
-  if (dg > 0.f) out += OMEGA * (rc - level_row_nb(L, code, i, j, k, c, xc, v, XP)) / dg;
+  if (dg > 0.f) out += OMEGA * (rc - level_row_sel(L, code, xc, v, ap)) / dg;
   Store<T>::st(as<T>(L.x2), c, out);
 }
 
@@ -1155,16 +1194,22 @@ __device__ __forceinline__ TailRow tail_row(const Lev& L, int c) {
 }
 
 // row_sums at cell c of a level with dims (nx, ny), the neighbours' values read from X (shared
-// memory); the terms are added in face order x-, x+, y-, y+, z-, z+.
+// memory); the terms are added in face order x-, x+, y-, y+, z-, z+.  As level_row_sel: the six
+// reads are issued together (indices clamped into the array; a face leading out of the level has
+// state 0 and its value is unused) and the terms selected, not branched on.
 __device__ __forceinline__ float tail_rowsum(const TailRow& w, int c, int nx, int nxny, float pc, const float* X,
                                              float inv) {
   const int mm[6] = {c - 1, c + 1, c - nx, c + nx, c - nxny, c + nxny};
+  float v[6];
+#pragma unroll
+  for (int f = 0; f < 6; ++f) v[f] = X[min(max(mm[f], 0), TAIL_REG_THREADS - 1)];
   float acc = 0.f;
 #pragma unroll
   for (int f = 0; f < 6; ++f) {
     const unsigned st = face_state(w.code, f);
-    if (st == 1) acc += w.a[f] * (pc - X[mm[f]]);
-    else if (st == 2) acc += 2.f * w.a[f] * pc;
+    const float t1 = w.a[f] * (pc - v[f]);
+    const float t2 = 2.f * w.a[f] * pc;
+    acc += st == 1u ? t1 : (st == 2u ? t2 : 0.f);
   }
   return acc * inv;
 }
@@ -1213,7 +1258,7 @@ __global__ void __launch_bounds__(TAIL_REG_THREADS) k_coarse_tail_reg(const Tail
         float xn = x;
         if (own) {
           if (s == 0) xn = w[l].diag > 0.f ? 0.f + OMEGA * (r - 0.f) / w[l].diag : 0.f;
-          else if (w[l].diag > 0.f) xn = x + OMEGA * (r - tail_rowsum(w[l], c, nx, nxny, x, in, inv)) / w[l].diag;
+          else xn = jacobi_sel(x, r, tail_rowsum(w[l], c, nx, nxny, x, in, inv), w[l].diag);
           out[c] = xn;
         }
         __syncthreads();
@@ -1264,7 +1309,7 @@ __global__ void __launch_bounds__(TAIL_REG_THREADS) k_coarse_tail_reg(const Tail
         float* out = (s & 1) ? XB[l] : XA[l];
         const float* in = (s & 1) ? XA[l] : XB[l];
         float xn = x;
-        if (own && w[l].diag > 0.f) xn = x + OMEGA * (r - tail_rowsum(w[l], c, nx, nxny, x, in, inv)) / w[l].diag;
+        if (own) xn = jacobi_sel(x, r, tail_rowsum(w[l], c, nx, nxny, x, in, inv), w[l].diag);
         if (own) out[c] = xn;
         __syncthreads();
         x = xn;
