@@ -66,6 +66,12 @@ BYTES_PER_CELL = {
     "kq_fine_post1": 2 + 4 + 4 + 4 + 0.5 + 4,
     "kq_fine_post2_rz": 2 + 4 + 4 + 4 + 4,
     "kq_residual": 2 + 4 * 3,
+    # the same passes on TMA-staged layers (f64 mode, the default from 2^23 cells with nx % 8 == 0)
+    "kt_dir_apply_dot": 2 + 4 + 4 + 4 + 4,
+    "kt_fine_pre": 2 + 4 + 4 + 4,
+    "kt_fine_restrict": 2 + 4 + 4 + 0.5,
+    "kt_fine_post1": 2 + 4 + 4 + 4 + 0.5 + 4,
+    "kt_fine_post2_rz": 2 + 4 + 4 + 4 + 4,
     # one-cell-per-thread kernels (ordered mode, and f64 mode with kernels = 1)
     "k_dir_apply_dot": 2 + 4 + 4 + 4 + 4,
     "k_update_rn": 4 * 6,
@@ -1225,9 +1231,9 @@ def main():
     ap.add_argument("--train-samples", type=int, default=20000,
                     help="training samples of the learned preconditioner (20,000 at 64^3, as config 4 asks)")
     ap.add_argument("--kernels", type=int, default=0,
-                    help="fine-level kernel family (fd3_options.kernels): 0 the default (four cells per thread from "
-                         "2^23 cells, else two), 3 two cells per thread, 4 four cells per thread, 2 one cell per "
-                         "thread in the same blocking")
+                    help="fine-level kernel family (fd3_options.kernels): 0 the default (TMA-staged layers from "
+                         "2^23 cells, else two cells per thread), 3 two cells per thread, 4 four cells per thread, "
+                         "5 TMA-staged layers, 2 one cell per thread in the same blocking")
     ap.add_argument("--graphs", type=int, default=1,
                     help="1: the inner loop as a CUDA graph with a WHILE node; 0: host-driven (for ncu launch lists)")
     args = ap.parse_args()

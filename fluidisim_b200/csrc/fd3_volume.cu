@@ -26,6 +26,7 @@
 #include "../../include/fluidisim_delta3d.h"
 #include "fd3_cut.cuh"
 #include "fd3_zmarch4.cuh"
+#include "fd3_tmarch.cuh"
 #include "fd3_batch.cuh"
 #include "fd3_linear.cuh"
 #include "fd3_levels.cuh"
@@ -173,6 +174,15 @@ struct fd3_volume {
   int loop_mode = -1;
   cudaStream_t loop_stream = nullptr;
   unsigned long long body_nodes = 0;
+  // tensor maps of the TMA-staged fine kernels (kernels = 5), made on first use; the buffers they
+  // describe are allocated once, so the maps stay valid for the volume's life
+  struct TmaSet {
+    CUtensorMap hz, hz2, hdir, hdir2, hprec, hres;  // halo boxes
+    CUtensorMap oprec, ores;                        // tile boxes
+    CUtensorMap codes, par;                         // row codes; level 0's x (parent box)
+  };
+  TmaSet* tma = nullptr;
+  int tma_state = 0;  // 0 not tried, 1 ready, -1 the driver refused a map
 
   Geo geo() const {
     Geo G;
@@ -195,7 +205,18 @@ struct fd3_volume {
   }
   bool ord() const { return opt.reduction == FD3_REDUCE_ORDERED_F32; }
   bool blocked() const { return !ord() && opt.kernels != 1; }
-  bool paired() const { return blocked() && (opt.kernels == 0 || opt.kernels == 3 || opt.kernels == 4) && nx % 2 == 0; }
+  bool paired() const {
+    return blocked() && (opt.kernels == 0 || opt.kernels == 3 || opt.kernels == 4 || opt.kernels == 5) && nx % 2 == 0;
+  }
+  // TMA-staged fine kernels (fd3_tmarch.cuh) for the V-cycle's and the direction's passes: f32 storage,
+  // nx % 8 == 0 and the multigrid, chosen explicitly (kernels = 5) or by default on volumes of at least
+  // kQuadMinCells, where the passes stream from HBM (measured on the 256^3 wave: 19.3 against 20.0 ms
+  // per projection with four cells per thread; on the 128^3 basin, which sits in L2, 3.07 against
+  // 3.03 ms with two cells per thread, which stays the default there)
+  bool tmaf() const {
+    if (!blocked() || nx % 8 != 0 || opt.storage == FD3_STORAGE_F16 || !mg_on() || tma_state < 0) return false;
+    return opt.kernels == 5 || (opt.kernels == 0 && (long long)n >= kQuadMinCells);
+  }
   // four cells per thread: with f32 storage and nx % 4 == 0, chosen explicitly (kernels = 4) or by
   // default on volumes of at least kQuadMinCells, where the passes stream from HBM (measured: 256^3
   // 20.9 against 21.5 ms per projection; at 128^3, where the working set sits in L2 and the passes
@@ -210,7 +231,7 @@ struct fd3_volume {
   int loop_key() const {
     return (ord() ? 1 : 0) | (mg_on() ? 2 : 0) | (blocked() ? 4 : 0) | (opt.no_overlap ? 8 : 0) | (linear ? 16 : 0) |
            (paired() ? 32 : 0) | (half() ? 64 : 0) | (sparse ? 128 : 0) |  // the captured Geo holds the set's mask
-           (opt.no_tile_skip ? 256 : 0) | (quad() ? 512 : 0);
+           (opt.no_tile_skip ? 256 : 0) | (quad() ? 512 : 0) | (tmaf() ? 1024 : 0);
   }
   Red red() const { return Red{p64, p32, count}; }
 };
@@ -235,6 +256,8 @@ void release(fd3_volume* V) {
   if (V->hflag) cudaFreeHost(V->hflag);
   if (V->hfsc) cudaFreeHost(V->hfsc);
   if (V->own_stream) cudaStreamDestroy(V->own_stream);
+  delete V->tma;
+  V->tma = nullptr;
 }
 
 cudaEvent_t next_event(fd3_volume* V) {
@@ -481,6 +504,134 @@ void quad_vcycle(fd3_volume* V, int gate, int op) {
   });
 }
 
+// ------------------------------------------------------------------ TMA-staged fine kernels
+// cuTensorMapEncodeTiled from the driver the runtime is bound to (no link against libcuda).
+typedef CUresult (*TmapEncodeFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+TmapEncodeFn tmap_encoder() {
+  static TmapEncodeFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<TmapEncodeFn>(f);
+  });
+  return fn;
+}
+
+// A 3-D map of an nx x ny x nz array (f32, or u16 row codes) copied in boxes of bw x bh x 1; cells
+// outside the array read as zero.
+bool make_tmap(CUtensorMap* m, const void* base, bool u16, int nx, int ny, int nz, int bw, int bh) {
+  TmapEncodeFn enc = tmap_encoder();
+  if (!enc) return false;
+  const cuuint64_t es = u16 ? 2 : 4;
+  const cuuint64_t dims[3] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz};
+  const cuuint64_t strides[2] = {(cuuint64_t)nx * es, (cuuint64_t)nx * ny * es};
+  const cuuint32_t box[3] = {(cuuint32_t)bw, (cuuint32_t)bh, 1u};
+  const cuuint32_t estr[3] = {1u, 1u, 1u};
+  return enc(m, u16 ? CU_TENSOR_MAP_DATA_TYPE_UINT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<void*>(base), dims,
+             strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// The volume's tensor maps, made once; false (and the family is off for good) if the driver refuses one.
+bool tma_ready(fd3_volume* V) {
+  if (V->tma_state != 0) return V->tma_state > 0;
+  V->tma_state = -1;
+  fd3_volume::TmaSet* T = new (std::nothrow) fd3_volume::TmaSet();
+  if (!T) return false;
+  const int nx = V->nx, ny = V->ny, nz = V->nz;
+  bool ok = make_tmap(&T->hz, V->z, false, nx, ny, nz, TMW, TMH) && make_tmap(&T->hz2, V->z2, false, nx, ny, nz, TMW, TMH) &&
+            make_tmap(&T->hdir, V->dir, false, nx, ny, nz, TMW, TMH) &&
+            make_tmap(&T->hdir2, V->dir2, false, nx, ny, nz, TMW, TMH) &&
+            make_tmap(&T->hprec, V->prec, false, nx, ny, nz, TMW, TMH) &&
+            make_tmap(&T->hres, V->res, false, nx, ny, nz, TMW, TMH) &&
+            make_tmap(&T->oprec, V->prec, false, nx, ny, nz, TMX, TMY) &&
+            make_tmap(&T->ores, V->res, false, nx, ny, nz, TMX, TMY) &&
+            make_tmap(&T->codes, V->codes, true, nx, ny, nz, TMX, TMY);
+  if (ok && !V->levels.empty()) {
+    const Lev& L = V->levels[0];
+    ok = L.nx * 2 == nx && L.ny * 2 == ny && L.nz * 2 == nz && make_tmap(&T->par, L.x, false, L.nx, L.ny, L.nz, TMPW, TMPH);
+  }
+  if (!ok) { delete T; return false; }
+  V->tma = T;
+  V->tma_state = 1;
+  return true;
+}
+
+template <int PASS, int K, int D, int Q>
+void launch_tpass(fd3_volume* V, const char* name, const TMaps& M, const TArgs& a) {
+  constexpr int MINB = Q == 4 ? 5 : FD3_TMINB;
+  static std::once_flag attr_once;  // one per instantiation: the opt-in above 48 KiB of shared memory
+  std::call_once(attr_once, [] {
+    cudaFuncSetAttribute(kt_pass<PASS, K, D, Q, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)TPass<PASS, D>::SMEM_LAUNCH);
+  });
+  launch_grid_smem(V, name, zblocks_t(V->nx, V->ny, V->nz, K), TQ<Q>::NT, TPass<PASS, D>::SMEM_LAUNCH,
+                   kt_pass<PASS, K, D, Q, MINB>, M, V->geo(), a, V->red(), V->dS);
+}
+
+// Layers per CTA of the TMA-staged kernels: 8 when the grid still gives two waves at four CTAs per SM,
+// else 4 (measured: at 128^3, 8 and 16 layers took 3.95 and 4.70 ms per projection against 3.07 with
+// 4; at 256^3, 16 layers were no faster than 8).  Two cells per thread and two layers in flight:
+// four cells per thread (CTAs of 128 threads) and deeper rings (fewer CTAs per SM) were slower at both
+// sizes, one layer in flight slower at 128^3.
+inline int pick_kt(int nx, int ny, int nz) { return zblocks_t(nx, ny, nz, 8) >= 2 * 4 * 148 ? 8 : 4; }
+template <class F>
+void kt_dispatch(const fd3_volume* V, F f) {
+  if (pick_kt(V->nx, V->ny, V->nz) == 8) f(IC<8>{}, IC<2>{}, IC<2>{});
+  else f(IC<4>{}, IC<2>{}, IC<2>{});
+}
+
+template <int K, int Q, int D>
+void tma_vcycle_k(fd3_volume* V, int gate, int op) {
+  const fd3_volume::TmaSet& T = *V->tma;
+  const bool levels = !V->levels.empty();
+  TArgs a{};
+  a.gate = gate;
+  a.L = levels ? V->levels[0] : Lev{};
+  TMaps M{};
+  // z = the two pre-sweeps from zero: halo prec, r
+  M.m[0] = T.hprec; M.m[1] = T.hres; M.m[2] = T.codes;
+  a.out0 = V->z;
+  launch_tpass<TP_PRE, K, D, Q>(V, "kt_fine_pre", M, a);
+  if (levels) {  // residual and its eight-child mean into level 0's r: halo z, tile r
+    M.m[0] = T.hz; M.m[1] = T.ores; M.m[2] = T.codes;
+    launch_tpass<TP_RESTRICT, K, D, Q>(V, "kt_fine_restrict", M, a);
+    coarse_cycle(V, gate);
+  }
+  // z2 = prolongation + the first post-sweep: halo z, prec; tile r; codes; parent
+  M.m[0] = T.hz; M.m[1] = T.hprec; M.m[2] = T.ores; M.m[3] = T.codes; M.m[4] = levels ? T.par : T.codes;
+  a.out0 = V->z2;
+  a.prolong = levels ? 1 : 0;
+  launch_tpass<TP_POST1, K, D, Q>(V, "kt_fine_post1", M, a);
+  // z = the second post-sweep with r.z: halo z2; tile prec, r
+  M.m[0] = T.hz2; M.m[1] = T.oprec; M.m[2] = T.ores; M.m[3] = T.codes;
+  a.out0 = V->z;
+  a.op = op;
+  launch_tpass<TP_POST2, K, D, Q>(V, "kt_fine_post2_rz", M, a);
+}
+void tma_vcycle(fd3_volume* V, int gate, int op) {
+  kt_dispatch(V, [&](auto k, auto q, auto d) {
+    tma_vcycle_k<decltype(k)::value, decltype(q)::value, decltype(d)::value>(V, gate, op);
+  });
+}
+// d = z (+ beta d) from din into dout, q = A d, d.q and alpha.
+void tma_dir(fd3_volume* V, int parity) {
+  const fd3_volume::TmaSet& T = *V->tma;
+  TMaps M{};
+  M.m[0] = T.hz; M.m[1] = parity ? T.hdir2 : T.hdir; M.m[2] = T.codes;
+  TArgs a{};
+  a.out0 = parity ? V->dir : V->dir2;
+  a.out1 = V->tmp;
+  kt_dispatch(V, [&](auto k, auto q, auto d) {
+    launch_tpass<TP_DIR, decltype(k)::value, decltype(d)::value, decltype(q)::value>(V, "kt_dir_apply_dot", M, a);
+  });
+}
+
 // v_cycle3 (delta3d_multigrid.rs:393-429) with res.z at its end (op FIN_RZ_PRIME or FIN_RZ_ITER);
 // z = M^-1 res is left in V->z.
 void vcycle(fd3_volume* V, int gate, int op) {
@@ -489,6 +640,10 @@ void vcycle(fd3_volume* V, int gate, int op) {
   const bool levels = !V->levels.empty();
   Lev L0 = levels ? V->levels[0] : Lev{};
   const unsigned short* codes = V->codes;
+  if (V->tmaf() && tma_ready(V)) {  // TMA-staged 2.5-D blocked kernels (f64 reductions, f32 storage)
+    tma_vcycle(V, gate, op);
+    return;
+  }
   if (V->quad()) {  // 2.5-D blocked kernels, four cells per thread (f64 reductions, f32 storage)
     quad_vcycle(V, gate, op);
     return;
@@ -553,7 +708,11 @@ void iteration(fd3_volume* V, int parity) {
   if (V->mg_on()) {
     float* din = parity ? V->dir2 : V->dir;
     float* dout = parity ? V->dir : V->dir2;
-    if (V->quad()) {
+    if (V->tmaf() && tma_ready(V)) {
+      tma_dir(V, parity);
+      LAUNCH_G(V, kv_update_rn, update_blocks(V->n), TPB, V->n, V->p, V->res, (const float*)dout,
+               (const float*)V->tmp, V->red(), V->dS, update_mask(V), V->ncol);
+    } else if (V->quad()) {
       quad_dispatch(V, [&](auto qx, auto k4) {
         constexpr int QX = decltype(qx)::value, K4 = decltype(k4)::value;
         launch_grid(V, "kq_dir_apply_dot", zblocks4<QX>(V->nx, V->ny, V->nz, K4), Z4T, kq_dir_apply_dot<QX, K4>, G,
@@ -1436,9 +1595,10 @@ void fd3_destroy(fd3_volume* v) {
 
 int fd3_set_options(fd3_volume* v, const fd3_options* o) {
   if (!v || !o) return FD3_ERR_INVALID_ARGUMENT;
-  if (o->reduction > 1 || o->kernels > 4 || o->no_overlap > 1 || o->storage > 1 || o->no_tile_skip > 1)
+  if (o->reduction > 1 || o->kernels > 5 || o->no_overlap > 1 || o->storage > 1 || o->no_tile_skip > 1)
     return FD3_ERR_DOMAIN;
   if (o->kernels == 4 && (v->nx % 4 != 0 || o->storage == FD3_STORAGE_F16)) return FD3_ERR_DOMAIN;
+  if (o->kernels == 5 && (v->nx % 8 != 0 || o->storage == FD3_STORAGE_F16)) return FD3_ERR_DOMAIN;
   // FP16 storage runs on the paired fine kernels: f64 reductions, kernels = 0 or 3 and an even nx
   if (o->storage == FD3_STORAGE_F16 &&
       (o->reduction != FD3_REDUCE_F64 || (o->kernels != 0 && o->kernels != 3) || v->nx % 2 != 0))

@@ -88,14 +88,16 @@ typedef struct fd3_options {
   uint32_t mg_max_levels; /* coarse levels kept by fd3_enable_multigrid; 0 = every level the
                              reference's coarsening rule allows (delta3d_multigrid.rs:73-88) */
   uint32_t use_graphs;    /* 1 = run the inner PCG loop as a CUDA graph with a WHILE node */
-  uint32_t kernels;       /* fine-level kernels in f64 mode: 0 = 2.5-D blocked (default): four cells
-                             per thread on volumes of 2^23 cells or more with nx % 4 == 0 and f32
-                             storage, else two cells per thread (one when nx is odd); 1 = one cell per
-                             thread (the family the ordered mode always uses); 2 = 2.5-D blocked with
-                             one cell per thread; 3 = 2.5-D blocked with two cells per thread; 4 =
-                             2.5-D blocked with four cells per thread (nx % 4 == 0, f32 storage).
-                             Every family gives the same cell values; only the order of the f64
-                             partial sums differs */
+  uint32_t kernels;       /* fine-level kernels in f64 mode: 0 = 2.5-D blocked (default): on volumes
+                             of 2^23 cells or more with f32 storage the TMA-staged kernels (nx % 8 ==
+                             0) or four cells per thread (nx % 4 == 0), else two cells per thread
+                             (one when nx is odd); 1 = one cell per thread (the family the ordered
+                             mode always uses); 2 = 2.5-D blocked with one cell per thread; 3 = 2.5-D
+                             blocked with two cells per thread; 4 = 2.5-D blocked with four cells per
+                             thread (nx % 4 == 0, f32 storage); 5 = 2.5-D blocked, two cells per
+                             thread, layers staged in shared memory by TMA copies (nx % 8 == 0, f32
+                             storage).  Every family gives the same cell values; only the order of
+                             the f64 partial sums differs */
   uint32_t no_overlap;    /* 1 = launch each kernel only after the previous one completes; 0 (default)
                              = programmatic dependent launch: the next kernel is scheduled early and
                              waits on the device (results are identical either way) */

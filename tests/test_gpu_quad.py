@@ -58,7 +58,7 @@ def test_vcycle_bits_are_the_same_in_every_family_and_the_oracle(shape):
     s = lake(*shape)
     x = scenes.noise(s["nx"] * s["ny"] * s["nz"], 5)
     zs = {}
-    for kernels in (0, 1, 2, 3, 4):
+    for kernels in (0, 1, 2, 3, 4, 5):
         d = device(s, kernels)
         zs[kernels] = d.vcycle_for_tests(x)
         d.close()

@@ -233,10 +233,11 @@ def test_a_sparse_set_over_a_cut_lake_matches_the_oracle():
         assert_bits(x, y, name)
 
 
-@pytest.mark.parametrize("kernels", [0, 2, 3, 4])
+@pytest.mark.parametrize("kernels", [0, 2, 3, 4, 5])
 def test_skipping_the_tiles_outside_the_set_changes_no_bit(kernels):
     """The blocked fine kernels skip the column tiles with no column of the set (32 x 8 with one cell
-    per thread, 64 x 8 with two, 128 x 8 with four: kernels 2, 3 (and 0 here) and 4, nx = 128).
+    per thread, 64 x 8 with two, 128 x 8 with four, 64 x 8 TMA-staged: kernels 2, 3 (and 0 here), 4
+    and 5, nx = 128).
     Against the same volume processing every tile: every field bit for bit, through steps, a set
     change that empties tiles and one that refills them."""
     nx, ny = 128, 64
