@@ -1400,6 +1400,21 @@ __global__ void __launch_bounds__(TPB) k_residual_c(Geo g, const unsigned short*
 }
 
 // Loop start: the host's view of the loop state; a pending NotFinite keeps the loop closed.
+// The first inner loop of a projection started from the device's own scalars (f64 reductions): the
+// host's test before it (b2 > 0, rr above tol b2, iterations left; delta3d_mobile.rs:513-516) is made
+// here, so the set-up, the loop and the outer checks go out without a host round trip between them.
+__global__ void k_loop_start_dev(Scalars* S, unsigned max_iters) {
+  KSTART();
+  const double tolb2 = 1e-12 * S->b2;
+  S->tolb2 = tolb2;
+  S->phys = (double)INFINITY;
+  S->it = 0;
+  S->max_iters = max_iters;
+  S->brk = 0;
+  S->body_runs = 0;
+  S->active = (S->status == 0 && S->b2 > 0.0 && S->rr > tolb2 && max_iters > 0u) ? 1 : 0;
+}
+
 __global__ void k_loop_start(Scalars* S, double rr, double tolb2, double phys, unsigned it, unsigned max_iters) {
   KSTART();
   S->rr = rr;

@@ -949,14 +949,34 @@ int project_mobile3(fd3_volume* V, float scale, float k1, uint32_t max_iters, fd
     if (V->has_mg) prepare_multigrid(V);
   }
   residual(V, (int)FIN_RR0);
-  TRY(pull(V));
-  if (V->hS->status) return V->hS->status;
+  // With f64 reductions and the loop graph, the first outer iteration is enqueued whole: the prime,
+  // the loop (started on the device from the set-up's scalars: it does not run when the host's test
+  // would not have started it) and the outer checks, with one synchronisation at their end.  A
+  // prime that turns out unneeded changes nothing the checks or the report read; a non-finite
+  // set-up stops the loop on the device and is reported after the checks, as before them.
+  const bool speculate = !ord && V->mg_on() && V->opt.use_graphs && !V->prof;
+  Checks ck{};
+  bool have_checks = false;
+  if (speculate) {
+    prime(V);
+    LAUNCH_G(V, k_loop_start_dev, 1, 1, V->dS, max_iters);
+    const int mode = V->loop_key();
+    if (!V->loop_exec || V->loop_mode != mode || V->loop_stream != V->stream) TRY(build_loop_graph(V));
+    CK(cudaGraphLaunch(V->loop_exec, V->stream));
+    TRY(outer_checks(V, k1, &ck));
+    if (V->hS->status) return V->hS->status;
+    V->launches += (unsigned long long)((std::max(V->hS->it, 1u) + 1) / 2) * V->body_nodes;
+    have_checks = true;
+  } else {
+    TRY(pull(V));
+    if (V->hS->status) return V->hS->status;
+  }
   const double b2 = V->hS->b2;
   double rr = V->hS->rr;
   // tol = 1e-12_f32 (delta3d_mobile.rs:507); tol*b2 in f32 in the reference's arithmetic
   const double tolb2 = ord ? (double)(1e-12f * (float)b2) : 1e-12 * b2;
-  bool primed = false;
-  uint32_t it = 0;
+  bool primed = have_checks;
+  uint32_t it = have_checks ? V->hS->it : 0;
   bool floor_stop = false;
   double phys = std::numeric_limits<double>::infinity();
   bool has_checkpoint = false;
@@ -965,13 +985,16 @@ int project_mobile3(fd3_volume* V, float scale, float k1, uint32_t max_iters, fd
   double actual_rr = 0;
   bool settled = false;
   double settled_d[2] = {0, 0};
-  Checks ck{};
   auto above = [&](double r) {
     if (ord) return (float)r > (float)tolb2 || (float)r > (float)phys;
     return r > tolb2 || r > phys;
   };
   for (;;) {
-    uint32_t before = it;
+    uint32_t before = have_checks ? 0u : it;
+    if (have_checks) {  // the first outer iteration ran whole on the device
+      have_checks = false;
+      rr = V->hS->rr;
+    } else {
     if (b2 > 0 && above(rr) && it < max_iters) {
       if (!primed) {
         prime(V);
@@ -985,6 +1008,7 @@ int project_mobile3(fd3_volume* V, float scale, float k1, uint32_t max_iters, fd
       rr = V->hS->rr;
     }
     TRY(outer_checks(V, k1, &ck));
+    }
     if (ck.status) return ck.status;
     const double actual = ck.actual;
     bool exhausted = it >= max_iters || it == before;
