@@ -617,11 +617,49 @@ __device__ __forceinline__ unsigned level_codes_at(const Lev& L, int c) {
   }
   return code;
 }
-__global__ void k_level_codes(Lev L) {
+// prepare_multigrid3 (delta3d_multigrid.rs:370-387) of one level in two passes: the kinds and the
+// apertures (coarsen3 from the fine volume, `fine`, or from level F; cells, then faces, in one index
+// space), then the diagonal and the row codes, which read only those.
+__global__ void k_level_prepare_a(Geo g, Lev F, Lev C, int fine) {
   KSTART();
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= L.n) return;
-  L.code[c] = (unsigned short)level_codes_at(L, c);
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < C.n) {
+    C.kind[q] = fine ? coarsen_kind_fine_at(g, C, q) : coarsen_kind_level_at(F, C, q);
+    return;
+  }
+  q -= C.n;
+  if (fine) coarsen_open_at(g.nx, g.ny, g.ou, g.ov, g.ow, g.act, C, q);
+  else coarsen_open_at(F.nx, F.ny, F.ou, F.ov, F.ow, nullptr, C, q);
+}
+__global__ void k_level_prepare_b(Lev C) {
+  KSTART();
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= C.n) return;
+  C.diag[c] = level_diag_at(C, c);
+  C.code[c] = (unsigned short)level_codes_at(C, c);
+}
+// The same for levels first .. last (first >= 1, every one small) in one CTA: the kinds and
+// apertures level by level, a barrier after each, then every level's diagonal and codes.
+constexpr int PREP_SMALL_THREADS = 1024;
+__global__ void __launch_bounds__(PREP_SMALL_THREADS) k_levels_prepare_small(const Lev* __restrict__ levs, int first,
+                                                                          int last) {
+  KSTART();
+  for (int l = first; l <= last; ++l) {
+    const Lev F = levs[l - 1], C = levs[l];
+    const int nfaces = (C.nx + 1) * C.ny * C.nz + C.nx * (C.ny + 1) * C.nz + C.nx * C.ny * (C.nz + 1);
+    for (int q = threadIdx.x; q < C.n + nfaces; q += blockDim.x) {
+      if (q < C.n) C.kind[q] = coarsen_kind_level_at(F, C, q);
+      else coarsen_open_at(F.nx, F.ny, F.ou, F.ov, F.ow, nullptr, C, q - C.n);
+    }
+    __syncthreads();
+  }
+  for (int l = first; l <= last; ++l) {
+    const Lev C = levs[l];
+    for (int c = threadIdx.x; c < C.n; c += blockDim.x) {
+      C.diag[c] = level_diag_at(C, c);
+      C.code[c] = (unsigned short)level_codes_at(C, c);
+    }
+  }
 }
 
 // One row of row_sums (with p) from its code: the same terms, in the same order, as level_row_f.

@@ -87,7 +87,7 @@ struct Lev {
   float* ou; float* ov; float* ow;
   float* kind; float* diag;
   float* x; float* x2; float* r; float* t;
-  unsigned short* code;   // row codes of the level (k_level_codes)
+  unsigned short* code;   // row codes of the level (k_level_prepare_b)
 };
 
 // Device-resident scalars of one projection.  Reduced values are held in double; in ordered
@@ -476,12 +476,6 @@ __device__ __forceinline__ float level_diag_at(const Lev& L, int c) {
   face(L.ow[((k + 1) * L.ny + j) * L.nx + i], k + 1 < L.nz, c + nxny, true);
   return acc * L.inv;
 }
-__global__ void k_level_diag(Lev L) {
-  KSTART();
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= L.n) return;
-  L.diag[c] = level_diag_at(L, c);
-}
 
 // Damped Jacobi sweep (smooth3): xout = xin + w (r - L xin) / diag where diag > 0.  zero_in = 1
 // is the first sweep after `x.fill(0)`: L 0 = +0 exactly, so xout = 0 + w (r - 0) / diag.
@@ -539,12 +533,6 @@ __device__ __forceinline__ float coarsen_kind_fine_at(const Geo& g, const Lev& C
   }
   return active ? 1.f : (air ? -1.f : 0.f);
 }
-__global__ void k_coarsen_kind_fine(Geo g, Lev C) {
-  KSTART();
-  int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= C.n) return;
-  C.kind[q] = coarsen_kind_fine_at(g, C, q);
-}
 
 __device__ __forceinline__ float coarsen_kind_level_at(const Lev& F, const Lev& C, int q) {
   int ci = q % C.nx, t = q / C.nx, cj = t % C.ny, ck = t / C.ny;
@@ -557,12 +545,6 @@ __device__ __forceinline__ float coarsen_kind_level_at(const Lev& F, const Lev& 
     else if (v < 0.f) air = true;
   }
   return active ? 1.f : (air ? -1.f : 0.f);
-}
-__global__ void k_coarsen_kind_level(Lev F, Lev C) {
-  KSTART();
-  int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= C.n) return;
-  C.kind[q] = coarsen_kind_level_at(F, C, q);
 }
 
 // Coarse apertures: mean of the 4 fine faces a coarse face covers.  `fo*` are the fine apertures
@@ -612,11 +594,6 @@ __device__ __forceinline__ void coarsen_open_at(int fnx, int fny, const float* _
     }
     C.ow[q] = 0.25f * s;
   }
-}
-__global__ void k_coarsen_open(int fnx, int fny, const float* __restrict__ fou, const float* __restrict__ fov,
-                               const float* __restrict__ fow, const unsigned char* __restrict__ act, Lev C) {
-  KSTART();
-  coarsen_open_at(fnx, fny, fou, fov, fow, act, C, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // ------------------------------------------------------------------------------------------------

@@ -349,25 +349,24 @@ inline const unsigned char* update_mask(const fd3_volume* V) {
 
 // ------------------------------------------------------------------------------------ multigrid
 // prepare_multigrid3 (delta3d_multigrid.rs:370-387): coarse geometry follows the surface.
+// Two launches per level (kinds and apertures, then diagonal and codes); the levels of at most
+// PREP_SMALL_CELLS cells below the first run in one CTA (measured: the 24 launches of a 128^3
+// hierarchy become 5).
+constexpr int PREP_SMALL_CELLS = 4096;
 void prepare_multigrid(fd3_volume* V) {
   if (!V->has_mg || V->levels.empty()) return;
   Geo G = V->geo();
-  for (size_t l = 0; l < V->levels.size(); ++l) {
-    Lev& C = V->levels[l];
-    long long nfaces = (long long)(C.nx + 1) * C.ny * C.nz + (long long)C.nx * (C.ny + 1) * C.nz +
-                       (long long)C.nx * C.ny * (C.nz + 1);
-    if (l == 0) {
-      LAUNCH(V, k_coarsen_kind_fine, C.n, G, C);
-      LAUNCH(V, k_coarsen_open, nfaces, V->nx, V->ny, (const float*)V->ou, (const float*)V->ov, (const float*)V->ow,
-             (const unsigned char*)G.act, C);
-    } else {
-      Lev& F = V->levels[l - 1];
-      LAUNCH(V, k_coarsen_kind_level, C.n, F, C);
-      LAUNCH(V, k_coarsen_open, nfaces, F.nx, F.ny, (const float*)F.ou, (const float*)F.ov, (const float*)F.ow,
-             (const unsigned char*)nullptr, C);
+  const int nl = (int)V->levels.size();
+  for (int l = 0; l < nl; ++l) {
+    const Lev& C = V->levels[l];
+    if (l > 0 && C.n <= PREP_SMALL_CELLS) {
+      LAUNCH_G(V, k_levels_prepare_small, 1, PREP_SMALL_THREADS, (const Lev*)V->dlev, l, nl - 1);
+      return;
     }
-    LAUNCH(V, k_level_diag, C.n, C);
-    LAUNCH(V, k_level_codes, C.n, C);
+    const long long nfaces = (long long)(C.nx + 1) * C.ny * C.nz + (long long)C.nx * (C.ny + 1) * C.nz +
+                             (long long)C.nx * C.ny * (C.nz + 1);
+    LAUNCH(V, k_level_prepare_a, C.n + nfaces, G, l > 0 ? V->levels[l - 1] : Lev{}, C, l == 0 ? 1 : 0);
+    LAUNCH(V, k_level_prepare_b, C.n, C);
   }
 }
 
