@@ -1738,12 +1738,17 @@ int fd3_set_surface(fd3_volume* V, const float* eta, size_t len) {
 }
 
 // delta3d.rs:631-645: the faces are staged in us/vs/ws, checked on the device, then published.
+// The staged faces are checked with one flag and one host round trip for the three arrays, then
+// copied into u, v, w (the published fields, which fd3_device_fields exposes: the call returns once
+// they are written).
 static int set_velocity_staged(fd3_volume* V) {
-  bool ok1, ok2, ok3;
-  TRY(check_finite_device(V, V->us, V->nu, &ok1));
-  TRY(check_finite_device(V, V->vs, V->nv, &ok2));
-  TRY(check_finite_device(V, V->ws, V->nw, &ok3));
-  if (!(ok1 && ok2 && ok3)) return FD3_ERR_NOT_FINITE;
+  CK(cudaMemsetAsync(V->dflag, 0, sizeof(int), V->stream));
+  LAUNCH_G(V, k_check_finite, 592, TPB, (long long)V->nu, (const float*)V->us, V->dflag);
+  LAUNCH_G(V, k_check_finite, 592, TPB, (long long)V->nv, (const float*)V->vs, V->dflag);
+  LAUNCH_G(V, k_check_finite, 592, TPB, (long long)V->nw, (const float*)V->ws, V->dflag);
+  CK(cudaMemcpyAsync(V->hflag, V->dflag, sizeof(int), cudaMemcpyDeviceToHost, V->stream));
+  TRY(sync(V));
+  if (*V->hflag != 0) return FD3_ERR_NOT_FINITE;
   CK(cudaMemcpyAsync(V->u, V->us, (size_t)V->nu * 4, cudaMemcpyDeviceToDevice, V->stream));
   CK(cudaMemcpyAsync(V->v, V->vs, (size_t)V->nv * 4, cudaMemcpyDeviceToDevice, V->stream));
   CK(cudaMemcpyAsync(V->w, V->ws, (size_t)V->nw * 4, cudaMemcpyDeviceToDevice, V->stream));
