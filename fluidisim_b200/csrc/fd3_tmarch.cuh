@@ -216,8 +216,10 @@ __global__ void __launch_bounds__(TQ<Q>::NT, MINB)
     const uint32_t bar0 = smem_u32(sm);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(sm + 64);
     unsigned char* const stages = sm + TM_CTRL_BYTES;
-    // Layers take the stages in turn (layer k0 - 1 the first), both in issue and in wait order.
-    int s_issue = 0, issued = k0 - 2;  // thread 0: the next stage to fill, the last layer issued
+    // Layers take the stages in turn (layer k0 - 1 the first), both in issue and in wait order.  One
+    // thread of the last warp issues the copies: the operand planes are formed by the first warps.
+    constexpr int ISSUER = NT - 32;
+    int s_issue = 0, issued = k0 - 2;  // the issuer: the next stage to fill, the last layer issued
     auto issue = [&](int L) {
       const int zc = min(max(L, 0), g.nz - 1);
       const uint32_t st = smem_u32(stages + s_issue * P::STAGE), bar = bar0 + 8u * s_issue;
@@ -233,7 +235,7 @@ __global__ void __launch_bounds__(TQ<Q>::NT, MINB)
       s_issue = s_issue + 1 == NS ? 0 : s_issue + 1;
       issued = L;
     };
-    if (tid == 0) {
+    if (tid == ISSUER) {
       for (int s = 0; s < NS; ++s) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar0 + 8u * s) : "memory");
       *abort_flag = 0;
       asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -315,7 +317,7 @@ __global__ void __launch_bounds__(TQ<Q>::NT, MINB)
       make_op(stages + skn * P::STAGE, (k + 1) & 3);
       __syncthreads();
       if (*abort_flag) break;
-      if (tid == 0 && k + D + 1 <= k1) {
+      if (tid == ISSUER && k + D + 1 <= k1) {
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // the generic reads of the stage before its refill
         issue(k + D + 1);
       }
@@ -424,7 +426,7 @@ __global__ void __launch_bounds__(TQ<Q>::NT, MINB)
       }
     }
     if (*abort_flag) {  // a wait ran out: drain this CTA's copies in flight, then fail the projection
-      if (tid == 0) {
+      if (tid == ISSUER) {
         while (waited < issued && wait_next()) {
         }
         S->status = 2;
