@@ -72,6 +72,7 @@ BYTES_PER_CELL = {
     "kt_fine_restrict": 2 + 4 + 4 + 0.5,
     "kt_fine_post1": 2 + 4 + 4 + 4 + 0.5 + 4,
     "kt_fine_post2_rz": 2 + 4 + 4 + 4 + 4,
+    "kt_residual": 2 + 4 * 3,                  # code, p, rhs, res out
     # one-cell-per-thread kernels (ordered mode, and f64 mode with kernels = 1)
     "k_dir_apply_dot": 2 + 4 + 4 + 4 + 4,
     "k_update_rn": 4 * 6,

@@ -177,8 +177,8 @@ struct fd3_volume {
   // tensor maps of the TMA-staged fine kernels (kernels = 5), made on first use; the buffers they
   // describe are allocated once, so the maps stay valid for the volume's life
   struct TmaSet {
-    CUtensorMap hz, hz2, hdir, hdir2, hprec, hres;  // halo boxes
-    CUtensorMap oprec, ores;                        // tile boxes
+    CUtensorMap hz, hz2, hdir, hdir2, hprec, hres, hp;  // halo boxes
+    CUtensorMap oprec, ores, orhs;                      // tile boxes
     CUtensorMap codes, par;                         // row codes; level 0's x (parent box)
   };
   TmaSet* tma = nullptr;
@@ -548,8 +548,10 @@ bool tma_ready(fd3_volume* V) {
             make_tmap(&T->hdir2, V->dir2, false, nx, ny, nz, TMW, TMH) &&
             make_tmap(&T->hprec, V->prec, false, nx, ny, nz, TMW, TMH) &&
             make_tmap(&T->hres, V->res, false, nx, ny, nz, TMW, TMH) &&
+            make_tmap(&T->hp, V->p, false, nx, ny, nz, TMW, TMH) &&
             make_tmap(&T->oprec, V->prec, false, nx, ny, nz, TMX, TMY) &&
             make_tmap(&T->ores, V->res, false, nx, ny, nz, TMX, TMY) &&
+            make_tmap(&T->orhs, V->rhs, false, nx, ny, nz, TMX, TMY) &&
             make_tmap(&T->codes, V->codes, true, nx, ny, nz, TMX, TMY);
   if (ok && !V->levels.empty()) {
     const Lev& L = V->levels[0];
@@ -628,6 +630,19 @@ void tma_dir(fd3_volume* V, int parity) {
   a.out1 = V->tmp;
   kt_dispatch(V, [&](auto k, auto q, auto d) {
     launch_tpass<TP_DIR, decltype(k)::value, decltype(d)::value, decltype(q)::value>(V, "kt_dir_apply_dot", M, a);
+  });
+}
+
+// res = rhs - A p with res.res (FIN_RR0 or FIN_ACTUAL): halo p, tile rhs.
+void tma_residual(fd3_volume* V, int op) {
+  const fd3_volume::TmaSet& T = *V->tma;
+  TMaps M{};
+  M.m[0] = T.hp; M.m[1] = T.orhs; M.m[2] = T.codes;
+  TArgs a{};
+  a.out0 = V->res;
+  a.op = op;
+  kt_dispatch(V, [&](auto k, auto q, auto d) {
+    launch_tpass<TP_RESID, decltype(k)::value, decltype(d)::value, decltype(q)::value>(V, "kt_residual", M, a);
   });
 }
 
@@ -848,6 +863,10 @@ void correct(fd3_volume* V, float k1) {
 // it (f64 reductions), else one cell per thread (the ordered mode's chunk order).
 void residual(fd3_volume* V, int op) {
   Geo G = V->geo();
+  if (V->tmaf() && tma_ready(V)) {
+    tma_residual(V, op);
+    return;
+  }
   if (V->quad()) {
     quad_dispatch(V, [&](auto qx, auto k4) {
       constexpr int QX = decltype(qx)::value, K4 = decltype(k4)::value;
