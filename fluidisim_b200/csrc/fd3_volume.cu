@@ -350,9 +350,9 @@ inline const unsigned char* update_mask(const fd3_volume* V) {
 // ------------------------------------------------------------------------------------ multigrid
 // prepare_multigrid3 (delta3d_multigrid.rs:370-387): coarse geometry follows the surface.
 // Two launches per level (kinds and apertures, then diagonal and codes); the levels of at most
-// PREP_SMALL_CELLS cells below the first run in one CTA (measured: the 24 launches of a 128^3
-// hierarchy become 5).
-constexpr int PREP_SMALL_CELLS = 4096;
+// PREP_SMALL_CELLS cells below the first run in one CTA (the 24 launches of a 128^3 hierarchy become
+// 7; with the 16^3 level in the one-CTA kernel too, that kernel alone took 27.7 us).
+constexpr int PREP_SMALL_CELLS = 512;
 void prepare_multigrid(fd3_volume* V) {
   if (!V->has_mg || V->levels.empty()) return;
   Geo G = V->geo();
