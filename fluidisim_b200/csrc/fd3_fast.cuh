@@ -130,50 +130,34 @@ struct LoadT {
 // built for), instead of rebuilding each row from the geometry.
 
 // One cell of divergence_mobile3 (delta3d_mobile.rs:398-433): |div u| of a wet row into the
-// maximum over all wet rows and, without a surface ghost (no face state 2), over the plain ones.
-__device__ __forceinline__ void div_metric_cell(const Geo& g, unsigned code, const float* __restrict__ u,
-                                                const float* __restrict__ v, const float* __restrict__ w, int c,
-                                                float& all, float& plain) {
-  if (!(code & RC_WET)) return;
-  int i, j, k; cell_ijk(g, c, i, j, k);
+// maximum over all wet rows and, without a surface ghost (no face state 2), over the plain ones;
+// the cell's six face velocities (x-, x+, y-, y+, z-, z+) are given.
+__device__ __forceinline__ void div_metric_vals(const Geo& g, unsigned code, int i, int j, int k, float ul, float ur,
+                                                float vf, float vk, float wb, float wt, float& all, float& plain) {
   float dv;
   if (g.cut) {
-    float fl = __ldg(g.ou + fu(g, i, j, k)) * u[fu(g, i, j, k)];
-    float fr = __ldg(g.ou + fu(g, i + 1, j, k)) * u[fu(g, i + 1, j, k)];
-    float ff = __ldg(g.ov + fv(g, i, j, k)) * v[fv(g, i, j, k)];
-    float fk = __ldg(g.ov + fv(g, i, j + 1, k)) * v[fv(g, i, j + 1, k)];
-    float fb = __ldg(g.ow + fw(g, i, j, k)) * w[fw(g, i, j, k)];
-    float ft = __ldg(g.ow + fw(g, i, j, k + 1)) * w[fw(g, i, j, k + 1)];
+    float fl = __ldg(g.ou + fu(g, i, j, k)) * ul;
+    float fr = __ldg(g.ou + fu(g, i + 1, j, k)) * ur;
+    float ff = __ldg(g.ov + fv(g, i, j, k)) * vf;
+    float fk = __ldg(g.ov + fv(g, i, j + 1, k)) * vk;
+    float fb = __ldg(g.ow + fw(g, i, j, k)) * wb;
+    float ft = __ldg(g.ow + fw(g, i, j, k + 1)) * wt;
     dv = ((fr - fl + ft - fb) + (fk - ff)) / g.dx;
     if (g.wall) dv = dv + wall_flux(g, i, j, k);
   } else {
-    float fl = u[fu(g, i, j, k)], fr = u[fu(g, i + 1, j, k)];
-    float ff = v[fv(g, i, j, k)], fk = v[fv(g, i, j + 1, k)];
-    float fb = w[fw(g, i, j, k)], ft = w[fw(g, i, j, k + 1)];
-    dv = ((fr - fl + ft - fb) + (fk - ff)) / g.dx;
+    dv = ((ur - ul + wt - wb) + (vk - vf)) / g.dx;
   }
   const float d = fabsf(dv);
   all = fmaxf(all, d);
   if (!(code & RC_GHOSTS)) plain = fmaxf(plain, d);
 }
-
-// divergence_mobile3 (delta3d_mobile.rs:398-433): max |div u| over the wet rows and over the
-// plain ones (no surface ghost: no face state 2), into S->fmax[0] and [1].  Each thread takes
-// METRIC_CELLS cells, a block's cells apart, and the block merges its maxima by one atomic each.
-__global__ void k_div_metric_c(Geo g, const unsigned short* __restrict__ codes, const float* __restrict__ u,
-                               const float* __restrict__ v, const float* __restrict__ w, Scalars* S) {
-  KSTART();
-  float all = 0.f, plain = 0.f;
-  const int c0 = blockIdx.x * (METRIC_CELLS * blockDim.x) + threadIdx.x;
-  unsigned code[METRIC_CELLS];
-#pragma unroll
-  for (int q = 0; q < METRIC_CELLS; ++q) {
-    const int c = c0 + q * blockDim.x;
-    code[q] = c < g.n ? codes[c] : 0u;
-  }
-#pragma unroll
-  for (int q = 0; q < METRIC_CELLS; ++q) div_metric_cell(g, code[q], u, v, w, c0 + q * blockDim.x, all, plain);
-  block_fmax2_atomic(all, plain, &S->fmax[0], &S->fmax[1]);
+__device__ __forceinline__ void div_metric_cell(const Geo& g, unsigned code, const float* __restrict__ u,
+                                                const float* __restrict__ v, const float* __restrict__ w, int c,
+                                                float& all, float& plain) {
+  if (!(code & RC_WET)) return;
+  int i, j, k; cell_ijk(g, c, i, j, k);
+  div_metric_vals(g, code, i, j, k, u[fu(g, i, j, k)], u[fu(g, i + 1, j, k)], v[fv(g, i, j, k)], v[fv(g, i, j + 1, k)],
+                  w[fw(g, i, j, k)], w[fw(g, i, j, k + 1)], all, plain);
 }
 
 // correct_mobile3 (delta3d_mobile.rs:284-343) from the row codes.  A u or v face between cells l
@@ -182,6 +166,35 @@ __global__ void k_div_metric_c(Geo g, const unsigned short* __restrict__ codes, 
 // exactly the faces the reference corrects: open, neither cell solid, at least one wet.  A w face
 // is corrected when the row of the cell below has it live.  Ghost coefficients and values are the
 // reference's (ghost_side3, ghost_up3).
+// The corrected value of the u (axis 0) or v (axis 1) face (i, j, k) whose staged value is `val`,
+// given the codes and pressures of the cells on its + side (cr, pr) and - side (cl, pl), which only
+// an interior face reads.
+__device__ __forceinline__ float corrected_uv_vals(const Geo& g, float k1, float val, int axis, int i, int j, int k,
+                                                  unsigned cr, unsigned cl, float pr, float pl) {
+  const bool interior = axis == 0 ? (i > 0 && i < g.nx) : (j > 0 && j < g.ny);
+  if (interior) {
+    const int x = axis == 0 ? i - 1 : i, y = axis == 0 ? j : j - 1;
+    const unsigned sr = face_state(cr, axis == 0 ? 0 : 2);  // r's face toward l
+    if (sr == 1) {
+      val -= k1 * (pr - pl) / g.dx;
+    } else if (sr == 2) {
+      float a, b; ghost_side3(g, i, j, k, x, y, a, b);
+      val -= k1 * (pr - b) * a / g.dx;
+    } else if (!(cr & RC_WET) && face_state(cl, axis == 0 ? 1 : 3) == 2) {  // l's face toward r
+      float a, b; ghost_side3(g, x, y, k, i, j, a, b);
+      val -= k1 * (b - pl) * a / g.dx;
+    }
+  }
+  return val;
+}
+__device__ __forceinline__ float corrected_uv(const Geo& g, const unsigned short* __restrict__ codes, float k1,
+                                             const float* __restrict__ p, float val, int axis, int i, int j, int k) {
+  const bool interior = axis == 0 ? (i > 0 && i < g.nx) : (j > 0 && j < g.ny);
+  if (!interior) return val;
+  const int x = axis == 0 ? i - 1 : i, y = axis == 0 ? j : j - 1;
+  const int l = (k * g.ny + y) * g.nx + x, r = (k * g.ny + j) * g.nx + i;
+  return corrected_uv_vals(g, k1, val, axis, i, j, k, codes[r], codes[l], p[r], p[l]);
+}
 __device__ __forceinline__ void correct_uv_at(const Geo& g, const unsigned short* __restrict__ codes, float k1,
                                               const float* __restrict__ p, const float* __restrict__ us,
                                               const float* __restrict__ vs, float* __restrict__ u,
@@ -191,57 +204,151 @@ __device__ __forceinline__ void correct_uv_at(const Geo& g, const unsigned short
   if (q < nu) { axis = 0; f = q; i = f % (g.nx + 1); int t = f / (g.nx + 1); j = t % g.ny; k = t / g.ny; }
   else if (q < nu + nv) { axis = 1; f = q - nu; i = f % g.nx; int t = f / g.nx; j = t % (g.ny + 1); k = t / (g.ny + 1); }
   else return;
-  float val = axis == 0 ? us[f] : vs[f];
-  const bool interior = axis == 0 ? (i > 0 && i < g.nx) : (j > 0 && j < g.ny);
-  if (interior) {
-    const int x = axis == 0 ? i - 1 : i, y = axis == 0 ? j : j - 1;
-    const int l = (k * g.ny + y) * g.nx + x, r = (k * g.ny + j) * g.nx + i;
-    const unsigned cr = codes[r];
-    const unsigned sr = face_state(cr, axis == 0 ? 0 : 2);  // r's face toward l
-    if (sr == 1) {
-      val -= k1 * (p[r] - p[l]) / g.dx;
-    } else if (sr == 2) {
-      float a, b; ghost_side3(g, i, j, k, x, y, a, b);
-      val -= k1 * (p[r] - b) * a / g.dx;
-    } else if (!(cr & RC_WET) && face_state(codes[l], axis == 0 ? 1 : 3) == 2) {  // l's face toward r
-      float a, b; ghost_side3(g, x, y, k, i, j, a, b);
-      val -= k1 * (b - p[l]) * a / g.dx;
-    }
-  }
+  const float val = corrected_uv(g, codes, k1, p, axis == 0 ? us[f] : vs[f], axis, i, j, k);
   if (axis == 0) u[f] = val; else v[f] = val;
 }
-__global__ void k_correct_uv_c(Geo g, const unsigned short* __restrict__ codes, float k1, const float* __restrict__ p,
-                               const float* __restrict__ us, const float* __restrict__ vs, float* __restrict__ u,
-                               float* __restrict__ v) {
-  KSTART();
-  correct_uv_at(g, codes, k1, p, us, vs, u, v, blockIdx.x * blockDim.x + threadIdx.x);
-}
 
+// The corrected value of the w face (i, j, k) (k its layer) whose staged value is `val`, given the
+// code and pressure of the cell below (cb, pb) and the pressure of the cell above (pa), which only
+// a face with a cell below reads.
+__device__ __forceinline__ float corrected_w_vals(const Geo& g, float k1, float val, int i, int j, int k, unsigned cb,
+                                                 float pb, float pa) {
+  if (k >= 1) {
+    const unsigned st = face_state(cb, 5);  // the face above the cell below
+    if (st == 1) {
+      val -= k1 * (pa - pb) / g.dx;
+    } else if (st == 2) {
+      float a, b; ghost_up3(g, i, j, k - 1, a, b);
+      val -= k1 * (b - pb) * a / g.dx;
+    }
+  }
+  return val;
+}
+__device__ __forceinline__ float corrected_w(const Geo& g, const unsigned short* __restrict__ codes, float k1,
+                                            const float* __restrict__ p, float val, int f, int i, int j, int k) {
+  if (k < 1) return val;
+  const int nxny = g.nx * g.ny;
+  const int below = f - nxny;
+  const unsigned cb = codes[below];
+  // the cell above exists wherever the face below it is live (state 1)
+  const float pa = face_state(cb, 5) == 1u ? p[below + nxny] : 0.f;
+  return corrected_w_vals(g, k1, val, i, j, k, cb, p[below], pa);
+}
 __device__ __forceinline__ void correct_w_at(const Geo& g, const unsigned short* __restrict__ codes, float k1,
                                              const float* __restrict__ p, const float* __restrict__ ws,
                                              float* __restrict__ w, int f) {
   const int nw = g.nx * g.ny * (g.nz + 1);
   if (f >= nw) return;
   const int nxny = g.nx * g.ny;
-  const int k = f / nxny;
-  float val = ws[f];
-  if (k >= 1) {
-    const int below = f - nxny;
-    const unsigned st = face_state(codes[below], 5);  // the face above the cell below
-    if (st == 1) {
-      val -= k1 * (p[below + nxny] - p[below]) / g.dx;
-    } else if (st == 2) {
-      const int col = f % nxny, i = col % g.nx, j = col / g.nx;
-      float a, b; ghost_up3(g, i, j, k - 1, a, b);
-      val -= k1 * (b - p[below]) * a / g.dx;
+  const int k = f / nxny, col = f % nxny, i = col % g.nx, j = col / g.nx;
+  w[f] = corrected_w(g, codes, k1, p, ws[f], f, i, j, k);
+}
+
+// correct_mobile3, divergence_mobile3 and the largest |u| (delta3d_mobile.rs:284-343, 398-433) in
+// one pass.  Cell c forms the corrected values of its six faces with the expressions of
+// correct_uv_at and correct_w_at (a face shared by two cells gets the same value from both), stores
+// the faces it owns (x-, y-, z-, and the + faces on the volume's upper edges, so every face is stored
+// once), takes |div u| of its row from the six values, and the largest |value| of its own faces.
+// Maxima into S->fmax[0] (all rows), [1] (plain rows), [2] (|u|), reset before, by one atomic each
+// per block.
+__device__ __forceinline__ void block_fmax3_atomic(float a, float b, float c, float* addr0, float* addr1,
+                                                   float* addr2) {
+  __shared__ float pa[32], pb[32], pc[32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    a = fmaxf(a, __shfl_down_sync(0xffffffffu, a, o));
+    b = fmaxf(b, __shfl_down_sync(0xffffffffu, b, o));
+    c = fmaxf(c, __shfl_down_sync(0xffffffffu, c, o));
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) { pa[wid] = a; pb[wid] = b; pc[wid] = c; }
+  __syncthreads();
+  if (wid == 0) {
+    const bool on = lane < (int)(blockDim.x >> 5);
+    a = on ? pa[lane] : 0.f;
+    b = on ? pb[lane] : 0.f;
+    c = on ? pc[lane] : 0.f;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      a = fmaxf(a, __shfl_down_sync(0xffffffffu, a, o));
+      b = fmaxf(b, __shfl_down_sync(0xffffffffu, b, o));
+      c = fmaxf(c, __shfl_down_sync(0xffffffffu, c, o));
+    }
+    if (lane == 0) {
+      atomic_fmax_nonneg(addr0, a);
+      atomic_fmax_nonneg(addr1, b);
+      atomic_fmax_nonneg(addr2, c);
     }
   }
-  w[f] = val;
 }
-__global__ void k_correct_w_c(Geo g, const unsigned short* __restrict__ codes, float k1, const float* __restrict__ p,
-                              const float* __restrict__ ws, float* __restrict__ w) {
+// Columns of 32 x 8 cells (a warp per row) marching CM_K layers: the indices advance by constant
+// strides, the codes and pressures of the cells below and above ride in registers from layer to
+// layer, and a cell's top w face is the next layer's bottom one, formed once and carried.
+constexpr int CM_X = 32, CM_Y = 8, CM_K = 8;
+inline int cm_blocks(int nx, int ny, int nz) {
+  return ((nx + CM_X - 1) / CM_X) * ((ny + CM_Y - 1) / CM_Y) * ((nz + CM_K - 1) / CM_K);
+}
+__global__ void __launch_bounds__(CM_X * CM_Y) k_correct_metric(Geo g, const unsigned short* __restrict__ codes,
+                                                                float k1, const float* __restrict__ p,
+                                                                const float* __restrict__ us,
+                                                                const float* __restrict__ vs,
+                                                                const float* __restrict__ ws, float* __restrict__ u,
+                                                                float* __restrict__ v, float* __restrict__ w,
+                                                                Scalars* S) {
   KSTART();
-  correct_w_at(g, codes, k1, p, ws, w, blockIdx.x * blockDim.x + threadIdx.x);
+  float all = 0.f, plain = 0.f, mx = 0.f;
+  const int ntx = (g.nx + CM_X - 1) / CM_X, nty = (g.ny + CM_Y - 1) / CM_Y;
+  int b = blockIdx.x;
+  const int bx = b % ntx; b /= ntx;
+  const int by = b % nty; b /= nty;
+  const int i = bx * CM_X + (int)(threadIdx.x & 31), j = by * CM_Y + (int)(threadIdx.x >> 5);
+  const int k0 = b * CM_K, ke = min(k0 + CM_K, g.nz);
+  if (i < g.nx && j < g.ny) {
+    const int nxny = g.nx * g.ny, su = g.ny * (g.nx + 1), sv = (g.ny + 1) * g.nx;
+    const bool xm = i > 0, xp = i + 1 < g.nx, ym = j > 0, yp = j + 1 < g.ny;
+    int c = (k0 * g.ny + j) * g.nx + i;                 // the cell, and its w face below (fw)
+    int ful = (k0 * g.ny + j) * (g.nx + 1) + i;         // its u face x-
+    int fvf = (k0 * (g.ny + 1) + j) * g.nx + i;         // its v face y-
+    unsigned cc = codes[c];
+    float pc = p[c];
+    float wb;
+    {
+      const unsigned cb = k0 > 0 ? codes[c - nxny] : 0u;
+      const float pb = k0 > 0 ? p[c - nxny] : 0.f;
+      wb = corrected_w_vals(g, k1, ws[c], i, j, k0, cb, pb, pc);
+    }
+    for (int k = k0; k < ke; ++k) {
+      const bool zp = k + 1 < g.nz;
+      const unsigned ca = zp ? codes[c + nxny] : 0u;
+      const float pa = zp ? p[c + nxny] : 0.f;
+      const unsigned cxm = xm ? codes[c - 1] : 0u, cxp = xp ? codes[c + 1] : 0u;
+      const unsigned cym = ym ? codes[c - g.nx] : 0u, cyp = yp ? codes[c + g.nx] : 0u;
+      const float pxm = xm ? p[c - 1] : 0.f, pxp = xp ? p[c + 1] : 0.f;
+      const float pym = ym ? p[c - g.nx] : 0.f, pyp = yp ? p[c + g.nx] : 0.f;
+      const float ul = corrected_uv_vals(g, k1, us[ful], 0, i, j, k, cc, cxm, pc, pxm);
+      const float ur = corrected_uv_vals(g, k1, us[ful + 1], 0, i + 1, j, k, cxp, cc, pxp, pc);
+      const float vf = corrected_uv_vals(g, k1, vs[fvf], 1, i, j, k, cc, cym, pc, pym);
+      const float vk = corrected_uv_vals(g, k1, vs[fvf + g.nx], 1, i, j + 1, k, cyp, cc, pyp, pc);
+      const float wt = corrected_w_vals(g, k1, ws[c + nxny], i, j, k + 1, cc, pc, pa);
+      u[ful] = ul;
+      v[fvf] = vf;
+      w[c] = wb;
+      mx = fmaxf(mx, fabsf(ul));
+      mx = fmaxf(mx, fabsf(vf));
+      mx = fmaxf(mx, fabsf(wb));
+      if (!xp) { u[ful + 1] = ur; mx = fmaxf(mx, fabsf(ur)); }
+      if (!yp) { v[fvf + g.nx] = vk; mx = fmaxf(mx, fabsf(vk)); }
+      if (!zp) { w[c + nxny] = wt; mx = fmaxf(mx, fabsf(wt)); }
+      if (cc & RC_WET) div_metric_vals(g, cc, i, j, k, ul, ur, vf, vk, wb, wt, all, plain);
+      cc = ca;
+      pc = pa;
+      wb = wt;
+      c += nxny;
+      ful += su;
+      fvf += sv;
+    }
+  }
+  block_fmax3_atomic(all, plain, mx, &S->fmax[0], &S->fmax[1], &S->fmax[2]);
 }
 
 // One row of backward_error_mobile3 (delta3d_mobile.rs:243-271): |r_i| / (|b| + |A||p|)_i of a wet
