@@ -352,50 +352,83 @@ __global__ void __launch_bounds__(CM_X * CM_Y) k_correct_metric(Geo g, const uns
 }
 
 // One row of backward_error_mobile3 (delta3d_mobile.rs:243-271): |r_i| / (|b| + |A||p|)_i of a wet
-// row (0 for a dry row or a zero scale).  The apertures and ghost coefficients are apply_code's.
+// row (0 for a dry row or a zero scale), from the pressures of the cell and its six neighbours (x-,
+// x+, y-, y+, z-, z+; a neighbour's is read only across a live face), b_i and r_i.  The apertures and
+// ghost coefficients are apply_code's.
+__device__ __forceinline__ float backward_error_vals(const Geo& g, unsigned code, int i, int j, int k, float pcv,
+                                                    float pxm, float pxp, float pym, float pyp, float pzm, float pzp,
+                                                    float bc, float rc) {
+  if (!(code & RC_WET)) return 0.f;
+  const bool unit = code & RC_UNIT;
+  const float pc = fabsf(pcv);
+  float acc = 0.f;
+  auto face = [&](int f, int axis, int fi, float pm, int x, int y) {
+    const unsigned st = face_state(code, f);
+    if (!st) return;
+    const float a = unit ? 1.f : aper3(g, axis, fi);
+    if (st == 1) acc += a * (pc + fabsf(pm));
+    else acc += a * pc * (f == 5 ? ghost_it_up(g, i, j, k) : ghost_it_side(g, i, j, k, x, y));
+  };
+  face(0, 0, fu(g, i, j, k), pxm, i - 1, j);
+  face(1, 0, fu(g, i + 1, j, k), pxp, i + 1, j);
+  face(2, 1, fv(g, i, j, k), pym, i, j - 1);
+  face(3, 1, fv(g, i, j + 1, k), pyp, i, j + 1);
+  face(4, 2, fw(g, i, j, k), pzm, i, j);
+  face(5, 2, fw(g, i, j, k + 1), pzp, i, j);
+  const float scale = fabsf(bc) + acc * g.inv;
+  return scale > 0.f ? fabsf(rc) / scale : 0.f;
+}
 __device__ __forceinline__ float backward_error_cell(const Geo& g, unsigned code, const float* __restrict__ p,
                                                      const float* __restrict__ rhs, const float* __restrict__ res,
                                                      int c) {
   if (!(code & RC_WET)) return 0.f;
   int i, j, k; cell_ijk(g, c, i, j, k);
   const int nxny = g.nx * g.ny;
-  const bool unit = code & RC_UNIT;
-  const float pc = fabsf(p[c]);
-  float acc = 0.f;
-  auto face = [&](int f, int axis, int fi, int m, int x, int y) {
-    const unsigned st = face_state(code, f);
-    if (!st) return;
-    const float a = unit ? 1.f : aper3(g, axis, fi);
-    if (st == 1) acc += a * (pc + fabsf(p[m]));
-    else acc += a * pc * (f == 5 ? ghost_it_up(g, i, j, k) : ghost_it_side(g, i, j, k, x, y));
-  };
-  face(0, 0, fu(g, i, j, k), c - 1, i - 1, j);
-  face(1, 0, fu(g, i + 1, j, k), c + 1, i + 1, j);
-  face(2, 1, fv(g, i, j, k), c - g.nx, i, j - 1);
-  face(3, 1, fv(g, i, j + 1, k), c + g.nx, i, j + 1);
-  face(4, 2, fw(g, i, j, k), c - nxny, i, j);
-  face(5, 2, fw(g, i, j, k + 1), c + nxny, i, j);
-  const float scale = fabsf(rhs[c]) + acc * g.inv;
-  return scale > 0.f ? fabsf(res[c]) / scale : 0.f;
+  return backward_error_vals(g, code, i, j, k, p[c], i > 0 ? p[c - 1] : 0.f, i + 1 < g.nx ? p[c + 1] : 0.f,
+                             j > 0 ? p[c - g.nx] : 0.f, j + 1 < g.ny ? p[c + g.nx] : 0.f, k > 0 ? p[c - nxny] : 0.f,
+                             k + 1 < g.nz ? p[c + nxny] : 0.f, rhs[c], res[c]);
 }
 
-// backward_error_mobile3 (delta3d_mobile.rs:243-271): max |r_i| / (|b| + |A||p|)_i over the wet
-// rows into S->fmax[3].  A row's apertures and ghost coefficients are the ones apply_code uses.
-// Each thread takes METRIC_CELLS cells, a block's cells apart; one atomic per block.
-__global__ void k_backward_error_c(Geo g, const unsigned short* __restrict__ codes, const float* __restrict__ p,
-                                   const float* __restrict__ rhs, const float* __restrict__ res, Scalars* S) {
+// backward_error_mobile3 (delta3d_mobile.rs:243-271) and the fingerprint of p in one pass, marching
+// the columns as k_correct_metric does (the pressures below and above ride in registers): the
+// largest |r_i| / (|b| + |A||p|)_i over the wet rows into S->fmax[3] (one atomic per block), and the
+// wrapping sum of hash_at over every cell into S->hash (one atomic per warp; the sum does not depend
+// on the order).  Both reset before.
+__global__ void __launch_bounds__(CM_X * CM_Y) k_backward_hash(Geo g, const unsigned short* __restrict__ codes,
+                                                               const float* __restrict__ p,
+                                                               const float* __restrict__ rhs,
+                                                               const float* __restrict__ res, Scalars* S) {
   KSTART();
   float worst = 0.f;
-  const int c0 = blockIdx.x * (METRIC_CELLS * blockDim.x) + threadIdx.x;
-  unsigned codev[METRIC_CELLS];
-#pragma unroll
-  for (int q = 0; q < METRIC_CELLS; ++q) {
-    const int c = c0 + q * blockDim.x;
-    codev[q] = c < g.n ? codes[c] : 0u;
+  unsigned long long h = 0ull;
+  const int ntx = (g.nx + CM_X - 1) / CM_X, nty = (g.ny + CM_Y - 1) / CM_Y;
+  int b = blockIdx.x;
+  const int bx = b % ntx; b /= ntx;
+  const int by = b % nty; b /= nty;
+  const int i = bx * CM_X + (int)(threadIdx.x & 31), j = by * CM_Y + (int)(threadIdx.x >> 5);
+  const int k0 = b * CM_K, ke = min(k0 + CM_K, g.nz);
+  if (i < g.nx && j < g.ny) {
+    const int nxny = g.nx * g.ny;
+    const bool xm = i > 0, xp = i + 1 < g.nx, ym = j > 0, yp = j + 1 < g.ny;
+    int c = (k0 * g.ny + j) * g.nx + i;
+    float pb = k0 > 0 ? p[c - nxny] : 0.f;
+    float pc = p[c];
+    for (int k = k0; k < ke; ++k, c += nxny) {
+      const float pa = k + 1 < g.nz ? p[c + nxny] : 0.f;
+      const unsigned code = codes[c];
+      const float pxm = xm ? p[c - 1] : 0.f, pxp = xp ? p[c + 1] : 0.f;
+      const float pym = ym ? p[c - g.nx] : 0.f, pyp = yp ? p[c + g.nx] : 0.f;
+      const float bc = rhs[c], rc = res[c];
+      worst = fmaxf(worst, backward_error_vals(g, code, i, j, k, pc, pxm, pxp, pym, pyp, pb, pa, bc, rc));
+      h += hash_val(pc, c);
+      pb = pc;
+      pc = pa;
+    }
   }
-#pragma unroll
-  for (int q = 0; q < METRIC_CELLS; ++q) worst = fmaxf(worst, backward_error_cell(g, codev[q], p, rhs, res, c0 + q * blockDim.x));
   block_fmax2_atomic(worst, 0.f, &S->fmax[3], nullptr);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) h += __shfl_down_sync(0xffffffffu, h, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(&S->hash, h);
 }
 
 // ------------------------------------------------------------------------------------------------

@@ -672,9 +672,10 @@ __device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
   z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
   return z ^ (z >> 31);
 }
-__device__ __forceinline__ unsigned long long hash_at(const float* __restrict__ p, int q) {
-  return mix64(((unsigned long long)(unsigned)__float_as_int(p[q]) << 32 | (unsigned)q) + 0x9E3779B97F4A7C15ull);
+__device__ __forceinline__ unsigned long long hash_val(float x, int q) {
+  return mix64(((unsigned long long)(unsigned)__float_as_int(x) << 32 | (unsigned)q) + 0x9E3779B97F4A7C15ull);
 }
+__device__ __forceinline__ unsigned long long hash_at(const float* __restrict__ p, int q) { return hash_val(p[q], q); }
 __global__ void k_hash(int n, const float* __restrict__ p, Scalars* S) {
   KSTART();
   unsigned long long h = 0;

@@ -907,12 +907,13 @@ int outer_checks(fd3_volume* V, float k1, Checks* out) {
              (const float*)V->p, (const float*)V->us, (const float*)V->vs, (const float*)V->ws, V->u, V->v, V->w,
              V->dS);
   }
-  if (V->linear)
+  if (V->linear) {
     LAUNCH(V, k_backward_error_linear, V->n, G, (const float*)V->p, (const float*)V->rhs, (const float*)V->res, V->dS);
-  else
-    LAUNCH(V, k_backward_error_c, ((long long)V->n + METRIC_CELLS - 1) / METRIC_CELLS, G,
-           (const unsigned short*)V->codes, (const float*)V->p, (const float*)V->rhs, (const float*)V->res, V->dS);
-  LAUNCH_G(V, k_hash, 592, TPB, V->n, (const float*)V->p, V->dS);
+    LAUNCH_G(V, k_hash, 592, TPB, V->n, (const float*)V->p, V->dS);
+  } else {  // the backward error and the fingerprint in one pass
+    LAUNCH_G(V, k_backward_hash, cm_blocks(V->nx, V->ny, V->nz), CM_X * CM_Y, G, (const unsigned short*)V->codes,
+             (const float*)V->p, (const float*)V->rhs, (const float*)V->res, V->dS);
+  }
   TRY(pull(V));
   const Scalars* S = V->hS;
   // delta3d_mobile.rs:426-432; the linear metric (delta3d.rs:1043-1052) has no velocity floor
