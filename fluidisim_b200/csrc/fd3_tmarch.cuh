@@ -343,8 +343,14 @@ __global__ void __launch_bounds__(TQ<Q>::NT, MINB)
         bool fast = true;
 #pragma unroll
         for (int e = 0; e < Q; ++e) fast = fast && rc_plain_or_dry(cd[e]);
+        unsigned any = 0u;
+#pragma unroll
+        for (int e = 0; e < Q; ++e) any |= cd[e];
         V av;
-        if (fast) {
+        if (any == 0u) {  // every cell dry: the masked sums are +0 (a warp of air skips them)
+#pragma unroll
+          for (int e = 0; e < Q; ++e) qs(av, e, 0.f);
+        } else if (fast) {
 #pragma unroll
           for (int e = 0; e < Q; ++e) {
             const float pe = qe(pc, e), xm = e == 0 ? xl : qe(pc, e - 1), xp = e == Q - 1 ? xr : qe(pc, e + 1);
