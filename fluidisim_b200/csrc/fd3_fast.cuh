@@ -485,7 +485,17 @@ template <>
 __device__ void finish_block<RED_F64>(Red red, int nparts, Scalars* S, int op) {
   __shared__ double sm[TPB];
   double s = 0.0;
-  for (int q = threadIdx.x; q < nparts; q += blockDim.x) s += __ldcg(red.p64 + q);
+  // each thread's partials in index order, their loads issued eight at a time (the sums are the same)
+  const int step = blockDim.x;
+  int q = threadIdx.x;
+  for (; q + 7 * step < nparts; q += 8 * step) {
+    double v[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) v[e] = __ldcg(red.p64 + q + e * step);
+#pragma unroll
+    for (int e = 0; e < 8; ++e) s += v[e];
+  }
+  for (; q < nparts; q += step) s += __ldcg(red.p64 + q);
   sm[threadIdx.x] = s;
   __syncthreads();
   for (int w = blockDim.x / 2; w > 0; w >>= 1) {

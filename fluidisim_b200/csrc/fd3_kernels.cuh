@@ -259,30 +259,44 @@ __device__ __forceinline__ void ghost_side3(const Geo& g, int i, int j, int k, i
 
 struct RowE { int n; float a, it, val; };  // n < 0: no fluid neighbour (a wall, a ghost or nothing)
 
-// mobile_row (delta3d_mobile.rs:152-188): order x-, x+, y-, y+, z-, z+.
+// mobile_row (delta3d_mobile.rs:152-188): order x-, x+, y-, y+, z-, z+.  Every operand the decisions
+// may need (apertures, the neighbours' solid tests and column heights) is loaded first, each behind
+// its bounds test, so the loads go out together; the decisions then follow the reference's order.
 __device__ __forceinline__ void mobile_row(const Geo& g, int i, int j, int k, RowE row[6]) {
 #pragma unroll
   for (int f = 0; f < 6; ++f) row[f] = RowE{-1, 0.f, 0.f, 0.f};
   const int nxny = g.nx * g.ny;
   const int c = (k * g.ny + j) * g.nx + i;
+  const bool ok[4] = {i > 0, i + 1 < g.nx, j > 0, j + 1 < g.ny};
+  const int xs[4] = {i - 1, i + 1, i, i}, ys[4] = {j, j, j - 1, j + 1};
+  const int fi[4] = {fu(g, i, j, k), fu(g, i + 1, j, k), fv(g, i, j, k), fv(g, i, j + 1, k)};
+  float a[4], hn[4];
+  bool sol[4];
 #pragma unroll
   for (int f = 0; f < 4; ++f) {
-    bool ok; int x, y; float a;
-    if (f == 0) { ok = i > 0; x = i - 1; y = j; a = ok ? open3(g, 0, fu(g, i, j, k)) : 0.f; }
-    else if (f == 1) { ok = i + 1 < g.nx; x = i + 1; y = j; a = ok ? open3(g, 0, fu(g, i + 1, j, k)) : 0.f; }
-    else if (f == 2) { ok = j > 0; x = i; y = j - 1; a = ok ? open3(g, 1, fv(g, i, j, k)) : 0.f; }
-    else { ok = j + 1 < g.ny; x = i; y = j + 1; a = ok ? open3(g, 1, fv(g, i, j + 1, k)) : 0.f; }
-    if (!ok) continue;
-    int cn = (k * g.ny + y) * g.nx + x;
-    if (a == 0.f || solid3(g, cn)) continue;
-    if (wet3(g, x, y, k)) row[f] = RowE{cn, a, 0.f, 0.f};
-    else { float it, b; ghost_side3(g, i, j, k, x, y, it, b); row[f] = RowE{-1, a, it, b}; }
+    const int cn = (k * g.ny + ys[f]) * g.nx + xs[f];
+    a[f] = ok[f] ? open3(g, f < 2 ? 0 : 1, fi[f]) : 0.f;
+    sol[f] = ok[f] ? solid3(g, cn) : true;
+    hn[f] = ok[f] ? __ldg(g.eta + ys[f] * g.nx + xs[f]) : 0.f;
   }
-  float down = open3(g, 2, fw(g, i, j, k));
-  if (k > 0 && down > 0.f && !solid3(g, c - nxny)) row[4] = RowE{c - nxny, down, 0.f, 0.f};
-  float up = open3(g, 2, fw(g, i, j, k + 1));
+  const float down = open3(g, 2, fw(g, i, j, k));
+  const bool sol_down = k > 0 ? solid3(g, c - nxny) : true;
+  const float up = open3(g, 2, fw(g, i, j, k + 1));
+  const bool above = k + 1 < g.nz;
+  const bool sol_up = above ? solid3(g, c + nxny) : true;
+  const float hc = __ldg(g.eta + j * g.nx + i);
+#pragma unroll
+  for (int f = 0; f < 4; ++f) {
+    if (!ok[f]) continue;
+    if (a[f] == 0.f || sol[f]) continue;
+    const int x = xs[f], y = ys[f];
+    const int cn = (k * g.ny + y) * g.nx + x;
+    if (((float)k + 0.5f) * g.dx < hn[f]) row[f] = RowE{cn, a[f], 0.f, 0.f};  // wet3 of the neighbour
+    else { float it, b; ghost_side3(g, i, j, k, x, y, it, b); row[f] = RowE{-1, a[f], it, b}; }
+  }
+  if (k > 0 && down > 0.f && !sol_down) row[4] = RowE{c - nxny, down, 0.f, 0.f};
   if (up > 0.f) {
-    if (k + 1 < g.nz && wet3(g, i, j, k + 1)) row[5] = RowE{c + nxny, up, 0.f, 0.f};
+    if (above && !sol_up && ((float)(k + 1) + 0.5f) * g.dx < hc) row[5] = RowE{c + nxny, up, 0.f, 0.f};
     else { float it, b; ghost_up3(g, i, j, k, it, b); row[5] = RowE{-1, up, it, b}; }
   }
 }
