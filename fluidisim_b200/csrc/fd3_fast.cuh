@@ -526,9 +526,15 @@ template <int MODE>
 __device__ __forceinline__ void reduce_finish(typename Acc<MODE>::T v, int c, int n, Red red, Scalars* S, int op) {
   block_reduce<MODE>(v, c, n, red);
   __shared__ bool last;
-  __threadfence();
+  // the partials must be visible before the block counts in: in f64 mode thread 0 wrote the block's
+  // one partial and alone fences (the other threads' stores need no ordering here: the next kernel
+  // sees them after the grid completes); in ordered mode several threads wrote chunk partials
+  if (MODE == RED_ORD) __threadfence();
   __syncthreads();
-  if (threadIdx.x == 0) last = atomicAdd(red.count, 1u) == gridDim.x - 1;
+  if (threadIdx.x == 0) {
+    if (MODE != RED_ORD) __threadfence();
+    last = atomicAdd(red.count, 1u) == gridDim.x - 1;
+  }
   __syncthreads();
   if (!last) return;
   __threadfence();

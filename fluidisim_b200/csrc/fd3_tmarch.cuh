@@ -153,14 +153,13 @@ __device__ __forceinline__ void kt_reduce_finish(double v, Red red, Scalars* S, 
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
   if ((threadIdx.x & 31) == 0) sw[threadIdx.x >> 5] = v;
   __syncthreads();
-  if (threadIdx.x == 0) {
+  if (threadIdx.x == 0) {  // the block's partial, visible before the block counts in
     double t = 0.0;
     for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sw[w];
     red.p64[blockIdx.x] = t;
+    __threadfence();
+    last = atomicAdd(red.count, 1u) == gridDim.x - 1;
   }
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) last = atomicAdd(red.count, 1u) == gridDim.x - 1;
   __syncthreads();
   if (!last) return;
   __threadfence();
