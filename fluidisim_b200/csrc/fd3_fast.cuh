@@ -284,6 +284,12 @@ __device__ __forceinline__ void block_fmax3_atomic(float a, float b, float c, fl
 // Columns of 32 x 8 cells (a warp per row) marching CM_K layers: the indices advance by constant
 // strides, the codes and pressures of the cells below and above ride in registers from layer to
 // layer, and a cell's top w face is the next layer's bottom one, formed once and carried.
+// Resident CTAs per SM for the assembly (k_rhs_b2) and the backward error pass: eight (32 registers,
+// a few spilled) measured 17.48 -> 16.79 ms per 256^3 projection against the unbounded 48-50
+// registers (six: 16.86), the same box.
+#ifndef FD3_SETUP_MINB
+#define FD3_SETUP_MINB 8
+#endif
 constexpr int CM_X = 32, CM_Y = 8, CM_K = 8;
 inline int cm_blocks(int nx, int ny, int nz) {
   return ((nx + CM_X - 1) / CM_X) * ((ny + CM_Y - 1) / CM_Y) * ((nz + CM_K - 1) / CM_K);
@@ -399,7 +405,7 @@ __device__ __forceinline__ float backward_error_cell(const Geo& g, unsigned code
 // largest |r_i| / (|b| + |A||p|)_i over the wet rows into S->fmax[3] (one atomic per block), and the
 // wrapping sum of hash_at over every cell into S->hash (one atomic per warp; the sum does not depend
 // on the order).  Both reset before.
-__global__ void __launch_bounds__(CM_X * CM_Y) k_backward_hash(Geo g, const unsigned short* __restrict__ codes,
+__global__ void __launch_bounds__(CM_X * CM_Y, FD3_SETUP_MINB) k_backward_hash(Geo g, const unsigned short* __restrict__ codes,
                                                                const float* __restrict__ p,
                                                                const float* __restrict__ rhs,
                                                                const float* __restrict__ res, Scalars* S) {
@@ -1568,7 +1574,7 @@ __device__ __forceinline__ float rhs_b2_at(const Geo& g, float scale, float* __r
 // With `codes` not null, the same pass also writes each cell's row code (row_code_of the same
 // row; 0 for a dry cell); with `pdry` not null it zeroes that pressure on the dry cells.
 template <int MODE>
-__global__ void __launch_bounds__(TPB) k_rhs_b2(Geo g, float scale, float* __restrict__ rhs, float* __restrict__ prec,
+__global__ void __launch_bounds__(TPB, FD3_SETUP_MINB) k_rhs_b2(Geo g, float scale, float* __restrict__ rhs, float* __restrict__ prec,
                                                 Red red, Scalars* S, int reduce, unsigned short* __restrict__ codes,
                                                 float* __restrict__ pdry) {
   KSTART();
