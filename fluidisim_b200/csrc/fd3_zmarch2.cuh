@@ -19,10 +19,15 @@
 
 namespace fd3 {
 
-// Resident CTAs per SM the register budget is cut for: 3 (up to 85 registers, no spills) measured
-// 344.6 against 342.1 projections/s at 128^3 with 4 (64 registers, the passes spilling).
+// Resident CTAs per SM the register budget is cut for: 3 (up to 85 registers, no spills) for the
+// sweeps, 4 (64) for the lighter direction and restriction passes; measured at 128^3 on one box:
+// 349.4 projections/s, against 345.7 with 3 for every pass; 3 for every pass against 4 for every
+// pass (the sweeps spilling), 344.6 against 342.1 on another.
 #ifndef FD3_ZMINB2
 #define FD3_ZMINB2 3
+#endif
+#ifndef FD3_ZMINB2_LIGHT
+#define FD3_ZMINB2_LIGHT 4
 #endif
 // Layers per CTA (K2) is a template parameter: 8 when the grid still yields two waves of CTAs at
 // four per SM (measured best at 256^3), else 4 (best at 128^3, where 8 leaves SMs idle).
@@ -265,7 +270,7 @@ __global__ void __launch_bounds__(Z2T, FD3_ZMINB2) kx_residual(Geo g, const unsi
 
 // d = z (+ beta d); q = A d; d.q; alpha (FIN_DQ).
 template <int K2, class T>
-__global__ void __launch_bounds__(Z2T, FD3_ZMINB2) kx_dir_apply_dot(Geo g, const unsigned short* __restrict__ codes,
+__global__ void __launch_bounds__(Z2T, FD3_ZMINB2_LIGHT) kx_dir_apply_dot(Geo g, const unsigned short* __restrict__ codes,
                                                                   const T* __restrict__ z,
                                                                   const float* __restrict__ din, float* __restrict__ dout,
                                                                   float* __restrict__ q, Red red, Scalars* S) {
@@ -345,7 +350,7 @@ __global__ void __launch_bounds__(Z2T, FD3_ZMINB2) kx_fine_post2_rz(Geo g, const
 // each thread's pair is one coarse cell's x children; the even rows sum the eight children, in the
 // reference's CHILDREN order, from the two layers kept in shared memory.
 template <int K2, class T>
-__global__ void __launch_bounds__(Z2T, FD3_ZMINB2) kx_fine_restrict(Geo g, const unsigned short* __restrict__ codes,
+__global__ void __launch_bounds__(Z2T, FD3_ZMINB2_LIGHT) kx_fine_restrict(Geo g, const unsigned short* __restrict__ codes,
                                                                   const float* __restrict__ r,
                                                                   const T* __restrict__ z, Lev L, const Scalars* S,
                                                                   int gate) {
